@@ -1,0 +1,108 @@
+"""ctypes binding of the matcha_b200 C ABI (include/matcha_b200.h).
+
+The library is the product's only compute path: importing this module on a machine
+without the built library, or calling an entry point without a CUDA device, raises
+instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import torch
+
+from . import build as _build
+
+MTB_OK = 0
+MTB_ERR_ARG = 1
+MTB_ERR_OOM = 2
+MTB_ERR_NUMERIC = 3
+MTB_ERR_TIMEOUT = 4
+MTB_ERR_CUDA = 5
+
+MTB_MAX_STAGES = 16
+MTB_SEARCH_COMPAT_TOP_BLOCK = 1
+MTB_SEARCH_GRADIENT_STEP = 2
+
+_lib = None
+
+
+class MtbSearchConfig(ctypes.Structure):
+    _fields_ = [
+        ("Lmax", ctypes.c_int),
+        ("n_stages", ctypes.c_int),
+        ("stages", ctypes.c_int * MTB_MAX_STAGES),
+        ("L0", ctypes.c_int),
+        ("K", ctypes.c_int),
+        ("candidates", ctypes.c_int),
+        ("num_steps", ctypes.c_int),
+        ("max_batch", ctypes.c_int),
+        ("flags", ctypes.c_int),
+    ]
+
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I64 = ctypes.c_int64
+
+# name -> (restype, argtypes); every symbol declared in include/matcha_b200.h
+SIGNATURES = {
+    "mtb_version": (_I, []),
+    "mtb_last_error": (ctypes.c_char_p, []),
+    "mtb_search_create": (_I, [ctypes.POINTER(MtbSearchConfig), ctypes.POINTER(_P)]),
+    "mtb_search_destroy": (None, [_P]),
+    "mtb_so3_grid_topk": (_I, [_P, _P, _I64, _I, _P, _P, _P, _P, _P]),
+    "mtb_newton_march": (_I, [_P, _P, _I64, _I, _P, _P, _P, _P, _P]),
+    "mtb_search_orientations": (_I, [_P, _P, _I64, _I, _P, _P, _P, _P, _P]),
+}
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = False):
+    """Load the shared library (optionally building it first) and declare its symbols."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = lib_path()
+    if not os.path.exists(path):
+        if build_if_missing:
+            _build.build()
+        else:
+            raise RuntimeError(
+                f"matcha_b200 CUDA library not found at {path}; build it with `python -m matcha_b200.build`")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int, what: str) -> None:
+    """Map a C status to the exception type the reference's callers expect."""
+    if rc == MTB_OK:
+        return
+    msg = load().mtb_last_error().decode(errors="replace")
+    text = f"{what} failed (status {rc}): {msg}"
+    if rc == MTB_ERR_OOM:
+        raise torch.cuda.OutOfMemoryError("CUDA out of memory. " + text)
+    if rc == MTB_ERR_ARG:
+        raise ValueError(text)
+    raise RuntimeError(text)
+
+
+def stream_ptr(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def require_cuda(t: torch.Tensor, name: str) -> None:
+    if not t.is_cuda:
+        raise RuntimeError(f"{name} must be a CUDA tensor: matcha_b200 runs on the GPU only")

@@ -1,0 +1,646 @@
+// Orientation search on sm_100a: SO(3) grid search with top-k, and the
+// frequency-marched Wigner-D Newton refinement.
+//
+// Reference behaviour restated here (paths inside swing-research/Matcha):
+//   grid      src/matcha/core/SOFFT.py:30-124, src/matcha/core/Matcha.py:27-58,207-236
+//   Newton    src/matcha/core/Matcha.py:150-205, 239-403
+//   D, d      src/matcha/core/WignerDMatrices.py:281-306, 673-801, 1291-1375
+//   g, H      src/matcha/core/WignerDGradients.py:155-302
+//
+// Design (B200): one CTA per (subtomogram, candidate) runs every march stage for
+// its candidate.  The small-d matrix of each degree l is produced by the three-term
+// recurrence in l for fixed (m', m) (state in registers, one fundamental wedge
+// m' >= |m| per thread, symmetric copies written to shared memory), and contracted
+// against sigma in the same sweep: value, Euler gradient and Hessian come out of one
+// pass over sigma with 10 register accumulators and a warp-shuffle block reduction.
+// No D matrix and no 15-column coefficient bank ever reach HBM.  The 3x3 Newton
+// solve runs in FP64.
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+#include <vector>
+#include "common.cuh"
+
+namespace {
+
+struct SearchParams {
+  int Lmax;
+  int n_stages;
+  int stages[MTB_MAX_STAGES];
+  int L0;
+  int K;
+  int C;
+  int num_steps;
+  int flags;
+};
+
+constexpr int kNewtonThreads = 256;
+constexpr int kGridThreads = 256;
+constexpr int kMaxCand = 32;
+
+// ------------------------------------------------------------------ Newton pass
+// Accumulator slots.
+enum { A_VAL = 0, A_GA, A_GB, A_GG, A_HAA, A_HAB, A_HAG, A_HBB, A_HBG, A_HGG, A_N };
+
+struct NewtonSmem {
+  float* dbuf[2];  // d^l blocks, width 2l+1, double-buffered by l parity
+  float* rowf[2];  // 5 row factors x (2 Lmax + 1), by l parity
+  float2* ea;      // exp(i m' alpha), m' = -Li..Li
+  float2* eg;      // exp(i m gamma)
+  float* red;      // (threads/32) x A_N
+  float* res;      // A_N reduced results
+};
+
+template <int KP>
+__device__ void newton_pass(const float2* __restrict__ sig, const double* __restrict__ logC,
+                            float a, float be, float ga, int Li, bool derivs, bool compat_top,
+                            int W, NewtonSmem sm) {
+  const int tid = threadIdx.x;
+  const int NT = blockDim.x;
+  // phases e^{i m a}, e^{i m g} in double, stored float
+  for (int r = tid; r < 2 * Li + 1; r += NT) {
+    double s, c;
+    sincos((double)(r - Li) * (double)a, &s, &c);
+    sm.ea[r] = make_float2((float)c, (float)s);
+    sincos((double)(r - Li) * (double)ga, &s, &c);
+    sm.eg[r] = make_float2((float)c, (float)s);
+  }
+  const float cb = cosf(be);
+  double hs, hc;
+  sincos(0.5 * (double)be, &hs, &hc);
+  const double lac = log(fabs(hc)), las = log(fabs(hs));
+  const int sgc = hc < 0.0 ? 1 : 0, sgs = hs < 0.0 ? 1 : 0;
+
+  float d1[KP], d0[KP];
+#pragma unroll
+  for (int k = 0; k < KP; ++k) { d1[k] = 0.f; d0[k] = 0.f; }
+
+  float acc[A_N];
+#pragma unroll
+  for (int i = 0; i < A_N; ++i) acc[i] = 0.f;
+
+  for (int l = 0; l <= Li; ++l) {
+    const int w = 2 * l + 1;
+    float* dcur = sm.dbuf[l & 1];
+    // ---- recurrence: wedge pairs p = m'^2 + (m + m'), m' = 0..l, |m| <= m'
+    const int npair = (l + 1) * (l + 1);
+#pragma unroll
+    for (int k = 0; k < KP; ++k) {
+      const int p = tid + k * NT;
+      if (p < npair) {
+        int mp = (int)sqrtf((float)p);
+        while (mp * mp > p) --mp;
+        while ((mp + 1) * (mp + 1) <= p) ++mp;
+        const int m = p - mp * mp - mp;
+        float v;
+        if (mp == l) {
+          // closed form at l0 = m': (-1)^(m'-m) sqrt((2m')!/((m'+m)!(m'-m)!)) c^(m'+m) s^(m'-m)
+          const int pc = mp + m, ps = mp - m;
+          double lg = logC[p];
+          if (pc) lg += pc * lac;
+          if (ps) lg += ps * las;
+          double dv = exp(lg);
+          const int sgn = (ps & 1) ^ ((pc & 1) & sgc) ^ ((ps & 1) & sgs);
+          v = (float)(sgn ? -dv : dv);
+          d0[k] = 0.f;
+        } else if (l == 1) {
+          v = cb * d1[k];  // (m', m) = (0, 0)
+          d0[k] = d1[k];
+        } else {
+          const float lm = (float)(l - 1);
+          const float fl = (float)l;
+          const float mm = (float)m, mmp = (float)mp;
+          const float aa = (2.f * fl - 1.f) * (lm * fl * cb - mm * mmp);
+          const float xp = (lm * lm - mm * mm) * (lm * lm - mmp * mmp);
+          const float xc = (fl * fl - mm * mm) * (fl * fl - mmp * mmp);
+          v = (aa * d1[k] - fl * sqrtf(xp) * d0[k]) / (lm * sqrtf(xc));
+          d0[k] = d1[k];
+        }
+        d1[k] = v;
+        // symmetric copies: d_{m m'} = d_{-m',-m} = (-1)^(m'-m) d_{m'm}; d_{-m,-m'} = d_{m'm}
+        const float vs = ((mp - m) & 1) ? -v : v;
+        dcur[(mp + l) * w + (m + l)] = v;
+        dcur[(m + l) * w + (mp + l)] = vs;
+        dcur[(-m + l) * w + (-mp + l)] = v;
+        dcur[(-mp + l) * w + (-m + l)] = vs;
+      }
+    }
+    // ---- row factors of WignerDGradients.py:45-79 for m' = -l..l
+    if (derivs) {
+      float* rf = sm.rowf[l & 1];
+      for (int r = tid; r < w; r += NT) {
+        const float fl = (float)l, mp = (float)(r - l);
+        rf[0 * W + r] = -0.5f * sqrtf(fmaxf((fl + mp) * (fl - mp + 1.f), 0.f));
+        rf[1 * W + r] = 0.5f * sqrtf(fmaxf((fl - mp) * (fl + mp + 1.f), 0.f));
+        rf[2 * W + r] = 0.25f * sqrtf(fmaxf((fl + mp) * (fl - mp + 1.f) * (fl + mp - 1.f) * (fl - mp + 2.f), 0.f));
+        rf[3 * W + r] = -0.25f * ((fl + mp) * (fl - mp + 1.f) + (fl + mp + 1.f) * (fl - mp));
+        rf[4 * W + r] = 0.25f * sqrtf(fmaxf((fl + mp + 1.f) * (fl - mp) * (fl + mp + 2.f) * (fl - mp - 1.f), 0.f));
+      }
+    }
+    __syncthreads();
+    // ---- contraction over the (2l+1)^2 entries of degree l
+    const float2* sl = sig + mtb_dsize(l - 1);
+    const bool zap = compat_top && (l == Li);
+    const float* rf = sm.rowf[l & 1];
+    for (int e = tid; e < w * w; e += NT) {
+      const int r = e / w;       // m' + l
+      const int c = e - r * w;   // m + l
+      const float2 s = __ldg(&sl[e]);
+      const float2 ph = cmul(sm.ea[r - l + Li], sm.eg[c - l + Li]);
+      const float er = ph.x * s.x - ph.y * s.y;
+      const float ei = ph.x * s.y + ph.y * s.x;
+      float dc = dcur[e];
+      if (zap && (r == 0 || c == 0)) dc = 0.f;
+      acc[A_VAL] += dc * er;
+      if (derivs) {
+        const float mp = (float)(r - l), m = (float)(c - l);
+        auto dat = [&](int rr) -> float {
+          if (rr < 0 || rr >= w) return 0.f;
+          if (zap && (rr == 0 || c == 0)) return 0.f;
+          return dcur[rr * w + c];
+        };
+        const float dm1 = dat(r - 1), dp1 = dat(r + 1), dm2 = dat(r - 2), dp2 = dat(r + 2);
+        const float db = rf[0 * W + r] * dm1 + rf[1 * W + r] * dp1;
+        const float dbb = rf[3 * W + r] * dc + rf[2 * W + r] * dm2 + rf[4 * W + r] * dp2;
+        const float t = dc * er, u = dc * ei;
+        acc[A_GA] -= mp * u;
+        acc[A_GG] -= m * u;
+        acc[A_HAA] -= mp * mp * t;
+        acc[A_HGG] -= m * m * t;
+        acc[A_HAG] -= mp * m * t;
+        acc[A_GB] += db * er;
+        const float x = db * ei;
+        acc[A_HAB] -= mp * x;
+        acc[A_HBG] -= m * x;
+        acc[A_HBB] += dbb * er;
+      }
+    }
+  }
+  // ---- block reduction of the accumulators
+  const int lane = tid & 31, warp = tid >> 5, nw = NT >> 5;
+#pragma unroll
+  for (int i = 0; i < A_N; ++i) {
+    const float v = warp_sum(acc[i]);
+    if (lane == 0) sm.red[warp * A_N + i] = v;
+  }
+  __syncthreads();
+  if (tid < A_N) {
+    float s = 0.f;
+    for (int q = 0; q < nw; ++q) s += sm.red[q * A_N + tid];
+    sm.res[tid] = s;
+  }
+  __syncthreads();
+}
+
+// Solve H x = g in FP64 with partial pivoting; false when a pivot is exactly zero
+// (torch.linalg.solve raises "singular" there and the reference takes a zero step,
+// Matcha.py:316-343).
+__device__ bool solve3(const double H[3][3], const double g[3], double x[3]) {
+  double A[3][4];
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) A[i][j] = H[i][j];
+    A[i][3] = g[i];
+  }
+  for (int c = 0; c < 3; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < 3; ++r)
+      if (fabs(A[r][c]) > fabs(A[piv][c])) piv = r;
+    if (A[piv][c] == 0.0 || !isfinite(A[piv][c])) return false;
+    if (piv != c)
+      for (int j = 0; j < 4; ++j) { double t = A[c][j]; A[c][j] = A[piv][j]; A[piv][j] = t; }
+    for (int r = c + 1; r < 3; ++r) {
+      const double f = A[r][c] / A[c][c];
+      for (int j = c; j < 4; ++j) A[r][j] -= f * A[c][j];
+    }
+  }
+  for (int r = 2; r >= 0; --r) {
+    double s = A[r][3];
+    for (int j = r + 1; j < 3; ++j) s -= A[r][j] * x[j];
+    x[r] = s / A[r][r];
+  }
+  return true;
+}
+
+template <int KP>
+__global__ void __launch_bounds__(kNewtonThreads)
+newton_march_kernel(const float2* __restrict__ sigma, int64_t stride, int BC,
+                    float* __restrict__ alpha, float* __restrict__ beta, float* __restrict__ gamma,
+                    float* __restrict__ score, const double* __restrict__ logC, SearchParams P) {
+  extern __shared__ __align__(16) float smem[];
+  const int W = 2 * P.Lmax + 1;
+  NewtonSmem sm;
+  sm.dbuf[0] = smem;
+  sm.dbuf[1] = smem + W * W;
+  sm.rowf[0] = smem + 2 * W * W;
+  sm.rowf[1] = sm.rowf[0] + 5 * W;
+  sm.ea = reinterpret_cast<float2*>(sm.rowf[1] + 5 * W);
+  sm.eg = sm.ea + W;
+  sm.red = reinterpret_cast<float*>(sm.eg + W);
+  sm.res = sm.red + (kNewtonThreads / 32) * A_N;
+  __shared__ float st[8];  // angles and control broadcast
+
+  const int cand = blockIdx.x;
+  if (cand >= BC) return;
+  const int b = cand / P.C;
+  const float2* sig = sigma + (int64_t)b * stride;
+  const bool compat = (P.flags & MTB_SEARCH_COMPAT_TOP_BLOCK) != 0;
+  const bool grad_step = (P.flags & MTB_SEARCH_GRADIENT_STEP) != 0;
+  const float base_lr = grad_step ? 5e-7f : 1.f;
+
+  float a = alpha[cand], be = beta[cand], ga = gamma[cand];
+  float best = 0.f;
+  for (int s = 0; s < P.n_stages; ++s) {
+    const int Li = P.stages[s];
+    const bool zap = compat && (Li == P.Lmax);
+    newton_pass<KP>(sig, logC, a, be, ga, Li, P.num_steps > 0, zap, W, sm);
+    best = sm.res[A_VAL];
+    double g[3] = {sm.res[A_GA], sm.res[A_GB], sm.res[A_GG]};
+    double H[3][3] = {{sm.res[A_HAA], sm.res[A_HAB], sm.res[A_HAG]},
+                      {sm.res[A_HAB], sm.res[A_HBB], sm.res[A_HBG]},
+                      {sm.res[A_HAG], sm.res[A_HBG], sm.res[A_HGG]}};
+    float lr = base_lr;
+    for (int it = 0; it < P.num_steps; ++it) {
+      double x[3] = {0.0, 0.0, 0.0};
+      if (grad_step) {
+        for (int i = 0; i < 3; ++i) x[i] = -g[i];
+      } else if (!solve3(H, g, x)) {
+        x[0] = x[1] = x[2] = 0.0;
+      }
+      const float ta = a - lr * (float)x[0];
+      const float tb = be - lr * (float)x[1];
+      const float tg = ga - lr * (float)x[2];
+      const bool last = (it == P.num_steps - 1);
+      newton_pass<KP>(sig, logC, ta, tb, tg, Li, !last, zap, W, sm);
+      const float ev = sm.res[A_VAL];
+      if (ev > best) {
+        a = ta; be = tb; ga = tg; best = ev;
+        lr *= 1.1f;
+        if (!last) {
+          g[0] = sm.res[A_GA]; g[1] = sm.res[A_GB]; g[2] = sm.res[A_GG];
+          H[0][0] = sm.res[A_HAA]; H[0][1] = H[1][0] = sm.res[A_HAB]; H[0][2] = H[2][0] = sm.res[A_HAG];
+          H[1][1] = sm.res[A_HBB]; H[1][2] = H[2][1] = sm.res[A_HBG]; H[2][2] = sm.res[A_HGG];
+        }
+      } else {
+        lr *= 0.5f;
+      }
+      // every thread evaluates the same branch on identical values; the next pass
+      // syncs before shared results are overwritten
+      __syncthreads();
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    alpha[cand] = a;
+    beta[cand] = be;
+    gamma[cand] = ga;
+    score[cand] = best;
+  }
+  (void)st;
+}
+
+// ------------------------------------------------------------------ grid + top-k
+__device__ __forceinline__ bool better(float v1, int i1, float v2, int i2) {
+  return v1 > v2 || (v1 == v2 && i1 < i2);
+}
+
+__global__ void __launch_bounds__(kGridThreads)
+so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
+                     const float* __restrict__ dtab, int L0, int n, int C,
+                     float* __restrict__ alpha, float* __restrict__ beta, float* __restrict__ gamma,
+                     float* __restrict__ grid_out) {
+  extern __shared__ __align__(16) float gsm[];
+  const int P = 2 * L0 - 1;
+  const int nk = mtb_dsize(L0 - 1);
+  float2* sg = reinterpret_cast<float2*>(gsm);  // nk
+  float2* F = sg + nk;                           // P*P
+  float2* G = F + P * P;                         // P*n
+  float2* tw = G + P * n;                        // n
+  __shared__ float mv[kGridThreads / 32];
+  __shared__ int mi[kGridThreads / 32];
+  __shared__ int mt[kGridThreads / 32];
+
+  const int b = blockIdx.x;
+  if (b >= B) return;
+  const int tid = threadIdx.x;
+  const float2* sig = sigma + (int64_t)b * stride;
+  for (int k = tid; k < nk; k += blockDim.x) sg[k] = sig[k];
+  for (int k = tid; k < n; k += blockDim.x) {
+    double s, c;
+    sincospi(2.0 * k / n, &s, &c);
+    tw[k] = make_float2((float)c, (float)s);
+  }
+  float tv[kMaxCand];
+  int ti[kMaxCand];
+  int cnt = 0, minp = 0;
+  const float inv_n2 = 1.f / (float)(n * n);
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    const float* dj = dtab + (int64_t)j * nk;
+    for (int q = tid; q < P * P; q += blockDim.x) {
+      const int mp = q / P - (L0 - 1), m = q % P - (L0 - 1);
+      const int l0 = max(abs(mp), abs(m));
+      float re = 0.f, im = 0.f;
+      for (int l = l0; l < L0; ++l) {
+        const int idx = mtb_dsize(l - 1) + (mp + l) * (2 * l + 1) + (m + l);
+        const float d = __ldg(&dj[idx]);
+        re += d * sg[idx].x;
+        im += d * sg[idx].y;
+      }
+      F[q] = make_float2(re, im);
+    }
+    __syncthreads();
+    for (int q = tid; q < P * n; q += blockDim.x) {
+      const int r = q / n, gg = q % n;
+      float re = 0.f, im = 0.f;
+      for (int c = 0; c < P; ++c) {
+        const int m = c - (L0 - 1);
+        int k = (gg * m) % n;
+        if (k < 0) k += n;
+        const float2 f = F[r * P + c], t = tw[k];
+        re += f.x * t.x - f.y * t.y;
+        im += f.x * t.y + f.y * t.x;
+      }
+      G[q] = make_float2(re, im);
+    }
+    __syncthreads();
+    for (int q = tid; q < n * n; q += blockDim.x) {
+      const int aa = q / n, gg = q % n;
+      float re = 0.f;
+      for (int r = 0; r < P; ++r) {
+        const int mp = r - (L0 - 1);
+        int k = (aa * mp) % n;
+        if (k < 0) k += n;
+        const float2 gv = G[r * n + gg], t = tw[k];
+        re += gv.x * t.x - gv.y * t.y;
+      }
+      const float v = re * inv_n2;
+      const int flat = j * n * n + q;
+      if (grid_out) grid_out[(int64_t)b * n * n * n + flat] = v;
+      if (cnt < C) {
+        tv[cnt] = v; ti[cnt] = flat; ++cnt;
+        if (cnt == C || !better(tv[minp], ti[minp], v, flat)) {
+          minp = 0;
+          for (int t = 1; t < cnt; ++t)
+            if (better(tv[minp], ti[minp], tv[t], ti[t])) minp = t;
+        }
+      } else if (better(v, flat, tv[minp], ti[minp])) {
+        tv[minp] = v; ti[minp] = flat;
+        minp = 0;
+        for (int t = 1; t < cnt; ++t)
+          if (better(tv[minp], ti[minp], tv[t], ti[t])) minp = t;
+      }
+    }
+    __syncthreads();
+  }
+  // block merge: C rounds of block argmax over each thread's best remaining entry
+  const int lane = tid & 31, warp = tid >> 5;
+  const float bstep = (float)(M_PI / (double)(n - 1));
+  const float astep = (float)(2.0 * M_PI / (double)n);
+  for (int c = 0; c < C; ++c) {
+    int hp = -1;
+    float hv = -INFINITY;
+    int hi = 0x7fffffff;
+    for (int t = 0; t < cnt; ++t)
+      if (hp < 0 || better(tv[t], ti[t], hv, hi)) { hp = t; hv = tv[t]; hi = ti[t]; }
+    float v = hv;
+    int i = hi, who = (hp < 0) ? -1 : tid;
+    for (int o = 16; o > 0; o >>= 1) {
+      const float v2 = __shfl_xor_sync(0xffffffffu, v, o);
+      const int i2 = __shfl_xor_sync(0xffffffffu, i, o);
+      const int w2 = __shfl_xor_sync(0xffffffffu, who, o);
+      if (w2 >= 0 && (who < 0 || better(v2, i2, v, i))) { v = v2; i = i2; who = w2; }
+    }
+    if (lane == 0) { mv[warp] = v; mi[warp] = i; mt[warp] = who; }
+    __syncthreads();
+    if (tid == 0) {
+      float bv = mv[0];
+      int bi = mi[0], bw = mt[0];
+      for (int q = 1; q < (int)(blockDim.x >> 5); ++q)
+        if (mt[q] >= 0 && (bw < 0 || better(mv[q], mi[q], bv, bi))) { bv = mv[q]; bi = mi[q]; bw = mt[q]; }
+      mt[0] = bw;
+      mi[0] = bi;
+      const int jj = bi / (n * n), aa = (bi / n) % n, gg = bi % n;
+      const int o = b * C + c;
+      beta[o] = (float)jj * bstep;
+      alpha[o] = (float)aa * astep;
+      gamma[o] = (float)gg * astep;
+    }
+    __syncthreads();
+    if (mt[0] == tid && hp >= 0) {
+      // remove the taken entry
+      tv[hp] = tv[cnt - 1];
+      ti[hp] = ti[cnt - 1];
+      --cnt;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void reduce_candidates_kernel(const float* __restrict__ ca, const float* __restrict__ cb,
+                                         const float* __restrict__ cg, const float* __restrict__ cs,
+                                         int B, int C, float* alpha, float* beta, float* gamma,
+                                         float* score) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  int best = 0;
+  float bv = cs[b * C];
+  for (int c = 1; c < C; ++c) {
+    const float v = cs[b * C + c];
+    if (v > bv) { bv = v; best = c; }
+  }
+  alpha[b] = ca[b * C + best];
+  beta[b] = cb[b * C + best];
+  gamma[b] = cg[b * C + best];
+  score[b] = bv;
+}
+
+// ------------------------------------------------------------------ host tables
+double host_small_d_start_log(int mp, int m) {
+  return 0.5 * (lgamma(2.0 * mp + 1.0) - lgamma((double)(mp + m) + 1.0) - lgamma((double)(mp - m) + 1.0));
+}
+
+// d^l_{m'm}(beta) for l < L0 in flat order, by the same recurrence in double.
+void host_small_d(int Lm, double beta, double* out) {
+  const double cb = cos(beta), c = cos(0.5 * beta), s = sin(0.5 * beta);
+  for (int mp = -Lm; mp <= Lm; ++mp)
+    for (int m = -Lm; m <= Lm; ++m) {
+      const int l0 = abs(mp) > abs(m) ? abs(mp) : abs(m);
+      // start value from the explicit sum at l0 (single term)
+      const int kmin = (m - mp) > 0 ? (m - mp) : 0;
+      const int k = kmin;
+      const int l = l0;
+      const double lognum = 0.5 * (lgamma(l + mp + 1.0) + lgamma(l - mp + 1.0) + lgamma(l + m + 1.0) + lgamma(l - m + 1.0));
+      const double logden = lgamma(l + m - k + 1.0) + lgamma(k + 1.0) + lgamma(mp - m + k + 1.0) + lgamma(l - mp - k + 1.0);
+      const int pc = 2 * l + m - mp - 2 * k, ps = mp - m + 2 * k;
+      double v = exp(lognum - logden) * (((mp - m + k) & 1) ? -1.0 : 1.0);
+      v *= (pc ? pow(c, pc) : 1.0) * (ps ? pow(s, ps) : 1.0);
+      double dl = v, dlm1 = 0.0;
+      out[mtb_dsize(l0 - 1) + (mp + l0) * (2 * l0 + 1) + (m + l0)] = dl;
+      for (int ll = l0; ll < Lm; ++ll) {
+        double dn;
+        if (ll == 0) {
+          dn = cb * dl;
+        } else {
+          const double a = (2.0 * ll + 1.0) * (ll * (ll + 1.0) * cb - (double)m * mp);
+          const double bb = (ll + 1.0) * sqrt((double)(ll * ll - m * m) * (double)(ll * ll - mp * mp));
+          const double cc = ll * sqrt((double)((ll + 1) * (ll + 1) - m * m) * (double)((ll + 1) * (ll + 1) - mp * mp));
+          dn = (a * dl - bb * dlm1) / cc;
+        }
+        dlm1 = dl;
+        dl = dn;
+        const int L1 = ll + 1;
+        out[mtb_dsize(L1 - 1) + (mp + L1) * (2 * L1 + 1) + (m + L1)] = dl;
+      }
+    }
+}
+
+template <int KP>
+int launch_newton(const float2* sigma, int64_t stride, int BC, float* a, float* b, float* g, float* s,
+                  const double* logC, const SearchParams& P, cudaStream_t st) {
+  const int W = 2 * P.Lmax + 1;
+  const size_t smem = (size_t)(2 * W * W + 10 * W) * sizeof(float) + (size_t)2 * W * sizeof(float2) +
+                      (size_t)((kNewtonThreads / 32) * A_N + A_N) * sizeof(float);
+  MTB_CUDA_TRY(cudaFuncSetAttribute(newton_march_kernel<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  newton_march_kernel<KP><<<BC, kNewtonThreads, smem, st>>>(sigma, stride, BC, a, b, g, s, logC, P);
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+struct mtb_search {
+  mtb_search_config cfg;
+  SearchParams P;
+  int n;            // grid size per axis
+  int device;
+  float* dtab;      // (n, dsize(L0-1))
+  double* logC;     // (Lmax+1)^2
+  float* cand;      // 4 x (max_batch * C): alpha, beta, gamma, score
+};
+
+extern "C" int mtb_search_create(const mtb_search_config* cfg, mtb_search** out) {
+  MTB_ARG_CHECK(cfg && out, "null argument");
+  *out = nullptr;
+  MTB_ARG_CHECK(cfg->Lmax >= 1 && cfg->Lmax <= 64, "Lmax must be in [1, 64]");
+  MTB_ARG_CHECK(cfg->n_stages >= 1 && cfg->n_stages <= MTB_MAX_STAGES, "n_stages out of range");
+  MTB_ARG_CHECK(cfg->L0 >= 1 && cfg->L0 <= cfg->Lmax, "L0 must be in [1, Lmax]");
+  MTB_ARG_CHECK(cfg->K >= 1 && 2 * cfg->L0 * cfg->K <= 128, "grid size 2*L0*K must be <= 128");
+  MTB_ARG_CHECK(cfg->candidates >= 1 && cfg->candidates <= kMaxCand, "candidates must be in [1, 32]");
+  MTB_ARG_CHECK(cfg->candidates <= 2 * cfg->L0 * cfg->K * 2 * cfg->L0 * cfg->K * 2 * cfg->L0 * cfg->K,
+                "more candidates than grid points");
+  MTB_ARG_CHECK(cfg->num_steps >= 0 && cfg->max_batch >= 1, "bad num_steps / max_batch");
+  for (int i = 0; i < cfg->n_stages; ++i)
+    MTB_ARG_CHECK(cfg->stages[i] >= 0 && cfg->stages[i] <= cfg->Lmax, "stage degree out of range");
+  {
+    const int n = 2 * cfg->L0 * cfg->K, P = 2 * cfg->L0 - 1;
+    const size_t gsm = (size_t)(mtb_dsize(cfg->L0 - 1) + P * P + P * n + n) * 8;
+    MTB_ARG_CHECK(gsm <= 200 * 1024, "grid search too large for shared memory (reduce L0 or K)");
+  }
+  mtb_search* h = new mtb_search();
+  memset(h, 0, sizeof(*h));
+  h->cfg = *cfg;
+  h->P.Lmax = cfg->Lmax;
+  h->P.n_stages = cfg->n_stages;
+  for (int i = 0; i < cfg->n_stages; ++i) h->P.stages[i] = cfg->stages[i];
+  h->P.L0 = cfg->L0;
+  h->P.K = cfg->K;
+  h->P.C = cfg->candidates;
+  h->P.num_steps = cfg->num_steps;
+  h->P.flags = cfg->flags;
+  h->n = 2 * cfg->L0 * cfg->K;
+  cudaGetDevice(&h->device);
+
+  const int n = h->n, L0 = cfg->L0, nk = mtb_dsize(L0 - 1);
+  std::vector<float> dt((size_t)n * nk);
+  std::vector<double> tmp(mtb_dsize(L0 - 1) > 0 ? mtb_dsize(L0 - 1) : 1);
+  for (int j = 0; j < n; ++j) {
+    // np.linspace(0, pi, n, endpoint=True)
+    const double beta = (n > 1) ? (j == n - 1 ? M_PI : j * (M_PI / (n - 1))) : 0.0;
+    host_small_d(L0 - 1, beta, tmp.data());
+    for (int k = 0; k < nk; ++k) dt[(size_t)j * nk + k] = (float)tmp[k];
+  }
+  const int Lm = cfg->Lmax;
+  std::vector<double> lc((size_t)(Lm + 1) * (Lm + 1));
+  for (int mp = 0; mp <= Lm; ++mp)
+    for (int m = -mp; m <= mp; ++m) lc[mp * mp + m + mp] = host_small_d_start_log(mp, m);
+
+  auto fail = [&](int code) { mtb_search_destroy(h); return code; };
+  if (cudaMalloc(&h->dtab, dt.size() * sizeof(float)) != cudaSuccess) return fail(MTB_ERR_OOM);
+  if (cudaMalloc(&h->logC, lc.size() * sizeof(double)) != cudaSuccess) return fail(MTB_ERR_OOM);
+  if (cudaMalloc(&h->cand, (size_t)4 * cfg->max_batch * cfg->candidates * sizeof(float)) != cudaSuccess)
+    return fail(MTB_ERR_OOM);
+  if (cudaMemcpy(h->dtab, dt.data(), dt.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(h->logC, lc.data(), lc.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(MTB_ERR_CUDA);
+  *out = h;
+  return MTB_OK;
+}
+
+extern "C" void mtb_search_destroy(mtb_search* h) {
+  if (!h) return;
+  if (h->dtab) cudaFree(h->dtab);
+  if (h->logC) cudaFree(h->logC);
+  if (h->cand) cudaFree(h->cand);
+  delete h;
+}
+
+extern "C" int mtb_so3_grid_topk(mtb_search* h, const float* sigma, int64_t sigma_stride, int B,
+                                 float* alpha, float* beta, float* gamma, float* grid,
+                                 mtb_stream_t stream) {
+  MTB_ARG_CHECK(h, "null handle");
+  MTB_ARG_CHECK(B >= 0 && B <= h->cfg.max_batch, "batch exceeds max_batch");
+  if (B == 0) return MTB_OK;
+  MTB_ARG_CHECK(sigma && alpha && beta && gamma, "null pointer");
+  MTB_ARG_CHECK(sigma_stride >= mtb_dsize(h->cfg.L0 - 1), "sigma row shorter than dsize(L0-1)");
+  const int L0 = h->cfg.L0, n = h->n, P = 2 * L0 - 1, nk = mtb_dsize(L0 - 1);
+  const size_t smem = (size_t)(nk + P * P + P * n + n) * sizeof(float2);
+  MTB_CUDA_TRY(cudaFuncSetAttribute(so3_grid_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  so3_grid_topk_kernel<<<B, kGridThreads, smem, (cudaStream_t)stream>>>(
+      reinterpret_cast<const float2*>(sigma), sigma_stride, B, h->dtab, L0, n, h->cfg.candidates,
+      alpha, beta, gamma, grid);
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
+}
+
+extern "C" int mtb_newton_march(mtb_search* h, const float* sigma, int64_t sigma_stride, int B,
+                                float* alpha, float* beta, float* gamma, float* score,
+                                mtb_stream_t stream) {
+  MTB_ARG_CHECK(h, "null handle");
+  MTB_ARG_CHECK(B >= 0 && B <= h->cfg.max_batch, "batch exceeds max_batch");
+  if (B == 0) return MTB_OK;
+  MTB_ARG_CHECK(sigma && alpha && beta && gamma && score, "null pointer");
+  MTB_ARG_CHECK(sigma_stride >= mtb_dsize(h->cfg.Lmax), "sigma row shorter than dsize(Lmax)");
+  const int BC = B * h->cfg.candidates;
+  const int pairs = (h->cfg.Lmax + 1) * (h->cfg.Lmax + 1);
+  const int kp = (pairs + kNewtonThreads - 1) / kNewtonThreads;
+  const float2* s = reinterpret_cast<const float2*>(sigma);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (kp <= 2) return launch_newton<2>(s, sigma_stride, BC, alpha, beta, gamma, score, h->logC, h->P, st);
+  if (kp <= 5) return launch_newton<5>(s, sigma_stride, BC, alpha, beta, gamma, score, h->logC, h->P, st);
+  if (kp <= 9) return launch_newton<9>(s, sigma_stride, BC, alpha, beta, gamma, score, h->logC, h->P, st);
+  return launch_newton<17>(s, sigma_stride, BC, alpha, beta, gamma, score, h->logC, h->P, st);
+}
+
+extern "C" int mtb_search_orientations(mtb_search* h, const float* sigma, int64_t sigma_stride, int B,
+                                       float* alpha, float* beta, float* gamma, float* score,
+                                       mtb_stream_t stream) {
+  MTB_ARG_CHECK(h, "null handle");
+  MTB_ARG_CHECK(B >= 0 && B <= h->cfg.max_batch, "batch exceeds max_batch");
+  if (B == 0) return MTB_OK;
+  MTB_ARG_CHECK(alpha && beta && gamma && score, "null pointer");
+  const int C = h->cfg.candidates;
+  const size_t cap = (size_t)h->cfg.max_batch * C;
+  float* ca = h->cand;
+  float* cb = ca + cap;
+  float* cg = cb + cap;
+  float* cs = cg + cap;
+  int rc = mtb_so3_grid_topk(h, sigma, sigma_stride, B, ca, cb, cg, nullptr, stream);
+  if (rc) return rc;
+  rc = mtb_newton_march(h, sigma, sigma_stride, B, ca, cb, cg, cs, stream);
+  if (rc) return rc;
+  reduce_candidates_kernel<<<(B + 127) / 128, 128, 0, (cudaStream_t)stream>>>(ca, cb, cg, cs, B, C, alpha,
+                                                                               beta, gamma, score);
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
+}
