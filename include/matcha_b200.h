@@ -90,6 +90,66 @@ int mtb_search_orientations(mtb_search* h, const float* sigma, int64_t sigma_str
                             float* alpha, float* beta, float* gamma, float* score,
                             mtb_stream_t stream);
 
+/* ------------------------------------------------------------------------------
+ * Ball expansion (FLE) and per-degree correlation coefficients sigma.
+ * Replaces FLEBasis3D.evaluate_t (src/matcha/core/FLEBasis3D.py:945-976; its
+ * cuFINUFFT + torch-harmonics + radial-interpolation pipeline, :1026-1267) and
+ * CrossCorrelationMatcher.compute_sigma / get_sigma
+ * (src/matcha/core/CrossCorrelationMatcher.py:183-249).
+ *
+ * The host supplies the basis in compact form (all pointers host, read during
+ * mtb_fle_create only): octant representatives of the voxel ball and their sign
+ * images, the real basis columns (Re or Im of conj(psi_{lkm}) for m >= 0) with their
+ * reflection-parity class, a table of j_l(lambda_{lk} r) per squared radius, and the
+ * maps from real columns back to the complex coefficients in the reference's order.
+ * ---------------------------------------------------------------------------- */
+typedef struct {
+  int N;                    /* volume edge; volumes are (B, N, N, N) float32, C order  */
+  int max_batch;            /* largest B any call will pass                            */
+  int ne;                   /* complex coefficients per volume (reference order)       */
+  int n_rep;                /* octant representatives (x, y, z >= 0) inside the ball   */
+  int n_cols;               /* real basis columns (== ne)                              */
+  int lmax;                 /* largest degree l                                        */
+  int n_lk;                 /* distinct (l, k) radial functions                        */
+  int n_r2;                 /* rows of jtab (squared radii)                            */
+  const int* rep_img;       /* [n_rep*8] flat voxel index of the sign image with bit0=x
+                               flipped, bit1=y, bit2=z; -1 if absent or a duplicate     */
+  const double* rep_cos;    /* [n_rep] cos(theta) of the representative                */
+  const double* rep_phi;    /* [n_rep] phi of the representative                       */
+  const int* rep_r2;        /* [n_rep] row of jtab                                      */
+  const double* jtab;       /* [n_r2*n_lk] j_l(lambda_lk * r / radius)                  */
+  const int* col_class;     /* [n_cols] parity class, bit0 = odd in x, bit1 = y, bit2 = z */
+  const int* col_l;         /* [n_cols]                                                */
+  const int* col_m;         /* [n_cols] m >= 0                                         */
+  const int* col_part;      /* [n_cols] 0: Re conj(Y) = P cos(m phi), 1: Im = -P sin(m phi) */
+  const int* col_lk;        /* [n_cols] column of jtab                                  */
+  const double* col_scale;  /* [n_cols] h * c_lk                                        */
+  const int* coef_col_re;   /* [ne] column giving Re a_i (times coef_sign_re)           */
+  const int* coef_col_im;   /* [ne] column giving Im a_i (times coef_sign_im), -1: zero */
+  const signed char* coef_sign_re; /* [ne] +-1                                          */
+  const signed char* coef_sign_im; /* [ne] +-1                                          */
+  const int* kpad;          /* [lmax+1] padded k-count of degree l                      */
+  const int* kidx;          /* [sum_l (2l+1) kpad[l]] coefficient index of (l, mu, k),
+                               rows mu = -l..l, -1 = padding                            */
+} mtb_fle_config;
+
+typedef struct mtb_fle mtb_fle;
+
+int mtb_fle_create(const mtb_fle_config* cfg, mtb_fle** out);
+void mtb_fle_destroy(mtb_fle* h);
+
+/* Ball coefficients of B real volumes: coeffs (B, coeff_stride) complex64 out, in the
+ * reference's order (FLEBasis3D.evaluate_t, without the in-place zeroing of the input);
+ * norms (B,) float32 out (|a|_2, CrossCorrelationMatcher.py:244) or NULL. */
+int mtb_fle_forward(mtb_fle* h, const float* vol, int B, float* coeffs, int64_t coeff_stride,
+                    float* norms, mtb_stream_t stream);
+
+/* sigma[b, Dindex(l, m, mp)] = (-1)^(m+mp) sum_k tmpl[l, -mp, k] conj(coeffs[b, l, -m, k])
+ * for l <= lmax (CrossCorrelationMatcher.py:183-212).  coeffs (B, coeff_stride) and
+ * tmpl (ne,) complex64; sigma (B, sigma_stride) complex64 out, dsize(lmax) entries. */
+int mtb_sigma(mtb_fle* h, const float* coeffs, int64_t coeff_stride, const float* tmpl, int B,
+              float* sigma, int64_t sigma_stride, mtb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,6 +41,19 @@ class MtbSearchConfig(ctypes.Structure):
     ]
 
 
+class MtbFleConfig(ctypes.Structure):
+    _fields_ = [
+        ("N", ctypes.c_int), ("max_batch", ctypes.c_int), ("ne", ctypes.c_int), ("n_rep", ctypes.c_int),
+        ("n_cols", ctypes.c_int), ("lmax", ctypes.c_int), ("n_lk", ctypes.c_int), ("n_r2", ctypes.c_int),
+        ("rep_img", ctypes.c_void_p), ("rep_cos", ctypes.c_void_p), ("rep_phi", ctypes.c_void_p),
+        ("rep_r2", ctypes.c_void_p), ("jtab", ctypes.c_void_p), ("col_class", ctypes.c_void_p),
+        ("col_l", ctypes.c_void_p), ("col_m", ctypes.c_void_p), ("col_part", ctypes.c_void_p),
+        ("col_lk", ctypes.c_void_p), ("col_scale", ctypes.c_void_p), ("coef_col_re", ctypes.c_void_p),
+        ("coef_col_im", ctypes.c_void_p), ("coef_sign_re", ctypes.c_void_p), ("coef_sign_im", ctypes.c_void_p),
+        ("kpad", ctypes.c_void_p), ("kidx", ctypes.c_void_p),
+    ]
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _I64 = ctypes.c_int64
@@ -54,6 +67,10 @@ SIGNATURES = {
     "mtb_so3_grid_topk": (_I, [_P, _P, _I64, _I, _P, _P, _P, _P, _P]),
     "mtb_newton_march": (_I, [_P, _P, _I64, _I, _P, _P, _P, _P, _P]),
     "mtb_search_orientations": (_I, [_P, _P, _I64, _I, _P, _P, _P, _P, _P]),
+    "mtb_fle_create": (_I, [ctypes.POINTER(MtbFleConfig), ctypes.POINTER(_P)]),
+    "mtb_fle_destroy": (None, [_P]),
+    "mtb_fle_forward": (_I, [_P, _P, _I, _P, _I64, _P, _P]),
+    "mtb_sigma": (_I, [_P, _P, _I64, _P, _I, _P, _I64, _P]),
 }
 
 

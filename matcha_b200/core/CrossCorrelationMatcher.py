@@ -1,0 +1,95 @@
+"""Drop-in ``CrossCorrelationMatcher`` (src/matcha/core/CrossCorrelationMatcher.py).
+
+``get_sigma`` runs the ball expansion of the whole batch (``mtb_fle_forward``) and the
+per-degree contraction with the template (``mtb_sigma``) on the current stream, and
+returns the persistent ``sigma`` / ``bh_norms`` buffers zeroed and refilled, as the
+reference does.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+import torch.nn.functional as F
+
+from .. import _native as N
+from .FLEBasis3D import FLEBasis3D
+from .fle_tables import sht_index as get_sht_index  # noqa: F401  (reference name)
+from .wigner_index import compute_size
+
+
+def _to_complex(dtype):
+    if dtype == torch.float32:
+        return torch.complex64
+    if dtype == torch.float64:
+        return torch.complex128
+    raise ValueError(f"Unsupported dtype {dtype} for conversion to complex.")
+
+
+class CrossCorrelationMatcher:
+    """Ball expansion + correlation coefficients sigma (CrossCorrelationMatcher.py:37-249)."""
+
+    def __init__(self, N: int, device: torch.device, expansion_epsilon: float = 1e-4, batchsize: int = 1,
+                 reduce_memory: bool = True, bandlimit: int = None, micro_batch_split: int = 2,
+                 dtype=torch.float32, radius: int = None, jl_zeros_path: str = None, cs_path: str = None,
+                 precision_mode: str = "accurate"):
+        self.N = N
+        self.fle_basis_eps = expansion_epsilon
+        self.batchsize = batchsize
+        self.reduce_memory = reduce_memory
+        self.bandlimit = bandlimit
+        self.micro_batch_split = int(micro_batch_split)
+        if self.micro_batch_split <= 0:
+            raise ValueError("micro_batch_split must be a positive integer.")
+        if self.batchsize == 1:
+            self.micro_batch_split = 1
+        self.micro_batch_size = max(1, min(self.batchsize, (self.batchsize + self.micro_batch_split - 1)
+                                          // self.micro_batch_split))
+        self.device = torch.device(device)
+        self.dtype_real = dtype
+        self.dtype = _to_complex(self.dtype_real)
+        self.radius = radius
+        # the whole batch is expanded in one pass; micro-batching only bounded the
+        # reference's NUFFT workspace
+        self.fle = FLEBasis3D(N=self.N, bandlimit=self.bandlimit, eps=self.fle_basis_eps,
+                              reduce_memory=self.reduce_memory, batchsize=self.batchsize, radius=self.radius,
+                              device=self.device, dtype=torch.complex64, jl_zeros_path=jl_zeros_path,
+                              cs_path=cs_path, precision_mode=precision_mode)
+        self.lmax = self.fle.lmax
+        self.sigma = torch.zeros((self.batchsize, compute_size(self.lmax + 1)), dtype=torch.complex64,
+                                 device=self.device)
+        self.bh_norms = torch.zeros((self.batchsize,), dtype=torch.float32, device=self.device)
+        self._coeffs = torch.zeros((self.batchsize, self.fle.ne), dtype=torch.complex64, device=self.device)
+        self.template_coefficients_alphas_torch = None
+        self.bh_norm_template = None
+
+    @torch.no_grad()
+    def set_template(self, template_data: np.ndarray, mask: torch.Tensor = None):
+        """Expand the template (N, N, N); keeps its coefficients and norm (:117-130)."""
+        t = torch.from_numpy(np.ascontiguousarray(template_data).copy()).to(dtype=torch.float32, device=self.device)
+        a, norms = self.fle._forward(t.unsqueeze(0), True)
+        self.template_coefficients_alphas_torch = F.pad(a[0], (0, 1))
+        self.bh_norm_template = norms[0]
+
+    @torch.no_grad()
+    def get_sigma(self, volumes: torch.Tensor):
+        """(sigma (batchsize, Dsize(lmax)) complex64, bh_norms (batchsize,)) (:214-249)."""
+        num_volumes = volumes.shape[0]
+        if num_volumes > self.batchsize:
+            raise ValueError(f"Input batch size {num_volumes} exceeds configured batchsize {self.batchsize}.")
+        if self.template_coefficients_alphas_torch is None:
+            raise RuntimeError("set_template must be called before get_sigma")
+        self.sigma.zero_()
+        self.bh_norms.zero_()
+        if num_volumes == 0:
+            return self.sigma, self.bh_norms
+        vol = volumes.to(device=self.device, dtype=torch.float32).contiguous()
+        dev = self.device
+        with torch.cuda.device(dev):
+            N.check(self.fle._lib.mtb_fle_forward(self.fle._h, N.ptr(vol), num_volumes, N.ptr(self._coeffs),
+                                                  self._coeffs.stride(0), N.ptr(self.bh_norms),
+                                                  N.stream_ptr(dev)), "mtb_fle_forward")
+            N.check(self.fle._lib.mtb_sigma(self.fle._h, N.ptr(self._coeffs), self._coeffs.stride(0),
+                                            N.ptr(self.template_coefficients_alphas_torch), num_volumes,
+                                            N.ptr(self.sigma), self.sigma.stride(0), N.stream_ptr(dev)),
+                    "mtb_sigma")
+        return self.sigma, self.bh_norms

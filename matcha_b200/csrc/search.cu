@@ -44,7 +44,7 @@ enum { A_VAL = 0, A_GA, A_GB, A_GG, A_HAA, A_HAB, A_HAG, A_HBB, A_HBG, A_HGG, A_
 
 struct NewtonSmem {
   float* dbuf[2];  // d^l blocks, width 2l+1, double-buffered by l parity
-  float* rowf[2];  // 5 row factors x (2 Lmax + 1), by l parity
+  float* rowf[2];  // 8 floats per row m' (5 row factors), by l parity
   float2* ea;      // exp(i m' alpha), m' = -Li..Li
   float2* eg;      // exp(i m gamma)
   float* red;      // (threads/32) x A_N
@@ -57,13 +57,18 @@ __device__ void newton_pass(const float2* __restrict__ sig, const double* __rest
                             int W, NewtonSmem sm) {
   const int tid = threadIdx.x;
   const int NT = blockDim.x;
-  // phases e^{i m a}, e^{i m g} in double, stored float
+  // phases e^{i m a}, e^{i m g}: argument reduced to [-pi, pi] in double, sincos in float
   for (int r = tid; r < 2 * Li + 1; r += NT) {
-    double s, c;
-    sincos((double)(r - Li) * (double)a, &s, &c);
-    sm.ea[r] = make_float2((float)c, (float)s);
-    sincos((double)(r - Li) * (double)ga, &s, &c);
-    sm.eg[r] = make_float2((float)c, (float)s);
+    const double two_pi = 6.283185307179586;
+    double t = (double)(r - Li) * (double)a;
+    t -= two_pi * rint(t / two_pi);
+    float s, c;
+    sincosf((float)t, &s, &c);
+    sm.ea[r] = make_float2(c, s);
+    t = (double)(r - Li) * (double)ga;
+    t -= two_pi * rint(t / two_pi);
+    sincosf((float)t, &s, &c);
+    sm.eg[r] = make_float2(c, s);
   }
   const float cb = cosf(be);
   double hs, hc;
@@ -71,9 +76,19 @@ __device__ void newton_pass(const float2* __restrict__ sig, const double* __rest
   const double lac = log(fabs(hc)), las = log(fabs(hs));
   const int sgc = hc < 0.0 ? 1 : 0, sgs = hs < 0.0 ? 1 : 0;
 
-  float d1[KP], d0[KP];
+  // wedge pairs p = m'^2 + (m + m') owned by this thread, decoded once per pass
+  float d1[KP], d0[KP], sq[KP];
+  int pmp[KP], pm[KP];
 #pragma unroll
-  for (int k = 0; k < KP; ++k) { d1[k] = 0.f; d0[k] = 0.f; }
+  for (int k = 0; k < KP; ++k) {
+    const int p = tid + k * NT;
+    int mp = (int)sqrtf((float)p);
+    while (mp * mp > p) --mp;
+    while ((mp + 1) * (mp + 1) <= p) ++mp;
+    pmp[k] = mp;
+    pm[k] = p - mp * mp - mp;
+    d1[k] = 0.f; d0[k] = 0.f; sq[k] = 0.f;
+  }
 
   float acc[A_N];
 #pragma unroll
@@ -82,16 +97,17 @@ __device__ void newton_pass(const float2* __restrict__ sig, const double* __rest
   for (int l = 0; l <= Li; ++l) {
     const int w = 2 * l + 1;
     float* dcur = sm.dbuf[l & 1];
-    // ---- recurrence: wedge pairs p = m'^2 + (m + m'), m' = 0..l, |m| <= m'
+    // ---- recurrence (l-1 -> l) for the wedge m' >= |m|, symmetric copies to shared
     const int npair = (l + 1) * (l + 1);
+    const float fl = (float)l;
+    const float inv_lm = (l > 1) ? 1.f / (float)(l - 1) : 0.f;
+    const float a1 = (2.f * fl - 1.f) * (fl - 1.f) * fl;
+    const float a2 = (2.f * fl - 1.f);
 #pragma unroll
     for (int k = 0; k < KP; ++k) {
       const int p = tid + k * NT;
       if (p < npair) {
-        int mp = (int)sqrtf((float)p);
-        while (mp * mp > p) --mp;
-        while ((mp + 1) * (mp + 1) <= p) ++mp;
-        const int m = p - mp * mp - mp;
+        const int mp = pmp[k], m = pm[k];
         float v;
         if (mp == l) {
           // closed form at l0 = m': (-1)^(m'-m) sqrt((2m')!/((m'+m)!(m'-m)!)) c^(m'+m) s^(m'-m)
@@ -99,25 +115,26 @@ __device__ void newton_pass(const float2* __restrict__ sig, const double* __rest
           double lg = logC[p];
           if (pc) lg += pc * lac;
           if (ps) lg += ps * las;
-          double dv = exp(lg);
+          const double dv = exp(lg);
           const int sgn = (ps & 1) ^ ((pc & 1) & sgc) ^ ((ps & 1) & sgs);
           v = (float)(sgn ? -dv : dv);
           d0[k] = 0.f;
+          sq[k] = 0.f;  // sqrt(X_l0) = 0
         } else if (l == 1) {
-          v = cb * d1[k];  // (m', m) = (0, 0)
+          v = cb * d1[k];  // (m', m) = (0, 0); X_1 = 1
           d0[k] = d1[k];
+          sq[k] = 1.f;
         } else {
-          const float lm = (float)(l - 1);
-          const float fl = (float)l;
-          const float mm = (float)m, mmp = (float)mp;
-          const float aa = (2.f * fl - 1.f) * (lm * fl * cb - mm * mmp);
-          const float xp = (lm * lm - mm * mm) * (lm * lm - mmp * mmp);
-          const float xc = (fl * fl - mm * mm) * (fl * fl - mmp * mmp);
-          v = (aa * d1[k] - fl * sqrtf(xp) * d0[k]) / (lm * sqrtf(xc));
+          const float mm = (float)(m * m), pp = (float)(mp * mp), l2 = fl * fl;
+          const float x = (l2 - mm) * (l2 - pp);
+          const float inv = rsqrtf(x);
+          const float aa = a1 * cb - a2 * (float)(m * mp);
+          v = (aa * d1[k] - fl * sq[k] * d0[k]) * inv * inv_lm;
           d0[k] = d1[k];
+          sq[k] = x * inv;
         }
         d1[k] = v;
-        // symmetric copies: d_{m m'} = d_{-m',-m} = (-1)^(m'-m) d_{m'm}; d_{-m,-m'} = d_{m'm}
+        // d_{m m'} = d_{-m',-m} = (-1)^(m'-m) d_{m'm};  d_{-m,-m'} = d_{m'm}
         const float vs = ((mp - m) & 1) ? -v : v;
         dcur[(mp + l) * w + (m + l)] = v;
         dcur[(m + l) * w + (mp + l)] = vs;
@@ -125,54 +142,65 @@ __device__ void newton_pass(const float2* __restrict__ sig, const double* __rest
         dcur[(-mp + l) * w + (-m + l)] = vs;
       }
     }
-    // ---- row factors of WignerDGradients.py:45-79 for m' = -l..l
+    // ---- row factors of WignerDGradients.py:45-79 for m' = -l..l, packed per row
     if (derivs) {
       float* rf = sm.rowf[l & 1];
       for (int r = tid; r < w; r += NT) {
-        const float fl = (float)l, mp = (float)(r - l);
-        rf[0 * W + r] = -0.5f * sqrtf(fmaxf((fl + mp) * (fl - mp + 1.f), 0.f));
-        rf[1 * W + r] = 0.5f * sqrtf(fmaxf((fl - mp) * (fl + mp + 1.f), 0.f));
-        rf[2 * W + r] = 0.25f * sqrtf(fmaxf((fl + mp) * (fl - mp + 1.f) * (fl + mp - 1.f) * (fl - mp + 2.f), 0.f));
-        rf[3 * W + r] = -0.25f * ((fl + mp) * (fl - mp + 1.f) + (fl + mp + 1.f) * (fl - mp));
-        rf[4 * W + r] = 0.25f * sqrtf(fmaxf((fl + mp + 1.f) * (fl - mp) * (fl + mp + 2.f) * (fl - mp - 1.f), 0.f));
+        const float mp = (float)(r - l);
+        rf[8 * r + 0] = -0.5f * sqrtf(fmaxf((fl + mp) * (fl - mp + 1.f), 0.f));
+        rf[8 * r + 1] = 0.5f * sqrtf(fmaxf((fl - mp) * (fl + mp + 1.f), 0.f));
+        rf[8 * r + 2] = 0.25f * sqrtf(fmaxf((fl + mp) * (fl - mp + 1.f) * (fl + mp - 1.f) * (fl - mp + 2.f), 0.f));
+        rf[8 * r + 3] = -0.25f * ((fl + mp) * (fl - mp + 1.f) + (fl + mp + 1.f) * (fl - mp));
+        rf[8 * r + 4] = 0.25f * sqrtf(fmaxf((fl + mp + 1.f) * (fl - mp) * (fl + mp + 2.f) * (fl - mp - 1.f), 0.f));
       }
     }
     __syncthreads();
-    // ---- contraction over the (2l+1)^2 entries of degree l
+    // ---- contraction over degree l: thread = (column c, chunk of rows), walking down
+    //      the column with a sliding window d(r-2..r+2) so each entry is read once
     const float2* sl = sig + mtb_dsize(l - 1);
     const bool zap = compat_top && (l == Li);
     const float* rf = sm.rowf[l & 1];
-    for (int e = tid; e < w * w; e += NT) {
-      const int r = e / w;       // m' + l
-      const int c = e - r * w;   // m + l
-      const float2 s = __ldg(&sl[e]);
-      const float2 ph = cmul(sm.ea[r - l + Li], sm.eg[c - l + Li]);
-      const float er = ph.x * s.x - ph.y * s.y;
-      const float ei = ph.x * s.y + ph.y * s.x;
-      float dc = dcur[e];
-      if (zap && (r == 0 || c == 0)) dc = 0.f;
-      acc[A_VAL] += dc * er;
-      if (derivs) {
-        const float mp = (float)(r - l), m = (float)(c - l);
-        auto dat = [&](int rr) -> float {
-          if (rr < 0 || rr >= w) return 0.f;
-          if (zap && (rr == 0 || c == 0)) return 0.f;
-          return dcur[rr * w + c];
-        };
-        const float dm1 = dat(r - 1), dp1 = dat(r + 1), dm2 = dat(r - 2), dp2 = dat(r + 2);
-        const float db = rf[0 * W + r] * dm1 + rf[1 * W + r] * dp1;
-        const float dbb = rf[3 * W + r] * dc + rf[2 * W + r] * dm2 + rf[4 * W + r] * dp2;
-        const float t = dc * er, u = dc * ei;
-        acc[A_GA] -= mp * u;
-        acc[A_GG] -= m * u;
-        acc[A_HAA] -= mp * mp * t;
-        acc[A_HGG] -= m * m * t;
-        acc[A_HAG] -= mp * m * t;
-        acc[A_GB] += db * er;
-        const float x = db * ei;
-        acc[A_HAB] -= mp * x;
-        acc[A_HBG] -= m * x;
-        acc[A_HBB] += dbb * er;
+    const int G = max(1, NT / w);
+    const int chunk = (w + G - 1) / G;
+    const int c = tid % w, g = tid / w;
+    if (g < G) {
+      const int r0 = g * chunk;
+      const int r1 = min(w, r0 + chunk);
+      const bool zc = zap && (c == 0);
+      auto ld = [&](int rr) -> float {
+        if (rr < 0 || rr >= w || zc || (zap && rr == 0)) return 0.f;
+        return dcur[rr * w + c];
+      };
+      const float2 egc = sm.eg[c - l + Li];
+      const float m = (float)(c - l);
+      float dm2 = ld(r0 - 2), dm1 = ld(r0 - 1), dc = ld(r0), dp1 = ld(r0 + 1);
+      for (int r = r0; r < r1; ++r) {
+        const float dp2 = ld(r + 2);
+        const float2 s = __ldg(&sl[r * w + c]);
+        const float2 q = cmul(egc, s);
+        const float2 ear = sm.ea[r - l + Li];
+        const float er = ear.x * q.x - ear.y * q.y;
+        const float ei = ear.x * q.y + ear.y * q.x;
+        acc[A_VAL] += dc * er;
+        if (derivs) {
+          const float mp = (float)(r - l);
+          const float4 f4 = *reinterpret_cast<const float4*>(&rf[8 * r]);
+          const float f5 = rf[8 * r + 4];
+          const float db = f4.x * dm1 + f4.y * dp1;
+          const float dbb = f4.w * dc + f4.z * dm2 + f5 * dp2;
+          const float t = dc * er, u = dc * ei;
+          acc[A_GA] -= mp * u;
+          acc[A_GG] -= m * u;
+          acc[A_HAA] -= mp * mp * t;
+          acc[A_HGG] -= m * m * t;
+          acc[A_HAG] -= mp * m * t;
+          acc[A_GB] += db * er;
+          const float x = db * ei;
+          acc[A_HAB] -= mp * x;
+          acc[A_HBG] -= m * x;
+          acc[A_HBB] += dbb * er;
+        }
+        dm2 = dm1; dm1 = dc; dc = dp1; dp1 = dp2;
       }
     }
   }
@@ -222,7 +250,7 @@ __device__ bool solve3(const double H[3][3], const double g[3], double x[3]) {
 }
 
 template <int KP>
-__global__ void __launch_bounds__(kNewtonThreads)
+__global__ void __launch_bounds__(kNewtonThreads, 2)
 newton_march_kernel(const float2* __restrict__ sigma, int64_t stride, int BC,
                     float* __restrict__ alpha, float* __restrict__ beta, float* __restrict__ gamma,
                     float* __restrict__ score, const double* __restrict__ logC, SearchParams P) {
@@ -231,9 +259,9 @@ newton_march_kernel(const float2* __restrict__ sigma, int64_t stride, int BC,
   NewtonSmem sm;
   sm.dbuf[0] = smem;
   sm.dbuf[1] = smem + W * W;
-  sm.rowf[0] = smem + 2 * W * W;
-  sm.rowf[1] = sm.rowf[0] + 5 * W;
-  sm.ea = reinterpret_cast<float2*>(sm.rowf[1] + 5 * W);
+  sm.rowf[0] = smem + 2 * W * W + 2;  // 16-byte aligned (W odd: 2 W^2 + 2 = 0 mod 4)
+  sm.rowf[1] = sm.rowf[0] + 8 * W;
+  sm.ea = reinterpret_cast<float2*>(sm.rowf[1] + 8 * W);
   sm.eg = sm.ea + W;
   sm.red = reinterpret_cast<float*>(sm.eg + W);
   sm.res = sm.red + (kNewtonThreads / 32) * A_N;
@@ -498,7 +526,7 @@ template <int KP>
 int launch_newton(const float2* sigma, int64_t stride, int BC, float* a, float* b, float* g, float* s,
                   const double* logC, const SearchParams& P, cudaStream_t st) {
   const int W = 2 * P.Lmax + 1;
-  const size_t smem = (size_t)(2 * W * W + 10 * W) * sizeof(float) + (size_t)2 * W * sizeof(float2) +
+  const size_t smem = (size_t)(2 * W * W + 2 + 16 * W) * sizeof(float) + (size_t)2 * W * sizeof(float2) +
                       (size_t)((kNewtonThreads / 32) * A_N + A_N) * sizeof(float);
   MTB_CUDA_TRY(cudaFuncSetAttribute(newton_march_kernel<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   newton_march_kernel<KP><<<BC, kNewtonThreads, smem, st>>>(sigma, stride, BC, a, b, g, s, logC, P);
