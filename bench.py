@@ -1,0 +1,425 @@
+#!/usr/bin/env python
+"""Throughput of one alignment alternation: subtomograms/s at 64^3, L=32 on B200.
+
+Workload (the plain-method benchmark shape): a 64^3 float32 template made of 400
+Gaussian blobs (sigma U[1, 2.5] voxels) in two lobes of radius 26 and 18 voxels,
+soft-masked; 1000 subtomograms, each the template rotated by a Haar-uniform rotation
+(trilinear resampling in the reference's convention), shifted by a uniform offset in
+[-5, 5]^3 voxels (Fourier phase ramp) and given white Gaussian noise at 0 dB SNR inside
+the mask.  One step is one alternation over the whole batch: ball expansion and
+correlation coefficients (L = 32), SO(3) grid search and Newton march over
+L = 8, 16, 24, 32 with 10 candidates and one Newton step, rotation-tracker update and
+the FFT shift match (search radius 5, upsample factor 8).  Synthetic data; inputs are
+generated on the device before the timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank aligns its own batch (no collective on the data path); the
+step time is the maximum over ranks.  ``--impl reference`` times the CPU restatement of
+the reference's algorithm (the oracle) on the host cores, on a bounded sample per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_BOX, L_MAX, LI = 64, 32, [8, 16, 24]
+SHIFT_RADIUS, UPSAMPLE = 5, 8
+METRIC = "subtomograms/s at 64^3 L=32 (one alternation: FLE+sigma, SO(3) grid, Newton march, shift)"
+KERNELS_PER_STEP = 15  # fold, gemm, expand, sigma, grid, newton, reduce, tracker, bg, rfft_x, fft_y,
+# fft_z, updft1, updft23, finalize
+
+
+def parse():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--batch", type=int, default=1000)
+    p.add_argument("--cpu-sample", type=int, default=2, help="subtomograms per CPU-baseline step")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--seed", type=int, default=0)
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------- synthetic data (numpy, host)
+def make_template(rng, N=N_BOX, n_blobs=400):
+    g = np.arange(N) - N // 2
+    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    vol = np.zeros((N, N, N))
+    lobes = [(26.0, np.array([-3.0, 1.0, 0.0])), (18.0, np.array([6.0, -4.0, 3.0]))]
+    for i in range(n_blobs):
+        r_l, off = lobes[i % 2]
+        d = rng.standard_normal(3)
+        c = off + d / np.linalg.norm(d) * r_l * rng.uniform() ** (1 / 3)
+        s = rng.uniform(1.0, 2.5)
+        vol += rng.uniform(0.5, 1.0) * np.exp(-((z - c[0]) ** 2 + (y - c[1]) ** 2 + (x - c[2]) ** 2) / (2 * s * s))
+    r = np.sqrt(x ** 2 + y ** 2 + z ** 2)
+    vol *= np.clip((0.45 * N + 2 - r) / 4, 0, 1)
+    return vol.astype(np.float32)
+
+
+def make_batch(template, rng, B, device):
+    """Rotated (reference rotate_volumes convention), shifted, noisy subtomograms on the device."""
+    import torch
+    import torch.nn.functional as TF
+    from scipy.spatial.transform import Rotation as R
+
+    N = template.shape[0]
+    q = rng.standard_normal((B, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    shifts = rng.uniform(-5, 5, (B, 3)).astype(np.float32)
+    mats = torch.tensor(R.from_quat(np.roll(q, -1, axis=1)).as_matrix(), dtype=torch.float32, device=device)
+    t = torch.from_numpy(template).to(device)
+    tp = TF.pad(t[None, None], (0, 1, 0, 1, 0, 1))
+    lin = torch.linspace(-1, 1, N + 1, device=device)
+    wg, hg, dg = torch.meshgrid(lin, lin, lin, indexing="ij")
+    coords = torch.stack([dg.flatten(), hg.flatten(), wg.flatten()], 0)
+    k = torch.fft.fftfreq(N, device=device)
+    kz, ky, kx = torch.meshgrid(k, k, k, indexing="ij")
+    g = torch.arange(N, device=device) - N // 2
+    zz, yy, xx = torch.meshgrid(g, g, g, indexing="ij")
+    mask = (torch.sqrt((xx ** 2 + yy ** 2 + zz ** 2).float()) < 0.45 * N)
+    out = torch.empty((B, N, N, N), device=device, dtype=torch.float32)
+    sh = torch.from_numpy(shifts).to(device)
+    noise_gen = torch.Generator(device=device)
+    noise_gen.manual_seed(int(rng.integers(1 << 31)))
+    for s in range(0, B, 50):
+        e = min(B, s + 50)
+        rc = (mats[s:e] @ coords).permute(0, 2, 1).reshape(e - s, N + 1, N + 1, N + 1, 3)
+        v = TF.grid_sample(tp.expand(e - s, -1, -1, -1, -1), rc, mode="bilinear", align_corners=True)
+        v = v[:, 0, :N, :N, :N]
+        ph = torch.exp(-2j * np.pi * (kz[None] * sh[s:e, 0, None, None, None] + ky[None] * sh[s:e, 1, None, None, None]
+                                      + kx[None] * sh[s:e, 2, None, None, None]))
+        v = torch.fft.ifftn(torch.fft.fftn(v, dim=(1, 2, 3)) * ph, dim=(1, 2, 3)).real
+        power = (v[:, mask] ** 2).mean(dim=1)
+        noise = torch.randn(v.shape, device=device, generator=noise_gen) * torch.sqrt(power)[:, None, None, None]
+        out[s:e] = v + noise
+    return out, q, shifts
+
+
+def rotation_error_deg(alpha, beta, gamma, q_true):
+    """Tracker angle after update_rotation_estimate from the true rotation (example.py:208-220)."""
+    from scipy.spatial.transform import Rotation as R
+
+    est = R.from_euler("ZYZ", np.stack([alpha, beta, gamma], -1)).as_quat()
+    qw = np.roll(est, 1, axis=1)
+    qw[:, [1, 3]] = qw[:, [3, 1]]
+    sw = R.from_quat(np.roll(qw, -1, axis=1))
+    tr = R.from_quat(np.roll(q_true, -1, axis=1))
+    return np.rad2deg((tr * sw.inv()).magnitude())
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"mtb_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU restatement (oracle)
+def cpu_align(sample, template, vols, q_true, threads=None):
+    """Oracle pipeline on a few subtomograms; returns (seconds per subtomogram, outputs)."""
+    from matcha_b200.core import fle_tables as T
+    from oracle import fle as OF
+    from oracle import pipeline as OP
+    from oracle import shift as OS
+
+    radius = min(N_BOX // 2, int(N_BOX // 2 * 0.95))
+    tb = T.lap_eig_ball(N_BOX, L_MAX, radius)
+    ff = OP.FoldedFLE(tb, N_BOX, float(radius))
+    a_t = ff.evaluate_t(template[None])[0]
+    ref = OS.load_reference_full(template, N_BOX, 1.0)
+    v = vols[:sample].astype(np.float64)
+    tracker = np.tile([1.0, 0, 0, 0], (sample, 1))
+    t0 = time.perf_counter()
+    out = OP.align_batch(ff, a_t, ref, v, v, tracker, np.zeros((sample, 3)), L_MAX, LI, uf=UPSAMPLE,
+                         shift_radius=SHIFT_RADIUS)
+    dt = time.perf_counter() - t0
+    return dt / sample, out
+
+
+# ---------------------------------------------------------------- our implementation
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device(f"cuda:{local}")
+    from matcha_b200.pipeline import AlignmentStep, StepConfig
+
+    rng = np.random.default_rng(args.seed)
+    template = make_template(rng)
+    B = args.batch
+    vols, q_true, shifts = make_batch(template, np.random.default_rng(args.seed + 1 + rank), B, dev)
+    step = AlignmentStep(StepConfig(N=N_BOX, L=L_MAX, Li=LI, batch=B, shift_search_radius=SHIFT_RADIUS,
+                                    shift_upsample_factor=UPSAMPLE), dev)
+    step.set_template(template)
+    ident = torch.zeros((B, 4), device=dev, dtype=torch.float64)
+    ident[:, 0] = 1
+    tracker = ident.clone()
+    zeros3 = torch.zeros((B, 3), device=dev, dtype=torch.float32)
+
+    def one():
+        tracker.copy_(ident)
+        return step(vols, vols, tracker, zeros3)
+
+    for _ in range(args.warmup):
+        out = one()
+    torch.cuda.synchronize()
+    # per-stage breakdown (one extra untimed step)
+    st = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    tracker.copy_(ident)
+    ev[0].record(st)
+    sigma, norms = step.correlator.get_sigma(vols)
+    ev[1].record(st)
+    a, b, g, sc = step.matcher.search_orientations(sigma)
+    ev[2].record(st)
+    step(vols, vols, tracker, zeros3)  # full step (includes a second sigma/search)
+    ev[3].record(st)
+    torch.cuda.synchronize()
+    t_sigma = ev[0].elapsed_time(ev[1])
+    t_search = ev[1].elapsed_time(ev[2])
+    t_full = ev[2].elapsed_time(ev[3])
+    stages = {"fle_sigma_ms": t_sigma, "search_ms": t_search, "shift_ms": max(0.0, t_full - t_sigma - t_search)}
+    # per-kernel timing of the candidates for the roofline (launch stream events)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0, b0, g0 = step.matcher._grid_search_so3fft(sigma)
+    torch.cuda.synchronize()
+    e0.record(st)
+    step.matcher.march(a0, b0, g0, sigma)
+    e1.record(st)
+    torch.cuda.synchronize()
+    t_march = e0.elapsed_time(e1)
+    # timed region
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        start.record(st)
+        for _ in range(args.steps):
+            out = one()
+        end.record(st)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end) / args.steps
+    if world > 1:
+        tms = torch.tensor([ms], device=dev)
+        dist.all_reduce(tms, op=dist.ReduceOp.MAX)
+        ms = float(tms.item())
+        dist.barrier()
+    # end-to-end through the public API with host buffers
+    host = vols.cpu().pin_memory()
+    dvol = torch.empty_like(vols)
+    res_host = torch.empty((B, 8), dtype=torch.float32).pin_memory()
+    res_dev = torch.empty((B, 8), device=dev, dtype=torch.float32)
+    e2e_start, e2e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e2e_steps = max(1, min(args.steps, 5))
+    e2e_start.record(st)
+    for _ in range(e2e_steps):
+        dvol.copy_(host, non_blocking=True)
+        tracker.copy_(ident)
+        o = step(dvol, dvol, tracker, zeros3)
+        res_dev[:, 0], res_dev[:, 1], res_dev[:, 2], res_dev[:, 3] = o["alpha"], o["beta"], o["gamma"], o["rotation_score"]
+        res_dev[:, 4:7] = o["shift"]
+        res_dev[:, 7] = o["shift_score"]
+        res_host.copy_(res_dev, non_blocking=True)
+    e2e_end.record(st)
+    torch.cuda.synchronize()
+    e2e_ms = e2e_start.elapsed_time(e2e_end) / e2e_steps
+    if world > 1:
+        t2 = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t2.item())
+    # accuracy of the last step
+    al, be, ga = (out[k].cpu().numpy() for k in ("alpha", "beta", "gamma"))
+    err = rotation_error_deg(al, be, ga, q_true)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    peaks = {}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peaks = json.load(open(pp))
+    # roofline of the Newton march (FP32 CUDA cores): algorithmic flops per launch,
+    # sum over stages of (15 + 2) * 8 * C * Dsize(Li) * steps + 8 * C * Dsize(Li), per subtomogram
+    from matcha_b200.core.wigner_index import dsize
+
+    C, steps_n = 10, 1
+    flop_sub = sum((15 + 2) * 8 * C * dsize(l) * steps_n + 8 * C * dsize(l) for l in LI + [L_MAX])
+    achieved = flop_sub * B / (t_march * 1e-3) / 1e12
+    clocks = clk.summary()
+    fp32_peak = 148 * 128 * 2 * (clocks["sm_mhz"] or 1965.0) * 1e6 / 1e12
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    line = {
+        "metric": METRIC,
+        "value": world * B / (ms * 1e-3),
+        "unit": "subtomograms/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{B} subtomograms 64^3, L=32, march 8/16/24/32, C=10, 1 Newton step, "
+                               f"shift r=5 uf=8, 0 dB", "batch_per_gpu": B, "box": N_BOX, "L": L_MAX,
+                   "parallelism": f"replicas x{world}", "l2": "inputs 1.05 GB per step > 126 MB L2"},
+        "median_rot_err_deg": float(np.median(err)),
+        "p90_rot_err_deg": float(np.percentile(err, 90)),
+        "stages_ms": stages,
+        "roofline": {"kernel": "newton_march_kernel", "bound": "tensor", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "fp32_core_peak_tflops": fp32_peak, "fp32_core_frac": achieved / fp32_peak,
+                     "kernel_ms": t_march, "traffic": None,
+                     "note": "FP32 CUDA-core kernel; peak is the measured bf16 tensor figure"},
+        "e2e": {"value": world * B / (e2e_ms * 1e-3), "unit": "subtomograms/s",
+                "h2d_bytes_per_step": int(B * N_BOX ** 3 * 4), "d2h_bytes_per_step": int(B * 8 * 4)},
+        "gpu_launches": KERNELS_PER_STEP * args.steps,
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            import torch as _t
+
+            sec, _ = cpu_align(args.cpu_sample, template, vols[: args.cpu_sample].cpu().numpy(), q_true)
+            line["cpu_baseline"] = {"value": 1.0 / sec, "unit": "subtomograms/s", "cores": os.cpu_count(),
+                                    "kind": "port", "sample": f"{args.cpu_sample} subtomograms through the oracle "
+                                                              f"(folded exact FLE, sigma, grid, march, shift)"}
+        except Exception as exc:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": "subtomograms/s", "cores": os.cpu_count(),
+                                    "kind": "port", "sample": f"failed: {exc!r}"[:200]}
+    print(json.dumps(line))
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    rng = np.random.default_rng(args.seed)
+    template = make_template(rng)
+    sample = max(1, args.cpu_sample)
+    # inputs: rotated, noisy subtomograms made on the host (no GPU on this arm)
+    from scipy.ndimage import map_coordinates
+    from scipy.spatial.transform import Rotation as R
+
+    q = rng.standard_normal((sample, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    g = np.linspace(-1, 1, N_BOX + 1)
+    wg, hg, dg = np.meshgrid(g, g, g, indexing="ij")
+    coords = np.stack([dg.ravel(), hg.ravel(), wg.ravel()], 0)
+    vols = np.zeros((sample, N_BOX, N_BOX, N_BOX), dtype=np.float32)
+    tp = np.pad(template, ((0, 1), (0, 1), (0, 1)))
+    for i in range(sample):
+        rc = R.from_quat(np.roll(q[i], -1)).as_matrix() @ coords
+        idx = (rc + 1) / 2 * N_BOX  # align_corners=True over N+1 samples
+        v = map_coordinates(tp, [idx[2], idx[1], idx[0]], order=1, mode="constant").reshape(N_BOX + 1, N_BOX + 1,
+                                                                                              N_BOX + 1)
+        v = v[:N_BOX, :N_BOX, :N_BOX]
+        vols[i] = v + rng.standard_normal(v.shape) * np.sqrt((v ** 2).mean())
+    times = []
+    for it in range(args.warmup + args.steps):
+        sec, _ = cpu_align(sample, template, vols, q)
+        if it >= args.warmup:
+            times.append(sec)
+    per = float(np.mean(times))
+    value = 1.0 / per
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "subtomograms/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": per * sample * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{args.batch} subtomograms 64^3, L=32, march 8/16/24/32, C=10, 1 Newton step, "
+                               f"shift r=5 uf=8, 0 dB", "batch_per_gpu": args.batch, "box": N_BOX, "L": L_MAX,
+                   "parallelism": "host cores"},
+        "cpu_baseline": {"value": value, "unit": "subtomograms/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"{sample} subtomograms per step through the oracle restatement"},
+        "e2e": {"value": value, "unit": "subtomograms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

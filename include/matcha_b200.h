@@ -150,6 +150,44 @@ int mtb_fle_forward(mtb_fle* h, const float* vol, int B, float* coeffs, int64_t 
 int mtb_sigma(mtb_fle* h, const float* coeffs, int64_t coeff_stride, const float* tmpl, int B,
               float* sigma, int64_t sigma_stride, mtb_stream_t stream);
 
+/* ------------------------------------------------------------------------------
+ * FFT shift match (RELION-style masked correlation with a local upsampled DFT).
+ * Replaces estimate_shift_like_relion and what it calls
+ * (src/matcha/core/ShiftMatcher.py:46-282, 491-674): rotate_complex_volume,
+ * extract_shifted_patch_batch, apply_cosine_mask, rfftn and compute_shift_local.
+ * ---------------------------------------------------------------------------- */
+typedef struct {
+  int N;                 /* box edge, power of two                                  */
+  int max_batch;         /* largest B any call will pass                            */
+  int upsample_factor;   /* shift_upsample_factor (ShiftMatcher.py:660)             */
+  int search_radius;     /* shift_search_radius; window 2r+1 (ShiftMatcher.py:661-662) */
+  float mask_radius;     /* box_size / (2 voxel_size), setup_utils.py:292-295; <0: N/2 */
+  float cosine_width;    /* 5.0 in the reference (setup_utils.py:295)               */
+} mtb_shift_config;
+
+typedef struct mtb_shift mtb_shift;
+
+int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out);
+void mtb_shift_destroy(mtb_shift* h);
+
+/* ref_fourier: (N, N, N) complex64, the fftshifted and masked Fourier reference of
+ * load_reference_full (ShiftMatcher.py:456-472); copied into the handle. */
+int mtb_shift_set_reference(mtb_shift* h, const float* ref_fourier, mtb_stream_t stream);
+
+/* subtomos (B, N, N, N) float32; shift_zyx (B, 3) prior shifts (z, y, x); rot (B, 9)
+ * row-major rotation matrices of the reference's ZYZ Euler angles
+ * (R.from_euler('ZYZ', angles, degrees=True), ShiftMatcher.py:503); ctf (B, N, N, N/2+1)
+ * float32 or NULL.  shift_xyz (B, 3) and score (B,) float32 out. */
+int mtb_shift_search(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot,
+                     const float* ctf, int B, float* shift_xyz, float* score, mtb_stream_t stream);
+
+/* Rotation bookkeeping on the device: tracker <- normalized(tracker * conj(swap_xz(q(a, b, g))))
+ * as update_rotation_estimate (src/matcha/utils/rotation_ops.py:23-34), and rot (B, 9), the
+ * matrix the shift match uses for the new tracker (ShiftMatcher.py:503, :913).  alpha, beta,
+ * gamma (B,) float32; tracker_in / tracker_out (B, 4) float64 (w, x, y, z), may alias. */
+int mtb_update_rotation(const float* alpha, const float* beta, const float* gamma, const double* tracker_in,
+                        int B, double* tracker_out, float* rot, mtb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

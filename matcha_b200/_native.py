@@ -54,6 +54,13 @@ class MtbFleConfig(ctypes.Structure):
     ]
 
 
+class MtbShiftConfig(ctypes.Structure):
+    _fields_ = [
+        ("N", ctypes.c_int), ("max_batch", ctypes.c_int), ("upsample_factor", ctypes.c_int),
+        ("search_radius", ctypes.c_int), ("mask_radius", ctypes.c_float), ("cosine_width", ctypes.c_float),
+    ]
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _I64 = ctypes.c_int64
@@ -71,6 +78,11 @@ SIGNATURES = {
     "mtb_fle_destroy": (None, [_P]),
     "mtb_fle_forward": (_I, [_P, _P, _I, _P, _I64, _P, _P]),
     "mtb_sigma": (_I, [_P, _P, _I64, _P, _I, _P, _I64, _P]),
+    "mtb_shift_create": (_I, [ctypes.POINTER(MtbShiftConfig), ctypes.POINTER(_P)]),
+    "mtb_shift_destroy": (None, [_P]),
+    "mtb_shift_set_reference": (_I, [_P, _P, _P]),
+    "mtb_shift_search": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P]),
+    "mtb_update_rotation": (_I, [_P, _P, _P, _P, _I, _P, _P, _P]),
 }
 
 

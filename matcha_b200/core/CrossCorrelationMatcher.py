@@ -11,7 +11,7 @@ import numpy as np
 import torch
 import torch.nn.functional as F
 
-from .. import _native as N
+from .. import _native as nat
 from .FLEBasis3D import FLEBasis3D
 from .fle_tables import sht_index as get_sht_index  # noqa: F401  (reference name)
 from .wigner_index import compute_size
@@ -85,11 +85,11 @@ class CrossCorrelationMatcher:
         vol = volumes.to(device=self.device, dtype=torch.float32).contiguous()
         dev = self.device
         with torch.cuda.device(dev):
-            N.check(self.fle._lib.mtb_fle_forward(self.fle._h, N.ptr(vol), num_volumes, N.ptr(self._coeffs),
-                                                  self._coeffs.stride(0), N.ptr(self.bh_norms),
-                                                  N.stream_ptr(dev)), "mtb_fle_forward")
-            N.check(self.fle._lib.mtb_sigma(self.fle._h, N.ptr(self._coeffs), self._coeffs.stride(0),
-                                            N.ptr(self.template_coefficients_alphas_torch), num_volumes,
-                                            N.ptr(self.sigma), self.sigma.stride(0), N.stream_ptr(dev)),
+            nat.check(self.fle._lib.mtb_fle_forward(self.fle._h, nat.ptr(vol), num_volumes, nat.ptr(self._coeffs),
+                                                  self._coeffs.stride(0), nat.ptr(self.bh_norms),
+                                                  nat.stream_ptr(dev)), "mtb_fle_forward")
+            nat.check(self.fle._lib.mtb_sigma(self.fle._h, nat.ptr(self._coeffs), self._coeffs.stride(0),
+                                            nat.ptr(self.template_coefficients_alphas_torch), num_volumes,
+                                            nat.ptr(self.sigma), self.sigma.stride(0), nat.stream_ptr(dev)),
                     "mtb_sigma")
         return self.sigma, self.bh_norms

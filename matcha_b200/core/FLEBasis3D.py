@@ -13,7 +13,7 @@ import ctypes
 import numpy as np
 import torch
 
-from .. import _native as N
+from .. import _native as nat
 from . import fle_tables as T
 
 
@@ -142,7 +142,7 @@ class FLEBasis3D:
         ct = build_compact_tables(tb, self.N1, float(radius))
         self.compact = ct
         keep = []
-        cfg = N.MtbFleConfig()
+        cfg = nat.MtbFleConfig()
         cfg.N, cfg.max_batch, cfg.ne, cfg.n_rep = self.N1, self.batchsize, tb.ne, ct["n_rep"]
         cfg.n_cols, cfg.lmax, cfg.n_lk, cfg.n_r2 = ct["n_cols"], tb.lmax, ct["jtab"].shape[1], ct["jtab"].shape[0]
         for name in ("rep_img", "rep_cos", "rep_phi", "rep_r2", "jtab", "col_class", "col_l", "col_m", "col_part",
@@ -151,10 +151,10 @@ class FLEBasis3D:
             arr = np.ascontiguousarray(ct[name])
             keep.append(arr)
             setattr(cfg, name, arr.ctypes.data)
-        lib = N.load()
+        lib = nat.load()
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
-            N.check(lib.mtb_fle_create(ctypes.byref(cfg), ctypes.byref(h)), "mtb_fle_create")
+            nat.check(lib.mtb_fle_create(ctypes.byref(cfg), ctypes.byref(h)), "mtb_fle_create")
         self._h = h
         self._lib = lib
 
@@ -165,7 +165,7 @@ class FLEBasis3D:
             self._h = None
 
     def _forward(self, f: torch.Tensor, want_norms: bool):
-        N.require_cuda(f, "volumes")
+        nat.require_cuda(f, "volumes")
         f = f.reshape(-1, self.N1, self.N1, self.N1)
         if f.dtype != torch.float32:
             f = f.real.to(torch.float32) if f.is_complex() else f.to(torch.float32)
@@ -176,8 +176,8 @@ class FLEBasis3D:
         out = torch.empty((b, self.ne), device=f.device, dtype=torch.complex64)
         norms = torch.empty((b,), device=f.device, dtype=torch.float32) if want_norms else None
         with torch.cuda.device(f.device):
-            N.check(self._lib.mtb_fle_forward(self._h, N.ptr(f), b, N.ptr(out), out.stride(0), N.ptr(norms),
-                                              N.stream_ptr(f.device)), "mtb_fle_forward")
+            nat.check(self._lib.mtb_fle_forward(self._h, nat.ptr(f), b, nat.ptr(out), out.stride(0), nat.ptr(norms),
+                                              nat.stream_ptr(f.device)), "mtb_fle_forward")
         return out, norms
 
     @torch.no_grad()

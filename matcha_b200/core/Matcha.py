@@ -11,7 +11,7 @@ import ctypes
 
 import torch
 
-from .. import _native as N
+from .. import _native as nat
 from .SOFFT import SOFFT
 from .wigner_index import dsize
 
@@ -94,14 +94,14 @@ class Matcha:
         self._truncate_dsize_cache = {int(l): dsize(int(l)) for l in set(self.Li)}
         flags = 0
         if self.compat_top_block:
-            flags |= N.MTB_SEARCH_COMPAT_TOP_BLOCK
+            flags |= nat.MTB_SEARCH_COMPAT_TOP_BLOCK
         if self.step_type == "gradient":
-            flags |= N.MTB_SEARCH_GRADIENT_STEP
-        self._cfg = N.MtbSearchConfig()
+            flags |= nat.MTB_SEARCH_GRADIENT_STEP
+        self._cfg = nat.MtbSearchConfig()
         self._cfg.Lmax = self.Lmax
         self._cfg.n_stages = len(self.stages)
-        if len(self.stages) > N.MTB_MAX_STAGES:
-            raise ValueError(f"at most {N.MTB_MAX_STAGES} march stages are supported")
+        if len(self.stages) > nat.MTB_MAX_STAGES:
+            raise ValueError(f"at most {nat.MTB_MAX_STAGES} march stages are supported")
         for i, l in enumerate(self.stages):
             self._cfg.stages[i] = l
         self._cfg.L0 = self.L0
@@ -110,10 +110,10 @@ class Matcha:
         self._cfg.num_steps = self.num_steps
         self._cfg.max_batch = self.batchsize
         self._cfg.flags = flags
-        lib = N.load()
+        lib = nat.load()
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
-            N.check(lib.mtb_search_create(ctypes.byref(self._cfg), ctypes.byref(h)), "mtb_search_create")
+            nat.check(lib.mtb_search_create(ctypes.byref(self._cfg), ctypes.byref(h)), "mtb_search_create")
         self._h = h
         self._lib = lib
 
@@ -134,7 +134,7 @@ class Matcha:
         return matcha_config
 
     def _prep_sigma(self, sigma: torch.Tensor) -> torch.Tensor:
-        N.require_cuda(sigma, "sigma")
+        nat.require_cuda(sigma, "sigma")
         if sigma.ndim != 2:
             raise ValueError("sigma must have shape (batch, Dsize)")
         if sigma.dtype != torch.complex64:
@@ -154,9 +154,9 @@ class Matcha:
         B = sigma.shape[0]
         out = torch.empty((3, B, self.candidates), device=sigma.device, dtype=torch.float32)
         with torch.cuda.device(sigma.device):
-            N.check(self._lib.mtb_so3_grid_topk(self._h, N.ptr(sigma), sigma.stride(0), B, N.ptr(out[0]),
-                                                N.ptr(out[1]), N.ptr(out[2]), None,
-                                                N.stream_ptr(sigma.device)), "mtb_so3_grid_topk")
+            nat.check(self._lib.mtb_so3_grid_topk(self._h, nat.ptr(sigma), sigma.stride(0), B, nat.ptr(out[0]),
+                                                nat.ptr(out[1]), nat.ptr(out[2]), None,
+                                                nat.stream_ptr(sigma.device)), "mtb_so3_grid_topk")
         return out[0], out[1], out[2]
 
     @torch.no_grad()
@@ -171,8 +171,8 @@ class Matcha:
             raise ValueError("angles must have shape (batch, candidates)")
         s = torch.empty_like(a)
         with torch.cuda.device(sigma.device):
-            N.check(self._lib.mtb_newton_march(self._h, N.ptr(sigma), sigma.stride(0), B, N.ptr(a), N.ptr(b),
-                                               N.ptr(g), N.ptr(s), N.stream_ptr(sigma.device)),
+            nat.check(self._lib.mtb_newton_march(self._h, nat.ptr(sigma), sigma.stride(0), B, nat.ptr(a), nat.ptr(b),
+                                               nat.ptr(g), nat.ptr(s), nat.stream_ptr(sigma.device)),
                     "mtb_newton_march")
         return a, b, g, s
 
@@ -183,7 +183,7 @@ class Matcha:
         B = sigma.shape[0]
         out = torch.empty((4, B), device=sigma.device, dtype=torch.float32)
         with torch.cuda.device(sigma.device):
-            N.check(self._lib.mtb_search_orientations(self._h, N.ptr(sigma), sigma.stride(0), B, N.ptr(out[0]),
-                                                      N.ptr(out[1]), N.ptr(out[2]), N.ptr(out[3]),
-                                                      N.stream_ptr(sigma.device)), "mtb_search_orientations")
+            nat.check(self._lib.mtb_search_orientations(self._h, nat.ptr(sigma), sigma.stride(0), B, nat.ptr(out[0]),
+                                                      nat.ptr(out[1]), nat.ptr(out[2]), nat.ptr(out[3]),
+                                                      nat.stream_ptr(sigma.device)), "mtb_search_orientations")
         return out[0], out[1], out[2], out[3]

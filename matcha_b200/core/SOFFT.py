@@ -11,7 +11,7 @@ import ctypes
 import numpy as np
 import torch
 
-from .. import _native as N
+from .. import _native as nat
 from .wigner_index import dsize
 
 
@@ -33,7 +33,7 @@ class SOFFT:
         h = self._handles.get(candidates)
         if h is not None:
             return h
-        cfg = N.MtbSearchConfig()
+        cfg = nat.MtbSearchConfig()
         cfg.Lmax = self.L
         cfg.n_stages = 1
         cfg.stages[0] = self.L
@@ -43,10 +43,10 @@ class SOFFT:
         cfg.num_steps = 0
         cfg.max_batch = self.batch_size
         cfg.flags = 0
-        lib = N.load()
+        lib = nat.load()
         hh = ctypes.c_void_p()
         with torch.cuda.device(self.device):
-            N.check(lib.mtb_search_create(ctypes.byref(cfg), ctypes.byref(hh)), "mtb_search_create")
+            nat.check(lib.mtb_search_create(ctypes.byref(cfg), ctypes.byref(hh)), "mtb_search_create")
         self._handles[candidates] = hh
         self._lib = lib
         return hh
@@ -58,7 +58,7 @@ class SOFFT:
         self._handles = {}
 
     def _run(self, flmn: torch.Tensor, candidates: int, want_grid: bool):
-        N.require_cuda(flmn, "flmn_coeffs_t")
+        nat.require_cuda(flmn, "flmn_coeffs_t")
         assert flmn.ndim == 2
         if flmn.dtype != torch.complex64:
             flmn = flmn.to(torch.complex64)
@@ -72,9 +72,9 @@ class SOFFT:
         grid = torch.empty((B, n, n, n), device=flmn.device, dtype=torch.float32) if want_grid else None
         h = self._handle(candidates)
         with torch.cuda.device(flmn.device):
-            N.check(self._lib.mtb_so3_grid_topk(h, N.ptr(flmn), flmn.stride(0), B, N.ptr(angles[0]),
-                                                N.ptr(angles[1]), N.ptr(angles[2]), N.ptr(grid),
-                                                N.stream_ptr(flmn.device)), "mtb_so3_grid_topk")
+            nat.check(self._lib.mtb_so3_grid_topk(h, nat.ptr(flmn), flmn.stride(0), B, nat.ptr(angles[0]),
+                                                nat.ptr(angles[1]), nat.ptr(angles[2]), nat.ptr(grid),
+                                                nat.stream_ptr(flmn.device)), "mtb_so3_grid_topk")
         return angles, grid
 
     @torch.no_grad()

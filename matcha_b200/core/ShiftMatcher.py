@@ -1,0 +1,209 @@
+"""Drop-in ``ShiftMatcher`` (src/matcha/core/ShiftMatcher.py) on the B200 kernels.
+
+``set_reference`` keeps the reference's once-per-template preparation on the host
+(``load_reference_full``: soft low-pass, gridding correction, centred FFT, spherical
+Fourier mask, FFT shift; ShiftMatcher.py:377-472) and uploads the result.
+``search_shifts`` turns each rotation tracker into the reference's ZYZ rotation matrix
+on the host (ShiftMatcher.py:503, :913) and runs the whole per-subtomogram shift match
+in ``mtb_shift_search``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+from scipy.spatial.transform import Rotation as R
+
+from .. import _native as nat
+
+
+# ---------------------------------------------------------------- host preparation
+def apply_soft_mask(Irefs, ori_size, pixel_size, ini_high, width_fmask_edge=6.0):
+    """Cosine-edged low-pass in Fourier space (ShiftMatcher.py:377-408)."""
+    if ini_high <= 0:
+        return Irefs
+    radius = ori_size * pixel_size / ini_high - width_fmask_edge / 2.0
+    radius_p = radius + width_fmask_edge
+    out = []
+    for vol in Irefs:
+        ft = np.fft.fftshift(np.fft.fftn(vol, norm="forward"))
+        zd, yd, xd = vol.shape
+        zz, yy, xx = np.indices(vol.shape)
+        r = np.sqrt((xx - xd // 2) ** 2 + (yy - yd // 2) ** 2 + (zz - zd // 2) ** 2)
+        mask = np.ones_like(r)
+        mask[r > radius_p] = 0
+        tz = (r >= radius) & (r <= radius_p)
+        mask[tz] = 0.5 - 0.5 * np.cos(np.pi * (radius_p - r[tz]) / width_fmask_edge)
+        ft *= mask
+        out.append(np.fft.ifftn(np.fft.ifftshift(ft), norm="forward").real.astype(np.float64))
+    return out
+
+
+def gridding_correct(vol_in, ori_size, padding_factor, interpolator, r_min_nn=0):
+    """Divide by sinc^2 (trilinear) or sinc (nearest) of the radius (ShiftMatcher.py:411-439)."""
+    z, y, x = vol_in.shape
+    kk, ii, jj = np.meshgrid(np.arange(-z // 2, z // 2), np.arange(-y // 2, y // 2), np.arange(-x // 2, x // 2),
+                             indexing="ij")
+    rval = np.sqrt(kk ** 2 + ii ** 2 + jj ** 2) / (ori_size * padding_factor)
+    sinc = np.ones_like(rval)
+    nz = rval > 0
+    sinc[nz] = np.sin(np.pi * rval[nz]) / (np.pi * rval[nz])
+    if interpolator == "nearest" and r_min_nn == 0:
+        corr = sinc
+    elif interpolator == "trilinear" or (interpolator == "nearest" and r_min_nn > 0):
+        corr = sinc ** 2
+    else:
+        raise ValueError("Unrecognized interpolator: must be 'nearest' or 'trilinear'")
+    corr[corr == 0] = 1.0
+    return vol_in / corr
+
+
+def get_mask_full(shape):
+    """Spherical mask on FFT index coordinates (ShiftMatcher.py:442-453)."""
+    nz, ny, nx = shape
+    cz, cy = nz // 2, ny // 2
+    Z, Y, X = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    kp = np.where(Z < cz, Z, Z - nz)
+    ip = np.where(Y < cy, Y, Y - ny)
+    jp = np.where(X < cy, X, X - nx)
+    return (kp ** 2 + ip ** 2 + jp ** 2) <= nz // 2 * nz // 2
+
+
+def load_reference_full(ref, volume_size, voxel_size):
+    """Fourier-domain reference used by the shift match (ShiftMatcher.py:456-472)."""
+    ref = np.asarray(ref).astype(np.float64)
+    iref = apply_soft_mask([ref], ori_size=volume_size, pixel_size=voxel_size, ini_high=4.0, width_fmask_edge=2.0)
+    g = gridding_correct(iref[0], ori_size=volume_size, padding_factor=1.0, interpolator="trilinear")
+    h = int(volume_size // 2)
+    faux = np.fft.fftn(np.roll(g, (-h, -h, -h), axis=(0, 1, 2)), norm="forward")
+    mask = np.fft.fftshift(get_mask_full(faux.shape), axes=(0, 1, 2))
+    return np.fft.fftshift(faux, axes=(0, 1, 2)) * mask
+
+
+def tracker_to_euler_deg(rotation_tracker) -> np.ndarray:
+    """np.rad2deg(quaternionic.array(tracker.conj()).to_euler_angles) for (w, x, y, z) trackers."""
+    q = np.asarray(rotation_tracker, dtype=np.float64).reshape(-1, 4) * np.array([1.0, -1.0, -1.0, -1.0])
+    n = (q ** 2).sum(-1)
+    a = np.arctan2(q[:, 3], q[:, 0]) + np.arctan2(-q[:, 1], q[:, 2])
+    b = 2 * np.arccos(np.sqrt((q[:, 0] ** 2 + q[:, 3] ** 2) / n))
+    g = np.arctan2(q[:, 3], q[:, 0]) - np.arctan2(-q[:, 1], q[:, 2])
+    return np.rad2deg(np.stack([a, b, g], -1))
+
+
+def _cfg(config, key, default=None):
+    try:
+        return config.get(key, default)
+    except AttributeError:
+        return getattr(config, key, default)
+
+
+class ShiftMatcher:
+    """Stateful shift-search wrapper (ShiftMatcher.py:766-928)."""
+
+    def __init__(self, config, device: torch.device, dtype: torch.dtype, micro_batch_size: int = None):
+        self.config = config
+        self.device = torch.device(device)
+        self.dtype = dtype
+        nb = _cfg(config, "num_subtomograms_per_batch", 1)
+        self.micro_batch_size = int(micro_batch_size) if micro_batch_size is not None else max(1, int(nb // 2))
+        self.reference_data_fourier = None
+        self.N = int(_cfg(config, "N"))
+        self.upsample_factor = int(_cfg(config, "shift_upsample_factor", 16))
+        self.radius = int(_cfg(config, "shift_search_radius", 2))
+        box = float(_cfg(config, "box_size", self.N))
+        vox = float(_cfg(config, "voxel_size", 1.0))
+        self.mask_radius = box / (2.0 * vox)
+        self._h = None
+        self._cap = 0
+        self._ref_version = 0      # bumped by set_reference
+        self._uploaded_version = -1
+        self._ref_dev = None
+        self._lib = nat.load()
+
+    def _handle(self, B: int):
+        if self._h is not None and B <= self._cap:
+            return self._h
+        self._free()
+        cfg = nat.MtbShiftConfig()
+        cfg.N = self.N
+        cfg.max_batch = max(B, int(_cfg(self.config, "num_subtomograms_per_batch", B) or B))
+        cfg.upsample_factor = self.upsample_factor
+        cfg.search_radius = self.radius
+        cfg.mask_radius = self.mask_radius
+        cfg.cosine_width = 5.0
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.mtb_shift_create(ctypes.byref(cfg), ctypes.byref(h)), "mtb_shift_create")
+        self._h, self._cap = h, cfg.max_batch
+        self._uploaded_version = -1
+        return h
+
+    def _free(self):
+        if self._h is not None and self._h.value:
+            self._lib.mtb_shift_destroy(self._h)
+        self._h = None
+        self._cap = 0
+
+    def __del__(self):
+        if getattr(self, "_lib", None) is not None:
+            self._free()
+
+    @torch.no_grad()
+    def set_reference(self, template_data: np.ndarray):
+        """Precompute and cache the Fourier-domain reference (ShiftMatcher.py:805-822)."""
+        ref = load_reference_full(template_data, volume_size=self.N,
+                                  voxel_size=float(_cfg(self.config, "voxel_size", 1.0)))
+        self.reference_data_fourier = torch.from_numpy(ref).unsqueeze(0).to(self.device, dtype=self.dtype)
+        self._ref_version += 1
+
+    def get_base_shifts(self, num_subtomograms_per_batch: int, num_base_shifts: int, dtype_real: torch.dtype):
+        """Base translation grid (B, S, 3) (ShiftMatcher.py:824-871)."""
+        execution = _cfg(self.config, "execution", None)
+        grid = None if execution is None else _cfg(execution, "translational_search_grid", None)
+        if grid is None:
+            base = torch.zeros((num_base_shifts, 3), device=self.device, dtype=dtype_real)
+        else:
+            base = torch.as_tensor(grid[0], device=self.device, dtype=dtype_real)
+            if base.ndim == 1:
+                base = base.unsqueeze(0)
+            if base.shape[0] != num_base_shifts:
+                if base.shape[0] > num_base_shifts:
+                    base = base[:num_base_shifts]
+                else:
+                    pad = torch.zeros((num_base_shifts - base.shape[0], 3), device=self.device, dtype=dtype_real)
+                    base = torch.cat((base, pad), dim=0)
+        return base.unsqueeze(0).expand(num_subtomograms_per_batch, -1, -1)
+
+    @torch.no_grad()
+    def search_shifts(self, *, subtomos: torch.Tensor, ctfs: torch.Tensor, shift_zyx: torch.Tensor,
+                      rotation_tracker, micro_batch_size: int = None):
+        """(shift (B, 3) in (x, y, z), score (B,)) at the current orientations (ShiftMatcher.py:873-928)."""
+        if self.reference_data_fourier is None:
+            raise RuntimeError("ShiftMatcher reference is not initialized. Call `set_reference` first.")
+        B = subtomos.shape[0]
+        angles = tracker_to_euler_deg(rotation_tracker)
+        if angles.shape[0] != B:
+            raise ValueError("rotation_tracker must hold one rotation per subtomogram")
+        rot = torch.from_numpy(R.from_euler("ZYZ", angles, degrees=True).as_matrix().reshape(B, 9)).to(
+            self.device, torch.float32)
+        vol = subtomos.to(self.device, torch.float32).contiguous()
+        nat.require_cuda(vol, "subtomos")
+        sz = torch.as_tensor(shift_zyx, device=self.device, dtype=torch.float32).reshape(B, 3).contiguous()
+        ctf = None
+        if bool(_cfg(self.config, "do_ctf_correction", True)) and isinstance(ctfs, torch.Tensor):
+            ctf = ctfs.to(self.device, torch.float32).reshape(B, self.N, self.N, self.N // 2 + 1).contiguous()
+        out = torch.empty((B, 3), device=self.device, dtype=torch.float32)
+        score = torch.empty((B,), device=self.device, dtype=torch.float32)
+        h = self._handle(B)
+        if self._uploaded_version != self._ref_version:
+            self._ref_dev = self.reference_data_fourier.to(torch.complex64).contiguous()
+            with torch.cuda.device(self.device):
+                nat.check(self._lib.mtb_shift_set_reference(h, nat.ptr(self._ref_dev), nat.stream_ptr(self.device)),
+                          "mtb_shift_set_reference")
+            self._uploaded_version = self._ref_version
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.mtb_shift_search(h, nat.ptr(vol), nat.ptr(sz), nat.ptr(rot), nat.ptr(ctf), B,
+                                                 nat.ptr(out), nat.ptr(score), nat.stream_ptr(self.device)),
+                      "mtb_shift_search")
+        return out, score

@@ -20,6 +20,7 @@
 #include <string.h>
 #include <vector>
 #include "common.cuh"
+#include "newton.cuh"
 
 namespace {
 
@@ -34,297 +35,8 @@ struct SearchParams {
   int flags;
 };
 
-constexpr int kNewtonThreads = 256;
 constexpr int kGridThreads = 256;
 constexpr int kMaxCand = 32;
-
-// ------------------------------------------------------------------ Newton pass
-// Accumulator slots.
-enum { A_VAL = 0, A_GA, A_GB, A_GG, A_HAA, A_HAB, A_HAG, A_HBB, A_HBG, A_HGG, A_N };
-
-struct NewtonSmem {
-  float* dbuf[2];  // d^l blocks, width 2l+1, double-buffered by l parity
-  float* rowf[2];  // 8 floats per row m' (5 row factors), by l parity
-  float2* ea;      // exp(i m' alpha), m' = -Li..Li
-  float2* eg;      // exp(i m gamma)
-  float* red;      // (threads/32) x A_N
-  float* res;      // A_N reduced results
-};
-
-template <int KP>
-__device__ void newton_pass(const float2* __restrict__ sig, const double* __restrict__ logC,
-                            float a, float be, float ga, int Li, bool derivs, bool compat_top,
-                            int W, NewtonSmem sm) {
-  const int tid = threadIdx.x;
-  const int NT = blockDim.x;
-  // phases e^{i m a}, e^{i m g}: argument reduced to [-pi, pi] in double, sincos in float
-  for (int r = tid; r < 2 * Li + 1; r += NT) {
-    const double two_pi = 6.283185307179586;
-    double t = (double)(r - Li) * (double)a;
-    t -= two_pi * rint(t / two_pi);
-    float s, c;
-    sincosf((float)t, &s, &c);
-    sm.ea[r] = make_float2(c, s);
-    t = (double)(r - Li) * (double)ga;
-    t -= two_pi * rint(t / two_pi);
-    sincosf((float)t, &s, &c);
-    sm.eg[r] = make_float2(c, s);
-  }
-  const float cb = cosf(be);
-  double hs, hc;
-  sincos(0.5 * (double)be, &hs, &hc);
-  const double lac = log(fabs(hc)), las = log(fabs(hs));
-  const int sgc = hc < 0.0 ? 1 : 0, sgs = hs < 0.0 ? 1 : 0;
-
-  // wedge pairs p = m'^2 + (m + m') owned by this thread, decoded once per pass
-  float d1[KP], d0[KP], sq[KP];
-  int pmp[KP], pm[KP];
-#pragma unroll
-  for (int k = 0; k < KP; ++k) {
-    const int p = tid + k * NT;
-    int mp = (int)sqrtf((float)p);
-    while (mp * mp > p) --mp;
-    while ((mp + 1) * (mp + 1) <= p) ++mp;
-    pmp[k] = mp;
-    pm[k] = p - mp * mp - mp;
-    d1[k] = 0.f; d0[k] = 0.f; sq[k] = 0.f;
-  }
-
-  float acc[A_N];
-#pragma unroll
-  for (int i = 0; i < A_N; ++i) acc[i] = 0.f;
-
-  for (int l = 0; l <= Li; ++l) {
-    const int w = 2 * l + 1;
-    float* dcur = sm.dbuf[l & 1];
-    // ---- recurrence (l-1 -> l) for the wedge m' >= |m|, symmetric copies to shared
-    const int npair = (l + 1) * (l + 1);
-    const float fl = (float)l;
-    const float inv_lm = (l > 1) ? 1.f / (float)(l - 1) : 0.f;
-    const float a1 = (2.f * fl - 1.f) * (fl - 1.f) * fl;
-    const float a2 = (2.f * fl - 1.f);
-#pragma unroll
-    for (int k = 0; k < KP; ++k) {
-      const int p = tid + k * NT;
-      if (p < npair) {
-        const int mp = pmp[k], m = pm[k];
-        float v;
-        if (mp == l) {
-          // closed form at l0 = m': (-1)^(m'-m) sqrt((2m')!/((m'+m)!(m'-m)!)) c^(m'+m) s^(m'-m)
-          const int pc = mp + m, ps = mp - m;
-          double lg = logC[p];
-          if (pc) lg += pc * lac;
-          if (ps) lg += ps * las;
-          const double dv = exp(lg);
-          const int sgn = (ps & 1) ^ ((pc & 1) & sgc) ^ ((ps & 1) & sgs);
-          v = (float)(sgn ? -dv : dv);
-          d0[k] = 0.f;
-          sq[k] = 0.f;  // sqrt(X_l0) = 0
-        } else if (l == 1) {
-          v = cb * d1[k];  // (m', m) = (0, 0); X_1 = 1
-          d0[k] = d1[k];
-          sq[k] = 1.f;
-        } else {
-          const float mm = (float)(m * m), pp = (float)(mp * mp), l2 = fl * fl;
-          const float x = (l2 - mm) * (l2 - pp);
-          const float inv = rsqrtf(x);
-          const float aa = a1 * cb - a2 * (float)(m * mp);
-          v = (aa * d1[k] - fl * sq[k] * d0[k]) * inv * inv_lm;
-          d0[k] = d1[k];
-          sq[k] = x * inv;
-        }
-        d1[k] = v;
-        // d_{m m'} = d_{-m',-m} = (-1)^(m'-m) d_{m'm};  d_{-m,-m'} = d_{m'm}
-        const float vs = ((mp - m) & 1) ? -v : v;
-        dcur[(mp + l) * w + (m + l)] = v;
-        dcur[(m + l) * w + (mp + l)] = vs;
-        dcur[(-m + l) * w + (-mp + l)] = v;
-        dcur[(-mp + l) * w + (-m + l)] = vs;
-      }
-    }
-    // ---- row factors of WignerDGradients.py:45-79 for m' = -l..l, packed per row
-    if (derivs) {
-      float* rf = sm.rowf[l & 1];
-      for (int r = tid; r < w; r += NT) {
-        const float mp = (float)(r - l);
-        rf[8 * r + 0] = -0.5f * sqrtf(fmaxf((fl + mp) * (fl - mp + 1.f), 0.f));
-        rf[8 * r + 1] = 0.5f * sqrtf(fmaxf((fl - mp) * (fl + mp + 1.f), 0.f));
-        rf[8 * r + 2] = 0.25f * sqrtf(fmaxf((fl + mp) * (fl - mp + 1.f) * (fl + mp - 1.f) * (fl - mp + 2.f), 0.f));
-        rf[8 * r + 3] = -0.25f * ((fl + mp) * (fl - mp + 1.f) + (fl + mp + 1.f) * (fl - mp));
-        rf[8 * r + 4] = 0.25f * sqrtf(fmaxf((fl + mp + 1.f) * (fl - mp) * (fl + mp + 2.f) * (fl - mp - 1.f), 0.f));
-      }
-    }
-    __syncthreads();
-    // ---- contraction over degree l: thread = (column c, chunk of rows), walking down
-    //      the column with a sliding window d(r-2..r+2) so each entry is read once
-    const float2* sl = sig + mtb_dsize(l - 1);
-    const bool zap = compat_top && (l == Li);
-    const float* rf = sm.rowf[l & 1];
-    const int G = max(1, NT / w);
-    const int chunk = (w + G - 1) / G;
-    const int c = tid % w, g = tid / w;
-    if (g < G) {
-      const int r0 = g * chunk;
-      const int r1 = min(w, r0 + chunk);
-      const bool zc = zap && (c == 0);
-      auto ld = [&](int rr) -> float {
-        if (rr < 0 || rr >= w || zc || (zap && rr == 0)) return 0.f;
-        return dcur[rr * w + c];
-      };
-      const float2 egc = sm.eg[c - l + Li];
-      const float m = (float)(c - l);
-      float dm2 = ld(r0 - 2), dm1 = ld(r0 - 1), dc = ld(r0), dp1 = ld(r0 + 1);
-      for (int r = r0; r < r1; ++r) {
-        const float dp2 = ld(r + 2);
-        const float2 s = __ldg(&sl[r * w + c]);
-        const float2 q = cmul(egc, s);
-        const float2 ear = sm.ea[r - l + Li];
-        const float er = ear.x * q.x - ear.y * q.y;
-        const float ei = ear.x * q.y + ear.y * q.x;
-        acc[A_VAL] += dc * er;
-        if (derivs) {
-          const float mp = (float)(r - l);
-          const float4 f4 = *reinterpret_cast<const float4*>(&rf[8 * r]);
-          const float f5 = rf[8 * r + 4];
-          const float db = f4.x * dm1 + f4.y * dp1;
-          const float dbb = f4.w * dc + f4.z * dm2 + f5 * dp2;
-          const float t = dc * er, u = dc * ei;
-          acc[A_GA] -= mp * u;
-          acc[A_GG] -= m * u;
-          acc[A_HAA] -= mp * mp * t;
-          acc[A_HGG] -= m * m * t;
-          acc[A_HAG] -= mp * m * t;
-          acc[A_GB] += db * er;
-          const float x = db * ei;
-          acc[A_HAB] -= mp * x;
-          acc[A_HBG] -= m * x;
-          acc[A_HBB] += dbb * er;
-        }
-        dm2 = dm1; dm1 = dc; dc = dp1; dp1 = dp2;
-      }
-    }
-  }
-  // ---- block reduction of the accumulators
-  const int lane = tid & 31, warp = tid >> 5, nw = NT >> 5;
-#pragma unroll
-  for (int i = 0; i < A_N; ++i) {
-    const float v = warp_sum(acc[i]);
-    if (lane == 0) sm.red[warp * A_N + i] = v;
-  }
-  __syncthreads();
-  if (tid < A_N) {
-    float s = 0.f;
-    for (int q = 0; q < nw; ++q) s += sm.red[q * A_N + tid];
-    sm.res[tid] = s;
-  }
-  __syncthreads();
-}
-
-// Solve H x = g in FP64 with partial pivoting; false when a pivot is exactly zero
-// (torch.linalg.solve raises "singular" there and the reference takes a zero step,
-// Matcha.py:316-343).
-__device__ bool solve3(const double H[3][3], const double g[3], double x[3]) {
-  double A[3][4];
-  for (int i = 0; i < 3; ++i) {
-    for (int j = 0; j < 3; ++j) A[i][j] = H[i][j];
-    A[i][3] = g[i];
-  }
-  for (int c = 0; c < 3; ++c) {
-    int piv = c;
-    for (int r = c + 1; r < 3; ++r)
-      if (fabs(A[r][c]) > fabs(A[piv][c])) piv = r;
-    if (A[piv][c] == 0.0 || !isfinite(A[piv][c])) return false;
-    if (piv != c)
-      for (int j = 0; j < 4; ++j) { double t = A[c][j]; A[c][j] = A[piv][j]; A[piv][j] = t; }
-    for (int r = c + 1; r < 3; ++r) {
-      const double f = A[r][c] / A[c][c];
-      for (int j = c; j < 4; ++j) A[r][j] -= f * A[c][j];
-    }
-  }
-  for (int r = 2; r >= 0; --r) {
-    double s = A[r][3];
-    for (int j = r + 1; j < 3; ++j) s -= A[r][j] * x[j];
-    x[r] = s / A[r][r];
-  }
-  return true;
-}
-
-template <int KP>
-__global__ void __launch_bounds__(kNewtonThreads, 2)
-newton_march_kernel(const float2* __restrict__ sigma, int64_t stride, int BC,
-                    float* __restrict__ alpha, float* __restrict__ beta, float* __restrict__ gamma,
-                    float* __restrict__ score, const double* __restrict__ logC, SearchParams P) {
-  extern __shared__ __align__(16) float smem[];
-  const int W = 2 * P.Lmax + 1;
-  NewtonSmem sm;
-  sm.dbuf[0] = smem;
-  sm.dbuf[1] = smem + W * W;
-  sm.rowf[0] = smem + 2 * W * W + 2;  // 16-byte aligned (W odd: 2 W^2 + 2 = 0 mod 4)
-  sm.rowf[1] = sm.rowf[0] + 8 * W;
-  sm.ea = reinterpret_cast<float2*>(sm.rowf[1] + 8 * W);
-  sm.eg = sm.ea + W;
-  sm.red = reinterpret_cast<float*>(sm.eg + W);
-  sm.res = sm.red + (kNewtonThreads / 32) * A_N;
-  __shared__ float st[8];  // angles and control broadcast
-
-  const int cand = blockIdx.x;
-  if (cand >= BC) return;
-  const int b = cand / P.C;
-  const float2* sig = sigma + (int64_t)b * stride;
-  const bool compat = (P.flags & MTB_SEARCH_COMPAT_TOP_BLOCK) != 0;
-  const bool grad_step = (P.flags & MTB_SEARCH_GRADIENT_STEP) != 0;
-  const float base_lr = grad_step ? 5e-7f : 1.f;
-
-  float a = alpha[cand], be = beta[cand], ga = gamma[cand];
-  float best = 0.f;
-  for (int s = 0; s < P.n_stages; ++s) {
-    const int Li = P.stages[s];
-    const bool zap = compat && (Li == P.Lmax);
-    newton_pass<KP>(sig, logC, a, be, ga, Li, P.num_steps > 0, zap, W, sm);
-    best = sm.res[A_VAL];
-    double g[3] = {sm.res[A_GA], sm.res[A_GB], sm.res[A_GG]};
-    double H[3][3] = {{sm.res[A_HAA], sm.res[A_HAB], sm.res[A_HAG]},
-                      {sm.res[A_HAB], sm.res[A_HBB], sm.res[A_HBG]},
-                      {sm.res[A_HAG], sm.res[A_HBG], sm.res[A_HGG]}};
-    float lr = base_lr;
-    for (int it = 0; it < P.num_steps; ++it) {
-      double x[3] = {0.0, 0.0, 0.0};
-      if (grad_step) {
-        for (int i = 0; i < 3; ++i) x[i] = -g[i];
-      } else if (!solve3(H, g, x)) {
-        x[0] = x[1] = x[2] = 0.0;
-      }
-      const float ta = a - lr * (float)x[0];
-      const float tb = be - lr * (float)x[1];
-      const float tg = ga - lr * (float)x[2];
-      const bool last = (it == P.num_steps - 1);
-      newton_pass<KP>(sig, logC, ta, tb, tg, Li, !last, zap, W, sm);
-      const float ev = sm.res[A_VAL];
-      if (ev > best) {
-        a = ta; be = tb; ga = tg; best = ev;
-        lr *= 1.1f;
-        if (!last) {
-          g[0] = sm.res[A_GA]; g[1] = sm.res[A_GB]; g[2] = sm.res[A_GG];
-          H[0][0] = sm.res[A_HAA]; H[0][1] = H[1][0] = sm.res[A_HAB]; H[0][2] = H[2][0] = sm.res[A_HAG];
-          H[1][1] = sm.res[A_HBB]; H[1][2] = H[2][1] = sm.res[A_HBG]; H[2][2] = sm.res[A_HGG];
-        }
-      } else {
-        lr *= 0.5f;
-      }
-      // every thread evaluates the same branch on identical values; the next pass
-      // syncs before shared results are overwritten
-      __syncthreads();
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    alpha[cand] = a;
-    beta[cand] = be;
-    gamma[cand] = ga;
-    score[cand] = best;
-  }
-  (void)st;
-}
 
 // ------------------------------------------------------------------ grid + top-k
 __device__ __forceinline__ bool better(float v1, int i1, float v2, int i2) {
@@ -522,18 +234,6 @@ void host_small_d(int Lm, double beta, double* out) {
     }
 }
 
-template <int KP>
-int launch_newton(const float2* sigma, int64_t stride, int BC, float* a, float* b, float* g, float* s,
-                  const double* logC, const SearchParams& P, cudaStream_t st) {
-  const int W = 2 * P.Lmax + 1;
-  const size_t smem = (size_t)(2 * W * W + 2 + 16 * W) * sizeof(float) + (size_t)2 * W * sizeof(float2) +
-                      (size_t)((kNewtonThreads / 32) * A_N + A_N) * sizeof(float);
-  MTB_CUDA_TRY(cudaFuncSetAttribute(newton_march_kernel<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  newton_march_kernel<KP><<<BC, kNewtonThreads, smem, st>>>(sigma, stride, BC, a, b, g, s, logC, P);
-  MTB_LAUNCH_CHECK();
-  return MTB_OK;
-}
-
 }  // namespace
 
 // ------------------------------------------------------------------ C ABI
@@ -543,7 +243,7 @@ struct mtb_search {
   int n;            // grid size per axis
   int device;
   float* dtab;      // (n, dsize(L0-1))
-  double* logC;     // (Lmax+1)^2
+  double* Ctab;     // (Lmax+1)^2 start-value coefficients of the recurrence
   float* cand;      // 4 x (max_batch * C): alpha, beta, gamma, score
 };
 
@@ -591,15 +291,15 @@ extern "C" int mtb_search_create(const mtb_search_config* cfg, mtb_search** out)
   const int Lm = cfg->Lmax;
   std::vector<double> lc((size_t)(Lm + 1) * (Lm + 1));
   for (int mp = 0; mp <= Lm; ++mp)
-    for (int m = -mp; m <= mp; ++m) lc[mp * mp + m + mp] = host_small_d_start_log(mp, m);
+    for (int m = -mp; m <= mp; ++m) lc[mp * mp + m + mp] = exp(host_small_d_start_log(mp, m));
 
   auto fail = [&](int code) { mtb_search_destroy(h); return code; };
   if (cudaMalloc(&h->dtab, dt.size() * sizeof(float)) != cudaSuccess) return fail(MTB_ERR_OOM);
-  if (cudaMalloc(&h->logC, lc.size() * sizeof(double)) != cudaSuccess) return fail(MTB_ERR_OOM);
+  if (cudaMalloc(&h->Ctab, lc.size() * sizeof(double)) != cudaSuccess) return fail(MTB_ERR_OOM);
   if (cudaMalloc(&h->cand, (size_t)4 * cfg->max_batch * cfg->candidates * sizeof(float)) != cudaSuccess)
     return fail(MTB_ERR_OOM);
   if (cudaMemcpy(h->dtab, dt.data(), dt.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(h->logC, lc.data(), lc.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+      cudaMemcpy(h->Ctab, lc.data(), lc.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(MTB_ERR_CUDA);
   *out = h;
   return MTB_OK;
@@ -608,7 +308,7 @@ extern "C" int mtb_search_create(const mtb_search_config* cfg, mtb_search** out)
 extern "C" void mtb_search_destroy(mtb_search* h) {
   if (!h) return;
   if (h->dtab) cudaFree(h->dtab);
-  if (h->logC) cudaFree(h->logC);
+  if (h->Ctab) cudaFree(h->Ctab);
   if (h->cand) cudaFree(h->cand);
   delete h;
 }
@@ -639,15 +339,14 @@ extern "C" int mtb_newton_march(mtb_search* h, const float* sigma, int64_t sigma
   if (B == 0) return MTB_OK;
   MTB_ARG_CHECK(sigma && alpha && beta && gamma && score, "null pointer");
   MTB_ARG_CHECK(sigma_stride >= mtb_dsize(h->cfg.Lmax), "sigma row shorter than dsize(Lmax)");
-  const int BC = B * h->cfg.candidates;
-  const int pairs = (h->cfg.Lmax + 1) * (h->cfg.Lmax + 1);
-  const int kp = (pairs + kNewtonThreads - 1) / kNewtonThreads;
-  const float2* s = reinterpret_cast<const float2*>(sigma);
-  cudaStream_t st = (cudaStream_t)stream;
-  if (kp <= 2) return launch_newton<2>(s, sigma_stride, BC, alpha, beta, gamma, score, h->logC, h->P, st);
-  if (kp <= 5) return launch_newton<5>(s, sigma_stride, BC, alpha, beta, gamma, score, h->logC, h->P, st);
-  if (kp <= 9) return launch_newton<9>(s, sigma_stride, BC, alpha, beta, gamma, score, h->logC, h->P, st);
-  return launch_newton<17>(s, sigma_stride, BC, alpha, beta, gamma, score, h->logC, h->P, st);
+  NewtonParams P;
+  P.Lmax = h->cfg.Lmax;
+  P.n_stages = h->cfg.n_stages;
+  for (int i = 0; i < MTB_MAX_STAGES; ++i) P.stages[i] = h->cfg.stages[i];
+  P.num_steps = h->cfg.num_steps;
+  P.flags = h->cfg.flags;
+  return newton_launch(sigma, sigma_stride, B, h->cfg.candidates, alpha, beta, gamma, score, h->Ctab, P,
+                       (cudaStream_t)stream);
 }
 
 extern "C" int mtb_search_orientations(mtb_search* h, const float* sigma, int64_t sigma_stride, int B,

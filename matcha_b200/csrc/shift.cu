@@ -1,0 +1,649 @@
+// RELION-style FFT shift match on sm_100a.
+//
+// Reference behaviour restated here (paths inside swing-research/Matcha):
+//   estimate_shift_like_relion   src/matcha/core/ShiftMatcher.py:619-674
+//   rotate_complex_volume        :491-537   (trilinear, align_corners=True, zero padding)
+//   extract_shifted_patch_batch  :558-616   (set_coords_to_zero=True, normalize=False)
+//   apply_cosine_mask            :540-555   masks: src/matcha/utils/setup_utils.py:239-270
+//   compute_shift (local)        :94-282    with _upsampled_dft :46-91
+//
+// Design (B200): per subtomogram the pipeline is
+//   bg      background sum of the shifted patch over the outer + cosine band
+//   rfft_x  patch sampled, zero planes, cosine fill, roll, 1/N^3 and the real FFT along
+//           the last axis in one pass (one CTA per (b, plane), FFT in shared memory)
+//   fft_y   FFT along the middle axis
+//   fft_z   FFT along the first axis, fused with the rotated, ifftshifted, masked
+//           Fourier reference (sampled on the fly), the product conj(S) T and both norms
+//   updft1  first pass of the local upsampled DFT (contract the first axis)
+//   updft23 second and third passes (middle axis, then the half axis, real part only)
+//           with a fused argmax: the U^3 refined correlation never reaches memory.
+// Contracting the half axis (N/2+1) last needs 51M instead of 87M complex MACs per
+// subtomogram at N=64, U=88; the separable sum is the same.
+#include <math.h>
+#include <string.h>
+#include <vector>
+#include "common.cuh"
+
+namespace {
+
+constexpr int kT = 256;
+
+struct ShiftGeom {
+  int N, H, U, h;        // box, half width N/2+1, upsampled region, N/2
+  float inv_n3;          // rfftn(norm="forward")
+  int r2_inner, r2_outer;// cosine band: r2 >= r2_inner (not inner), r2 > r2_outer (outer)
+  float rp, width;       // raised cosine: 0.5 + 0.5 cos(pi (rp - r) / width)
+  float wsum;            // number of outer voxels + sum of raised cosine weights
+  int mask_r2;           // mask_full: kp^2 + ip^2 + jp^2 <= (N/2)^2
+  float dftshift;        // floor(U / 2)
+  float uf;
+};
+
+__device__ __forceinline__ float trilinear(const float* __restrict__ v, int N, float z, float y, float x) {
+  const float z0 = floorf(z), y0 = floorf(y), x0 = floorf(x);
+  const int iz = (int)z0, iy = (int)y0, ix = (int)x0;
+  const float fz = z - z0, fy = y - y0, fx = x - x0;
+  float acc = 0.f;
+#pragma unroll
+  for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+      for (int dx = 0; dx < 2; ++dx) {
+        const int zz = iz + dz, yy = iy + dy, xx = ix + dx;
+        if (zz < 0 || zz >= N || yy < 0 || yy >= N || xx < 0 || xx >= N) continue;
+        const float w = (dz ? fz : 1.f - fz) * (dy ? fy : 1.f - fy) * (dx ? fx : 1.f - fx);
+        acc += w * __ldg(&v[((int64_t)zz * N + yy) * N + xx]);
+      }
+  return acc;
+}
+
+__device__ __forceinline__ float2 trilinear_c(const float2* __restrict__ v, int N, float z, float y, float x) {
+  const float z0 = floorf(z), y0 = floorf(y), x0 = floorf(x);
+  const int iz = (int)z0, iy = (int)y0, ix = (int)x0;
+  const float fz = z - z0, fy = y - y0, fx = x - x0;
+  float ar = 0.f, ai = 0.f;
+#pragma unroll
+  for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+      for (int dx = 0; dx < 2; ++dx) {
+        const int zz = iz + dz, yy = iy + dy, xx = ix + dx;
+        if (zz < 0 || zz >= N || yy < 0 || yy >= N || xx < 0 || xx >= N) continue;
+        const float w = (dz ? fz : 1.f - fz) * (dy ? fy : 1.f - fy) * (dx ? fx : 1.f - fx);
+        const float2 q = __ldg(&v[((int64_t)zz * N + yy) * N + xx]);
+        ar += w * q.x;
+        ai += w * q.y;
+      }
+  return make_float2(ar, ai);
+}
+
+// Per-subtomogram shift parameters: f = flip(shift_zyx) and the zeroed planes.
+struct PatchShift {
+  float f[3];
+  int zp[3];
+};
+
+__device__ __forceinline__ PatchShift patch_shift(const float* __restrict__ shift_zyx, int b, int N) {
+  PatchShift p;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float s = shift_zyx[b * 3 + (2 - d)];
+    p.f[d] = s;
+    const float a = fabsf(s);
+    const float fl = floorf(a);
+    if (a - fl > 0.f) {
+      p.zp[d] = (s < 0.f) ? (int)fl : N - (int)ceilf(a);
+    } else {
+      p.zp[d] = -1;
+    }
+  }
+  return p;
+}
+
+__device__ __forceinline__ float patch_value(const float* __restrict__ v, int N, const PatchShift& ps, int i, int j,
+                                             int k) {
+  if (i == ps.zp[0] || j == ps.zp[1] || k == ps.zp[2]) return 0.f;
+  return trilinear(v, N, (float)i + ps.f[0], (float)j + ps.f[1], (float)k + ps.f[2]);
+}
+
+__device__ __forceinline__ float block_sum(float v, float* red) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  float s = 0.f;
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (int)(blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
+    s = warp_sum(s);
+  }
+  __syncthreads();
+  return s;  // valid in thread 0
+}
+
+// ------------------------------------------------------------------ background sum
+__global__ void __launch_bounds__(kT)
+bg_kernel(const float* __restrict__ vol, const float* __restrict__ shift_zyx, const int* __restrict__ bg_idx,
+          const float* __restrict__ bg_w, int n_bg, ShiftGeom g, float* __restrict__ bg) {
+  __shared__ float red[32];
+  const int b = blockIdx.y;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const float* v = vol + (int64_t)b * g.N * g.N * g.N;
+  const PatchShift ps = patch_shift(shift_zyx, b, g.N);
+  float s = 0.f;
+  if (e < n_bg) {
+    const int idx = bg_idx[e];
+    const int k = idx % g.N, j = (idx / g.N) % g.N, i = idx / (g.N * g.N);
+    s = bg_w[e] * patch_value(v, g.N, ps, i, j, k);
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) atomicAdd(&bg[b], s);
+}
+
+// ------------------------------------------------------------------ radix-2 FFT in shared memory
+// In-place forward FFT (e^{-2 pi i k n / L}) of `lines` sequences of length L (power of two),
+// element t of line q at buf[q * ls + t * es].  tw[k] = e^{-2 pi i k / L}, k < L/2.
+__device__ void smem_fft(float2* buf, int lines, int L, int ls, int es, const float2* tw) {
+  const int NT = blockDim.x;
+  int logL = 0;
+  while ((1 << logL) < L) ++logL;
+  // bit reversal
+  for (int e = threadIdx.x; e < lines * L; e += NT) {
+    const int q = e / L, t = e % L;
+    const int r = __brev(t) >> (32 - logL);
+    if (r > t) {
+      float2* a = &buf[q * ls + t * es];
+      float2* c = &buf[q * ls + r * es];
+      const float2 tmp = *a;
+      *a = *c;
+      *c = tmp;
+    }
+  }
+  __syncthreads();
+  for (int s = 1; s <= logL; ++s) {
+    const int half = 1 << (s - 1);
+    const int stride = L >> s;
+    for (int e = threadIdx.x; e < lines * (L / 2); e += NT) {
+      const int q = e / (L / 2), t = e % (L / 2);
+      const int grp = t / half, pos = t % half;
+      const int i0 = grp * 2 * half + pos, i1 = i0 + half;
+      float2* p0 = &buf[q * ls + i0 * es];
+      float2* p1 = &buf[q * ls + i1 * es];
+      const float2 w = tw[pos * stride];
+      const float2 a = *p0, c = *p1;
+      const float2 wc = cmul(w, c);
+      *p0 = make_float2(a.x + wc.x, a.y + wc.y);
+      *p1 = make_float2(a.x - wc.x, a.y - wc.y);
+    }
+    __syncthreads();
+  }
+}
+
+__device__ void load_twiddles(float2* tw, int L) {
+  for (int k = threadIdx.x; k < L / 2; k += blockDim.x) {
+    double s, c;
+    sincospi(-2.0 * k / L, &s, &c);
+    tw[k] = make_float2((float)c, (float)s);
+  }
+}
+
+// ------------------------------------------------------------------ patch -> rfft along x
+// One CTA per (b, rolled plane i').  T[b][i'][j'][m2], m2 < H.
+__global__ void __launch_bounds__(kT)
+rfft_x_kernel(const float* __restrict__ vol, const float* __restrict__ shift_zyx, const float* __restrict__ bg,
+              ShiftGeom g, float2* __restrict__ T) {
+  extern __shared__ __align__(16) float2 sm2[];
+  const int N = g.N;
+  float2* tw = sm2;
+  float2* buf = sm2 + N / 2;  // N lines x N
+  const int ip = blockIdx.x, b = blockIdx.y;
+  const float* v = vol + (int64_t)b * N * N * N;
+  const PatchShift ps = patch_shift(shift_zyx, b, N);
+  const float avg = g.wsum > 0.f ? bg[b] / g.wsum : 0.f;
+  load_twiddles(tw, N);
+  const int i = (ip + g.h) % N;
+  const int di = i - g.h;
+  for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+    const int jp = e / N, kp = e % N;
+    const int j = (jp + g.h) % N, k = (kp + g.h) % N;
+    float p = patch_value(v, N, ps, i, j, k);
+    const int dj = j - g.h, dk = k - g.h;
+    const int r2 = di * di + dj * dj + dk * dk;
+    if (r2 > g.r2_outer) {
+      p = avg;
+    } else if (r2 >= g.r2_inner) {
+      const float r = sqrtf((float)r2);
+      const float w = 0.5f + 0.5f * cospif((g.rp - r) / g.width);
+      p = (1.f - w) * p + w * avg;
+    }
+    buf[jp * N + kp] = make_float2(p * g.inv_n3, 0.f);
+  }
+  __syncthreads();
+  smem_fft(buf, N, N, N, 1, tw);
+  float2* out = T + ((int64_t)b * N + ip) * N * g.H;
+  for (int e = threadIdx.x; e < N * g.H; e += blockDim.x) {
+    const int jp = e / g.H, m2 = e % g.H;
+    out[e] = buf[jp * N + m2];
+  }
+}
+
+// ------------------------------------------------------------------ FFT along y
+__global__ void __launch_bounds__(kT)
+fft_y_kernel(ShiftGeom g, float2* __restrict__ T) {
+  extern __shared__ __align__(16) float2 sm2[];
+  const int N = g.N, H = g.H;
+  float2* tw = sm2;
+  float2* buf = sm2 + N / 2;  // N x H, row j'
+  const int ip = blockIdx.x, b = blockIdx.y;
+  float2* slab = T + ((int64_t)b * N + ip) * N * H;
+  load_twiddles(tw, N);
+  for (int e = threadIdx.x; e < N * H; e += blockDim.x) buf[e] = slab[e];
+  __syncthreads();
+  smem_fft(buf, H, N, 1, H, tw);
+  for (int e = threadIdx.x; e < N * H; e += blockDim.x) slab[e] = buf[e];
+}
+
+// ------------------------------------------------------------------ FFT along z + product
+// One CTA per (b, j').  P = conj(S) * T in place; norms |T|^2, |S|^2 per subtomogram.
+__global__ void __launch_bounds__(kT)
+fft_z_product_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ ref,
+                     const float* __restrict__ rot, const float* __restrict__ ctf, float* __restrict__ nrm) {
+  extern __shared__ __align__(16) float2 sm2[];
+  __shared__ float red[32];
+  const int N = g.N, H = g.H;
+  float2* tw = sm2;
+  float2* buf = sm2 + N / 2;  // N (i') x H
+  const int jp = blockIdx.x, b = blockIdx.y;
+  float2* base = T + (int64_t)b * N * N * H + (int64_t)jp * H;
+  load_twiddles(tw, N);
+  for (int e = threadIdx.x; e < N * H; e += blockDim.x) {
+    const int ip = e / H, m2 = e % H;
+    buf[e] = base[(int64_t)ip * N * H + m2];
+  }
+  __syncthreads();
+  smem_fft(buf, H, N, 1, H, tw);
+  float R[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) R[q] = __ldg(&rot[b * 9 + q]);
+  const float c = (float)g.h;  // centre of the odd-padded grid, (N+1-1)/2
+  float st = 0.f, ss = 0.f;
+  for (int e = threadIdx.x; e < N * H; e += blockDim.x) {
+    const int ip = e / H, m2 = e % H;
+    const float2 t = buf[e];
+    // mask_full on the (N, N, N/2+1) index grid (setup_utils.py:239-249)
+    const int kp = ip < N / 2 ? ip : ip - N;
+    const int jq = jp < N / 2 ? jp : jp - N;
+    const int xq = m2 < N / 2 ? m2 : m2 - H;
+    float2 s = make_float2(0.f, 0.f);
+    if (kp * kp + jq * jq + xq * xq <= g.mask_r2) {
+      // ifftshift over (z, y) of the slice [..., N/2:] of the rotated reference
+      const int zo = (ip + g.h) % N, yo = (jp + g.h) % N, xw = m2 + g.h;
+      const float bx = (float)xw - c, by = (float)yo - c, bz = (float)zo - c;
+      const float rx = R[0] * bx + R[1] * by + R[2] * bz + c;
+      const float ry = R[3] * bx + R[4] * by + R[5] * bz + c;
+      const float rz = R[6] * bx + R[7] * by + R[8] * bz + c;
+      s = trilinear_c(ref, N, rz, ry, rx);
+      if (ctf) {
+        const float cv = __ldg(&ctf[(((int64_t)b * N + ip) * N + jp) * H + m2]);
+        s.x *= cv;
+        s.y *= cv;
+      }
+    }
+    st += t.x * t.x + t.y * t.y;
+    ss += s.x * s.x + s.y * s.y;
+    // conj(s) * t
+    const float2 p = make_float2(s.x * t.x + s.y * t.y, s.x * t.y - s.y * t.x);
+    base[(int64_t)ip * N * H + m2] = p;
+  }
+  st = block_sum(st, red);
+  ss = block_sum(ss, red);
+  if (threadIdx.x == 0) {
+    atomicAdd(&nrm[2 * b], st);
+    atomicAdd(&nrm[2 * b + 1], ss);
+  }
+}
+
+// ------------------------------------------------------------------ upsampled DFT, pass 1
+// X1[b][u0][m1][m2] = sum_{m0} E0[u0][m0] P[b][m0][m1][m2].  CTA: (column tile of 64, b).
+constexpr int kColTile = 64;
+
+__global__ void __launch_bounds__(kT)
+updft1_kernel(ShiftGeom g, const float2* __restrict__ P, const float2* __restrict__ E0, float2* __restrict__ X1) {
+  extern __shared__ __align__(16) float2 sm2[];
+  const int N = g.N, H = g.H, U = g.U;
+  const int NC = N * H;
+  float2* e0 = sm2;             // U x N
+  float2* pt = e0 + U * N;      // N x kColTile
+  const int c0 = blockIdx.x * kColTile, b = blockIdx.y;
+  const float2* Pb = P + (int64_t)b * N * NC;
+  for (int e = threadIdx.x; e < U * N; e += blockDim.x) e0[e] = E0[e];
+  for (int e = threadIdx.x; e < N * kColTile; e += blockDim.x) {
+    const int m0 = e / kColTile, cc = e % kColTile;
+    pt[e] = (c0 + cc < NC) ? Pb[(int64_t)m0 * NC + c0 + cc] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  // thread: column cc = tid % 64, rows u0 = tid / 64 + 4 q
+  const int cc = threadIdx.x % kColTile;
+  const int r0 = threadIdx.x / kColTile;
+  const int nr = blockDim.x / kColTile;
+  float2* Xb = X1 + (int64_t)b * U * NC;
+  for (int u0 = r0; u0 < U; u0 += nr) {
+    float re = 0.f, im = 0.f;
+    const float2* er = e0 + u0 * N;
+    for (int m0 = 0; m0 < N; ++m0) {
+      const float2 w = er[m0], x = pt[m0 * kColTile + cc];
+      re += w.x * x.x - w.y * x.y;
+      im += w.x * x.y + w.y * x.x;
+    }
+    if (c0 + cc < NC) Xb[(int64_t)u0 * NC + c0 + cc] = make_float2(re, im);
+  }
+}
+
+// ------------------------------------------------------------------ passes 2 and 3 + argmax
+// For each u0: X2[u1][m2] = sum_{m1} E1[u1][m1] X1[u0][m1][m2];
+//              V[u1][u2]  = Re sum_{m2} E2[u2][m2] X2[u1][m2];   running argmax.
+__device__ __forceinline__ bool better(float v1, int i1, float v2, int i2) {
+  // torch.argmax order: NaN is the largest value, the first index wins ties
+  if (isnan(v1) || isnan(v2)) return isnan(v1) && (!isnan(v2) || i1 < i2);
+  return v1 > v2 || (v1 == v2 && i1 < i2);
+}
+
+__global__ void __launch_bounds__(kT)
+updft23_kernel(ShiftGeom g, const float2* __restrict__ X1, const float2* __restrict__ E1,
+               const float2* __restrict__ E2, int rows_per_cta, float* __restrict__ pval, int* __restrict__ pidx) {
+  extern __shared__ __align__(16) float2 sm2[];
+  __shared__ float rv[32];
+  __shared__ int ri[32];
+  const int N = g.N, H = g.H, U = g.U;
+  float2* e1 = sm2;            // U x N
+  float2* e2 = e1 + U * N;     // U x H
+  float2* x1 = e2 + U * H;     // N x H
+  float2* x2 = x1 + N * H;     // U x H
+  const int grp = blockIdx.x, b = blockIdx.y;
+  for (int e = threadIdx.x; e < U * N; e += blockDim.x) e1[e] = E1[e];
+  for (int e = threadIdx.x; e < U * H; e += blockDim.x) e2[e] = E2[e];
+  float bv = -INFINITY;
+  int bi = 0x7fffffff;
+  const int u0a = grp * rows_per_cta;
+  const int u0b = min(U, u0a + rows_per_cta);
+  for (int u0 = u0a; u0 < u0b; ++u0) {
+    __syncthreads();
+    const float2* src = X1 + ((int64_t)b * U + u0) * N * H;
+    for (int e = threadIdx.x; e < N * H; e += blockDim.x) x1[e] = src[e];
+    __syncthreads();
+    for (int e = threadIdx.x; e < U * H; e += blockDim.x) {
+      const int u1 = e / H, m2 = e % H;
+      float re = 0.f, im = 0.f;
+      const float2* er = e1 + u1 * N;
+      for (int m1 = 0; m1 < N; ++m1) {
+        const float2 w = er[m1], x = x1[m1 * H + m2];
+        re += w.x * x.x - w.y * x.y;
+        im += w.x * x.y + w.y * x.x;
+      }
+      x2[e] = make_float2(re, im);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < U * U; e += blockDim.x) {
+      const int u1 = e / U, u2 = e % U;
+      float re = 0.f;
+      const float2* er = e2 + u2 * H;
+      const float2* xr = x2 + u1 * H;
+      for (int m2 = 0; m2 < H; ++m2) {
+        const float2 w = er[m2], x = xr[m2];
+        re += w.x * x.x - w.y * x.y;
+      }
+      const int flat = (u0 * U + u1) * U + u2;
+      if (better(re, flat, bv, bi)) { bv = re; bi = flat; }
+    }
+  }
+  // block argmax
+  for (int o = 16; o > 0; o >>= 1) {
+    const float v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+    const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (better(v2, i2, bv, bi)) { bv = v2; bi = i2; }
+  }
+  if ((threadIdx.x & 31) == 0) { rv[threadIdx.x >> 5] = bv; ri[threadIdx.x >> 5] = bi; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float v = rv[0];
+    int i = ri[0];
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q)
+      if (better(rv[q], ri[q], v, i)) { v = rv[q]; i = ri[q]; }
+    pval[b * gridDim.x + grp] = v;
+    pidx[b * gridDim.x + grp] = i;
+  }
+}
+
+__global__ void finalize_kernel(ShiftGeom g, int B, int ngrp, const float* __restrict__ pval,
+                                const int* __restrict__ pidx, const float* __restrict__ nrm,
+                                float* __restrict__ shift_xyz, float* __restrict__ score) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  float bv = pval[b * ngrp];
+  int bi = pidx[b * ngrp];
+  for (int q = 1; q < ngrp; ++q)
+    if (better(pval[b * ngrp + q], pidx[b * ngrp + q], bv, bi)) { bv = pval[b * ngrp + q]; bi = pidx[b * ngrp + q]; }
+  const int U = g.U;
+  const int u2 = bi % U, u1 = (bi / U) % U, u0 = bi / (U * U);
+  // (dim1, dim2, dim3) = (u0, u1, u2) - dftshift, / uf; returned flipped to (x, y, z)
+  shift_xyz[b * 3 + 0] = ((float)u2 - g.dftshift) / g.uf;
+  shift_xyz[b * 3 + 1] = ((float)u1 - g.dftshift) / g.uf;
+  shift_xyz[b * 3 + 2] = ((float)u0 - g.dftshift) / g.uf;
+  const float den = sqrtf(nrm[2 * b]) * sqrtf(nrm[2 * b + 1]);
+  score[b] = bv / den;
+}
+
+}  // namespace
+
+struct mtb_shift {
+  mtb_shift_config cfg;
+  ShiftGeom g;
+  int n_bg;
+  int* bg_idx;
+  float* bg_w;
+  float2* ref;     // (N, N, N) Fourier reference, fftshifted and masked
+  float2* E0;      // (U, N)
+  float2* E1;      // (U, N)
+  float2* E2;      // (U, H)
+  float* bg;       // (max_batch)
+  float* nrm;      // (max_batch, 2)
+  float2* T;       // (max_batch, N, N, H)
+  float2* X1;      // (max_batch, U, N, H)
+  float* pval;     // (max_batch, ngrp)
+  int* pidx;
+  int ngrp, rows_per_cta;
+  bool has_ref;
+};
+
+extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
+  MTB_ARG_CHECK(cfg && out, "null argument");
+  *out = nullptr;
+  const int N = cfg->N;
+  MTB_ARG_CHECK(N >= 4 && N <= 128 && (N & (N - 1)) == 0, "N must be a power of two in [4, 128]");
+  MTB_ARG_CHECK(cfg->max_batch >= 1 && cfg->max_batch <= 65535, "max_batch out of range");
+  MTB_ARG_CHECK(cfg->upsample_factor >= 2 && cfg->search_radius >= 0, "upsample_factor must be > 1");
+  MTB_ARG_CHECK(cfg->cosine_width > 0.f, "cosine_width must be positive");
+  mtb_shift* h = new mtb_shift();
+  memset(h, 0, sizeof(*h));
+  h->cfg = *cfg;
+  ShiftGeom& g = h->g;
+  g.N = N;
+  g.H = N / 2 + 1;
+  g.h = N / 2;
+  const int window = 2 * cfg->search_radius + 1;
+  g.U = (int)ceil((double)cfg->upsample_factor * window);
+  g.uf = (float)cfg->upsample_factor;
+  g.dftshift = floorf(g.U / 2.f);
+  g.inv_n3 = 1.f / ((float)N * N * N);
+  double radius = cfg->mask_radius;
+  if (radius < 0) radius = N / 2.0;
+  const double rp = radius + cfg->cosine_width;
+  g.rp = (float)rp;
+  g.width = cfg->cosine_width;
+  g.mask_r2 = (N / 2) * (N / 2);
+  // background voxels: r > rp (weight 1) and radius <= r <= rp (raised cosine)
+  std::vector<int> idx;
+  std::vector<float> w;
+  double wsum = 0.0;
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j)
+      for (int k = 0; k < N; ++k) {
+        const int di = i - N / 2, dj = j - N / 2, dk = k - N / 2;
+        const int r2 = di * di + dj * dj + dk * dk;
+        const double r = sqrt((double)r2);
+        if (r > rp) {
+          idx.push_back((i * N + j) * N + k);
+          w.push_back(1.f);
+          wsum += 1.0;
+        } else if (!(r < radius)) {
+          const float rc = (float)(0.5 + 0.5 * cos(M_PI * (rp - r) / cfg->cosine_width));
+          idx.push_back((i * N + j) * N + k);
+          w.push_back(rc);
+          wsum += rc;
+        }
+      }
+  // same sets by integer squared radius: outer r2 > floor(rp^2); band r2 >= ceil(radius^2)
+  const int r2_outer = (int)floor(rp * rp);
+  const int r2_inner = (int)ceil(radius * radius);
+  g.r2_inner = r2_inner;
+  g.r2_outer = r2_outer;
+  g.wsum = (float)wsum;
+  h->n_bg = (int)idx.size();
+  // DFT kernels exp(+2 pi i (u - dftshift) f_m), f = fftfreq(n, d=uf)
+  auto kern = [&](int n, std::vector<float2>& E) {
+    E.resize((size_t)g.U * n);
+    for (int u = 0; u < g.U; ++u)
+      for (int m = 0; m < n; ++m) {
+        const int mm = (m < (n + 1) / 2) ? m : m - n;
+        const double f = (double)mm / ((double)cfg->upsample_factor * n);
+        const double ph = 2.0 * M_PI * ((double)u - g.dftshift) * f;
+        E[(size_t)u * n + m] = make_float2((float)cos(ph), (float)sin(ph));
+      }
+  };
+  std::vector<float2> e0, e2;
+  kern(N, e0);
+  kern(g.H, e2);
+  h->rows_per_cta = 2;
+  h->ngrp = (g.U + h->rows_per_cta - 1) / h->rows_per_cta;
+  const size_t B = cfg->max_batch;
+  auto fail = [&](int code) { mtb_shift_destroy(h); return code; };
+  auto alloc = [&](void** p, size_t bytes) { return cudaMalloc(p, bytes > 0 ? bytes : 4) == cudaSuccess; };
+  if (!alloc((void**)&h->bg_idx, idx.size() * 4) || !alloc((void**)&h->bg_w, w.size() * 4) ||
+      !alloc((void**)&h->ref, (size_t)N * N * N * 8) || !alloc((void**)&h->E0, e0.size() * 8) ||
+      !alloc((void**)&h->E1, e0.size() * 8) || !alloc((void**)&h->E2, e2.size() * 8) ||
+      !alloc((void**)&h->bg, B * 4) || !alloc((void**)&h->nrm, B * 8) ||
+      !alloc((void**)&h->T, B * N * N * g.H * 8) || !alloc((void**)&h->X1, B * g.U * N * g.H * 8) ||
+      !alloc((void**)&h->pval, B * h->ngrp * 4) || !alloc((void**)&h->pidx, B * h->ngrp * 4))
+    return fail(MTB_ERR_OOM);
+  if (cudaMemcpy(h->bg_idx, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(h->bg_w, w.data(), w.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(h->E0, e0.data(), e0.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(h->E1, e0.data(), e0.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(h->E2, e2.data(), e2.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(MTB_ERR_CUDA);
+  *out = h;
+  return MTB_OK;
+}
+
+extern "C" void mtb_shift_destroy(mtb_shift* h) {
+  if (!h) return;
+  void* ptrs[] = {h->bg_idx, h->bg_w, h->ref, h->E0, h->E1, h->E2, h->bg, h->nrm, h->T, h->X1, h->pval, h->pidx};
+  for (void* p : ptrs) if (p) cudaFree(p);
+  delete h;
+}
+
+extern "C" int mtb_shift_set_reference(mtb_shift* h, const float* ref_fourier, mtb_stream_t stream) {
+  MTB_ARG_CHECK(h && ref_fourier, "null argument");
+  const size_t n = (size_t)h->g.N * h->g.N * h->g.N;
+  MTB_CUDA_TRY(cudaMemcpyAsync(h->ref, ref_fourier, n * 8, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  h->has_ref = true;
+  return MTB_OK;
+}
+
+extern "C" int mtb_shift_search(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot,
+                                const float* ctf, int B, float* shift_xyz, float* score, mtb_stream_t stream) {
+  MTB_ARG_CHECK(h, "null handle");
+  MTB_ARG_CHECK(h->has_ref, "shift reference is not set");
+  MTB_ARG_CHECK(B >= 0 && B <= h->cfg.max_batch, "batch exceeds max_batch");
+  if (B == 0) return MTB_OK;
+  MTB_ARG_CHECK(subtomos && shift_zyx && rot && shift_xyz && score, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  const ShiftGeom& g = h->g;
+  const int N = g.N, H = g.H, U = g.U;
+  MTB_CUDA_TRY(cudaMemsetAsync(h->bg, 0, (size_t)B * 4, st));
+  MTB_CUDA_TRY(cudaMemsetAsync(h->nrm, 0, (size_t)B * 8, st));
+  bg_kernel<<<dim3((h->n_bg + kT - 1) / kT, B), kT, 0, st>>>(subtomos, shift_zyx, h->bg_idx, h->bg_w, h->n_bg, g,
+                                                             h->bg);
+  MTB_LAUNCH_CHECK();
+  const size_t smx = (size_t)(N / 2 + N * N) * 8;
+  MTB_CUDA_TRY(cudaFuncSetAttribute(rfft_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+  rfft_x_kernel<<<dim3(N, B), kT, smx, st>>>(subtomos, shift_zyx, h->bg, g, h->T);
+  MTB_LAUNCH_CHECK();
+  const size_t smy = (size_t)(N / 2 + N * H) * 8;
+  MTB_CUDA_TRY(cudaFuncSetAttribute(fft_y_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
+  fft_y_kernel<<<dim3(N, B), kT, smy, st>>>(g, h->T);
+  MTB_LAUNCH_CHECK();
+  MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_product_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
+  fft_z_product_kernel<<<dim3(N, B), kT, smy, st>>>(g, h->T, h->ref, rot, ctf, h->nrm);
+  MTB_LAUNCH_CHECK();
+  const size_t sm1 = (size_t)(U * N + N * kColTile) * 8;
+  MTB_CUDA_TRY(cudaFuncSetAttribute(updft1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+  updft1_kernel<<<dim3((N * H + kColTile - 1) / kColTile, B), kT, sm1, st>>>(g, h->T, h->E0, h->X1);
+  MTB_LAUNCH_CHECK();
+  const size_t sm2 = (size_t)(U * N + U * H + N * H + U * H) * 8;
+  MTB_ARG_CHECK(sm2 <= 220 * 1024 && sm1 <= 220 * 1024, "upsampled region too large for shared memory");
+  MTB_CUDA_TRY(cudaFuncSetAttribute(updft23_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+  updft23_kernel<<<dim3(h->ngrp, B), kT, sm2, st>>>(g, h->X1, h->E1, h->E2, h->rows_per_cta, h->pval, h->pidx);
+  MTB_LAUNCH_CHECK();
+  finalize_kernel<<<(B + 127) / 128, 128, 0, st>>>(g, B, h->ngrp, h->pval, h->pidx, h->nrm, shift_xyz, score);
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
+}
+
+// ------------------------------------------------------------------ rotation tracker update
+// update_rotation_estimate (src/matcha/utils/rotation_ops.py:23-34) followed by the
+// rotation the shift match uses, R.from_euler('ZYZ', euler(conj(tracker))) (ShiftMatcher.py:503,
+// :913), which is the rotation matrix of conj(tracker).  FP64 quaternion arithmetic.
+namespace {
+__global__ void tracker_update_kernel(const float* __restrict__ alpha, const float* __restrict__ beta,
+                                      const float* __restrict__ gamma, const double* __restrict__ tin, int B,
+                                      double* __restrict__ tout, float* __restrict__ rot) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const double a = alpha[b], be = beta[b], g = gamma[b];
+  double sb, cb, sp, cp, sm, cm;
+  sincos(0.5 * be, &sb, &cb);
+  sincos(0.5 * (a + g), &sp, &cp);
+  sincos(0.5 * (a - g), &sm, &cm);
+  // quaternionic.array.from_euler_angles: exp(a z/2) exp(b y/2) exp(g z/2)
+  const double w = cb * cp, x = -sb * sm, y = sb * cm, z = cb * sp;
+  // components 1 and 3 swapped, then conjugated
+  const double qw = w, qx = -z, qy = -y, qz = -x;
+  const double tw = tin[4 * b], tx = tin[4 * b + 1], ty = tin[4 * b + 2], tz = tin[4 * b + 3];
+  double nw = tw * qw - tx * qx - ty * qy - tz * qz;
+  double nx = tw * qx + tx * qw + ty * qz - tz * qy;
+  double ny = tw * qy - tx * qz + ty * qw + tz * qx;
+  double nz = tw * qz + tx * qy - ty * qx + tz * qw;
+  const double inv = 1.0 / sqrt(nw * nw + nx * nx + ny * ny + nz * nz);
+  nw *= inv; nx *= inv; ny *= inv; nz *= inv;
+  tout[4 * b] = nw; tout[4 * b + 1] = nx; tout[4 * b + 2] = ny; tout[4 * b + 3] = nz;
+  // rotation matrix of conj(tracker)
+  const double cw = nw, cx = -nx, cy = -ny, cz = -nz;
+  float* R = rot + 9 * b;
+  R[0] = (float)(1 - 2 * (cy * cy + cz * cz)); R[1] = (float)(2 * (cx * cy - cw * cz)); R[2] = (float)(2 * (cx * cz + cw * cy));
+  R[3] = (float)(2 * (cx * cy + cw * cz)); R[4] = (float)(1 - 2 * (cx * cx + cz * cz)); R[5] = (float)(2 * (cy * cz - cw * cx));
+  R[6] = (float)(2 * (cx * cz - cw * cy)); R[7] = (float)(2 * (cy * cz + cw * cx)); R[8] = (float)(1 - 2 * (cx * cx + cy * cy));
+}
+}  // namespace
+
+extern "C" int mtb_update_rotation(const float* alpha, const float* beta, const float* gamma, const double* tracker_in,
+                                   int B, double* tracker_out, float* rot, mtb_stream_t stream) {
+  MTB_ARG_CHECK(B >= 0, "negative batch");
+  if (B == 0) return MTB_OK;
+  MTB_ARG_CHECK(alpha && beta && gamma && tracker_in && tracker_out && rot, "null pointer");
+  tracker_update_kernel<<<(B + 127) / 128, 128, 0, (cudaStream_t)stream>>>(alpha, beta, gamma, tracker_in, B,
+                                                                            tracker_out, rot);
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
+}

@@ -1,0 +1,100 @@
+"""One alternation of the alignment hot path for a batch, entirely on the device.
+
+Mirrors ``BatchProcessor._search_rotation`` + ``_search_shift``
+(src/matcha/align_subtomograms.py:254-285): correlation coefficients of the batch
+(``CrossCorrelationMatcher.get_sigma``), orientation search (``Matcha.search_orientations``),
+rotation-tracker update (``update_rotation_estimate``, src/matcha/utils/rotation_ops.py:23-34)
+and the shift match (``ShiftMatcher.search_shifts``).  The tracker update and the
+rotation the shift match needs are computed on the device (``mtb_update_rotation``), so a
+step issues no host synchronisation and can be captured in a CUDA graph.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from .core.CrossCorrelationMatcher import CrossCorrelationMatcher
+from .core.Matcha import Matcha
+from .core.ShiftMatcher import ShiftMatcher
+
+
+@dataclass
+class StepConfig:
+    N: int = 64
+    L: int = 32                      # L_max of the march; FLE bandlimit = L (align_subtomograms.py:125-134)
+    Li: list = field(default_factory=lambda: [8, 16, 24])
+    batch: int = 1000
+    radius: int | None = None        # ball radius; default min(N//2, int(0.95 N/2)) (align_subtomograms.py:94)
+    candidates: int = 10
+    num_steps: int = 1
+    K: int = 2
+    shift_upsample_factor: int = 8
+    shift_search_radius: int = 5
+    box_size: float | None = None
+    voxel_size: float = 1.0
+
+
+class _Cfg(dict):
+    def __getattr__(self, k):
+        try:
+            return self[k]
+        except KeyError as exc:
+            raise AttributeError(k) from exc
+
+
+class AlignmentStep:
+    """get_sigma -> search_orientations -> tracker update -> search_shifts for one batch."""
+
+    def __init__(self, cfg: StepConfig, device="cuda:0"):
+        self.cfg = cfg
+        self.device = torch.device(device)
+        radius = cfg.radius if cfg.radius is not None else min(cfg.N // 2, int(cfg.N // 2 * 0.95))
+        self.correlator = CrossCorrelationMatcher(N=cfg.N, device=self.device, batchsize=cfg.batch,
+                                                  bandlimit=cfg.L, radius=radius, precision_mode="fast")
+        self.matcher = Matcha(batchsize=cfg.batch, device=self.device, L_max=cfg.L,
+                              matcha_config=dict(Li=list(cfg.Li) + [cfg.L], candidates=cfg.candidates,
+                                                 num_steps=cfg.num_steps, oversampling_factor_K=cfg.K))
+        self.shifter = ShiftMatcher(_Cfg(N=cfg.N, voxel_size=cfg.voxel_size, num_subtomograms_per_batch=cfg.batch,
+                                         shift_upsample_factor=cfg.shift_upsample_factor,
+                                         shift_search_radius=cfg.shift_search_radius, do_ctf_correction=False,
+                                         box_size=cfg.box_size if cfg.box_size is not None else cfg.N),
+                                    self.device, torch.complex64)
+        B = cfg.batch
+        self.rot = torch.empty((B, 9), device=self.device, dtype=torch.float32)
+        self.shift = torch.empty((B, 3), device=self.device, dtype=torch.float32)
+        self.shift_score = torch.empty((B,), device=self.device, dtype=torch.float32)
+
+    def set_template(self, template: np.ndarray):
+        self.correlator.set_template(template)
+        self.shifter.set_reference(template)
+        # upload the shift reference now so that steps issue no host work
+        self.shifter._handle(self.cfg.batch)
+        ref = self.shifter.reference_data_fourier.to(torch.complex64).contiguous()
+        with torch.cuda.device(self.device):
+            nat.check(self.shifter._lib.mtb_shift_set_reference(self.shifter._h, nat.ptr(ref),
+                                                                nat.stream_ptr(self.device)), "mtb_shift_set_reference")
+        self.shifter._ref_dev = ref
+        self.shifter._uploaded_version = self.shifter._ref_version
+
+    @torch.no_grad()
+    def __call__(self, volumes: torch.Tensor, subtomos: torch.Tensor, tracker: torch.Tensor,
+                 shift_zyx: torch.Tensor):
+        """volumes: (B, N, N, N) input of the expansion; subtomos: (B, N, N, N) for the shift
+        match; tracker: (B, 4) float64 (w, x, y, z), updated in place; shift_zyx (B, 3)."""
+        B = volumes.shape[0]
+        sigma, norms = self.correlator.get_sigma(volumes)
+        a, b, g, score = self.matcher.search_orientations(sigma[:B])
+        dev = self.device
+        with torch.cuda.device(dev):
+            nat.check(self.matcher._lib.mtb_update_rotation(nat.ptr(a), nat.ptr(b), nat.ptr(g), nat.ptr(tracker), B,
+                                                            nat.ptr(tracker), nat.ptr(self.rot), nat.stream_ptr(dev)),
+                      "mtb_update_rotation")
+            nat.check(self.shifter._lib.mtb_shift_search(self.shifter._h, nat.ptr(subtomos), nat.ptr(shift_zyx),
+                                                         nat.ptr(self.rot), None, B, nat.ptr(self.shift),
+                                                         nat.ptr(self.shift_score), nat.stream_ptr(dev)),
+                      "mtb_shift_search")
+        return dict(alpha=a, beta=b, gamma=g, rotation_score=score, bh_norms=norms[:B], tracker=tracker,
+                    shift=self.shift[:B], shift_score=self.shift_score[:B])

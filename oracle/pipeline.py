@@ -1,0 +1,172 @@
+"""Oracle (test infrastructure only): one alignment alternation on the CPU.
+
+Chains the restatements of this package in the order of
+src/matcha/align_subtomograms.py:254-285 (get_sigma -> search_orientations ->
+update_rotation_estimate -> search_shifts) for a handful of subtomograms.  It is the
+CPU baseline the benchmark reports beside the GPU numbers, and a checker for the
+GPU pipeline; nothing in the product imports it.
+
+``FoldedFLE`` evaluates the same discrete adjoint as ``fle.evaluate_t`` but folds each
+volume over the 8 sign images of the positive octant first, which keeps the 64^3 basis
+at 1/8 of the dense size (float64, built once per configuration).
+"""
+from __future__ import annotations
+
+import numpy as np
+from scipy.spatial.transform import Rotation as R
+from scipy.special import spherical_jn
+
+from . import fle as F
+from . import matcha as M
+from . import shift as S
+
+
+class FoldedFLE:
+    """a = h B^H f through the octant folding; exact to float64 rounding."""
+
+    def __init__(self, tables, N1: int, radius: float):
+        self.tables = tables
+        N = N1 + (N1 % 2)
+        R_ = N // 2
+        g = np.arange(-R_, R_ + N % 2)
+        x, y, z = np.meshgrid(g, g, g, indexing="ij")
+        inside = (np.sqrt(x ** 2 + y ** 2 + z ** 2) / radius) <= 1 + 1e-13
+        if N > N1:
+            inside[N1:], inside[:, N1:], inside[:, :, N1:] = False, False, False
+        reps = np.unique(np.abs(np.stack([x[inside], y[inside], z[inside]], 1)), axis=0)
+        self.reps = reps
+        self.N1, self.R = N1, R_
+        # flat voxel index of each sign image (bit0 flips x, bit1 y, bit2 z); -1 absent/duplicate
+        img = np.full((reps.shape[0], 8), -1, dtype=np.int64)
+        for s in range(8):
+            sg = np.array([-1 if s & (1 << d) else 1 for d in range(3)])
+            c = reps * sg + R_
+            ok = np.all((c >= 0) & (c < N1), axis=1)
+            for d in range(3):
+                if s & (1 << d):
+                    ok &= reps[:, d] != 0
+            img[ok, s] = (c[ok, 0] * N1 + c[ok, 1]) * N1 + c[ok, 2]
+        self.img = img
+        r = np.sqrt((reps ** 2).sum(1)) / radius
+        th = np.arctan2(np.sqrt(reps[:, 0] ** 2 + reps[:, 1] ** 2), reps[:, 2])
+        ph = np.arctan2(reps[:, 1], reps[:, 0])
+        tb = tables
+        self.pos = np.nonzero(tb.ms >= 0)[0]
+        cols = np.zeros((reps.shape[0], self.pos.size), dtype=np.complex128)
+        ylm = _sph_harm_table(tb.lmax, th, ph)
+        radial = {}
+        for j, i in enumerate(self.pos):
+            l, m, k = int(tb.ls[i]), int(tb.ms[i]), int(tb.ks[i])
+            if (l, k) not in radial:
+                radial[(l, k)] = spherical_jn(l, tb.lmds[i] * r)
+            cols[:, j] = tb.h * tb.cs[i] * radial[(l, k)] * np.conj(ylm[(l, m)])
+        self.cols = cols
+        # parity of Re / Im of each column under the flips of x, y, z
+        m = tb.ms[self.pos]
+        l = tb.ls[self.pos]
+        self.par_re = np.stack([(-1.0) ** m, np.ones_like(m, dtype=float), (-1.0) ** (l + m)], 1)
+        self.par_im = np.stack([-(-1.0) ** m, -np.ones_like(m, dtype=float), (-1.0) ** (l + m)], 1)
+        self.partner = {}
+        for i in range(tb.ne):
+            self.partner[(int(tb.ls[i]), int(tb.ks[i]), int(tb.ms[i]))] = i
+
+    def _channel(self, vols, par):
+        """sum over images of f(image) * prod over flipped axes of par -> (b, n_rep) per column class."""
+        b = vols.shape[0]
+        v = vols.reshape(b, -1)
+        out = {}
+        for key in {tuple(p) for p in par}:
+            acc = np.zeros((b, self.reps.shape[0]))
+            for s in range(8):
+                idx = self.img[:, s]
+                ok = idx >= 0
+                w = np.prod([key[d] if s & (1 << d) else 1.0 for d in range(3)])
+                acc[:, ok] += w * v[:, idx[ok]]
+            out[key] = acc
+        return out
+
+    def evaluate_t(self, vols):
+        vols = np.asarray(vols, dtype=np.float64)
+        b = vols.shape[0]
+        tb = self.tables
+        ch_re = self._channel(vols, self.par_re)
+        ch_im = self._channel(vols, self.par_im)
+        re = np.zeros((b, self.pos.size))
+        im = np.zeros((b, self.pos.size))
+        for key, A in ch_re.items():
+            sel = np.all(self.par_re == key, axis=1)
+            re[:, sel] = A @ self.cols[:, sel].real
+        for key, A in ch_im.items():
+            sel = np.all(self.par_im == key, axis=1)
+            im[:, sel] = A @ self.cols[:, sel].imag
+        a = np.zeros((b, tb.ne), dtype=np.complex128)
+        a[:, self.pos] = re + 1j * im
+        for i in range(tb.ne):
+            m = int(tb.ms[i])
+            if m < 0:
+                j = self.partner[(int(tb.ls[i]), int(tb.ks[i]), -m)]
+                a[:, i] = (-1.0) ** m * np.conj(a[:, j])
+        return a
+
+
+def _sph_harm_table(lmax, theta, phi):
+    """Y_l^m(theta, phi) for 0 <= m <= l <= lmax: orthonormal, Condon-Shortley phase, by the
+    standard normalised associated-Legendre recurrences (checked against scipy's sph_harm_y
+    in the tests)."""
+    x = np.cos(theta)
+    s = np.sqrt(np.maximum(0.0, 1.0 - x * x))
+    out = {}
+    pmm = np.full_like(x, 1.0 / np.sqrt(4 * np.pi))
+    for m in range(lmax + 1):
+        if m > 0:
+            pmm = -np.sqrt((2 * m + 1) / (2 * m)) * s * pmm
+        e = np.exp(1j * m * phi)
+        p2, p1 = np.zeros_like(x), pmm
+        out[(m, m)] = pmm * e
+        for l in range(m + 1, lmax + 1):
+            if l == m + 1:
+                p = np.sqrt(2 * m + 3) * x * pmm
+            else:
+                a = np.sqrt((4 * l * l - 1) / (l * l - m * m))
+                b = np.sqrt(((l - 1) ** 2 - m * m) / (4 * (l - 1) ** 2 - 1))
+                p = a * (x * p1 - b * p2)
+            p2, p1 = p1, p
+            out[(l, m)] = p * e
+    return out
+
+
+def update_rotation_estimate(alpha, beta, gamma, tracker):
+    """src/matcha/utils/rotation_ops.py:23-34 with (w, x, y, z) float64 trackers."""
+    cb, sb = np.cos(0.5 * beta), np.sin(0.5 * beta)
+    q = np.stack([cb * np.cos(0.5 * (alpha + gamma)), -sb * np.sin(0.5 * (alpha - gamma)),
+                  sb * np.cos(0.5 * (alpha - gamma)), cb * np.sin(0.5 * (alpha + gamma))], -1)
+    q[:, [1, 3]] = q[:, [3, 1]]
+    qc = q * np.array([1, -1, -1, -1])
+    t = np.asarray(tracker, dtype=np.float64)
+    w1, v1 = t[:, :1], t[:, 1:]
+    w2, v2 = qc[:, :1], qc[:, 1:]
+    out = np.concatenate([w1 * w2 - (v1 * v2).sum(1, keepdims=True), w1 * v2 + w2 * v1 + np.cross(v1, v2)], 1)
+    return out / np.linalg.norm(out, axis=1, keepdims=True)
+
+
+def align_batch(fle: FoldedFLE, a_template, ref_fourier, vols, subtomos, tracker, shift_zyx, L, Li, K=2,
+                candidates=10, num_steps=1, uf=8, shift_radius=5, dtype=np.float32):
+    """One alternation for a few subtomograms: returns the same quantities as the GPU step."""
+    a = fle.evaluate_t(vols)
+    sigma = F.compute_sigma(fle.tables, a_template, a)
+    al, be, ga, score = M.search_orientations(sigma, list(Li) + [L], L, K=K, candidates=candidates,
+                                              num_steps=num_steps, dtype=dtype)
+    tr = update_rotation_estimate(al.astype(np.float64), be.astype(np.float64), ga.astype(np.float64), tracker)
+    ang = S.euler_zyz_deg_from_quat_conj(tr)
+    shifts, scores = [], []
+    for i in range(vols.shape[0]):
+        s, sc = S.estimate_shift_like_relion(ref_fourier, subtomos[i], shift_zyx[i], ang[i], uf, shift_radius)
+        shifts.append(s)
+        scores.append(sc)
+    return dict(alpha=al, beta=be, gamma=ga, rotation_score=score, bh_norms=np.linalg.norm(a, axis=1),
+                tracker=tr, shift=np.array(shifts), shift_score=np.array(scores))
+
+
+def rotation_matrix_of_tracker(tr):
+    """Matrix the shift match uses for a tracker (ShiftMatcher.py:503, :913)."""
+    return R.from_euler("ZYZ", S.euler_zyz_deg_from_quat_conj(tr), degrees=True).as_matrix()

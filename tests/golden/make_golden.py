@@ -13,6 +13,9 @@ What each fixture holds and which reference code produced it:
   the reference returns when truncate == ell_max).
 * ``grad_ref.npz``     -- ``WignerDGradients.set_so3_coeffs`` + ``get_derivatives``
   (src/matcha/core/WignerDGradients.py:155-302) on a seeded sigma and D.
+* ``shift_ref.npz``    -- ``load_reference_full`` and ``estimate_shift_like_relion``
+  (src/matcha/core/ShiftMatcher.py:456-472, 619-674) with the masks of
+  src/matcha/utils/setup_utils.py:239-270, on three seeded 32^3 subtomograms.
 * ``search_ref.npz``   -- ``Matcha.search_orientations`` (src/matcha/core/Matcha.py:369-403) and
   ``SOFFT.eval`` (src/matcha/core/SOFFT.py:67-98), run as reference code on the CPU.
   Two inputs the reference takes from packages absent here are supplied by the
@@ -169,6 +172,49 @@ def gen_search():
     print("search_ref.npz")
 
 
+def gen_shift():
+    """ShiftMatcher reference path on the CPU: load_reference_full + estimate_shift_like_relion."""
+    import torch
+
+    refharness._install_stubs()
+    S = refharness.load_module("matcha.core.ShiftMatcher")
+    U = refharness.load_module("matcha.utils.setup_utils")
+    sys.path.insert(0, ROOT)
+    from tests.helpers import blob_template, haar_quaternions, rotate_volumes_reference
+    from oracle import shift as OS
+
+    N, uf, r = 32, 8, 3
+    rng = np.random.default_rng(31)
+    tmpl = blob_template(rng, N, 40, 9, (1.5, 3.0), mask_radius=13)
+    q = haar_quaternions(rng, 3)
+    vols = rotate_volumes_reference(np.repeat(tmpl[None], 3, 0), q)
+    # integer and fractional true shifts via a Fourier phase ramp, plus noise
+    true = np.array([[0.0, 0.0, 0.0], [1.0, -2.0, 0.5], [-1.25, 0.75, 2.0]])
+    k = np.fft.fftfreq(N)
+    kz, ky, kx = np.meshgrid(k, k, k, indexing="ij")
+    for i in range(3):
+        ph = np.exp(-2j * np.pi * (kz * true[i, 0] + ky * true[i, 1] + kx * true[i, 2]))
+        vols[i] = np.fft.ifftn(np.fft.fftn(vols[i]) * ph).real
+    vols = (vols + 0.3 * rng.standard_normal(vols.shape)).astype(np.float32)
+    prior = np.array([[0.0, 0.0, 0.0], [0.5, -1.0, 0.25], [0.0, 0.0, 0.0]], dtype=np.float32)
+    angles = OS.euler_zyz_deg_from_quat_conj(q)
+    ref = S.load_reference_full(tmpl, volume_size=N, voxel_size=1.0)
+    mask_full = torch.from_numpy(U._get_mask_full((N, N, N // 2 + 1))).unsqueeze(0)
+    mo, mc, rc = U._compute_masks((N, N, N), N / 2.0, 5.0)
+    cfg = refharness._ConfigDict(N=N, shift_upsample_factor=uf, shift_search_radius=r, do_ctf_correction=False,
+                                 device=torch.device("cpu"),
+                                 execution=refharness._ConfigDict(shape=torch.tensor((N, N, N)),
+                                                                  dtype=torch.complex64))
+    shift, score = S.estimate_shift_like_relion(
+        torch.from_numpy(ref).unsqueeze(0).to(torch.complex64).expand(3, -1, -1, -1), torch.from_numpy(vols), None,
+        torch.from_numpy(prior)[:, None, :], angles, mask_full, torch.from_numpy(mo), torch.from_numpy(mc),
+        torch.from_numpy(rc).to(torch.float32), cfg)
+    np.savez_compressed(os.path.join(HERE, "shift_ref.npz"), template=tmpl, subtomos=vols, quats=q, prior_zyx=prior,
+                        angles_deg=angles, ref_fourier=ref.astype(np.complex64), shift_xyz=shift.numpy(),
+                        score=score.numpy(), N=N, uf=uf, radius=r, true_zyx=true)
+    print("shift_ref.npz", shift.numpy(), score.numpy())
+
+
 if __name__ == "__main__":
     what = sys.argv[1] if len(sys.argv) > 1 else "all"
     if what in ("wigner", "all"):
@@ -177,3 +223,5 @@ if __name__ == "__main__":
         gen_grad()
     if what in ("search", "all"):
         gen_search()
+    if what in ("shift", "all"):
+        gen_shift()

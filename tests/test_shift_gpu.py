@@ -1,0 +1,69 @@
+"""Shift match on the GPU against the oracle and the reference fixture."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import shift as OS
+from tests.helpers import blob_template, golden, haar_quaternions, rotate_volumes_reference
+
+pytestmark = pytest.mark.gpu
+
+
+class Cfg(dict):
+    __getattr__ = dict.__getitem__
+
+
+def _matcher(N, B, uf, r, device, box=None):
+    from matcha_b200.core.ShiftMatcher import ShiftMatcher
+
+    cfg = Cfg(N=N, voxel_size=1.0, num_subtomograms_per_batch=B, shift_upsample_factor=uf, shift_search_radius=r,
+              do_ctf_correction=False, box_size=box if box is not None else N)
+    return ShiftMatcher(cfg, device, torch.complex64)
+
+
+def test_shift_matches_reference_fixture(cuda_device):
+    z = golden("shift_ref.npz")
+    N, uf, r = int(z["N"]), int(z["uf"]), int(z["radius"])
+    sm = _matcher(N, 3, uf, r, cuda_device)
+    sm.set_reference(z["template"])
+    ref_host = sm.reference_data_fourier[0].cpu().numpy()
+    np.testing.assert_allclose(ref_host, z["ref_fourier"], atol=1e-6 * np.abs(z["ref_fourier"]).max())
+    # trackers whose conjugate has the fixture's Euler angles
+    q = z["quats"]
+    shift, score = sm.search_shifts(subtomos=torch.from_numpy(z["subtomos"]).to(cuda_device), ctfs=None,
+                                    shift_zyx=torch.from_numpy(z["prior_zyx"]).to(cuda_device), rotation_tracker=q)
+    np.testing.assert_allclose(shift.cpu().numpy(), z["shift_xyz"], atol=1e-6)
+    np.testing.assert_allclose(score.cpu().numpy(), z["score"], rtol=2e-5)
+
+
+@pytest.mark.parametrize("N,uf,r", [(32, 8, 3), (64, 8, 5), (32, 4, 2)])
+def test_shift_matches_oracle(cuda_device, N, uf, r):
+    rng = np.random.default_rng(N + uf + r)
+    tmpl = blob_template(rng, N, 60, N * 0.3, (1.5, 3.0), mask_radius=N * 0.4)
+    B = 3
+    q = haar_quaternions(rng, B)
+    vols = rotate_volumes_reference(np.repeat(tmpl[None], B, 0), q)
+    vols = (vols + 0.5 * rng.standard_normal(vols.shape)).astype(np.float32)
+    prior = rng.uniform(-1.5, 1.5, (B, 3)).astype(np.float32)
+    sm = _matcher(N, B, uf, r, cuda_device)
+    sm.set_reference(tmpl)
+    shift, score = sm.search_shifts(subtomos=torch.from_numpy(vols).to(cuda_device), ctfs=None,
+                                    shift_zyx=torch.from_numpy(prior).to(cuda_device), rotation_tracker=q)
+    shift, score = shift.cpu().numpy(), score.cpu().numpy()
+    ref = OS.load_reference_full(tmpl, N, 1.0)
+    ang = OS.euler_zyz_deg_from_quat_conj(q)
+    for b in range(B):
+        (s_ref, sc_ref), parts = OS.estimate_shift_like_relion(ref, vols[b], prior[b], ang[b], uf, r,
+                                                               return_parts=True)
+        grid = parts["grid"].ravel()
+        top2 = np.sort(grid)[-2:]
+        if (top2[1] - top2[0]) > 1e-5 * abs(top2[1]):  # unique peak
+            np.testing.assert_allclose(shift[b], s_ref, atol=1e-6)
+        np.testing.assert_allclose(score[b], sc_ref, rtol=3e-5)
+
+
+def test_shift_requires_reference(cuda_device):
+    sm = _matcher(16, 1, 4, 1, cuda_device)
+    with pytest.raises(RuntimeError):
+        sm.search_shifts(subtomos=torch.zeros((1, 16, 16, 16), device=cuda_device), ctfs=None,
+                         shift_zyx=torch.zeros((1, 3), device=cuda_device), rotation_tracker=np.array([[1.0, 0, 0, 0]]))
