@@ -131,7 +131,12 @@ typedef struct {
   const int* kpad;          /* [lmax+1] padded k-count of degree l                      */
   const int* kidx;          /* [sum_l (2l+1) kpad[l]] coefficient index of (l, mu, k),
                                rows mu = -l..l, -1 = padding                            */
+  int precision;            /* MTB_FLE_FP32: FP32 CUDA-core GEMM; MTB_FLE_BF16X3: tcgen05
+                               BF16 GEMM with a hi+lo split correction                  */
 } mtb_fle_config;
+
+#define MTB_FLE_FP32 0
+#define MTB_FLE_BF16X3 1
 
 typedef struct mtb_fle mtb_fle;
 
@@ -149,6 +154,10 @@ int mtb_fle_forward(mtb_fle* h, const float* vol, int B, float* coeffs, int64_t 
  * tmpl (ne,) complex64; sigma (B, sigma_stride) complex64 out, dsize(lmax) entries. */
 int mtb_sigma(mtb_fle* h, const float* coeffs, int64_t coeff_stride, const float* tmpl, int B,
               float* sigma, int64_t sigma_stride, mtb_stream_t stream);
+
+/* Synchronises stream and returns MTB_ERR_TIMEOUT if a bounded device-side wait of the
+ * tensor-core path gave up since the handle was created (then its results are invalid). */
+int mtb_fle_status(mtb_fle* h, mtb_stream_t stream);
 
 /* ------------------------------------------------------------------------------
  * FFT shift match (RELION-style masked correlation with a local upsampled DFT).

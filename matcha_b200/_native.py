@@ -21,6 +21,8 @@ MTB_ERR_TIMEOUT = 4
 MTB_ERR_CUDA = 5
 
 MTB_MAX_STAGES = 16
+MTB_FLE_FP32 = 0
+MTB_FLE_BF16X3 = 1
 MTB_SEARCH_COMPAT_TOP_BLOCK = 1
 MTB_SEARCH_GRADIENT_STEP = 2
 
@@ -50,7 +52,7 @@ class MtbFleConfig(ctypes.Structure):
         ("col_l", ctypes.c_void_p), ("col_m", ctypes.c_void_p), ("col_part", ctypes.c_void_p),
         ("col_lk", ctypes.c_void_p), ("col_scale", ctypes.c_void_p), ("coef_col_re", ctypes.c_void_p),
         ("coef_col_im", ctypes.c_void_p), ("coef_sign_re", ctypes.c_void_p), ("coef_sign_im", ctypes.c_void_p),
-        ("kpad", ctypes.c_void_p), ("kidx", ctypes.c_void_p),
+        ("kpad", ctypes.c_void_p), ("kidx", ctypes.c_void_p), ("precision", ctypes.c_int),
     ]
 
 
@@ -78,6 +80,7 @@ SIGNATURES = {
     "mtb_fle_destroy": (None, [_P]),
     "mtb_fle_forward": (_I, [_P, _P, _I, _P, _I64, _P, _P]),
     "mtb_sigma": (_I, [_P, _P, _I64, _P, _I, _P, _I64, _P]),
+    "mtb_fle_status": (_I, [_P, _P]),
     "mtb_shift_create": (_I, [ctypes.POINTER(MtbShiftConfig), ctypes.POINTER(_P)]),
     "mtb_shift_destroy": (None, [_P]),
     "mtb_shift_set_reference": (_I, [_P, _P, _P]),

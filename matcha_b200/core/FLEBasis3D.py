@@ -116,7 +116,7 @@ class FLEBasis3D:
     def __init__(self, N, bandlimit, eps, maxitr=None, maxfun=None, max_l=None, mode="complex",
                  sph_harm_solver="nvidia_torch", reduce_memory=True, batchsize=1, radius=1, device="cuda",
                  dtype=torch.complex128, jl_zeros_path="jl_zeros_l=3000_k=2500.mat",
-                 cs_path="cs_l=3000_k=2500.mat", precision_mode="accurate"):
+                 cs_path="cs_l=3000_k=2500.mat", precision_mode="accurate", precision="fp32"):
         if mode not in ("complex", "real"):
             raise AssertionError("mode must be 'real' or 'complex'")
         if mode == "real":
@@ -130,6 +130,9 @@ class FLEBasis3D:
         self.dtype = dtype
         self.precision_mode = precision_mode
         self.eps = eps
+        if precision not in ("fp32", "bf16x3"):
+            raise ValueError("precision must be 'fp32' (CUDA cores) or 'bf16x3' (tensor cores, hi+lo split)")
+        self.precision = precision
         tb = T.lap_eig_ball(int(N), bandlimit, float(radius), jl_zeros_path, cs_path, maxfun=maxfun, max_l=max_l)
         self.tables = tb
         self.N1, self.N, self.ne, self.lmax = tb.N1, tb.N, tb.ne, tb.lmax
@@ -151,6 +154,7 @@ class FLEBasis3D:
             arr = np.ascontiguousarray(ct[name])
             keep.append(arr)
             setattr(cfg, name, arr.ctypes.data)
+        cfg.precision = nat.MTB_FLE_BF16X3 if precision == "bf16x3" else nat.MTB_FLE_FP32
         lib = nat.load()
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
@@ -179,6 +183,11 @@ class FLEBasis3D:
             nat.check(self._lib.mtb_fle_forward(self._h, nat.ptr(f), b, nat.ptr(out), out.stride(0), nat.ptr(norms),
                                               nat.stream_ptr(f.device)), "mtb_fle_forward")
         return out, norms
+
+    def status(self):
+        """Raise if a bounded device-side wait of the tensor-core path gave up (synchronises)."""
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.mtb_fle_status(self._h, nat.stream_ptr(self.device)), "mtb_fle_status")
 
     @torch.no_grad()
     def evaluate_t(self, f: torch.Tensor, return_step=3):

@@ -19,6 +19,7 @@
 #include <string.h>
 #include <vector>
 #include "common.cuh"
+#include "fle_tc.cuh"
 
 namespace {
 
@@ -270,6 +271,8 @@ struct mtb_fle {
   int* kpad;
   int* koff;
   int* kidx;
+  FleTc tc;
+  bool use_tc;
 };
 
 extern "C" int mtb_fle_create(const mtb_fle_config* cfg, mtb_fle** out) {
@@ -374,6 +377,13 @@ extern "C" int mtb_fle_create(const mtb_fle_config* cfg, mtb_fle** out) {
   cudaFree(d_cos); cudaFree(d_phi); cudaFree(d_r2); cudaFree(d_j); cudaFree(d_lms); cudaFree(d_cl);
   cudaFree(d_cls); cudaFree(d_pos); cudaFree(d_part); cudaFree(d_lk); cudaFree(d_scale);
   if (rc) return fail(rc);
+  if (cfg->precision == MTB_FLE_BF16X3) {
+    rc = fle_tc_prepare(&h->tc, h->basis, h->class_cols, h->class_off, nr, cfg->max_batch, nc);
+    if (rc) return fail(rc);
+    h->use_tc = true;
+  } else if (cfg->precision != MTB_FLE_FP32) {
+    return fail(MTB_ERR_ARG);
+  }
   *out = h;
   return MTB_OK;
 }
@@ -381,6 +391,7 @@ extern "C" int mtb_fle_create(const mtb_fle_config* cfg, mtb_fle** out) {
 extern "C" void mtb_fle_destroy(mtb_fle* h) {
   if (!h) return;
   for (int k = 0; k < kClasses; ++k) if (h->basis[k]) cudaFree(h->basis[k]);
+  fle_tc_release(&h->tc);
   void* ptrs[] = {h->d_basis, h->d_class_cols, h->d_class_off, h->rep_img, h->col_re, h->col_im, h->s_re, h->s_im,
                   h->A, h->C, h->kpad, h->koff, h->kidx};
   for (void* p : ptrs) if (p) cudaFree(p);
@@ -398,15 +409,20 @@ extern "C" int mtb_fle_forward(mtb_fle* h, const float* vol, int B, float* coeff
   const int nr = h->cfg.n_rep, N = h->cfg.N;
   const int64_t vstride = (int64_t)N * N * N;
   const int64_t astride = (int64_t)h->cfg.max_batch * nr;
-  dim3 fg((nr + 255) / 256, B);
-  fold_kernel<<<fg, 256, 0, st>>>(vol, vstride, B, nr, h->rep_img, h->A, astride);
-  MTB_LAUNCH_CHECK();
-  int maxc = 0;
-  for (int k = 0; k < kClasses; ++k) maxc = h->class_cols[k] > maxc ? h->class_cols[k] : maxc;
-  dim3 gg((maxc + GN - 1) / GN, (B + GM - 1) / GM, kClasses);
-  gemm_fp32_kernel<<<gg, 256, 0, st>>>(h->A, astride, B, nr, h->d_basis, h->d_class_cols, h->C, h->cfg.n_cols,
-                                       h->d_class_off);
-  MTB_LAUNCH_CHECK();
+  if (h->use_tc) {
+    const int rc = fle_tc_forward(&h->tc, vol, vstride, B, h->rep_img, h->C, st);
+    if (rc) return rc;
+  } else {
+    dim3 fg((nr + 255) / 256, B);
+    fold_kernel<<<fg, 256, 0, st>>>(vol, vstride, B, nr, h->rep_img, h->A, astride);
+    MTB_LAUNCH_CHECK();
+    int maxc = 0;
+    for (int k = 0; k < kClasses; ++k) maxc = h->class_cols[k] > maxc ? h->class_cols[k] : maxc;
+    dim3 gg((maxc + GN - 1) / GN, (B + GM - 1) / GM, kClasses);
+    gemm_fp32_kernel<<<gg, 256, 0, st>>>(h->A, astride, B, nr, h->d_basis, h->d_class_cols, h->C, h->cfg.n_cols,
+                                         h->d_class_off);
+    MTB_LAUNCH_CHECK();
+  }
   expand_kernel<<<B, 256, 0, st>>>(h->C, h->cfg.n_cols, B, h->cfg.ne, h->col_re, h->col_im, h->s_re, h->s_im,
                                    reinterpret_cast<float2*>(coeffs), coeff_stride, norms);
   MTB_LAUNCH_CHECK();
@@ -429,4 +445,15 @@ extern "C" int mtb_sigma(mtb_fle* h, const float* coeffs, int64_t coeff_stride, 
                                                     h->koff, h->kidx, reinterpret_cast<float2*>(sigma), sigma_stride);
   MTB_LAUNCH_CHECK();
   return MTB_OK;
+}
+
+extern "C" int mtb_fle_status(mtb_fle* h, mtb_stream_t stream) {
+  MTB_ARG_CHECK(h, "null handle");
+  if (!h->use_tc) {
+    MTB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    return MTB_OK;
+  }
+  const int rc = fle_tc_check(&h->tc, (cudaStream_t)stream);
+  if (rc) mtb_set_last_error("tensor-core FLE GEMM: a bounded wait ran out", __FILE__, __LINE__);
+  return rc;
 }

@@ -1,0 +1,387 @@
+// Tensor-core path of the ball expansion: BF16 hi+lo split GEMM on tcgen05 (sm_100a).
+//
+// The 8 octant-parity GEMMs of fle.cu, C_p = A_p * B_p (A: folded volumes, B: basis
+// columns), run here as BF16 x BF16 -> FP32 products with a split correction:
+//     A B ~= A_hi B_hi + A_lo B_hi + A_hi B_lo,   A_hi = bf16(A), A_lo = bf16(A - A_hi)
+// (the dropped A_lo B_lo term is ~2^-16 relative).  The three products are one GEMM over
+// a K axis three times as long: k-block j of [0, 3 KB) selects (A_hi, B_hi), (A_lo, B_hi)
+// or (A_hi, B_lo), so every pipeline stage moves one A tile and one B tile.
+//
+// Layout: both operands K-major bf16, 128-byte swizzled tiles staged by TMA
+// (cp.async.bulk.tensor.2d), tile M = 128 (a batch block), N = 256 (basis columns),
+// K = 64 per stage, 4 stages.  One thread issues tcgen05.mma (kind::f16, M128 N256 K16)
+// into a 256-column FP32 accumulator in tensor memory; four warps read it back with
+// tcgen05.ld and store FP32 C.  A and B of all classes and both parts share two tensor
+// maps: rows (class * 2 + part) * Mpad + m of A, (class * 2 + part) * Npad + n of B.
+//
+// Every mbarrier wait is bounded; on expiry the kernel records an error code, stops
+// issuing, and still frees its tensor memory before returning.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+#include <string.h>
+#include "common.cuh"
+#include "fle_tc.cuh"
+
+namespace {
+
+constexpr int TM = 128, TN = 256, TK = 64;
+constexpr int STAGES = 4;
+constexpr int A_TILE = TM * TK * 2;  // 16 KB
+constexpr int B_TILE = TN * TK * 2;  // 32 KB
+constexpr int STAGE_BYTES = A_TILE + B_TILE;
+constexpr int kThreads = 192;        // warp 0: TMA, warp 1: MMA, warps 2-5: epilogue
+constexpr uint32_t kTmemCols = 256;
+constexpr long long kSpinLimit = 1LL << 26;
+
+struct TcParams {
+  int Mpad, Npad, KB;   // padded batch rows per (class, part), padded columns, K blocks of 64
+  int M;                // valid batch rows
+  int ncols[8];         // valid columns per class
+  int coff[8];          // column offset of the class inside C
+  int ldc;              // row stride of C (floats)
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (long long i = 0; i < kSpinLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int c0, int c1, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t smem_desc(const void* p) {
+  const uint64_t addr = smem_u32(p);
+  uint64_t d = 0;
+  d |= (addr >> 4) & 0x3FFFull;           // start address
+  d |= (uint64_t)1 << 16;                 // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset
+  d |= (uint64_t)1 << 46;                 // descriptor version for tcgen05
+  d |= (uint64_t)2 << 61;                 // SWIZZLE_128B
+  return d;
+}
+
+// Instruction descriptor, kind::f16: D f32, A/B bf16, both K-major, M=128, N=256.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+gemm_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcParams P,
+               float* __restrict__ C, int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  // 1024-byte alignment for the swizzled tiles
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ __align__(8) uint64_t full_bar[STAGES];
+  __shared__ __align__(8) uint64_t empty_bar[STAGES];
+  __shared__ __align__(8) uint64_t done_bar;
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag;
+
+  const int cls = blockIdx.z;
+  const int n0 = blockIdx.x * TN, m0 = blockIdx.y * TM;
+  if (n0 >= P.ncols[cls]) return;  // uniform per CTA
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&done_bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  const int KB3 = 3 * P.KB;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer
+    for (int j = 0; j < KB3; ++j) {
+      const int s = j % STAGES;
+      const uint32_t use = j / STAGES;
+      if (j >= STAGES && !mbar_wait(&empty_bar[s], (use - 1) & 1)) {
+        atomicExch(err, 1);
+        abort_flag = 1;
+        break;
+      }
+      if (abort_flag) break;
+      const int part = j / P.KB;           // 0: (hi, hi), 1: (lo, hi), 2: (hi, lo)
+      const int kb = j - part * P.KB;
+      const int apart = (part == 1) ? 1 : 0, bpart = (part == 2) ? 1 : 0;
+      uint8_t* sa = smem + s * STAGE_BYTES;
+      uint8_t* sb = sa + A_TILE;
+      mbar_expect_tx(&full_bar[s], STAGE_BYTES);
+      tma_load_2d(sa, &mapA, kb * TK, (cls * 2 + apart) * P.Mpad + m0, &full_bar[s]);
+      tma_load_2d(sb, &mapB, kb * TK, (cls * 2 + bpart) * P.Npad + n0, &full_bar[s]);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer
+    bool ok = true;
+    for (int j = 0; j < KB3; ++j) {
+      const int s = j % STAGES;
+      const uint32_t use = j / STAGES;
+      if (!mbar_wait(&full_bar[s], use & 1)) {
+        atomicExch(err, 2);
+        abort_flag = 1;
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint8_t* sa = smem + s * STAGE_BYTES;
+      const uint8_t* sb = sa + A_TILE;
+      const uint64_t ad = smem_desc(sa), bd = smem_desc(sb);
+#pragma unroll
+      for (int kk = 0; kk < TK / 16; ++kk) {
+        // 16 bf16 = 32 bytes further along K inside the swizzle atom: +2 in the >>4 address field
+        mma_bf16(tmem, ad + (uint64_t)(kk * 2), bd + (uint64_t)(kk * 2), (j > 0 || kk > 0) ? 1u : 0u);
+      }
+      mma_commit(&empty_bar[s]);
+    }
+    if (ok) mma_commit(&done_bar);
+  } else if (warp >= 2) {
+    // ---- epilogue: TMEM lanes 32*(warp%4) .. +31 hold rows m0 + that range
+    const bool ok = mbar_wait(&done_bar, 0);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!ok) {
+      atomicExch(err, 3);
+    } else {
+      const int q = warp & 3;
+      const int row = m0 + q * 32 + lane;
+      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16);
+      float* crow = C + (int64_t)row * P.ldc + P.coff[cls];
+      const int nc = P.ncols[cls];
+#pragma unroll 1
+      for (int cb = 0; cb < TN; cb += 32) {
+        uint32_t v[32];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+              "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+              "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+              "=r"(v[30]), "=r"(v[31])
+            : "r"(taddr + (uint32_t)cb));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < P.M) {
+          const int nb = n0 + cb;
+#pragma unroll
+          for (int t = 0; t < 32; ++t)
+            if (nb + t < nc) crow[nb + t] = __uint_as_float(v[t]);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+  }
+}
+
+// ---------------------------------------------------------------- operand preparation
+// Folded channels, split into bf16 hi/lo: Aall[((cls*2 + part) * Mpad + b) * Kpad + rep].
+__global__ void fold_split_kernel(const float* __restrict__ vol, int64_t vol_stride, int B, int n_rep, int Mpad,
+                                  int Kpad, const int* __restrict__ rep_img, __nv_bfloat16* __restrict__ A) {
+  const int rep = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  if (rep >= Kpad || b >= B) return;
+  float f[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    const int idx = rep < n_rep ? __ldg(&rep_img[rep * 8 + s]) : -1;
+    f[s] = idx >= 0 ? __ldg(&vol[(int64_t)b * vol_stride + idx]) : 0.f;
+  }
+#pragma unroll
+  for (int bit = 1; bit < 8; bit <<= 1)
+#pragma unroll
+    for (int s = 0; s < 8; ++s)
+      if (!(s & bit)) {
+        const float u = f[s], w = f[s | bit];
+        f[s] = u + w;
+        f[s | bit] = u - w;
+      }
+#pragma unroll
+  for (int p = 0; p < 8; ++p) {
+    const __nv_bfloat16 hi = __float2bfloat16_rn(f[p]);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(f[p] - __bfloat162float(hi));
+    A[((int64_t)(p * 2 + 0) * Mpad + b) * Kpad + rep] = hi;
+    A[((int64_t)(p * 2 + 1) * Mpad + b) * Kpad + rep] = lo;
+  }
+}
+
+// Basis (K x n_p, row-major FP32 per class) -> Ball[((cls*2 + part) * Npad + n) * Kpad + k], K-major bf16.
+__global__ void basis_split_kernel(const float* __restrict__ basis, int n_rep, int ncls, int cls, int Npad, int Kpad,
+                                   __nv_bfloat16* __restrict__ Bm) {
+  __shared__ float tile[32][33];
+  const int k0 = blockIdx.x * 32, n0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int k = k0 + i, n = n0 + threadIdx.x;
+    tile[i][threadIdx.x] = (k < n_rep && n < ncls) ? basis[(int64_t)k * ncls + n] : 0.f;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int n = n0 + i, k = k0 + threadIdx.x;
+    if (n >= Npad || k >= Kpad) continue;
+    const float v = tile[threadIdx.x][i];
+    const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+    Bm[((int64_t)(cls * 2 + 0) * Npad + n) * Kpad + k] = hi;
+    Bm[((int64_t)(cls * 2 + 1) * Npad + n) * Kpad + k] = lo;
+  }
+}
+
+typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int make_map(CUtensorMap* map, void* base, uint64_t inner, uint64_t rows, uint32_t box_rows) {
+  static EncodeTiled fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p)
+      return MTB_ERR_CUDA;
+    fn = reinterpret_cast<EncodeTiled>(p);
+  }
+  const cuuint64_t dims[2] = {inner, rows};
+  const cuuint64_t strides[1] = {inner * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)TK, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? MTB_OK : MTB_ERR_CUDA;
+}
+
+}  // namespace
+
+size_t fle_tc_a_elems(int max_batch, int n_rep) {
+  const int Mpad = (max_batch + TM - 1) / TM * TM;
+  const int Kpad = (n_rep + TK - 1) / TK * TK;
+  return (size_t)16 * Mpad * Kpad;
+}
+
+int fle_tc_prepare(FleTc* t, float* const* basis, const int* class_cols, const int* class_off, int n_rep,
+                   int max_batch, int n_cols) {
+  memset(t, 0, sizeof(*t));
+  t->Mpad = (max_batch + TM - 1) / TM * TM;
+  t->Kpad = (n_rep + TK - 1) / TK * TK;
+  int maxc = 0;
+  for (int k = 0; k < 8; ++k) maxc = class_cols[k] > maxc ? class_cols[k] : maxc;
+  t->Npad = (maxc + TN - 1) / TN * TN;
+  t->n_rep = n_rep;
+  t->n_cols = n_cols;
+  for (int k = 0; k < 8; ++k) {
+    t->ncols[k] = class_cols[k];
+    t->coff[k] = class_off[k];
+  }
+  const size_t asz = (size_t)16 * t->Mpad * t->Kpad, bsz = (size_t)16 * t->Npad * t->Kpad;
+  if (cudaMalloc(&t->A, asz * 2) != cudaSuccess) return MTB_ERR_OOM;
+  if (cudaMalloc(&t->B, bsz * 2) != cudaSuccess) return MTB_ERR_OOM;
+  if (cudaMalloc(&t->err, sizeof(int)) != cudaSuccess) return MTB_ERR_OOM;
+  if (cudaMemset(t->B, 0, bsz * 2) != cudaSuccess || cudaMemset(t->A, 0, asz * 2) != cudaSuccess ||
+      cudaMemset(t->err, 0, sizeof(int)) != cudaSuccess)
+    return MTB_ERR_CUDA;
+  for (int k = 0; k < 8; ++k) {
+    if (!class_cols[k]) continue;
+    dim3 g((t->Kpad + 31) / 32, (t->Npad + 31) / 32);
+    basis_split_kernel<<<g, dim3(32, 8)>>>(basis[k], n_rep, class_cols[k], k, t->Npad, t->Kpad,
+                                           reinterpret_cast<__nv_bfloat16*>(t->B));
+    if (cudaGetLastError() != cudaSuccess) return MTB_ERR_CUDA;
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return MTB_ERR_CUDA;
+  int rc = make_map(reinterpret_cast<CUtensorMap*>(t->mapA), t->A, (uint64_t)t->Kpad, (uint64_t)16 * t->Mpad, TM);
+  if (!rc) rc = make_map(reinterpret_cast<CUtensorMap*>(t->mapB), t->B, (uint64_t)t->Kpad, (uint64_t)16 * t->Npad, TN);
+  return rc;
+}
+
+void fle_tc_release(FleTc* t) {
+  if (t->A) cudaFree(t->A);
+  if (t->B) cudaFree(t->B);
+  if (t->err) cudaFree(t->err);
+  memset(t, 0, sizeof(*t));
+}
+
+int fle_tc_forward(FleTc* t, const float* vol, int64_t vol_stride, int B, const int* rep_img, float* C,
+                   cudaStream_t st) {
+  dim3 fg((t->Kpad + 255) / 256, B);
+  fold_split_kernel<<<fg, 256, 0, st>>>(vol, vol_stride, B, t->n_rep, t->Mpad, t->Kpad, rep_img,
+                                        reinterpret_cast<__nv_bfloat16*>(t->A));
+  MTB_LAUNCH_CHECK();
+  TcParams P;
+  P.Mpad = t->Mpad;
+  P.Npad = t->Npad;
+  P.KB = t->Kpad / TK;
+  P.M = B;
+  for (int k = 0; k < 8; ++k) {
+    P.ncols[k] = t->ncols[k];
+    P.coff[k] = t->coff[k];
+  }
+  P.ldc = t->n_cols;
+  const size_t smem = (size_t)STAGES * STAGE_BYTES + 1024;
+  MTB_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 gg(t->Npad / TN, (B + TM - 1) / TM, 8);
+  gemm_tc_kernel<<<gg, kThreads, smem, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA),
+                                             *reinterpret_cast<const CUtensorMap*>(t->mapB), P, C, t->err);
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
+}
+
+int fle_tc_check(FleTc* t, cudaStream_t st) {
+  int h = 0;
+  MTB_CUDA_TRY(cudaMemcpyAsync(&h, t->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MTB_CUDA_TRY(cudaStreamSynchronize(st));
+  return h ? MTB_ERR_TIMEOUT : MTB_OK;
+}

@@ -1,0 +1,26 @@
+// Tensor-core (tcgen05, BF16 hi+lo split) GEMM of the ball expansion; used by fle.cu.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+struct FleTc {
+  alignas(64) unsigned char mapA[128];  // CUtensorMap of the folded channels (bf16 hi/lo)
+  alignas(64) unsigned char mapB[128];  // CUtensorMap of the basis (bf16 hi/lo, K-major)
+  int Mpad, Npad, Kpad, n_rep, n_cols;
+  int ncols[8], coff[8];
+  void* A;   // (8 classes x 2 parts x Mpad, Kpad) bf16
+  void* B;   // (8 classes x 2 parts x Npad, Kpad) bf16
+  int* err;  // nonzero after a bounded wait ran out
+};
+
+// Split the FP32 class bases into bf16 hi/lo K-major operands and build the tensor maps.
+int fle_tc_prepare(FleTc* t, float* const* basis, const int* class_cols, const int* class_off, int n_rep,
+                   int max_batch, int n_cols);
+void fle_tc_release(FleTc* t);
+// Fold + split the volumes, then C (B, n_cols) = sum over classes of the split GEMMs.
+int fle_tc_forward(FleTc* t, const float* vol, int64_t vol_stride, int B, const int* rep_img, float* C,
+                   cudaStream_t st);
+// Synchronises st and reports MTB_ERR_TIMEOUT if a device-side wait gave up.
+int fle_tc_check(FleTc* t, cudaStream_t st);
+size_t fle_tc_a_elems(int max_batch, int n_rep);

@@ -35,6 +35,7 @@ class StepConfig:
     shift_search_radius: int = 5
     box_size: float | None = None
     voxel_size: float = 1.0
+    precision: str = "bf16x3"        # ball-expansion GEMM: "bf16x3" (tcgen05) or "fp32" (CUDA cores)
 
 
 class _Cfg(dict):
@@ -53,7 +54,8 @@ class AlignmentStep:
         self.device = torch.device(device)
         radius = cfg.radius if cfg.radius is not None else min(cfg.N // 2, int(cfg.N // 2 * 0.95))
         self.correlator = CrossCorrelationMatcher(N=cfg.N, device=self.device, batchsize=cfg.batch,
-                                                  bandlimit=cfg.L, radius=radius, precision_mode="fast")
+                                                  bandlimit=cfg.L, radius=radius, precision_mode="fast",
+                                                  precision=cfg.precision)
         self.matcher = Matcha(batchsize=cfg.batch, device=self.device, L_max=cfg.L,
                               matcha_config=dict(Li=list(cfg.Li) + [cfg.L], candidates=cfg.candidates,
                                                  num_steps=cfg.num_steps, oversampling_factor_K=cfg.K))

@@ -67,3 +67,39 @@ def test_rotation_recovery_end_to_end(cuda_device):
     a, b, g, s = (x.cpu().numpy() for x in m.search_orientations(sig))
     err = alignment_error_deg(a, b, g, q)
     assert np.median(err) < 3.0, err
+
+
+@pytest.mark.parametrize("N1,bl,radius", [(32, 16, 14), (31, 12, 13)])
+def test_tensor_core_split_matches_dense_definition(cuda_device, N1, bl, radius):
+    """BF16 hi+lo split GEMM on tcgen05: within 1e-4 relative of the exact adjoint."""
+    from matcha_b200.core.FLEBasis3D import FLEBasis3D
+
+    fle = FLEBasis3D(N=N1, bandlimit=bl, eps=1e-4, batchsize=130, radius=radius, device=cuda_device,
+                     dtype=torch.complex64, precision="bf16x3")
+    rng = np.random.default_rng(3 * N1 + radius)
+    vols = rng.standard_normal((130, N1, N1, N1)).astype(np.float32)  # two M tiles, the second ragged
+    a = fle.evaluate_t(torch.from_numpy(vols).to(cuda_device))
+    fle.status()
+    a = a.cpu().numpy()
+    idx = [0, 1, 127, 128, 129]
+    ref = F.evaluate_t(fle.tables, vols[idx], float(radius))
+    err = np.linalg.norm(a[idx] - ref) / np.linalg.norm(ref)
+    assert err < 1e-4, err
+    # and agrees with the FP32 CUDA-core path on every volume
+    f32 = FLEBasis3D(N=N1, bandlimit=bl, eps=1e-4, batchsize=130, radius=radius, device=cuda_device,
+                     dtype=torch.complex64, precision="fp32")
+    b = f32.evaluate_t(torch.from_numpy(vols).to(cuda_device)).cpu().numpy()
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-4
+
+
+def test_tensor_core_split_at_benchmark_shape(cuda_device):
+    from matcha_b200.core.FLEBasis3D import FLEBasis3D
+
+    kw = dict(N=64, bandlimit=32, eps=1e-4, batchsize=200, radius=30, device=cuda_device, dtype=torch.complex64)
+    tc = FLEBasis3D(precision="bf16x3", **kw)
+    fp = FLEBasis3D(precision="fp32", **kw)
+    v = torch.randn(200, 64, 64, 64, device=cuda_device)
+    a, b = tc.evaluate_t(v), fp.evaluate_t(v)
+    tc.status()
+    rel = (torch.linalg.norm(a - b) / torch.linalg.norm(b)).item()
+    assert rel < 1e-4, rel
