@@ -32,7 +32,7 @@ constexpr int B_TILE = TN * TK * 2;  // 32 KB
 constexpr int STAGE_BYTES = A_TILE + B_TILE;
 constexpr int kThreads = 192;        // warp 0: TMA, warp 1: MMA, warps 2-5: epilogue
 constexpr uint32_t kTmemCols = 256;
-constexpr long long kSpinLimit = 1LL << 26;
+constexpr long long kSpinLimit = 1LL << 22;
 
 struct TcParams {
   int Mpad, Npad, KB;   // padded batch rows per (class, part), padded columns, K blocks of 64

@@ -1,0 +1,32 @@
+"""The reference's hot-path imports resolve to matcha_b200 after shim.install()."""
+import sys
+import types
+
+from matcha_b200 import shim
+
+
+def test_install_routes_reference_modules(monkeypatch):
+    # parents as the installed reference would provide them
+    for name in ("matcha", "matcha.core"):
+        if name not in sys.modules:
+            mod = types.ModuleType(name)
+            mod.__path__ = []
+            monkeypatch.setitem(sys.modules, name, mod)
+    for name in shim.ALIASES:
+        monkeypatch.delitem(sys.modules, name, raising=False)
+    done = shim.install()
+    try:
+        from matcha.core.CrossCorrelationMatcher import CrossCorrelationMatcher
+        from matcha.core.Matcha import Matcha
+        from matcha.core.ShiftMatcher import ShiftMatcher
+
+        import matcha_b200.core.CrossCorrelationMatcher as C
+        import matcha_b200.core.Matcha as M
+        import matcha_b200.core.ShiftMatcher as S
+
+        assert Matcha is M.Matcha and CrossCorrelationMatcher is C.CrossCorrelationMatcher
+        assert ShiftMatcher is S.ShiftMatcher
+        assert set(done) == set(shim.ALIASES)
+    finally:
+        shim.uninstall()
+    assert "matcha.core.Matcha" not in sys.modules
