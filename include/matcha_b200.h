@@ -90,6 +90,26 @@ int mtb_search_orientations(mtb_search* h, const float* sigma, int64_t sigma_str
                             float* alpha, float* beta, float* gamma, float* score,
                             mtb_stream_t stream);
 
+/* Allocation-free orientation search.  No counterpart in the reference: it is
+ * mtb_search_orientations for callers that must not allocate device memory -- a host
+ * program that hands all device memory to its own allocator or runs under a fixed
+ * device-memory budget, or a pipeline that cannot take the device-wide synchronisation a
+ * cudaMalloc/cudaFree implies.  It needs no handle and calls no allocator: its tables and
+ * its candidate workspace live in one file-scope device array of
+ * MTB_SEARCH_STATIC_SCRATCH_BYTES, which every GPU that loads this library holds until
+ * the process exits.  The first call on a device looks up that array's device address
+ * (once per device, with the device current); make that first call before any stream
+ * capture.  All calls share the array: calls that can overlap on the GPU (different
+ * streams, or threads without ordering between them) race with each other and must be
+ * serialised by the caller.  The tables are rebuilt and every workspace entry is written
+ * by each call before it is read.  Returns MTB_ERR_ARG when B x candidates (with the grid
+ * tables) does not fit the array (about 250 000 candidate slots).  cfg is a host pointer
+ * (its max_batch is ignored); the other arguments are those of mtb_search_orientations. */
+#define MTB_SEARCH_STATIC_SCRATCH_BYTES (4 * 1024 * 1024)
+int mtb_search_orientations_static(const mtb_search_config* cfg, const float* sigma, int64_t sigma_stride,
+                                   int B, float* alpha, float* beta, float* gamma, float* score,
+                                   mtb_stream_t stream);
+
 /* ------------------------------------------------------------------------------
  * Ball expansion (FLE) and per-degree correlation coefficients sigma.
  * Replaces FLEBasis3D.evaluate_t (src/matcha/core/FLEBasis3D.py:945-976; its

@@ -371,3 +371,141 @@ extern "C" int mtb_search_orientations(mtb_search* h, const float* sigma, int64_
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }
+
+// ------------------------------------------------------------------ allocation-free search
+// mtb_search_orientations_static: the same grid search, Newton march and reduction as
+// mtb_search_orientations, for callers that cannot allocate device memory.  Its tables
+// (grid d-table, recurrence start coefficients) and the candidate workspace live in the
+// file-scope array g_search_scratch; the tables are rebuilt on the device by every call,
+// and every workspace entry is written before it is read, so nothing needs clearing.
+#include <mutex>
+
+namespace {
+
+constexpr size_t kStaticScratchBytes = (size_t)MTB_SEARCH_STATIC_SCRATCH_BYTES;
+__device__ __align__(256) unsigned char g_search_scratch[MTB_SEARCH_STATIC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+void* g_static_ptr[kMaxDevices] = {nullptr};
+
+size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+// Grid d-table d^l_{m'm}(beta_j), beta_j = j pi / (n - 1), l < L0, and the start
+// coefficients sqrt((2m')!/((m'+m)!(m'-m)!)) of the Newton recurrence, FP64 on the device.
+__global__ void static_tables_kernel(int L0, int n, int Lmax, float* __restrict__ dtab, double* __restrict__ Ctab) {
+  const int Lm = L0 - 1;
+  const int P = 2 * Lm + 1;
+  const int nk = mtb_dsize(Lm);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int npairs = n * P * P;
+  if (t < npairs) {
+    const int j = t / (P * P), q = t % (P * P);
+    const int mp = q / P - Lm, m = q % P - Lm;
+    const double beta = (n > 1) ? (j == n - 1 ? M_PI : j * (M_PI / (n - 1))) : 0.0;
+    const double cb = cos(beta), c = cos(0.5 * beta), s = sin(0.5 * beta);
+    const int l0 = abs(mp) > abs(m) ? abs(mp) : abs(m);
+    const int k = (m - mp) > 0 ? (m - mp) : 0;
+    const int l = l0;
+    const double lognum = 0.5 * (lgamma(l + mp + 1.0) + lgamma(l - mp + 1.0) + lgamma(l + m + 1.0) + lgamma(l - m + 1.0));
+    const double logden = lgamma(l + m - k + 1.0) + lgamma(k + 1.0) + lgamma(mp - m + k + 1.0) + lgamma(l - mp - k + 1.0);
+    const int pc = 2 * l + m - mp - 2 * k, ps = mp - m + 2 * k;
+    double v = exp(lognum - logden) * (((mp - m + k) & 1) ? -1.0 : 1.0);
+    v *= (pc ? pow(c, (double)pc) : 1.0) * (ps ? pow(s, (double)ps) : 1.0);
+    double dl = v, dlm1 = 0.0;
+    float* row = dtab + (int64_t)j * nk;
+    row[mtb_dsize(l0 - 1) + (mp + l0) * (2 * l0 + 1) + (m + l0)] = (float)dl;
+    for (int ll = l0; ll < Lm; ++ll) {
+      double dn;
+      if (ll == 0) {
+        dn = cb * dl;
+      } else {
+        const double a = (2.0 * ll + 1.0) * (ll * (ll + 1.0) * cb - (double)m * mp);
+        const double bb = (ll + 1.0) * sqrt((double)(ll * ll - m * m) * (double)(ll * ll - mp * mp));
+        const double cc = ll * sqrt((double)((ll + 1) * (ll + 1) - m * m) * (double)((ll + 1) * (ll + 1) - mp * mp));
+        dn = (a * dl - bb * dlm1) / cc;
+      }
+      dlm1 = dl;
+      dl = dn;
+      const int L1 = ll + 1;
+      row[mtb_dsize(L1 - 1) + (mp + L1) * (2 * L1 + 1) + (m + L1)] = (float)dl;
+    }
+  }
+  const int u = t - npairs;
+  if (u >= 0 && u < (Lmax + 1) * (Lmax + 1)) {
+    int mp = (int)sqrt((double)u);
+    while (mp * mp > u) --mp;
+    while ((mp + 1) * (mp + 1) <= u) ++mp;
+    const int m = u - mp * mp - mp;
+    Ctab[u] = exp(0.5 * (lgamma(2.0 * mp + 1.0) - lgamma((double)(mp + m) + 1.0) - lgamma((double)(mp - m) + 1.0)));
+  }
+}
+
+}  // namespace
+
+extern "C" int mtb_search_orientations_static(const mtb_search_config* cfg, const float* sigma, int64_t sigma_stride,
+                                              int B, float* alpha, float* beta, float* gamma, float* score,
+                                              mtb_stream_t stream) {
+  MTB_ARG_CHECK(cfg, "null config");
+  MTB_ARG_CHECK(cfg->Lmax >= 1 && cfg->Lmax <= 64, "Lmax must be in [1, 64]");
+  MTB_ARG_CHECK(cfg->n_stages >= 1 && cfg->n_stages <= MTB_MAX_STAGES, "n_stages out of range");
+  MTB_ARG_CHECK(cfg->L0 >= 1 && cfg->L0 <= cfg->Lmax, "L0 must be in [1, Lmax]");
+  MTB_ARG_CHECK(cfg->K >= 1 && 2 * cfg->L0 * cfg->K <= 128, "grid size 2*L0*K must be <= 128");
+  MTB_ARG_CHECK(cfg->candidates >= 1 && cfg->candidates <= kMaxCand, "candidates must be in [1, 32]");
+  MTB_ARG_CHECK(cfg->num_steps >= 0, "bad num_steps");
+  for (int i = 0; i < cfg->n_stages; ++i)
+    MTB_ARG_CHECK(cfg->stages[i] >= 0 && cfg->stages[i] <= cfg->Lmax, "stage degree out of range");
+  MTB_ARG_CHECK(B >= 0, "negative batch");
+  if (B == 0) return MTB_OK;
+  MTB_ARG_CHECK(sigma && alpha && beta && gamma && score, "null pointer");
+  MTB_ARG_CHECK(sigma_stride >= mtb_dsize(cfg->Lmax), "sigma row shorter than dsize(Lmax)");
+  const int n = 2 * cfg->L0 * cfg->K, L0 = cfg->L0, P = 2 * L0 - 1, nk = mtb_dsize(L0 - 1);
+  MTB_ARG_CHECK(cfg->candidates <= n * n * n, "more candidates than grid points");
+  const size_t gsm = (size_t)(nk + P * P + P * n + n) * sizeof(float2);
+  MTB_ARG_CHECK(gsm <= 200 * 1024, "grid search too large for shared memory (reduce L0 or K)");
+  const int C = cfg->candidates;
+  const size_t dtab_b = align256((size_t)n * nk * sizeof(float));
+  const size_t ctab_b = align256((size_t)(cfg->Lmax + 1) * (cfg->Lmax + 1) * sizeof(double));
+  const size_t cand_b = align256((size_t)4 * B * C * sizeof(float));
+  MTB_ARG_CHECK(dtab_b + ctab_b + cand_b <= kStaticScratchBytes,
+                "batch x candidates (or grid size) exceeds the static scratch of "
+                "MTB_SEARCH_STATIC_SCRATCH_BYTES; use mtb_search_orientations");
+  int dev = 0;
+  MTB_CUDA_TRY(cudaGetDevice(&dev));
+  MTB_ARG_CHECK(dev >= 0 && dev < kMaxDevices, "device ordinal out of range");
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_ptr[dev]) {
+      void* p = nullptr;
+      MTB_CUDA_TRY(cudaGetSymbolAddress(&p, g_search_scratch));
+      g_static_ptr[dev] = p;
+    }
+    base = static_cast<unsigned char*>(g_static_ptr[dev]);
+  }
+  float* dtab = reinterpret_cast<float*>(base);
+  double* Ctab = reinterpret_cast<double*>(base + dtab_b);
+  float* ca = reinterpret_cast<float*>(base + dtab_b + ctab_b);
+  float* cb = ca + (size_t)B * C;
+  float* cg = cb + (size_t)B * C;
+  float* cs = cg + (size_t)B * C;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int work = n * P * P + (cfg->Lmax + 1) * (cfg->Lmax + 1);
+  static_tables_kernel<<<(work + 127) / 128, 128, 0, st>>>(L0, n, cfg->Lmax, dtab, Ctab);
+  MTB_LAUNCH_CHECK();
+  MTB_CUDA_TRY(cudaFuncSetAttribute(so3_grid_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
+  so3_grid_topk_kernel<<<B, kGridThreads, gsm, st>>>(reinterpret_cast<const float2*>(sigma), sigma_stride, B, dtab, L0,
+                                                     n, C, ca, cb, cg, nullptr);
+  MTB_LAUNCH_CHECK();
+  NewtonParams NP;
+  NP.Lmax = cfg->Lmax;
+  NP.n_stages = cfg->n_stages;
+  for (int i = 0; i < MTB_MAX_STAGES; ++i) NP.stages[i] = i < cfg->n_stages ? cfg->stages[i] : 0;
+  NP.num_steps = cfg->num_steps;
+  NP.flags = cfg->flags;
+  const int rc = newton_launch(sigma, sigma_stride, B, C, ca, cb, cg, cs, Ctab, NP, st);
+  if (rc) return rc;
+  reduce_candidates_kernel<<<(B + 127) / 128, 128, 0, st>>>(ca, cb, cg, cs, B, C, alpha, beta, gamma, score);
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
+}
