@@ -192,7 +192,12 @@ typedef struct {
   int search_radius;     /* shift_search_radius; window 2r+1 (ShiftMatcher.py:661-662) */
   float mask_radius;     /* box_size / (2 voxel_size), setup_utils.py:292-295; <0: N/2 */
   float cosine_width;    /* 5.0 in the reference (setup_utils.py:295)               */
+  int precision;         /* MTB_SHIFT_FP32: upsampled DFT on CUDA cores; MTB_SHIFT_BF16X3:
+                            tcgen05 BF16 GEMMs with a hi+lo split (needs N % 32 == 0)  */
 } mtb_shift_config;
+
+#define MTB_SHIFT_FP32 0
+#define MTB_SHIFT_BF16X3 1
 
 typedef struct mtb_shift mtb_shift;
 
@@ -209,6 +214,10 @@ int mtb_shift_set_reference(mtb_shift* h, const float* ref_fourier, mtb_stream_t
  * float32 or NULL.  shift_xyz (B, 3) and score (B,) float32 out. */
 int mtb_shift_search(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot,
                      const float* ctf, int B, float* shift_xyz, float* score, mtb_stream_t stream);
+
+/* Synchronises stream; MTB_ERR_TIMEOUT if a bounded device-side wait of the tensor-core
+ * path gave up since the handle was created (then its results are invalid). */
+int mtb_shift_status(mtb_shift* h, mtb_stream_t stream);
 
 /* Rotation bookkeeping on the device: tracker <- normalized(tracker * conj(swap_xz(q(a, b, g))))
  * as update_rotation_estimate (src/matcha/utils/rotation_ops.py:23-34), and rot (B, 9), the

@@ -23,6 +23,8 @@ MTB_ERR_CUDA = 5
 MTB_MAX_STAGES = 16
 MTB_FLE_FP32 = 0
 MTB_FLE_BF16X3 = 1
+MTB_SHIFT_FP32 = 0
+MTB_SHIFT_BF16X3 = 1
 MTB_SEARCH_COMPAT_TOP_BLOCK = 1
 MTB_SEARCH_GRADIENT_STEP = 2
 
@@ -60,6 +62,7 @@ class MtbShiftConfig(ctypes.Structure):
     _fields_ = [
         ("N", ctypes.c_int), ("max_batch", ctypes.c_int), ("upsample_factor", ctypes.c_int),
         ("search_radius", ctypes.c_int), ("mask_radius", ctypes.c_float), ("cosine_width", ctypes.c_float),
+        ("precision", ctypes.c_int),
     ]
 
 
@@ -85,6 +88,7 @@ SIGNATURES = {
     "mtb_shift_create": (_I, [ctypes.POINTER(MtbShiftConfig), ctypes.POINTER(_P)]),
     "mtb_shift_destroy": (None, [_P]),
     "mtb_shift_set_reference": (_I, [_P, _P, _P]),
+    "mtb_shift_status": (_I, [_P, _P]),
     "mtb_shift_search": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P]),
     "mtb_update_rotation": (_I, [_P, _P, _P, _P, _I, _P, _P, _P]),
 }

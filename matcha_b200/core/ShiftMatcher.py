@@ -101,7 +101,11 @@ def _cfg(config, key, default=None):
 class ShiftMatcher:
     """Stateful shift-search wrapper (ShiftMatcher.py:766-928)."""
 
-    def __init__(self, config, device: torch.device, dtype: torch.dtype, micro_batch_size: int = None):
+    def __init__(self, config, device: torch.device, dtype: torch.dtype, micro_batch_size: int = None,
+                 precision: str = "fp32"):
+        if precision not in ("fp32", "bf16x3"):
+            raise ValueError("precision must be 'fp32' (CUDA cores) or 'bf16x3' (tensor cores, hi+lo split)")
+        self.precision = precision
         self.config = config
         self.device = torch.device(device)
         self.dtype = dtype
@@ -132,12 +136,19 @@ class ShiftMatcher:
         cfg.search_radius = self.radius
         cfg.mask_radius = self.mask_radius
         cfg.cosine_width = 5.0
+        cfg.precision = nat.MTB_SHIFT_BF16X3 if self.precision == "bf16x3" else nat.MTB_SHIFT_FP32
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             nat.check(self._lib.mtb_shift_create(ctypes.byref(cfg), ctypes.byref(h)), "mtb_shift_create")
         self._h, self._cap = h, cfg.max_batch
         self._uploaded_version = -1
         return h
+
+    def status(self):
+        """Raise if a bounded device-side wait of the tensor-core path gave up (synchronises)."""
+        if self._h is not None:
+            with torch.cuda.device(self.device):
+                nat.check(self._lib.mtb_shift_status(self._h, nat.stream_ptr(self.device)), "mtb_shift_status")
 
     def _free(self):
         if self._h is not None and self._h.value:

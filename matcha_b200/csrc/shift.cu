@@ -22,7 +22,9 @@
 #include <math.h>
 #include <string.h>
 #include <vector>
+#include <cuda_bf16.h>
 #include "common.cuh"
+#include "shift_tc.cuh"
 
 namespace {
 
@@ -246,9 +248,13 @@ fft_y_kernel(ShiftGeom g, float2* __restrict__ T) {
 
 // ------------------------------------------------------------------ FFT along z + product
 // One CTA per (b, j').  P = conj(S) * T in place; norms |T|^2, |S|^2 per subtomogram.
+// SPLIT: instead of P in place, write the pass-1 operand of the tensor-core upsampled DFT,
+// A1[part][(b, m2, m1)][2 m0 + c] as bf16 hi/lo pairs (a1_ws pairs per row, a1_R rows per part).
+template <bool SPLIT>
 __global__ void __launch_bounds__(kT)
 fft_z_product_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ ref,
-                     const float* __restrict__ rot, const float* __restrict__ ctf, float* __restrict__ nrm) {
+                     const float* __restrict__ rot, const float* __restrict__ ctf, float* __restrict__ nrm,
+                     uint32_t* __restrict__ a1, int a1_ws, int a1_R) {
   extern __shared__ __align__(16) float2 sm2[];
   __shared__ float red[32];
   const int N = g.N, H = g.H;
@@ -269,8 +275,9 @@ fft_z_product_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restri
   const float c = (float)g.h;  // centre of the odd-padded grid, (N+1-1)/2
   float st = 0.f, ss = 0.f;
   for (int e = threadIdx.x; e < N * H; e += blockDim.x) {
-    const int ip = e / H, m2 = e % H;
-    const float2 t = buf[e];
+    // SPLIT walks m0 fastest so the bf16 rows are written contiguously
+    const int ip = SPLIT ? e % N : e / H, m2 = SPLIT ? e / N : e % H;
+    const float2 t = buf[ip * H + m2];
     // mask_full on the (N, N, N/2+1) index grid (setup_utils.py:239-249)
     const int kp = ip < N / 2 ? ip : ip - N;
     const int jq = jp < N / 2 ? jp : jp - N;
@@ -294,7 +301,16 @@ fft_z_product_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restri
     ss += s.x * s.x + s.y * s.y;
     // conj(s) * t
     const float2 p = make_float2(s.x * t.x + s.y * t.y, s.x * t.y - s.y * t.x);
-    base[(int64_t)ip * N * H + m2] = p;
+    if (SPLIT) {
+      const __nv_bfloat16 rh = __float2bfloat16_rn(p.x), ih = __float2bfloat16_rn(p.y);
+      const __nv_bfloat162 hi = __halves2bfloat162(rh, ih);
+      const __nv_bfloat162 lo = __floats2bfloat162_rn(p.x - __bfloat162float(rh), p.y - __bfloat162float(ih));
+      const size_t row = ((size_t)b * H + m2) * N + jp;
+      a1[row * a1_ws + ip] = *reinterpret_cast<const uint32_t*>(&hi);
+      a1[((size_t)a1_R + row) * a1_ws + ip] = *reinterpret_cast<const uint32_t*>(&lo);
+    } else {
+      base[(int64_t)ip * N * H + m2] = p;
+    }
   }
   st = block_sum(st, red);
   ss = block_sum(ss, red);
@@ -434,6 +450,25 @@ __global__ void finalize_kernel(ShiftGeom g, int B, int ngrp, const float* __res
   score[b] = bv / den;
 }
 
+// Tensor-core path: decode the per-subtomogram argmax key of the third pass.
+__global__ void finalize_tc_kernel(ShiftGeom g, int B, const unsigned long long* __restrict__ best,
+                                   const float* __restrict__ nrm, float* __restrict__ shift_xyz,
+                                   float* __restrict__ score) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const unsigned long long key = best[b];
+  uint32_t vb = (uint32_t)(key >> 32);
+  vb = (vb & 0x80000000u) ? (vb & 0x7FFFFFFFu) : ~vb;
+  const float bv = __uint_as_float(vb);
+  const int bi = (int)(0xFFFFFFFFu - (uint32_t)(key & 0xFFFFFFFFull));
+  const int U = g.U;
+  const int u2 = bi % U, u1 = (bi / U) % U, u0 = bi / (U * U);
+  shift_xyz[b * 3 + 0] = ((float)u2 - g.dftshift) / g.uf;
+  shift_xyz[b * 3 + 1] = ((float)u1 - g.dftshift) / g.uf;
+  shift_xyz[b * 3 + 2] = ((float)u0 - g.dftshift) / g.uf;
+  score[b] = bv / (sqrtf(nrm[2 * b]) * sqrtf(nrm[2 * b + 1]));
+}
+
 }  // namespace
 
 struct mtb_shift {
@@ -454,6 +489,8 @@ struct mtb_shift {
   int* pidx;
   int ngrp, rows_per_cta;
   bool has_ref;
+  ShiftTc tc;
+  bool use_tc;
 };
 
 extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
@@ -542,15 +579,34 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
       cudaMemcpy(h->E1, e0.data(), e0.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->E2, e2.data(), e2.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(MTB_ERR_CUDA);
+  if (cfg->precision == MTB_SHIFT_BF16X3) {
+    const int rc = shift_tc_prepare(&h->tc, N, g.H, g.U, cfg->upsample_factor, g.dftshift, cfg->max_batch);
+    if (rc) return fail(rc);
+    h->use_tc = true;
+  } else if (cfg->precision != MTB_SHIFT_FP32) {
+    return fail(MTB_ERR_ARG);
+  }
   *out = h;
   return MTB_OK;
 }
 
 extern "C" void mtb_shift_destroy(mtb_shift* h) {
   if (!h) return;
+  shift_tc_release(&h->tc);
   void* ptrs[] = {h->bg_idx, h->bg_w, h->ref, h->E0, h->E1, h->E2, h->bg, h->nrm, h->T, h->X1, h->pval, h->pidx};
   for (void* p : ptrs) if (p) cudaFree(p);
   delete h;
+}
+
+extern "C" int mtb_shift_status(mtb_shift* h, mtb_stream_t stream) {
+  MTB_ARG_CHECK(h, "null handle");
+  if (!h->use_tc) {
+    MTB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    return MTB_OK;
+  }
+  const int rc = shift_tc_check(&h->tc, (cudaStream_t)stream);
+  if (rc) mtb_set_last_error("tensor-core shift DFT: a bounded wait ran out", __FILE__, __LINE__);
+  return rc;
 }
 
 extern "C" int mtb_shift_set_reference(mtb_shift* h, const float* ref_fourier, mtb_stream_t stream) {
@@ -584,8 +640,19 @@ extern "C" int mtb_shift_search(mtb_shift* h, const float* subtomos, const float
   MTB_CUDA_TRY(cudaFuncSetAttribute(fft_y_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
   fft_y_kernel<<<dim3(N, B), kT, smy, st>>>(g, h->T);
   MTB_LAUNCH_CHECK();
-  MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_product_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
-  fft_z_product_kernel<<<dim3(N, B), kT, smy, st>>>(g, h->T, h->ref, rot, ctf, h->nrm);
+  if (h->use_tc) {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_product_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
+    fft_z_product_kernel<true><<<dim3(N, B), kT, smy, st>>>(g, h->T, h->ref, rot, ctf, h->nrm, (uint32_t*)h->tc.A1,
+                                                          h->tc.KB12 * 32, h->tc.R1);
+    MTB_LAUNCH_CHECK();
+    const int rc = shift_tc_passes(&h->tc, B, st);
+    if (rc) return rc;
+    finalize_tc_kernel<<<(B + 127) / 128, 128, 0, st>>>(g, B, h->tc.best, h->nrm, shift_xyz, score);
+    MTB_LAUNCH_CHECK();
+    return MTB_OK;
+  }
+  MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_product_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
+  fft_z_product_kernel<false><<<dim3(N, B), kT, smy, st>>>(g, h->T, h->ref, rot, ctf, h->nrm, nullptr, 0, 0);
   MTB_LAUNCH_CHECK();
   const size_t sm1 = (size_t)(U * N + N * kColTile) * 8;
   MTB_CUDA_TRY(cudaFuncSetAttribute(updft1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));

@@ -35,7 +35,8 @@ class StepConfig:
     shift_search_radius: int = 5
     box_size: float | None = None
     voxel_size: float = 1.0
-    precision: str = "bf16x3"        # ball-expansion GEMM: "bf16x3" (tcgen05) or "fp32" (CUDA cores)
+    precision: str = "bf16x3"        # dense contractions (ball expansion, upsampled DFT): "bf16x3" on
+                                     # tcgen05 with a hi+lo split, or "fp32" on CUDA cores
 
 
 class _Cfg(dict):
@@ -63,7 +64,7 @@ class AlignmentStep:
                                          shift_upsample_factor=cfg.shift_upsample_factor,
                                          shift_search_radius=cfg.shift_search_radius, do_ctf_correction=False,
                                          box_size=cfg.box_size if cfg.box_size is not None else cfg.N),
-                                    self.device, torch.complex64)
+                                    self.device, torch.complex64, precision=cfg.precision)
         B = cfg.batch
         self.rot = torch.empty((B, 9), device=self.device, dtype=torch.float32)
         self.shift = torch.empty((B, 3), device=self.device, dtype=torch.float32)
