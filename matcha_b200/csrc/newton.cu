@@ -34,6 +34,7 @@ struct Smem {
   float2* eg;      // e^{i m g},  index m + Li
   float* red;      // (threads/32) x A_N
   float* res;      // A_N
+  int4* level;     // per degree l: {magic = ceil(65536 / w), G = 256 / w, chunk = ceil(w / G), w}
 };
 
 __device__ __forceinline__ double ipow(double x, int n) {
@@ -130,7 +131,10 @@ __device__ void pass(const float2* __restrict__ sig, const double* __restrict__ 
       }
     }
     // rows w, w+1 below the block read as zero
-    for (int e = tid; e < 2 * w; e += kNT) dcur[(w + e / w) * W + (e % w)] = 0.f;
+    for (int e = tid; e < 2 * w; e += kNT) {
+      const int hi = e >= w;
+      dcur[(w + hi) * W + (e - hi * w)] = 0.f;
+    }
     // per-row data of this level
     {
       float4* ra = sm.rowa[l & 1];
@@ -153,10 +157,13 @@ __device__ void pass(const float2* __restrict__ sig, const double* __restrict__ 
     }
     __syncthreads();
     // ---- contraction: thread (column c, row chunk g)
-    const int G = kNT / w;  // w <= 129 < kNT
-    const int c = tid % w, g = tid / w;
-    if (g < G) {
-      const int r0 = (g * w) / G, r1 = ((g + 1) * w) / G;
+    // g = tid / w and c = tid % w by a multiply with ceil(2^16 / w) (exact for tid < 256,
+    // w <= 129); groups of `chunk` rows, G = 256 / w groups per column
+    const int4 lv = sm.level[l];  // {magic, G, chunk, w}
+    const int g = (tid * lv.x) >> 16;
+    const int c = tid - g * w;
+    const int r0 = g * lv.z, r1 = min(w, r0 + lv.z);
+    if (g < lv.y && r0 < r1) {
       const float4* ra = sm.rowa[l & 1];
       const float4* rb = sm.rowb[l & 1];
       const float2 egc = sm.eg[c - l + Li];
@@ -165,6 +172,7 @@ __device__ void pass(const float2* __restrict__ sig, const double* __restrict__ 
       if (DERIVS) {
         float dm2 = dp[-2 * W], dm1 = dp[-W], dc = dp[0], dp1 = dp[W];
         float T = 0.f, U = 0.f, X = 0.f, MT = 0.f;
+#pragma unroll 2
         for (int r = r0; r < r1; ++r) {
           const float dp2 = dp[2 * W];
           const float2 s = __ldg(sp);
@@ -198,6 +206,7 @@ __device__ void pass(const float2* __restrict__ sig, const double* __restrict__ 
         acc[A_HBG] -= m * X;
       } else {
         float T = 0.f;
+#pragma unroll 4
         for (int r = r0; r < r1; ++r) {
           const float2 s = __ldg(sp);
           const float4 A = ra[r];
@@ -269,12 +278,17 @@ newton_march_kernel(const float2* __restrict__ sigma, int64_t stride, int BC, in
   sm.rowa[1] = f4 + W;
   sm.rowb[0] = f4 + 2 * W;
   sm.rowb[1] = f4 + 3 * W;
-  sm.ea = reinterpret_cast<float2*>(f4 + 4 * W);
+  sm.level = reinterpret_cast<int4*>(f4 + 4 * W);
+  sm.ea = reinterpret_cast<float2*>(sm.level + (P.Lmax + 1));
   sm.eg = sm.ea + W;
   sm.red = reinterpret_cast<float*>(sm.eg + W);
   sm.res = sm.red + (kNT / 32) * A_N;
   sm.dbuf[0] = sm.res + A_N + 2;
   sm.dbuf[1] = sm.dbuf[0] + (W + 4) * W;
+  for (int l = threadIdx.x; l <= P.Lmax; l += kNT) {
+    const int w = 2 * l + 1, G = kNT / w;
+    sm.level[l] = make_int4((65536 + w - 1) / w, G, (w + G - 1) / G, w);
+  }
 
   const int cand = blockIdx.x;
   if (cand >= BC) return;
@@ -358,7 +372,7 @@ int launch(const float2* sigma, int64_t stride, int BC, int C, float* a, float* 
 
 size_t newton_smem_bytes(int Lmax) {
   const int W = 2 * Lmax + 1;
-  return (size_t)4 * W * sizeof(float4) + (size_t)2 * W * sizeof(float2) +
+  return (size_t)4 * W * sizeof(float4) + (size_t)(Lmax + 1) * sizeof(int4) + (size_t)2 * W * sizeof(float2) +
          (size_t)((kNT / 32) * A_N + A_N + 2) * sizeof(float) + (size_t)2 * (W + 4) * W * sizeof(float);
 }
 

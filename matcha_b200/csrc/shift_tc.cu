@@ -175,6 +175,7 @@ updft_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
 #pragma unroll
             for (int t = 0; t < 8; ++t) {
               const int u0 = cb / 2 + t;
+              if (u0 >= P.U) break;
               uint32_t hi, lo;
               split2(v[2 * t], v[2 * t + 1], hi, lo);
               const size_t row = base_row + (size_t)u0 * P.H;
@@ -196,6 +197,7 @@ updft_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
 #pragma unroll
             for (int t = 0; t < 8; ++t) {
               const int u1 = cb / 2 + t;
+              if (u1 >= P.U) break;
               uint32_t hi, lo;
               split2(v[2 * t], v[2 * t + 1], hi, lo);
               const size_t row = base_row + u1;
@@ -308,11 +310,12 @@ int launch_pass(const ShiftTc* t, const void* mapA, const void* mapB, const UPar
 
 int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, int max_batch) {
   memset(t, 0, sizeof(*t));
-  // N-tile of passes 1, 2 is 2U (<= 256, multiple of 16); of pass 3 round_up(U, 16)
-  if (2 * U > 256 || (2 * U) % 16 || N % 32) return MTB_ERR_ARG;
+  // N-tile of passes 1, 2 is round_up(2U, 16) <= 256; of pass 3 round_up(U, 16)
+  if (U < 1 || 2 * U > 256 || N < 2) return MTB_ERR_ARG;
   t->N = N;
   t->H = H;
   t->U = U;
+  t->NT12 = (2 * U + 15) / 16 * 16;
   t->NT3 = (U + 15) / 16 * 16;
   t->KB12 = (2 * N + TK - 1) / TK;
   t->KB3 = (2 * H + TK - 1) / TK;
@@ -326,7 +329,7 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
   if (cudaMalloc(&t->A1, a1) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->A2, a2) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->A3, a3) != cudaSuccess) return MTB_ERR_OOM;
-  if (cudaMalloc(&t->E1, (size_t)2 * 2 * U * k12 * 2) != cudaSuccess) return MTB_ERR_OOM;
+  if (cudaMalloc(&t->E1, (size_t)2 * t->NT12 * k12 * 2) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->E3, (size_t)2 * t->NT3 * k3 * 2) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->best, (size_t)max_batch * 8) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->err, 4) != cudaSuccess) return MTB_ERR_OOM;
@@ -342,7 +345,7 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
     *re = cos(ph);
     *im = sin(ph);
   };
-  std::vector<uint16_t> e1((size_t)2 * 2 * U * k12, 0), e3((size_t)2 * t->NT3 * k3, 0);
+  std::vector<uint16_t> e1((size_t)2 * t->NT12 * k12, 0), e3((size_t)2 * t->NT3 * k3, 0);
   auto put = [&](std::vector<uint16_t>& dst, size_t k, int rows, int r, int kk, double v) {
     const uint16_t hi = f2bf((float)v);
     const uint16_t lo = f2bf((float)(v - (double)bf2f(hi)));
@@ -353,10 +356,10 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
     for (int m = 0; m < N; ++m) {
       double er, ei;
       E(N, u, m, &er, &ei);
-      put(e1, k12, 2 * U, 2 * u + 0, 2 * m + 0, er);
-      put(e1, k12, 2 * U, 2 * u + 0, 2 * m + 1, -ei);
-      put(e1, k12, 2 * U, 2 * u + 1, 2 * m + 0, ei);
-      put(e1, k12, 2 * U, 2 * u + 1, 2 * m + 1, er);
+      put(e1, k12, t->NT12, 2 * u + 0, 2 * m + 0, er);
+      put(e1, k12, t->NT12, 2 * u + 0, 2 * m + 1, -ei);
+      put(e1, k12, t->NT12, 2 * u + 1, 2 * m + 0, ei);
+      put(e1, k12, t->NT12, 2 * u + 1, 2 * m + 1, er);
     }
   for (int u = 0; u < U; ++u)
     for (int m = 0; m < H; ++m) {
@@ -371,7 +374,7 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
   int rc = make_map(t->mapA1, t->A1, k12, (uint64_t)2 * t->R1, TM);
   if (!rc) rc = make_map(t->mapA2, t->A2, k12, (uint64_t)2 * t->R2, TM);
   if (!rc) rc = make_map(t->mapA3, t->A3, k3, (uint64_t)2 * t->R3, TM);
-  if (!rc) rc = make_map(t->mapE1, t->E1, k12, (uint64_t)2 * 2 * U, 2 * U);
+  if (!rc) rc = make_map(t->mapE1, t->E1, k12, (uint64_t)2 * t->NT12, t->NT12);
   if (!rc) rc = make_map(t->mapE3, t->E3, k3, (uint64_t)2 * t->NT3, t->NT3);
   return rc;
 }
@@ -386,13 +389,20 @@ template <int MODE>
 int dispatch(const ShiftTc* t, int nt, const void* mapA, const void* mapB, const UParams& P, uint32_t* out,
              cudaStream_t st) {
   switch (nt) {
+    case 16: return launch_pass<16, MODE>(t, mapA, mapB, P, out, st);
+    case 32: return launch_pass<32, MODE>(t, mapA, mapB, P, out, st);
+    case 48: return launch_pass<48, MODE>(t, mapA, mapB, P, out, st);
     case 64: return launch_pass<64, MODE>(t, mapA, mapB, P, out, st);
+    case 80: return launch_pass<80, MODE>(t, mapA, mapB, P, out, st);
     case 96: return launch_pass<96, MODE>(t, mapA, mapB, P, out, st);
     case 112: return launch_pass<112, MODE>(t, mapA, mapB, P, out, st);
     case 128: return launch_pass<128, MODE>(t, mapA, mapB, P, out, st);
     case 144: return launch_pass<144, MODE>(t, mapA, mapB, P, out, st);
+    case 160: return launch_pass<160, MODE>(t, mapA, mapB, P, out, st);
     case 176: return launch_pass<176, MODE>(t, mapA, mapB, P, out, st);
+    case 192: return launch_pass<192, MODE>(t, mapA, mapB, P, out, st);
     case 208: return launch_pass<208, MODE>(t, mapA, mapB, P, out, st);
+    case 224: return launch_pass<224, MODE>(t, mapA, mapB, P, out, st);
     case 240: return launch_pass<240, MODE>(t, mapA, mapB, P, out, st);
     case 256: return launch_pass<256, MODE>(t, mapA, mapB, P, out, st);
     default: return MTB_ERR_ARG;
@@ -414,7 +424,7 @@ int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st) {
   P.rows = B * P.rpb;
   P.R_out = t->R2;
   P.rpb_out = U * H;
-  int rc = dispatch<1>(t, 2 * U, t->mapA1, t->mapE1, P, (uint32_t*)t->A2, st);
+  int rc = dispatch<1>(t, t->NT12, t->mapA1, t->mapE1, P, (uint32_t*)t->A2, st);
   if (rc) return rc;
   // pass 2: rows (b, u0, m2) -> A3 rows (b, u0, u1)
   P.KB = t->KB12;
@@ -424,7 +434,7 @@ int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st) {
   P.rows = B * P.rpb;
   P.R_out = t->R3;
   P.rpb_out = U * U;
-  rc = dispatch<2>(t, 2 * U, t->mapA2, t->mapE1, P, (uint32_t*)t->A3, st);
+  rc = dispatch<2>(t, t->NT12, t->mapA2, t->mapE1, P, (uint32_t*)t->A3, st);
   if (rc) return rc;
   // pass 3: rows (b, u0, u1) -> argmax keys
   P.KB = t->KB3;

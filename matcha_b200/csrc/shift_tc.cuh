@@ -9,7 +9,7 @@ struct ShiftTc {
   alignas(64) unsigned char mapA3[128];  // pass-3 A: rows (b, u0, u1), K (m2, re/im)
   alignas(64) unsigned char mapE1[128];  // B of passes 1, 2: rows (u, re/im)
   alignas(64) unsigned char mapE3[128];  // B of pass 3: rows u2
-  int N, H, U, NT3, KB12, KB3, Bmax;
+  int N, H, U, NT12, NT3, KB12, KB3, Bmax;
   int R1, R2, R3;                        // padded rows per hi/lo part
   void *A1, *A2, *A3, *E1, *E3;          // bf16, [part][row][K]
   unsigned long long* best;              // (Bmax) argmax keys: ordered value << 32 | ~flat index
