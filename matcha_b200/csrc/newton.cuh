@@ -5,7 +5,8 @@
 #include <stdint.h>
 #include "../../include/matcha_b200.h"
 
-constexpr int kNewtonThreads = 256;
+constexpr int kNewtonThreads = 128;
+constexpr int kNewtonMaxL = 64;
 
 struct NewtonParams {
   int Lmax;
@@ -15,10 +16,24 @@ struct NewtonParams {
   int flags;
 };
 
-// Dynamic shared memory of one Newton CTA for degrees up to Lmax.
-size_t newton_smem_bytes(int Lmax);
+// Entries of one subtomogram's folded sigma (and of the recurrence-factor table) for
+// degrees up to Lmax: sum_{l <= Lmax} (l + 1)^2, 16 bytes each.
+int64_t newton_fold_entries(int Lmax);
+
+// Fill the candidate-independent recurrence-factor table (newton_fold_entries(Lmax) float4).
+int newton_build_coef(int Lmax, float4* coef, cudaStream_t st);
 
 // Launch the march for B subtomograms x C candidates on stream st.  Ctab holds
-// sqrt((2m')!/((m'+m)!(m'-m)!)) at index m'^2 + m + m' for 0 <= |m| <= m' <= Lmax.
+// sqrt((2m')!/((m'+m)!(m'-m)!)) at index m'^2 + m + m' for 0 <= |m| <= m' <= Lmax; coef is
+// the table of newton_build_coef.  With fold (B x newton_fold_entries(Lmax) float4 of
+// workspace) sigma is folded once per subtomogram first; with fold == nullptr every step
+// reads the four sigma images itself (no workspace, more sigma traffic).
 int newton_launch(const float* sigma, int64_t stride, int B, int C, float* alpha, float* beta, float* gamma,
-                  float* score, const double* Ctab, const NewtonParams& P, cudaStream_t st);
+                  float* score, const double* Ctab, const float4* coef, float4* fold, const NewtonParams& P,
+                  cudaStream_t st);
+
+// The march that reproduces the reference's final-stage top block (flag
+// MTB_SEARCH_COMPAT_TOP_BLOCK): full d blocks in shared memory and the reference's row-shift
+// derivative stencil on the zeroed block.
+int newton_stencil_launch(const float* sigma, int64_t stride, int B, int C, float* alpha, float* beta,
+                          float* gamma, float* score, const double* Ctab, const NewtonParams& P, cudaStream_t st);

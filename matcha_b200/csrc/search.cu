@@ -244,6 +244,8 @@ struct mtb_search {
   int device;
   float* dtab;      // (n, dsize(L0-1))
   double* Ctab;     // (Lmax+1)^2 start-value coefficients of the recurrence
+  float4* coef;     // recurrence factors, newton_fold_entries(Lmax)
+  float4* fold;     // folded sigma, max_batch x newton_fold_entries(Lmax)
   float* cand;      // 4 x (max_batch * C): alpha, beta, gamma, score
 };
 
@@ -298,9 +300,14 @@ extern "C" int mtb_search_create(const mtb_search_config* cfg, mtb_search** out)
   if (cudaMalloc(&h->Ctab, lc.size() * sizeof(double)) != cudaSuccess) return fail(MTB_ERR_OOM);
   if (cudaMalloc(&h->cand, (size_t)4 * cfg->max_batch * cfg->candidates * sizeof(float)) != cudaSuccess)
     return fail(MTB_ERR_OOM);
+  const int64_t nf = newton_fold_entries(Lm);
+  if (cudaMalloc(&h->coef, (size_t)nf * sizeof(float4)) != cudaSuccess) return fail(MTB_ERR_OOM);
+  if (cudaMalloc(&h->fold, (size_t)cfg->max_batch * nf * sizeof(float4)) != cudaSuccess) return fail(MTB_ERR_OOM);
   if (cudaMemcpy(h->dtab, dt.data(), dt.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->Ctab, lc.data(), lc.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(MTB_ERR_CUDA);
+  if (newton_build_coef(Lm, h->coef, 0) != MTB_OK) return fail(MTB_ERR_CUDA);
+  if (cudaStreamSynchronize(0) != cudaSuccess) return fail(MTB_ERR_CUDA);
   *out = h;
   return MTB_OK;
 }
@@ -310,6 +317,8 @@ extern "C" void mtb_search_destroy(mtb_search* h) {
   if (h->dtab) cudaFree(h->dtab);
   if (h->Ctab) cudaFree(h->Ctab);
   if (h->cand) cudaFree(h->cand);
+  if (h->coef) cudaFree(h->coef);
+  if (h->fold) cudaFree(h->fold);
   delete h;
 }
 
@@ -345,8 +354,8 @@ extern "C" int mtb_newton_march(mtb_search* h, const float* sigma, int64_t sigma
   for (int i = 0; i < MTB_MAX_STAGES; ++i) P.stages[i] = h->cfg.stages[i];
   P.num_steps = h->cfg.num_steps;
   P.flags = h->cfg.flags;
-  return newton_launch(sigma, sigma_stride, B, h->cfg.candidates, alpha, beta, gamma, score, h->Ctab, P,
-                       (cudaStream_t)stream);
+  return newton_launch(sigma, sigma_stride, B, h->cfg.candidates, alpha, beta, gamma, score, h->Ctab, h->coef,
+                       h->fold, P, (cudaStream_t)stream);
 }
 
 extern "C" int mtb_search_orientations(mtb_search* h, const float* sigma, int64_t sigma_stride, int B,
@@ -466,8 +475,9 @@ extern "C" int mtb_search_orientations_static(const mtb_search_config* cfg, cons
   const int C = cfg->candidates;
   const size_t dtab_b = align256((size_t)n * nk * sizeof(float));
   const size_t ctab_b = align256((size_t)(cfg->Lmax + 1) * (cfg->Lmax + 1) * sizeof(double));
+  const size_t coef_b = align256((size_t)newton_fold_entries(cfg->Lmax) * sizeof(float4));
   const size_t cand_b = align256((size_t)4 * B * C * sizeof(float));
-  MTB_ARG_CHECK(dtab_b + ctab_b + cand_b <= kStaticScratchBytes,
+  MTB_ARG_CHECK(dtab_b + ctab_b + coef_b + cand_b <= kStaticScratchBytes,
                 "batch x candidates (or grid size) exceeds the static scratch of "
                 "MTB_SEARCH_STATIC_SCRATCH_BYTES; use mtb_search_orientations");
   int dev = 0;
@@ -485,7 +495,8 @@ extern "C" int mtb_search_orientations_static(const mtb_search_config* cfg, cons
   }
   float* dtab = reinterpret_cast<float*>(base);
   double* Ctab = reinterpret_cast<double*>(base + dtab_b);
-  float* ca = reinterpret_cast<float*>(base + dtab_b + ctab_b);
+  float4* coef = reinterpret_cast<float4*>(base + dtab_b + ctab_b);
+  float* ca = reinterpret_cast<float*>(base + dtab_b + ctab_b + coef_b);
   float* cb = ca + (size_t)B * C;
   float* cg = cb + (size_t)B * C;
   float* cs = cg + (size_t)B * C;
@@ -493,6 +504,8 @@ extern "C" int mtb_search_orientations_static(const mtb_search_config* cfg, cons
   const int work = n * P * P + (cfg->Lmax + 1) * (cfg->Lmax + 1);
   static_tables_kernel<<<(work + 127) / 128, 128, 0, st>>>(L0, n, cfg->Lmax, dtab, Ctab);
   MTB_LAUNCH_CHECK();
+  int rc = newton_build_coef(cfg->Lmax, coef, st);
+  if (rc) return rc;
   MTB_CUDA_TRY(cudaFuncSetAttribute(so3_grid_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
   so3_grid_topk_kernel<<<B, kGridThreads, gsm, st>>>(reinterpret_cast<const float2*>(sigma), sigma_stride, B, dtab, L0,
                                                      n, C, ca, cb, cg, nullptr);
@@ -503,7 +516,7 @@ extern "C" int mtb_search_orientations_static(const mtb_search_config* cfg, cons
   for (int i = 0; i < MTB_MAX_STAGES; ++i) NP.stages[i] = i < cfg->n_stages ? cfg->stages[i] : 0;
   NP.num_steps = cfg->num_steps;
   NP.flags = cfg->flags;
-  const int rc = newton_launch(sigma, sigma_stride, B, C, ca, cb, cg, cs, Ctab, NP, st);
+  rc = newton_launch(sigma, sigma_stride, B, C, ca, cb, cg, cs, Ctab, coef, nullptr, NP, st);
   if (rc) return rc;
   reduce_candidates_kernel<<<(B + 127) / 128, 128, 0, st>>>(ca, cb, cg, cs, B, C, alpha, beta, gamma, score);
   MTB_LAUNCH_CHECK();
