@@ -8,12 +8,13 @@
 //   compute_shift (local)        :94-282    with _upsampled_dft :46-91
 //
 // Design (B200): per subtomogram the pipeline is
-//   bg      background sum of the shifted patch over the outer + cosine band
-//   rfft_x  patch sampled, zero planes, cosine fill, roll, 1/N^3 and the real FFT along
-//           the last axis in one pass (one CTA per (b, plane), FFT in shared memory)
-//   fft_y   FFT along the middle axis
-//   fft_z   FFT along the first axis, fused with the rotated, ifftshifted, masked
-//           Fourier reference (sampled on the fly), the product conj(S) T and both norms
+//   xy      patch sampled from two input planes staged in shared memory, zero planes,
+//           roll, 1/N^3, the real FFT along the last axis and the FFT along the middle
+//           axis in one pass (one CTA per (b, plane)); the background fill enters linearly
+//           (see patch_fft_xy_kernel), its weighted sum is accumulated on the way
+//   z       background fill term, FFT along the first axis, fused with the rotated,
+//           ifftshifted, masked Fourier reference (sampled on the fly), the product
+//           conj(S) T and both norms
 //   updft1  first pass of the local upsampled DFT (contract the first axis)
 //   updft23 second and third passes (middle axis, then the half axis, real part only)
 //           with a fused argmax: the U^3 refined correlation never reaches memory.
@@ -40,25 +41,6 @@ struct ShiftGeom {
   float dftshift;        // floor(U / 2)
   float uf;
 };
-
-__device__ __forceinline__ float trilinear(const float* __restrict__ v, int N, float z, float y, float x) {
-  const float z0 = floorf(z), y0 = floorf(y), x0 = floorf(x);
-  const int iz = (int)z0, iy = (int)y0, ix = (int)x0;
-  const float fz = z - z0, fy = y - y0, fx = x - x0;
-  float acc = 0.f;
-#pragma unroll
-  for (int dz = 0; dz < 2; ++dz)
-#pragma unroll
-    for (int dy = 0; dy < 2; ++dy)
-#pragma unroll
-      for (int dx = 0; dx < 2; ++dx) {
-        const int zz = iz + dz, yy = iy + dy, xx = ix + dx;
-        if (zz < 0 || zz >= N || yy < 0 || yy >= N || xx < 0 || xx >= N) continue;
-        const float w = (dz ? fz : 1.f - fz) * (dy ? fy : 1.f - fy) * (dx ? fx : 1.f - fx);
-        acc += w * __ldg(&v[((int64_t)zz * N + yy) * N + xx]);
-      }
-  return acc;
-}
 
 __device__ __forceinline__ float2 trilinear_c(const float2* __restrict__ v, int N, float z, float y, float x) {
   const float z0 = floorf(z), y0 = floorf(y), x0 = floorf(x);
@@ -104,12 +86,6 @@ __device__ __forceinline__ PatchShift patch_shift(const float* __restrict__ shif
   return p;
 }
 
-__device__ __forceinline__ float patch_value(const float* __restrict__ v, int N, const PatchShift& ps, int i, int j,
-                                             int k) {
-  if (i == ps.zp[0] || j == ps.zp[1] || k == ps.zp[2]) return 0.f;
-  return trilinear(v, N, (float)i + ps.f[0], (float)j + ps.f[1], (float)k + ps.f[2]);
-}
-
 __device__ __forceinline__ float block_sum(float v, float* red) {
   v = warp_sum(v);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -124,62 +100,13 @@ __device__ __forceinline__ float block_sum(float v, float* red) {
   return s;  // valid in thread 0
 }
 
-// ------------------------------------------------------------------ background sum
-__global__ void __launch_bounds__(kT)
-bg_kernel(const float* __restrict__ vol, const float* __restrict__ shift_zyx, const int* __restrict__ bg_idx,
-          const float* __restrict__ bg_w, int n_bg, ShiftGeom g, float* __restrict__ bg) {
-  __shared__ float red[32];
-  const int b = blockIdx.y;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  const float* v = vol + (int64_t)b * g.N * g.N * g.N;
-  const PatchShift ps = patch_shift(shift_zyx, b, g.N);
-  float s = 0.f;
-  if (e < n_bg) {
-    const int idx = bg_idx[e];
-    const int k = idx % g.N, j = (idx / g.N) % g.N, i = idx / (g.N * g.N);
-    s = bg_w[e] * patch_value(v, g.N, ps, i, j, k);
-  }
-  s = block_sum(s, red);
-  if (threadIdx.x == 0) atomicAdd(&bg[b], s);
-}
-
 // ------------------------------------------------------------------ radix-2 FFT in shared memory
-// In-place forward FFT (e^{-2 pi i k n / L}) of `lines` sequences of length L (power of two),
-// element t of line q at buf[q * ls + t * es].  tw[k] = e^{-2 pi i k / L}, k < L/2.
-__device__ void smem_fft(float2* buf, int lines, int L, int ls, int es, const float2* tw) {
-  const int NT = blockDim.x;
-  int logL = 0;
-  while ((1 << logL) < L) ++logL;
-  // bit reversal
-  for (int e = threadIdx.x; e < lines * L; e += NT) {
-    const int q = e / L, t = e % L;
-    const int r = __brev(t) >> (32 - logL);
-    if (r > t) {
-      float2* a = &buf[q * ls + t * es];
-      float2* c = &buf[q * ls + r * es];
-      const float2 tmp = *a;
-      *a = *c;
-      *c = tmp;
-    }
-  }
-  __syncthreads();
-  for (int s = 1; s <= logL; ++s) {
-    const int half = 1 << (s - 1);
-    const int stride = L >> s;
-    for (int e = threadIdx.x; e < lines * (L / 2); e += NT) {
-      const int q = e / (L / 2), t = e % (L / 2);
-      const int grp = t / half, pos = t % half;
-      const int i0 = grp * 2 * half + pos, i1 = i0 + half;
-      float2* p0 = &buf[q * ls + i0 * es];
-      float2* p1 = &buf[q * ls + i1 * es];
-      const float2 w = tw[pos * stride];
-      const float2 a = *p0, c = *p1;
-      const float2 wc = cmul(w, c);
-      *p0 = make_float2(a.x + wc.x, a.y + wc.y);
-      *p1 = make_float2(a.x - wc.x, a.y - wc.y);
-    }
-    __syncthreads();
-  }
+__host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n >> 1); }
+
+template <int N>
+__device__ __forceinline__ int brev(int k) {
+  constexpr int kShift = 32 - ilog2c(N);
+  return (int)(__brev((unsigned)k) >> kShift);
 }
 
 __device__ void load_twiddles(float2* tw, int L) {
@@ -190,102 +117,195 @@ __device__ void load_twiddles(float2* tw, int L) {
   }
 }
 
-// ------------------------------------------------------------------ patch -> rfft along x
-// One CTA per (b, rolled plane i').  T[b][i'][j'][m2], m2 < H.
-__global__ void __launch_bounds__(kT)
-rfft_x_kernel(const float* __restrict__ vol, const float* __restrict__ shift_zyx, const float* __restrict__ bg,
-              ShiftGeom g, float2* __restrict__ T) {
-  extern __shared__ __align__(16) float2 sm2[];
-  const int N = g.N;
-  float2* tw = sm2;
-  float2* buf = sm2 + N / 2;  // N lines x N
-  const int ip = blockIdx.x, b = blockIdx.y;
-  const float* v = vol + (int64_t)b * N * N * N;
-  const PatchShift ps = patch_shift(shift_zyx, b, N);
-  const float avg = g.wsum > 0.f ? bg[b] / g.wsum : 0.f;
-  load_twiddles(tw, N);
-  const int i = (ip + g.h) % N;
-  const int di = i - g.h;
-  for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
-    const int jp = e / N, kp = e % N;
-    const int j = (jp + g.h) % N, k = (kp + g.h) % N;
-    float p = patch_value(v, N, ps, i, j, k);
-    const int dj = j - g.h, dk = k - g.h;
-    const int r2 = di * di + dj * dj + dk * dk;
-    if (r2 > g.r2_outer) {
-      p = avg;
-    } else if (r2 >= g.r2_inner) {
-      const float r = sqrtf((float)r2);
-      const float w = 0.5f + 0.5f * cospif((g.rp - r) / g.width);
-      p = (1.f - w) * p + w * avg;
+// In-place decimation-in-frequency forward FFT (e^{-2 pi i k n / N}) of `lines` sequences,
+// element t of line q at buf[q * ls + t * es]; the output of line q is left in bit-reversed
+// order (frequency k at position brev<N>(k)).  tw[k] = e^{-2 pi i k / N}, k < N/2.  Ends
+// with a barrier.
+template <int N>
+__device__ __forceinline__ void fft_dif(float2* buf, int lines, int ls, int es, const float2* __restrict__ tw) {
+  constexpr int HALF = N / 2;
+#pragma unroll
+  for (int span = HALF; span >= 1; span >>= 1) {
+    const int tstride = HALF / span;
+    for (int e = threadIdx.x; e < lines * HALF; e += blockDim.x) {
+      const int q = e / HALF, t = e % HALF;
+      const int pos = t & (span - 1);
+      const int i0 = 2 * t - pos, i1 = i0 + span;
+      float2* p0 = buf + q * ls + i0 * es;
+      float2* p1 = buf + q * ls + i1 * es;
+      const float2 u = *p0, c = *p1;
+      *p0 = make_float2(u.x + c.x, u.y + c.y);
+      *p1 = cmul(make_float2(u.x - c.x, u.y - c.y), tw[pos * tstride]);
     }
-    buf[jp * N + kp] = make_float2(p * g.inv_n3, 0.f);
-  }
-  __syncthreads();
-  smem_fft(buf, N, N, N, 1, tw);
-  float2* out = T + ((int64_t)b * N + ip) * N * g.H;
-  for (int e = threadIdx.x; e < N * g.H; e += blockDim.x) {
-    const int jp = e / g.H, m2 = e % g.H;
-    out[e] = buf[jp * N + m2];
+    __syncthreads();
   }
 }
 
-// ------------------------------------------------------------------ FFT along y
+// Raised-cosine fill weight of the band between the mask radius and rp (integer squared
+// radius r2 >= r2_inner, <= r2_outer); 1 outside, 0 inside.
+__device__ __forceinline__ float fill_weight(int r2, const ShiftGeom& g) {
+  if (r2 > g.r2_outer) return 1.f;
+  if (r2 < g.r2_inner) return 0.f;
+  const float r = sqrtf((float)r2);
+  return 0.5f + 0.5f * cospif((g.rp - r) / g.width);
+}
+
+// ------------------------------------------------------------------ patch -> 2-D rfft of a plane
+// One CTA per (b, rolled plane i').  The patch of a plane (trilinear at a constant shift, so
+// two input planes staged in shared memory cover it), its zeroed planes, the background
+// weights and 1/N^3 are applied, then the real FFT along x (two rows per complex FFT) and the
+// FFT along y; T[b][i'][j'][m2], m2 < N/2+1.
+//
+// The background fill is linear: the reference's filled patch is (1 - W) p + W avg with W the
+// outer/raised-cosine weight, and avg (the W-weighted mean of the patch) is known only after
+// every plane is done.  This kernel therefore transforms (1 - W) p / N^3 and accumulates the
+// weighted background sum into bg[b]; the z pass adds avg times the transform of W / N^3
+// (PATTERN = true computes that transform, once per geometry).
+template <int N, bool PATTERN>
 __global__ void __launch_bounds__(kT)
-fft_y_kernel(ShiftGeom g, float2* __restrict__ T) {
+patch_fft_xy_kernel(const float* __restrict__ vol, const float* __restrict__ shift_zyx,
+                    const float* __restrict__ bgw_tab, ShiftGeom g, float2* __restrict__ T,
+                    float* __restrict__ bg) {
+  constexpr int HN = N / 2, H = N / 2 + 1;
   extern __shared__ __align__(16) float2 sm2[];
-  const int N = g.N, H = g.H;
-  float2* tw = sm2;
-  float2* buf = sm2 + N / 2;  // N x H, row j'
+  __shared__ float red[32];
+  float2* tw = sm2;                                       // N/2
+  float2* zb = sm2 + HN;                                  // HN x N: rows q (re) and q + HN (im)
+  float* planes = reinterpret_cast<float*>(zb + HN * N);  // 2 x N x N input planes
+  float2* yb = reinterpret_cast<float2*>(planes);         // N x H, after the patch is built
   const int ip = blockIdx.x, b = blockIdx.y;
-  float2* slab = T + ((int64_t)b * N + ip) * N * H;
+  const int i = (ip + HN) & (N - 1);
+  const int di = i - HN;
   load_twiddles(tw, N);
-  for (int e = threadIdx.x; e < N * H; e += blockDim.x) buf[e] = slab[e];
+  auto put = [&](int jp, int kp, float val) {
+    reinterpret_cast<float*>(zb + (jp & (HN - 1)) * N + kp)[jp >= HN ? 1 : 0] = val;
+  };
+  float part = 0.f;
+  if (PATTERN) {
+    for (int e = threadIdx.x; e < N * N; e += kT) {
+      const int jp = e / N, kp = e % N;
+      const int dj = ((jp + HN) & (N - 1)) - HN, dk = ((kp + HN) & (N - 1)) - HN;
+      put(jp, kp, fill_weight(di * di + dj * dj + dk * dk, g) * g.inv_n3);
+    }
+  } else {
+    const float* v = vol + (int64_t)b * N * N * N;
+    const PatchShift ps = patch_shift(shift_zyx, b, N);
+    const float z = (float)i + ps.f[0];
+    const float z0 = floorf(z);
+    const int iz = (int)z0;
+    const float fz = z - z0;
+    // planes iz and iz + 1 (zero outside the box, which is what skipping them gives)
+    constexpr int P4 = N * N / 4;
+    float4* pl4 = reinterpret_cast<float4*>(planes);
+    for (int e = threadIdx.x; e < 2 * P4; e += kT) {
+      const int hi = e >= P4 ? 1 : 0;
+      const int zz = iz + hi;
+      pl4[e] = (zz >= 0 && zz < N) ? __ldg(reinterpret_cast<const float4*>(v + (int64_t)zz * N * N) + (e - hi * P4))
+                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();
+    const bool zplane = (i == ps.zp[0]);
+    for (int e = threadIdx.x; e < N * N; e += kT) {
+      const int jp = e / N, kp = e % N;
+      const int j = (jp + HN) & (N - 1), k = (kp + HN) & (N - 1);
+      float p = 0.f;
+      if (!zplane && j != ps.zp[1] && k != ps.zp[2]) {
+        const float y = (float)j + ps.f[1], x = (float)k + ps.f[2];
+        const float y0 = floorf(y), x0 = floorf(x);
+        const int iy = (int)y0, ix = (int)x0;
+        const float fy = y - y0, fx = x - x0;
+#pragma unroll
+        for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+          for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < 2; ++dx) {
+              const int yy = iy + dy, xx = ix + dx;
+              if (yy < 0 || yy >= N || xx < 0 || xx >= N) continue;
+              const float w = (dz ? fz : 1.f - fz) * (dy ? fy : 1.f - fy) * (dx ? fx : 1.f - fx);
+              p += w * planes[(dz * N + yy) * N + xx];
+            }
+      }
+      const int dj = j - HN, dk = k - HN;
+      const int r2 = di * di + dj * dj + dk * dk;
+      part += __ldg(bgw_tab + r2) * p;
+      put(jp, kp, (1.f - fill_weight(r2, g)) * p * g.inv_n3);
+    }
+  }
   __syncthreads();
-  smem_fft(buf, H, N, 1, H, tw);
-  for (int e = threadIdx.x; e < N * H; e += blockDim.x) slab[e] = buf[e];
+  fft_dif<N>(zb, HN, N, 1, tw);
+  // split the packed transforms: Z = A + i B with A, B the transforms of rows q and q + HN
+  for (int e = threadIdx.x; e < HN * H; e += kT) {
+    const int q = e / H, k = e % H;
+    const float2 zk = zb[q * N + brev<N>(k)];
+    const float2 zm = zb[q * N + brev<N>((N - k) & (N - 1))];
+    yb[q * H + k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    yb[(q + HN) * H + k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+  }
+  __syncthreads();
+  fft_dif<N>(yb, H, 1, H, tw);
+  float2* out = T + ((int64_t)b * N + ip) * N * H;
+  for (int e = threadIdx.x; e < N * H; e += kT) {
+    const int jp = e / H, m2 = e % H;
+    out[e] = yb[brev<N>(jp) * H + m2];
+  }
+  if (!PATTERN) {
+    part = block_sum(part, red);
+    if (threadIdx.x == 0) atomicAdd(&bg[b], part);
+  }
+}
+
+template <int N>
+constexpr size_t xy_smem_bytes() {
+  return (size_t)(N / 2 + (N / 2) * N) * sizeof(float2) + (size_t)2 * N * N * sizeof(float);
 }
 
 // ------------------------------------------------------------------ FFT along z + product
-// One CTA per (b, j').  P = conj(S) * T in place; norms |T|^2, |S|^2 per subtomogram.
-// SPLIT: instead of P in place, write the pass-1 operand of the tensor-core upsampled DFT,
+// One CTA per (b, j').  Adds avg_b times the plane transforms of W / N^3 (what), the FFT
+// along z, then P = conj(S) T with the rotated, ifftshifted, masked Fourier reference S
+// sampled on the fly, and the norms |T|^2, |S|^2 per subtomogram.  Without SPLIT P overwrites
+// T; with SPLIT the pass-1 operand of the tensor-core upsampled DFT is written instead,
 // A1[part][(b, m2, m1)][2 m0 + c] as bf16 hi/lo pairs (a1_ws pairs per row, a1_R rows per part).
-template <bool SPLIT>
+template <int N, bool SPLIT>
 __global__ void __launch_bounds__(kT)
-fft_z_product_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ ref,
-                     const float* __restrict__ rot, const float* __restrict__ ctf, float* __restrict__ nrm,
-                     uint32_t* __restrict__ a1, int a1_ws, int a1_R) {
+fft_z_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ what, const float* __restrict__ bg,
+             const float2* __restrict__ ref, const float* __restrict__ rot, const float* __restrict__ ctf,
+             float* __restrict__ nrm, uint32_t* __restrict__ a1, int a1_ws, int a1_R) {
+  constexpr int HN = N / 2, H = N / 2 + 1;
   extern __shared__ __align__(16) float2 sm2[];
   __shared__ float red[32];
-  const int N = g.N, H = g.H;
   float2* tw = sm2;
-  float2* buf = sm2 + N / 2;  // N (i') x H
+  float2* buf = sm2 + HN;  // N (i') x H
   const int jp = blockIdx.x, b = blockIdx.y;
   float2* base = T + (int64_t)b * N * N * H + (int64_t)jp * H;
+  const float2* wb = what + (int64_t)jp * H;
+  const float avg = g.wsum > 0.f ? __ldg(&bg[b]) / g.wsum : 0.f;
   load_twiddles(tw, N);
-  for (int e = threadIdx.x; e < N * H; e += blockDim.x) {
+  for (int e = threadIdx.x; e < N * H; e += kT) {
     const int ip = e / H, m2 = e % H;
-    buf[e] = base[(int64_t)ip * N * H + m2];
+    const float2 t = base[(int64_t)ip * N * H + m2];
+    const float2 w = __ldg(&wb[(int64_t)ip * N * H + m2]);
+    buf[e] = make_float2(fmaf(avg, w.x, t.x), fmaf(avg, w.y, t.y));
   }
   __syncthreads();
-  smem_fft(buf, H, N, 1, H, tw);
+  fft_dif<N>(buf, H, 1, H, tw);
   float R[9];
 #pragma unroll
   for (int q = 0; q < 9; ++q) R[q] = __ldg(&rot[b * 9 + q]);
   const float c = (float)g.h;  // centre of the odd-padded grid, (N+1-1)/2
   float st = 0.f, ss = 0.f;
-  for (int e = threadIdx.x; e < N * H; e += blockDim.x) {
+  for (int e = threadIdx.x; e < N * H; e += kT) {
     // SPLIT walks m0 fastest so the bf16 rows are written contiguously
     const int ip = SPLIT ? e % N : e / H, m2 = SPLIT ? e / N : e % H;
-    const float2 t = buf[ip * H + m2];
+    const float2 t = buf[brev<N>(ip) * H + m2];
     // mask_full on the (N, N, N/2+1) index grid (setup_utils.py:239-249)
-    const int kp = ip < N / 2 ? ip : ip - N;
-    const int jq = jp < N / 2 ? jp : jp - N;
-    const int xq = m2 < N / 2 ? m2 : m2 - H;
+    const int kp = ip < HN ? ip : ip - N;
+    const int jq = jp < HN ? jp : jp - N;
+    const int xq = m2 < HN ? m2 : m2 - H;
     float2 s = make_float2(0.f, 0.f);
     if (kp * kp + jq * jq + xq * xq <= g.mask_r2) {
       // ifftshift over (z, y) of the slice [..., N/2:] of the rotated reference
-      const int zo = (ip + g.h) % N, yo = (jp + g.h) % N, xw = m2 + g.h;
+      const int zo = (ip + HN) & (N - 1), yo = (jp + HN) & (N - 1), xw = m2 + HN;
       const float bx = (float)xw - c, by = (float)yo - c, bz = (float)zo - c;
       const float rx = R[0] * bx + R[1] * by + R[2] * bz + c;
       const float ry = R[3] * bx + R[4] * by + R[5] * bz + c;
@@ -318,6 +338,11 @@ fft_z_product_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restri
     atomicAdd(&nrm[2 * b], st);
     atomicAdd(&nrm[2 * b + 1], ss);
   }
+}
+
+template <int N>
+constexpr size_t z_smem_bytes() {
+  return (size_t)(N / 2 + N * (N / 2 + 1)) * sizeof(float2);
 }
 
 // ------------------------------------------------------------------ upsampled DFT, pass 1
@@ -474,9 +499,8 @@ __global__ void finalize_tc_kernel(ShiftGeom g, int B, const unsigned long long*
 struct mtb_shift {
   mtb_shift_config cfg;
   ShiftGeom g;
-  int n_bg;
-  int* bg_idx;
-  float* bg_w;
+  float* bgw_tab;  // background weight by integer squared radius, 0 .. 3 (N/2)^2
+  float2* what;    // (N, N, N/2+1) plane transforms of the fill weight W / N^3
   float2* ref;     // (N, N, N) Fourier reference, fftshifted and masked
   float2* E0;      // (U, N)
   float2* E1;      // (U, N)
@@ -492,6 +516,49 @@ struct mtb_shift {
   ShiftTc tc;
   bool use_tc;
 };
+
+// The front of the pipeline for box size N: with B > 0 the patch / xy-FFT and the z-FFT +
+// product of B subtomograms (into T, or into the tensor-core operand A1); with B == 0 the
+// plane transforms of the background fill weight, once per geometry, into h->what.
+template <int N>
+int shift_front_n(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
+                  int B, cudaStream_t st) {
+  const ShiftGeom& g = h->g;
+  const int sxy = (int)xy_smem_bytes<N>(), sz = (int)z_smem_bytes<N>();
+  if (B == 0) {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
+    patch_fft_xy_kernel<N, true><<<dim3(N, 1), kT, sxy, st>>>(nullptr, nullptr, nullptr, g, h->what, nullptr);
+    MTB_LAUNCH_CHECK();
+    return MTB_OK;
+  }
+  MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
+  patch_fft_xy_kernel<N, false><<<dim3(N, B), kT, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, g, h->T, h->bg);
+  MTB_LAUNCH_CHECK();
+  if (h->use_tc) {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+    fft_z_kernel<N, true><<<dim3(N, B), kT, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm,
+                                                       (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1);
+  } else {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+    fft_z_kernel<N, false><<<dim3(N, B), kT, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm, nullptr,
+                                                        0, 0);
+  }
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
+}
+
+int shift_front(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
+                int B, cudaStream_t st) {
+  switch (h->g.N) {
+    case 4: return shift_front_n<4>(h, subtomos, shift_zyx, rot, ctf, B, st);
+    case 8: return shift_front_n<8>(h, subtomos, shift_zyx, rot, ctf, B, st);
+    case 16: return shift_front_n<16>(h, subtomos, shift_zyx, rot, ctf, B, st);
+    case 32: return shift_front_n<32>(h, subtomos, shift_zyx, rot, ctf, B, st);
+    case 64: return shift_front_n<64>(h, subtomos, shift_zyx, rot, ctf, B, st);
+    case 128: return shift_front_n<128>(h, subtomos, shift_zyx, rot, ctf, B, st);
+    default: MTB_ARG_CHECK(false, "N must be a power of two in [4, 128]");
+  }
+}
 
 extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
   MTB_ARG_CHECK(cfg && out, "null argument");
@@ -519,26 +586,21 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
   g.rp = (float)rp;
   g.width = cfg->cosine_width;
   g.mask_r2 = (N / 2) * (N / 2);
-  // background voxels: r > rp (weight 1) and radius <= r <= rp (raised cosine)
-  std::vector<int> idx;
-  std::vector<float> w;
+  // background voxels: r > rp (weight 1) and radius <= r <= rp (raised cosine); the weight
+  // depends on the integer squared radius only
+  const int r2max = 3 * (N / 2) * (N / 2);
+  std::vector<float> wtab(r2max + 1, 0.f);
+  for (int r2 = 0; r2 <= r2max; ++r2) {
+    const double r = sqrt((double)r2);
+    if (r > rp) wtab[r2] = 1.f;
+    else if (!(r < radius)) wtab[r2] = (float)(0.5 + 0.5 * cos(M_PI * (rp - r) / cfg->cosine_width));
+  }
   double wsum = 0.0;
   for (int i = 0; i < N; ++i)
     for (int j = 0; j < N; ++j)
       for (int k = 0; k < N; ++k) {
         const int di = i - N / 2, dj = j - N / 2, dk = k - N / 2;
-        const int r2 = di * di + dj * dj + dk * dk;
-        const double r = sqrt((double)r2);
-        if (r > rp) {
-          idx.push_back((i * N + j) * N + k);
-          w.push_back(1.f);
-          wsum += 1.0;
-        } else if (!(r < radius)) {
-          const float rc = (float)(0.5 + 0.5 * cos(M_PI * (rp - r) / cfg->cosine_width));
-          idx.push_back((i * N + j) * N + k);
-          w.push_back(rc);
-          wsum += rc;
-        }
+        wsum += wtab[di * di + dj * dj + dk * dk];
       }
   // same sets by integer squared radius: outer r2 > floor(rp^2); band r2 >= ceil(radius^2)
   const int r2_outer = (int)floor(rp * rp);
@@ -546,7 +608,6 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
   g.r2_inner = r2_inner;
   g.r2_outer = r2_outer;
   g.wsum = (float)wsum;
-  h->n_bg = (int)idx.size();
   // DFT kernels exp(+2 pi i (u - dftshift) f_m), f = fftfreq(n, d=uf)
   auto kern = [&](int n, std::vector<float2>& E) {
     E.resize((size_t)g.U * n);
@@ -566,19 +627,20 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
   const size_t B = cfg->max_batch;
   auto fail = [&](int code) { mtb_shift_destroy(h); return code; };
   auto alloc = [&](void** p, size_t bytes) { return cudaMalloc(p, bytes > 0 ? bytes : 4) == cudaSuccess; };
-  if (!alloc((void**)&h->bg_idx, idx.size() * 4) || !alloc((void**)&h->bg_w, w.size() * 4) ||
+  if (!alloc((void**)&h->bgw_tab, wtab.size() * 4) || !alloc((void**)&h->what, (size_t)N * N * g.H * 8) ||
       !alloc((void**)&h->ref, (size_t)N * N * N * 8) || !alloc((void**)&h->E0, e0.size() * 8) ||
       !alloc((void**)&h->E1, e0.size() * 8) || !alloc((void**)&h->E2, e2.size() * 8) ||
       !alloc((void**)&h->bg, B * 4) || !alloc((void**)&h->nrm, B * 8) ||
       !alloc((void**)&h->T, B * N * N * g.H * 8) || !alloc((void**)&h->X1, B * g.U * N * g.H * 8) ||
       !alloc((void**)&h->pval, B * h->ngrp * 4) || !alloc((void**)&h->pidx, B * h->ngrp * 4))
     return fail(MTB_ERR_OOM);
-  if (cudaMemcpy(h->bg_idx, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(h->bg_w, w.data(), w.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+  if (cudaMemcpy(h->bgw_tab, wtab.data(), wtab.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->E0, e0.data(), e0.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->E1, e0.data(), e0.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->E2, e2.data(), e2.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(MTB_ERR_CUDA);
+  if (shift_front(h, nullptr, nullptr, nullptr, nullptr, 0, 0) != MTB_OK) return fail(MTB_ERR_CUDA);
+  if (cudaStreamSynchronize(0) != cudaSuccess) return fail(MTB_ERR_CUDA);
   if (cfg->precision == MTB_SHIFT_BF16X3) {
     const int rc = shift_tc_prepare(&h->tc, N, g.H, g.U, cfg->upsample_factor, g.dftshift, cfg->max_batch);
     if (rc) return fail(rc);
@@ -593,7 +655,7 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
 extern "C" void mtb_shift_destroy(mtb_shift* h) {
   if (!h) return;
   shift_tc_release(&h->tc);
-  void* ptrs[] = {h->bg_idx, h->bg_w, h->ref, h->E0, h->E1, h->E2, h->bg, h->nrm, h->T, h->X1, h->pval, h->pidx};
+  void* ptrs[] = {h->bgw_tab, h->what, h->ref, h->E0, h->E1, h->E2, h->bg, h->nrm, h->T, h->X1, h->pval, h->pidx};
   for (void* p : ptrs) if (p) cudaFree(p);
   delete h;
 }
@@ -629,31 +691,15 @@ extern "C" int mtb_shift_search(mtb_shift* h, const float* subtomos, const float
   const int N = g.N, H = g.H, U = g.U;
   MTB_CUDA_TRY(cudaMemsetAsync(h->bg, 0, (size_t)B * 4, st));
   MTB_CUDA_TRY(cudaMemsetAsync(h->nrm, 0, (size_t)B * 8, st));
-  bg_kernel<<<dim3((h->n_bg + kT - 1) / kT, B), kT, 0, st>>>(subtomos, shift_zyx, h->bg_idx, h->bg_w, h->n_bg, g,
-                                                             h->bg);
-  MTB_LAUNCH_CHECK();
-  const size_t smx = (size_t)(N / 2 + N * N) * 8;
-  MTB_CUDA_TRY(cudaFuncSetAttribute(rfft_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
-  rfft_x_kernel<<<dim3(N, B), kT, smx, st>>>(subtomos, shift_zyx, h->bg, g, h->T);
-  MTB_LAUNCH_CHECK();
-  const size_t smy = (size_t)(N / 2 + N * H) * 8;
-  MTB_CUDA_TRY(cudaFuncSetAttribute(fft_y_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
-  fft_y_kernel<<<dim3(N, B), kT, smy, st>>>(g, h->T);
-  MTB_LAUNCH_CHECK();
+  int rc = shift_front(h, subtomos, shift_zyx, rot, ctf, B, st);
+  if (rc) return rc;
   if (h->use_tc) {
-    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_product_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
-    fft_z_product_kernel<true><<<dim3(N, B), kT, smy, st>>>(g, h->T, h->ref, rot, ctf, h->nrm, (uint32_t*)h->tc.A1,
-                                                          h->tc.KB12 * 32, h->tc.R1);
-    MTB_LAUNCH_CHECK();
-    const int rc = shift_tc_passes(&h->tc, B, st);
+    rc = shift_tc_passes(&h->tc, B, st);
     if (rc) return rc;
     finalize_tc_kernel<<<(B + 127) / 128, 128, 0, st>>>(g, B, h->tc.best, h->nrm, shift_xyz, score);
     MTB_LAUNCH_CHECK();
     return MTB_OK;
   }
-  MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_product_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
-  fft_z_product_kernel<false><<<dim3(N, B), kT, smy, st>>>(g, h->T, h->ref, rot, ctf, h->nrm, nullptr, 0, 0);
-  MTB_LAUNCH_CHECK();
   const size_t sm1 = (size_t)(U * N + N * kColTile) * 8;
   MTB_CUDA_TRY(cudaFuncSetAttribute(updft1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
   updft1_kernel<<<dim3((N * H + kColTile - 1) / kColTile, B), kT, sm1, st>>>(g, h->T, h->E0, h->X1);
