@@ -63,6 +63,32 @@ __device__ __forceinline__ float2 trilinear_c(const float2* __restrict__ v, int 
   return make_float2(ar, ai);
 }
 
+// trilinear_c with clamped corner indices and zero weights outside the box: the same sum,
+// with eight unconditional loads that can all be in flight together.
+__device__ __forceinline__ float2 trilinear_c_nb(const float2* __restrict__ v, int N, float z, float y, float x) {
+  const float z0 = floorf(z), y0 = floorf(y), x0 = floorf(x);
+  const int iz = (int)z0, iy = (int)y0, ix = (int)x0;
+  const float fz = z - z0, fy = y - y0, fx = x - x0;
+  const float wz[2] = {(iz >= 0 && iz < N) ? 1.f - fz : 0.f, (iz + 1 >= 0 && iz + 1 < N) ? fz : 0.f};
+  const float wy[2] = {(iy >= 0 && iy < N) ? 1.f - fy : 0.f, (iy + 1 >= 0 && iy + 1 < N) ? fy : 0.f};
+  const float wx[2] = {(ix >= 0 && ix < N) ? 1.f - fx : 0.f, (ix + 1 >= 0 && ix + 1 < N) ? fx : 0.f};
+  const int cz[2] = {min(max(iz, 0), N - 1), min(max(iz + 1, 0), N - 1)};
+  const int cy[2] = {min(max(iy, 0), N - 1), min(max(iy + 1, 0), N - 1)};
+  const int cx[2] = {min(max(ix, 0), N - 1), min(max(ix + 1, 0), N - 1)};
+  float2 q[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c)
+    q[c] = __ldg(&v[((int64_t)cz[c >> 2] * N + cy[(c >> 1) & 1]) * N + cx[c & 1]]);
+  float ar = 0.f, ai = 0.f;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const float w = wz[c >> 2] * wy[(c >> 1) & 1] * wx[c & 1];
+    ar += w * q[c].x;
+    ai += w * q[c].y;
+  }
+  return make_float2(ar, ai);
+}
+
 // Per-subtomogram shift parameters: f = flip(shift_zyx) and the zeroed planes.
 struct PatchShift {
   float f[3];
@@ -345,6 +371,290 @@ constexpr size_t z_smem_bytes() {
   return (size_t)(N / 2 + N * (N / 2 + 1)) * sizeof(float2);
 }
 
+// ------------------------------------------------------------------ box 64: radix-8 x 8 path
+// The same two passes for N = 64 with the FFTs done by groups of 8 threads: a 64-point line
+// is x[r + 8 s] (thread r, register s), an 8-point DFT in registers, the twiddles W64^(r k1),
+// one transpose through the line's shared scratch (warp-synchronous: a line's 8 threads share
+// a warp) and a second 8-point DFT, which leaves X[r + 8 k2] in thread r.  The patch is built
+// by three separable linear interpolations (z, then x, then y) from the two staged planes.
+constexpr int kT64 = 288;  // 36 groups of 8: 33 lines for the (N/2+1)-column passes
+constexpr int kXS = 72;    // per-line scratch (float2): transpose slot (k1, r) at 9 k1 + r
+constexpr int kYS = 34;    // row stride (float2) of the 64 x 33 column buffers
+
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 c_mi(float2 a) { return make_float2(a.y, -a.x); }  // a * (-i)
+
+// 8-point forward DFT, natural order in and out (radix-2 decimation in frequency).
+__device__ __forceinline__ void dft8(float2 (&v)[8]) {
+  const float c = 0.70710678118654752f;
+  const float2 a0 = c_add(v[0], v[4]), a4 = c_sub(v[0], v[4]);
+  const float2 a1 = c_add(v[1], v[5]), d1 = c_sub(v[1], v[5]);
+  const float2 a2 = c_add(v[2], v[6]), d2 = c_sub(v[2], v[6]);
+  const float2 a3 = c_add(v[3], v[7]), d3 = c_sub(v[3], v[7]);
+  const float2 a5 = make_float2(c * (d1.x + d1.y), c * (d1.y - d1.x));  // d1 W8
+  const float2 a6 = c_mi(d2);                                           // d2 W8^2
+  const float2 a7 = make_float2(c * (d3.y - d3.x), -c * (d3.x + d3.y)); // d3 W8^3
+  const float2 b0 = c_add(a0, a2), b2 = c_sub(a0, a2);
+  const float2 b1 = c_add(a1, a3), b3 = c_mi(c_sub(a1, a3));
+  const float2 b4 = c_add(a4, a6), b6 = c_sub(a4, a6);
+  const float2 b5 = c_add(a5, a7), b7 = c_mi(c_sub(a5, a7));
+  v[0] = c_add(b0, b1); v[4] = c_sub(b0, b1);
+  v[2] = c_add(b2, b3); v[6] = c_sub(b2, b3);
+  v[1] = c_add(b4, b5); v[5] = c_sub(b4, b5);
+  v[3] = c_add(b6, b7); v[7] = c_sub(b6, b7);
+}
+
+// 64-point forward FFT of one line by its 8 threads (r = lane % 8): v[s] = x[r + 8 s] on
+// entry, v[k2] = X[r + 8 k2] on exit.  xs is the line's scratch (kXS float2); tw[m] = W64^m.
+__device__ __forceinline__ void fft64_group(float2 (&v)[8], int r, float2* xs, const float2* tw) {
+  dft8(v);
+#pragma unroll
+  for (int k1 = 1; k1 < 8; ++k1) v[k1] = cmul(v[k1], tw[r * k1]);
+  __syncwarp();
+#pragma unroll
+  for (int k1 = 0; k1 < 8; ++k1) xs[9 * k1 + r] = v[k1];
+  __syncwarp();
+#pragma unroll
+  for (int t = 0; t < 8; ++t) v[t] = xs[9 * r + t];
+  dft8(v);
+}
+
+// FFT along the rows of a 64 x 33 column buffer (element (n, col) at buf[n * kYS + col]) in
+// place, one column per group of 8 threads; xs: 36 line scratches.
+__device__ __forceinline__ void fft64_columns(float2* buf, float2* xs, const float2* tw) {
+  const int L = threadIdx.x >> 3, r = threadIdx.x & 7;
+  const int col = L < 33 ? L : 32;  // groups 33..35 shadow column 32 inside its own warp
+  float2 v[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) v[s] = buf[(r + 8 * s) * kYS + col];
+  fft64_group(v, r, xs + L * kXS, tw);
+  __syncwarp();
+  if (L < 33) {
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) buf[(r + 8 * k2) * kYS + col] = v[k2];
+  }
+}
+
+__device__ void load_twiddles64(float2* tw) {
+  for (int k = threadIdx.x; k < 64; k += blockDim.x) {
+    double s, c;
+    sincospi(-2.0 * k / 64, &s, &c);
+    tw[k] = make_float2((float)c, (float)s);
+  }
+}
+
+// patch_fft_xy_kernel<64, false> with the radix-8 x 8 FFTs; fill_tab[r2] is fill_weight(r2).
+__global__ void __launch_bounds__(kT64, 4)
+patch_fft_xy64_kernel(const float* __restrict__ vol, const float* __restrict__ shift_zyx,
+                      const float* __restrict__ bgw_tab, const float* __restrict__ fill_tab, ShiftGeom g,
+                      float2* __restrict__ T, float* __restrict__ bg) {
+  constexpr int N = 64, HN = 32, H = 33;
+  extern __shared__ __align__(16) float2 sm2[];
+  __shared__ float red[32];
+  __shared__ int s_c[2][2][N];      // [y/x][tap] clamped source index
+  __shared__ float s_w[2][2][N];    // [y/x][tap] weight (0 for taps outside the box or zeroed)
+  float2* tw = sm2;                                     // 64
+  float* P0 = reinterpret_cast<float*>(sm2 + 64);       // plane iz, then the z-interpolated plane
+  float* P1 = P0 + N * N;                               // plane iz+1, then the x-interpolated plane
+  float2* yb = reinterpret_cast<float2*>(P0);           // 64 x kYS, after the patch is built
+  float2* zb = reinterpret_cast<float2*>(P1 + N * N);   // 36 x kXS: packed rows, then scratch
+  const int ip = blockIdx.x, b = blockIdx.y;
+  const int i = (ip + HN) & (N - 1);
+  const int di = i - HN;
+  const float* v = vol + (int64_t)b * N * N * N;
+  const PatchShift ps = patch_shift(shift_zyx, b, N);
+  const float z = (float)i + ps.f[0];
+  const float z0 = floorf(z);
+  const int iz = (int)z0;
+  const float fz = z - z0;
+  load_twiddles64(tw);
+  if (threadIdx.x < 2 * N) {
+    const int ax = threadIdx.x / N, j = threadIdx.x % N;  // ax 0: y (index j), 1: x (index k)
+    const float y = (float)j + ps.f[1 + ax];
+    const float y0 = floorf(y);
+    const int iy = (int)y0;
+    const float fy = y - y0;
+    const bool zero = (j == ps.zp[1 + ax]);
+    s_c[ax][0][j] = min(max(iy, 0), N - 1);
+    s_c[ax][1][j] = min(max(iy + 1, 0), N - 1);
+    s_w[ax][0][j] = (zero || iy < 0 || iy >= N) ? 0.f : 1.f - fy;
+    s_w[ax][1][j] = (zero || iy + 1 < 0 || iy + 1 >= N) ? 0.f : fy;
+  }
+  constexpr int P4 = N * N / 4;
+  float4* pl4 = reinterpret_cast<float4*>(P0);
+  for (int e = threadIdx.x; e < 2 * P4; e += kT64) {
+    const int hi = e >= P4 ? 1 : 0;
+    const int zz = iz + hi;
+    pl4[e] = (zz >= 0 && zz < N) ? __ldg(reinterpret_cast<const float4*>(v + (int64_t)zz * N * N) + (e - hi * P4))
+                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
+  // z: P0 <- (1 - fz) P0 + fz P1 (a zeroed plane interpolates to zero)
+  {
+    const bool zplane = (i == ps.zp[0]);
+    const float w0 = zplane ? 0.f : 1.f - fz, w1 = zplane ? 0.f : fz;
+    const float4* q1 = reinterpret_cast<const float4*>(P1);
+    for (int e = threadIdx.x; e < P4; e += kT64) {
+      const float4 a = pl4[e], c = q1[e];
+      pl4[e] = make_float4(w0 * a.x + w1 * c.x, w0 * a.y + w1 * c.y, w0 * a.z + w1 * c.z, w0 * a.w + w1 * c.w);
+    }
+  }
+  __syncthreads();
+  // x: P1[yy][k] <- w0(k) P0[yy][c0(k)] + w1(k) P0[yy][c1(k)]; a thread keeps one column k
+  // (its taps in registers) and walks every fourth row
+  float part = 0.f;
+  if (threadIdx.x < 256) {
+    const int k = threadIdx.x & (N - 1), y0r = threadIdx.x >> 6;
+    const float w0 = s_w[1][0][k], w1 = s_w[1][1][k];
+    const int c0 = s_c[1][0][k], c1 = s_c[1][1][k];
+#pragma unroll 4
+    for (int yy = y0r; yy < N; yy += 4) P1[yy * N + k] = w0 * P0[yy * N + c0] + w1 * P0[yy * N + c1];
+  }
+  __syncthreads();
+  // y, background, fill weight, 1/N^3, roll, pack rows j' and j' + 32 into one complex line
+  if (threadIdx.x < 256) {
+    const int k = threadIdx.x & (N - 1), j0 = threadIdx.x >> 6;
+    const int dk = k - HN, kp = (k + HN) & (N - 1);
+    const int rk = di * di + dk * dk;
+#pragma unroll 2
+    for (int j = j0; j < N; j += 4) {
+      const float p = s_w[0][0][j] * P1[s_c[0][0][j] * N + k] + s_w[0][1][j] * P1[s_c[0][1][j] * N + k];
+      const int dj = j - HN;
+      const int r2 = rk + dj * dj;
+      float keep = 1.f;  // 1 - W
+      if (r2 > g.r2_outer) {
+        part += p;
+        keep = 0.f;
+      } else if (r2 >= g.r2_inner) {
+        part += __ldg(bgw_tab + r2) * p;
+        keep = 1.f - __ldg(fill_tab + r2);
+      }
+      const int jp = (j + HN) & (N - 1);
+      reinterpret_cast<float*>(zb + (jp & (HN - 1)) * kXS + kp)[jp >> 5] = keep * p * g.inv_n3;
+    }
+  }
+  __syncthreads();
+  // x FFT of the 32 packed lines (groups 32..35 work on their own scratch lines and are dropped)
+  {
+    const int L = threadIdx.x >> 3, r = threadIdx.x & 7;
+    float2* line = zb + L * kXS;
+    float2 w[8];
+#pragma unroll
+    for (int s8 = 0; s8 < 8; ++s8) w[s8] = line[r + 8 * s8];
+    fft64_group(w, r, line, tw);
+    __syncwarp();
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) line[r + 8 * k2] = w[k2];
+  }
+  __syncthreads();
+  // split Z = A + i B into the transforms of rows q and q + 32, columns m2 < 33
+  for (int e = threadIdx.x; e < HN * H; e += kT64) {
+    const int q = e / H, k = e - (e / H) * H;
+    const float2 zk = zb[q * kXS + k];
+    const float2 zm = zb[q * kXS + ((N - k) & (N - 1))];
+    yb[q * kYS + k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    yb[(q + HN) * kYS + k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+  }
+  __syncthreads();
+  fft64_columns(yb, zb, tw);
+  __syncthreads();
+  float2* out = T + ((int64_t)b * N + ip) * N * H;
+  for (int e = threadIdx.x; e < N * H; e += kT64) {
+    const int jq = e / H, m2 = e - (e / H) * H;
+    out[e] = yb[jq * kYS + m2];
+  }
+  part = block_sum(part, red);
+  if (threadIdx.x == 0) atomicAdd(&bg[b], part);
+}
+
+constexpr size_t xy64_smem_bytes() {
+  return (size_t)64 * sizeof(float2) + (size_t)2 * 64 * 64 * sizeof(float) + (size_t)36 * kXS * sizeof(float2);
+}
+
+// fft_z_kernel<64, SPLIT> with the radix-8 x 8 FFT.
+template <bool SPLIT>
+__global__ void __launch_bounds__(kT64, 4)
+fft_z64_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ what, const float* __restrict__ bg,
+               const float2* __restrict__ ref, const float* __restrict__ rot, const float* __restrict__ ctf,
+               float* __restrict__ nrm, uint32_t* __restrict__ a1, int a1_ws, int a1_R) {
+  constexpr int N = 64, HN = 32, H = 33;
+  extern __shared__ __align__(16) float2 sm2[];
+  __shared__ float red[32];
+  float2* tw = sm2;              // 64
+  float2* buf = sm2 + 64;        // 64 (i') x kYS
+  float2* xs = buf + N * kYS;    // 36 x kXS
+  const int jp = blockIdx.x, b = blockIdx.y;
+  float2* base = T + (int64_t)b * N * N * H + (int64_t)jp * H;
+  const float2* wb = what + (int64_t)jp * H;
+  const float avg = g.wsum > 0.f ? __ldg(&bg[b]) / g.wsum : 0.f;
+  load_twiddles64(tw);
+  for (int e = threadIdx.x; e < N * H; e += kT64) {
+    const int ip = e / H, m2 = e - (e / H) * H;
+    const float2 t = base[(int64_t)ip * N * H + m2];
+    const float2 w = __ldg(&wb[(int64_t)ip * N * H + m2]);
+    buf[ip * kYS + m2] = make_float2(fmaf(avg, w.x, t.x), fmaf(avg, w.y, t.y));
+  }
+  __syncthreads();
+  fft64_columns(buf, xs, tw);
+  __syncthreads();
+  float R[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) R[q] = __ldg(&rot[b * 9 + q]);
+  const float c = (float)g.h;
+  float st = 0.f, ss = 0.f;
+#pragma unroll 2
+  for (int e = threadIdx.x; e < N * H; e += kT64) {
+    const int ip = SPLIT ? e & (N - 1) : e / H, m2 = SPLIT ? e >> 6 : e - (e / H) * H;
+    const float2 t = buf[ip * kYS + m2];
+    const int kp = ip < HN ? ip : ip - N;
+    const int jq = jp < HN ? jp : jp - N;
+    const int xq = m2 < HN ? m2 : m2 - H;
+    float2 s = make_float2(0.f, 0.f);
+    if (kp * kp + jq * jq + xq * xq <= g.mask_r2) {
+      const int zo = (ip + HN) & (N - 1), yo = (jp + HN) & (N - 1), xw = m2 + HN;
+      const float bx = (float)xw - c, by = (float)yo - c, bz = (float)zo - c;
+      const float rx = R[0] * bx + R[1] * by + R[2] * bz + c;
+      const float ry = R[3] * bx + R[4] * by + R[5] * bz + c;
+      const float rz = R[6] * bx + R[7] * by + R[8] * bz + c;
+      s = trilinear_c_nb(ref, N, rz, ry, rx);
+      if (ctf) {
+        const float cv = __ldg(&ctf[(((int64_t)b * N + ip) * N + jp) * H + m2]);
+        s.x *= cv;
+        s.y *= cv;
+      }
+    }
+    st += t.x * t.x + t.y * t.y;
+    ss += s.x * s.x + s.y * s.y;
+    const float2 p = make_float2(s.x * t.x + s.y * t.y, s.x * t.y - s.y * t.x);
+    if (SPLIT) {
+      const __nv_bfloat16 rh = __float2bfloat16_rn(p.x), ih = __float2bfloat16_rn(p.y);
+      const __nv_bfloat162 hi = __halves2bfloat162(rh, ih);
+      const __nv_bfloat162 lo = __floats2bfloat162_rn(p.x - __bfloat162float(rh), p.y - __bfloat162float(ih));
+      const size_t row = ((size_t)b * H + m2) * N + jp;
+      a1[row * a1_ws + ip] = *reinterpret_cast<const uint32_t*>(&hi);
+      a1[((size_t)a1_R + row) * a1_ws + ip] = *reinterpret_cast<const uint32_t*>(&lo);
+    } else {
+      base[(int64_t)ip * N * H + m2] = p;
+    }
+  }
+  st = block_sum(st, red);
+  ss = block_sum(ss, red);
+  if (threadIdx.x == 0) {
+    atomicAdd(&nrm[2 * b], st);
+    atomicAdd(&nrm[2 * b + 1], ss);
+  }
+}
+
+constexpr size_t z64_smem_bytes() {
+  return (size_t)64 * sizeof(float2) + (size_t)64 * kYS * sizeof(float2) + (size_t)36 * kXS * sizeof(float2);
+}
+
+__global__ void fill_table_kernel(ShiftGeom g, int n, float* __restrict__ tab) {
+  const int r2 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r2 < n) tab[r2] = fill_weight(r2, g);
+}
+
 // ------------------------------------------------------------------ upsampled DFT, pass 1
 // X1[b][u0][m1][m2] = sum_{m0} E0[u0][m0] P[b][m0][m1][m2].  CTA: (column tile of 64, b).
 constexpr int kColTile = 64;
@@ -500,6 +810,7 @@ struct mtb_shift {
   mtb_shift_config cfg;
   ShiftGeom g;
   float* bgw_tab;  // background weight by integer squared radius, 0 .. 3 (N/2)^2
+  float* fill_tab; // fill weight W by integer squared radius (device formula)
   float2* what;    // (N, N, N/2+1) plane transforms of the fill weight W / N^3
   float2* ref;     // (N, N, N) Fourier reference, fftshifted and masked
   float2* E0;      // (U, N)
@@ -547,6 +858,26 @@ int shift_front_n(mtb_shift* h, const float* subtomos, const float* shift_zyx, c
   return MTB_OK;
 }
 
+int shift_front_64(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
+                   int B, cudaStream_t st) {
+  const ShiftGeom& g = h->g;
+  const int sxy = (int)xy64_smem_bytes(), sz = (int)z64_smem_bytes();
+  MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
+  patch_fft_xy64_kernel<<<dim3(64, B), kT64, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, h->fill_tab, g, h->T, h->bg);
+  MTB_LAUNCH_CHECK();
+  if (h->use_tc) {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+    fft_z64_kernel<true><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm,
+                                                         (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1);
+  } else {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+    fft_z64_kernel<false><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm, nullptr,
+                                                          0, 0);
+  }
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
+}
+
 int shift_front(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
                 int B, cudaStream_t st) {
   switch (h->g.N) {
@@ -554,7 +885,8 @@ int shift_front(mtb_shift* h, const float* subtomos, const float* shift_zyx, con
     case 8: return shift_front_n<8>(h, subtomos, shift_zyx, rot, ctf, B, st);
     case 16: return shift_front_n<16>(h, subtomos, shift_zyx, rot, ctf, B, st);
     case 32: return shift_front_n<32>(h, subtomos, shift_zyx, rot, ctf, B, st);
-    case 64: return shift_front_n<64>(h, subtomos, shift_zyx, rot, ctf, B, st);
+    case 64: return B > 0 ? shift_front_64(h, subtomos, shift_zyx, rot, ctf, B, st)
+                          : shift_front_n<64>(h, subtomos, shift_zyx, rot, ctf, B, st);
     case 128: return shift_front_n<128>(h, subtomos, shift_zyx, rot, ctf, B, st);
     default: MTB_ARG_CHECK(false, "N must be a power of two in [4, 128]");
   }
@@ -627,7 +959,7 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
   const size_t B = cfg->max_batch;
   auto fail = [&](int code) { mtb_shift_destroy(h); return code; };
   auto alloc = [&](void** p, size_t bytes) { return cudaMalloc(p, bytes > 0 ? bytes : 4) == cudaSuccess; };
-  if (!alloc((void**)&h->bgw_tab, wtab.size() * 4) || !alloc((void**)&h->what, (size_t)N * N * g.H * 8) ||
+  if (!alloc((void**)&h->bgw_tab, wtab.size() * 4) || !alloc((void**)&h->fill_tab, wtab.size() * 4) || !alloc((void**)&h->what, (size_t)N * N * g.H * 8) ||
       !alloc((void**)&h->ref, (size_t)N * N * N * 8) || !alloc((void**)&h->E0, e0.size() * 8) ||
       !alloc((void**)&h->E1, e0.size() * 8) || !alloc((void**)&h->E2, e2.size() * 8) ||
       !alloc((void**)&h->bg, B * 4) || !alloc((void**)&h->nrm, B * 8) ||
@@ -639,6 +971,8 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
       cudaMemcpy(h->E1, e0.data(), e0.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->E2, e2.data(), e2.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(MTB_ERR_CUDA);
+  fill_table_kernel<<<(r2max + 256) / 256, 256>>>(g, r2max + 1, h->fill_tab);
+  if (cudaGetLastError() != cudaSuccess) return fail(MTB_ERR_CUDA);
   if (shift_front(h, nullptr, nullptr, nullptr, nullptr, 0, 0) != MTB_OK) return fail(MTB_ERR_CUDA);
   if (cudaStreamSynchronize(0) != cudaSuccess) return fail(MTB_ERR_CUDA);
   if (cfg->precision == MTB_SHIFT_BF16X3) {
@@ -655,7 +989,7 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
 extern "C" void mtb_shift_destroy(mtb_shift* h) {
   if (!h) return;
   shift_tc_release(&h->tc);
-  void* ptrs[] = {h->bgw_tab, h->what, h->ref, h->E0, h->E1, h->E2, h->bg, h->nrm, h->T, h->X1, h->pval, h->pidx};
+  void* ptrs[] = {h->bgw_tab, h->fill_tab, h->what, h->ref, h->E0, h->E1, h->E2, h->bg, h->nrm, h->T, h->X1, h->pval, h->pidx};
   for (void* p : ptrs) if (p) cudaFree(p);
   delete h;
 }
