@@ -63,28 +63,51 @@ __device__ __forceinline__ float2 trilinear_c(const float2* __restrict__ v, int 
   return make_float2(ar, ai);
 }
 
-// trilinear_c with clamped corner indices and zero weights outside the box: the same sum,
-// with eight unconditional loads that can all be in flight together.
-__device__ __forceinline__ float2 trilinear_c_nb(const float2* __restrict__ v, int N, float z, float y, float x) {
+// Corner quads of the Fourier reference for the gathers of the box-64 path: entry
+// (zi, yi, xi), 0 <= zi <= N + 1, 0 <= yi, xi <= N, holds the four values at z = zi - 1,
+// y = yi - 1 + {0, 1}, x = xi - 1 + {0, 1} (zero outside the box), so one trilinear sample is
+// two aligned 32-byte entries.
+__global__ void ref_quad_kernel(const float2* __restrict__ ref, int N, float4* __restrict__ q) {
+  const int n1 = N + 1;
+  const int64_t n = (int64_t)(N + 2) * n1 * n1;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    const int xi = (int)(t % n1), yi = (int)((t / n1) % n1), zi = (int)(t / ((int64_t)n1 * n1));
+    const int z = zi - 1;
+    float2 c[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int y = yi - 1 + (k >> 1), x = xi - 1 + (k & 1);
+      c[k] = (z >= 0 && z < N && y >= 0 && y < N && x >= 0 && x < N) ? ref[((int64_t)z * N + y) * N + x]
+                                                                      : make_float2(0.f, 0.f);
+    }
+    q[2 * t] = make_float4(c[0].x, c[0].y, c[1].x, c[1].y);
+    q[2 * t + 1] = make_float4(c[2].x, c[2].y, c[3].x, c[3].y);
+  }
+}
+
+// trilinear_c from the corner quads (same weights and summation order).
+__device__ __forceinline__ float2 trilinear_quad(const float4* __restrict__ q, int N, float z, float y, float x) {
   const float z0 = floorf(z), y0 = floorf(y), x0 = floorf(x);
   const int iz = (int)z0, iy = (int)y0, ix = (int)x0;
   const float fz = z - z0, fy = y - y0, fx = x - x0;
-  const float wz[2] = {(iz >= 0 && iz < N) ? 1.f - fz : 0.f, (iz + 1 >= 0 && iz + 1 < N) ? fz : 0.f};
-  const float wy[2] = {(iy >= 0 && iy < N) ? 1.f - fy : 0.f, (iy + 1 >= 0 && iy + 1 < N) ? fy : 0.f};
-  const float wx[2] = {(ix >= 0 && ix < N) ? 1.f - fx : 0.f, (ix + 1 >= 0 && ix + 1 < N) ? fx : 0.f};
-  const int cz[2] = {min(max(iz, 0), N - 1), min(max(iz + 1, 0), N - 1)};
-  const int cy[2] = {min(max(iy, 0), N - 1), min(max(iy + 1, 0), N - 1)};
-  const int cx[2] = {min(max(ix, 0), N - 1), min(max(ix + 1, 0), N - 1)};
-  float2 q[8];
-#pragma unroll
-  for (int c = 0; c < 8; ++c)
-    q[c] = __ldg(&v[((int64_t)cz[c >> 2] * N + cy[(c >> 1) & 1]) * N + cx[c & 1]]);
+  const bool in = iz >= -1 && iz < N && iy >= -1 && iy < N && ix >= -1 && ix < N;
+  const int n1 = N + 1;
+  const int64_t e0 = in ? ((int64_t)(iz + 1) * n1 + (iy + 1)) * n1 + (ix + 1) : 0;
+  const int64_t e1 = e0 + (int64_t)n1 * n1;
+  const float4 a0 = __ldg(q + 2 * e0), a1 = __ldg(q + 2 * e0 + 1);
+  const float4 b0 = __ldg(q + 2 * e1), b1 = __ldg(q + 2 * e1 + 1);
+  const float2 v[8] = {make_float2(a0.x, a0.y), make_float2(a0.z, a0.w), make_float2(a1.x, a1.y),
+                       make_float2(a1.z, a1.w), make_float2(b0.x, b0.y), make_float2(b0.z, b0.w),
+                       make_float2(b1.x, b1.y), make_float2(b1.z, b1.w)};
   float ar = 0.f, ai = 0.f;
+  if (in) {
 #pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    const float w = wz[c >> 2] * wy[(c >> 1) & 1] * wx[c & 1];
-    ar += w * q[c].x;
-    ai += w * q[c].y;
+    for (int c = 0; c < 8; ++c) {
+      const int dz = c >> 2, dy = (c >> 1) & 1, dx = c & 1;
+      const float w = (dz ? fz : 1.f - fz) * (dy ? fy : 1.f - fy) * (dx ? fx : 1.f - fx);
+      ar += w * v[c].x;
+      ai += w * v[c].y;
+    }
   }
   return make_float2(ar, ai);
 }
@@ -483,6 +506,7 @@ patch_fft_xy64_kernel(const float* __restrict__ vol, const float* __restrict__ s
   }
   constexpr int P4 = N * N / 4;
   float4* pl4 = reinterpret_cast<float4*>(P0);
+#pragma unroll 4
   for (int e = threadIdx.x; e < 2 * P4; e += kT64) {
     const int hi = e >= P4 ? 1 : 0;
     const int zz = iz + hi;
@@ -576,7 +600,7 @@ constexpr size_t xy64_smem_bytes() {
 template <bool SPLIT>
 __global__ void __launch_bounds__(kT64, 4)
 fft_z64_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ what, const float* __restrict__ bg,
-               const float2* __restrict__ ref, const float* __restrict__ rot, const float* __restrict__ ctf,
+               const float4* __restrict__ refq, const float* __restrict__ rot, const float* __restrict__ ctf,
                float* __restrict__ nrm, uint32_t* __restrict__ a1, int a1_ws, int a1_R) {
   constexpr int N = 64, HN = 32, H = 33;
   extern __shared__ __align__(16) float2 sm2[];
@@ -589,6 +613,7 @@ fft_z64_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ w
   const float2* wb = what + (int64_t)jp * H;
   const float avg = g.wsum > 0.f ? __ldg(&bg[b]) / g.wsum : 0.f;
   load_twiddles64(tw);
+#pragma unroll 4
   for (int e = threadIdx.x; e < N * H; e += kT64) {
     const int ip = e / H, m2 = e - (e / H) * H;
     const float2 t = base[(int64_t)ip * N * H + m2];
@@ -610,14 +635,18 @@ fft_z64_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ w
     const int kp = ip < HN ? ip : ip - N;
     const int jq = jp < HN ? jp : jp - N;
     const int xq = m2 < HN ? m2 : m2 - H;
-    float2 s = make_float2(0.f, 0.f);
-    if (kp * kp + jq * jq + xq * xq <= g.mask_r2) {
+    // outside the mask the sample is taken far outside the box, which reads zero (entry 0)
+    const bool in_mask = kp * kp + jq * jq + xq * xq <= g.mask_r2;
+    float2 s;
+    {
       const int zo = (ip + HN) & (N - 1), yo = (jp + HN) & (N - 1), xw = m2 + HN;
       const float bx = (float)xw - c, by = (float)yo - c, bz = (float)zo - c;
       const float rx = R[0] * bx + R[1] * by + R[2] * bz + c;
       const float ry = R[3] * bx + R[4] * by + R[5] * bz + c;
-      const float rz = R[6] * bx + R[7] * by + R[8] * bz + c;
-      s = trilinear_c_nb(ref, N, rz, ry, rx);
+      const float rz = in_mask ? R[6] * bx + R[7] * by + R[8] * bz + c : -4.f;
+      s = trilinear_quad(refq, N, rz, ry, rx);
+    }
+    if (in_mask) {
       if (ctf) {
         const float cv = __ldg(&ctf[(((int64_t)b * N + ip) * N + jp) * H + m2]);
         s.x *= cv;
@@ -813,6 +842,7 @@ struct mtb_shift {
   float* fill_tab; // fill weight W by integer squared radius (device formula)
   float2* what;    // (N, N, N/2+1) plane transforms of the fill weight W / N^3
   float2* ref;     // (N, N, N) Fourier reference, fftshifted and masked
+  float4* refq;    // box 64: corner quads of ref, (N + 2) (N + 1)^2 x 32 bytes
   float2* E0;      // (U, N)
   float2* E1;      // (U, N)
   float2* E2;      // (U, H)
@@ -867,11 +897,11 @@ int shift_front_64(mtb_shift* h, const float* subtomos, const float* shift_zyx, 
   MTB_LAUNCH_CHECK();
   if (h->use_tc) {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
-    fft_z64_kernel<true><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm,
+    fft_z64_kernel<true><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
                                                          (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1);
   } else {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
-    fft_z64_kernel<false><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm, nullptr,
+    fft_z64_kernel<false><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm, nullptr,
                                                           0, 0);
   }
   MTB_LAUNCH_CHECK();
@@ -966,6 +996,7 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
       !alloc((void**)&h->T, B * N * N * g.H * 8) || !alloc((void**)&h->X1, B * g.U * N * g.H * 8) ||
       !alloc((void**)&h->pval, B * h->ngrp * 4) || !alloc((void**)&h->pidx, B * h->ngrp * 4))
     return fail(MTB_ERR_OOM);
+  if (N == 64 && !alloc((void**)&h->refq, (size_t)(N + 2) * (N + 1) * (N + 1) * 32)) return fail(MTB_ERR_OOM);
   if (cudaMemcpy(h->bgw_tab, wtab.data(), wtab.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->E0, e0.data(), e0.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->E1, e0.data(), e0.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -989,7 +1020,7 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
 extern "C" void mtb_shift_destroy(mtb_shift* h) {
   if (!h) return;
   shift_tc_release(&h->tc);
-  void* ptrs[] = {h->bgw_tab, h->fill_tab, h->what, h->ref, h->E0, h->E1, h->E2, h->bg, h->nrm, h->T, h->X1, h->pval, h->pidx};
+  void* ptrs[] = {h->bgw_tab, h->fill_tab, h->what, h->refq, h->ref, h->E0, h->E1, h->E2, h->bg, h->nrm, h->T, h->X1, h->pval, h->pidx};
   for (void* p : ptrs) if (p) cudaFree(p);
   delete h;
 }
@@ -1009,6 +1040,10 @@ extern "C" int mtb_shift_set_reference(mtb_shift* h, const float* ref_fourier, m
   MTB_ARG_CHECK(h && ref_fourier, "null argument");
   const size_t n = (size_t)h->g.N * h->g.N * h->g.N;
   MTB_CUDA_TRY(cudaMemcpyAsync(h->ref, ref_fourier, n * 8, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  if (h->refq) {
+    ref_quad_kernel<<<1024, 256, 0, (cudaStream_t)stream>>>(h->ref, h->g.N, h->refq);
+    MTB_LAUNCH_CHECK();
+  }
   h->has_ref = true;
   return MTB_OK;
 }
