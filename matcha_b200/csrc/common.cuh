@@ -37,6 +37,30 @@ __device__ __forceinline__ float warp_sum(float v) {
   return v;
 }
 
+// Round a finite float to the nearest bf16 (ties to even) with integer operations, which keeps
+// the split below off the conversion unit; the bf16 bits are returned in the low half.
+__device__ __forceinline__ uint32_t bf16_bits_rne(float x) {
+  const uint32_t u = __float_as_uint(x);
+  return (u + 0x7FFFu + ((u >> 16) & 1u)) >> 16;
+}
+
+// BF16 hi + lo split of x: hi = bf16(x), lo = bf16(x - hi).
+__device__ __forceinline__ void split_bf16(float x, uint32_t& hi, uint32_t& lo) {
+  hi = bf16_bits_rne(x);
+  lo = bf16_bits_rne(x - __uint_as_float(hi << 16));
+}
+
+// The same for a complex value, packed as bf16 pairs (real part in the low half), with the
+// paired round-to-nearest-even conversion (cvt.rn.bf16x2.f32).
+__device__ __forceinline__ void split_bf16x2(float re, float im, uint32_t& hi, uint32_t& lo) {
+  uint32_t h, l;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(h) : "f"(im), "f"(re));
+  const float rr = re - __uint_as_float(h << 16), ri = im - __uint_as_float(h & 0xFFFF0000u);
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(l) : "f"(ri), "f"(rr));
+  hi = h;
+  lo = l;
+}
+
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }

@@ -206,10 +206,10 @@ __global__ void fold_split_kernel(const float* __restrict__ vol, int64_t vol_str
       }
 #pragma unroll
   for (int p = 0; p < 8; ++p) {
-    const __nv_bfloat16 hi = __float2bfloat16_rn(f[p]);
-    const __nv_bfloat16 lo = __float2bfloat16_rn(f[p] - __bfloat162float(hi));
-    A[((int64_t)(p * 2 + 0) * Mpad + b) * Kpad + rep] = hi;
-    A[((int64_t)(p * 2 + 1) * Mpad + b) * Kpad + rep] = lo;
+    uint32_t hi, lo;
+    split_bf16(f[p], hi, lo);
+    A[((int64_t)(p * 2 + 0) * Mpad + b) * Kpad + rep] = __ushort_as_bfloat16((unsigned short)hi);
+    A[((int64_t)(p * 2 + 1) * Mpad + b) * Kpad + rep] = __ushort_as_bfloat16((unsigned short)lo);
   }
 }
 
@@ -227,10 +227,10 @@ __global__ void basis_split_kernel(const float* __restrict__ basis, int n_rep, i
     const int n = n0 + i, k = k0 + threadIdx.x;
     if (n >= Npad || k >= Kpad) continue;
     const float v = tile[threadIdx.x][i];
-    const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-    const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
-    Bm[((int64_t)(cls * 2 + 0) * Npad + n) * Kpad + k] = hi;
-    Bm[((int64_t)(cls * 2 + 1) * Npad + n) * Kpad + k] = lo;
+    uint32_t hi, lo;
+    split_bf16(v, hi, lo);
+    Bm[((int64_t)(cls * 2 + 0) * Npad + n) * Kpad + k] = __ushort_as_bfloat16((unsigned short)hi);
+    Bm[((int64_t)(cls * 2 + 1) * Npad + n) * Kpad + k] = __ushort_as_bfloat16((unsigned short)lo);
   }
 }
 

@@ -314,12 +314,13 @@ constexpr size_t xy_smem_bytes() {
 // along z, then P = conj(S) T with the rotated, ifftshifted, masked Fourier reference S
 // sampled on the fly, and the norms |T|^2, |S|^2 per subtomogram.  Without SPLIT P overwrites
 // T; with SPLIT the pass-1 operand of the tensor-core upsampled DFT is written instead,
-// A1[part][(b, m2, m1)][2 m0 + c] as bf16 hi/lo pairs (a1_ws pairs per row, a1_R rows per part).
+// A1[part][(b, m2, m1)][2 m0 + c] for m2 < N/2 as bf16 hi/lo pairs (a1_ws pairs per row, a1_R
+// rows per part), and the Nyquist plane m2 = N/2 in FP32 to p32[b][m1][m0].
 template <int N, bool SPLIT>
 __global__ void __launch_bounds__(kT)
 fft_z_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ what, const float* __restrict__ bg,
              const float2* __restrict__ ref, const float* __restrict__ rot, const float* __restrict__ ctf,
-             float* __restrict__ nrm, uint32_t* __restrict__ a1, int a1_ws, int a1_R) {
+             float* __restrict__ nrm, uint32_t* __restrict__ a1, int a1_ws, int a1_R, float2* __restrict__ p32) {
   constexpr int HN = N / 2, H = N / 2 + 1;
   extern __shared__ __align__(16) float2 sm2[];
   __shared__ float red[32];
@@ -371,12 +372,15 @@ fft_z_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ wha
     // conj(s) * t
     const float2 p = make_float2(s.x * t.x + s.y * t.y, s.x * t.y - s.y * t.x);
     if (SPLIT) {
-      const __nv_bfloat16 rh = __float2bfloat16_rn(p.x), ih = __float2bfloat16_rn(p.y);
-      const __nv_bfloat162 hi = __halves2bfloat162(rh, ih);
-      const __nv_bfloat162 lo = __floats2bfloat162_rn(p.x - __bfloat162float(rh), p.y - __bfloat162float(ih));
-      const size_t row = ((size_t)b * H + m2) * N + jp;
-      a1[row * a1_ws + ip] = *reinterpret_cast<const uint32_t*>(&hi);
-      a1[((size_t)a1_R + row) * a1_ws + ip] = *reinterpret_cast<const uint32_t*>(&lo);
+      if (m2 < HN) {
+        uint32_t hi, lo;
+        split_bf16x2(p.x, p.y, hi, lo);
+        const size_t row = ((size_t)b * HN + m2) * N + jp;
+        a1[row * a1_ws + ip] = hi;
+        a1[((size_t)a1_R + row) * a1_ws + ip] = lo;
+      } else {
+        p32[((size_t)b * N + jp) * N + ip] = p;  // the Nyquist plane m2 = N/2, FP32
+      }
     } else {
       base[(int64_t)ip * N * H + m2] = p;
     }
@@ -601,7 +605,7 @@ template <bool SPLIT>
 __global__ void __launch_bounds__(kT64, 4)
 fft_z64_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ what, const float* __restrict__ bg,
                const float4* __restrict__ refq, const float* __restrict__ rot, const float* __restrict__ ctf,
-               float* __restrict__ nrm, uint32_t* __restrict__ a1, int a1_ws, int a1_R) {
+               float* __restrict__ nrm, uint32_t* __restrict__ a1, int a1_ws, int a1_R, float2* __restrict__ p32) {
   constexpr int N = 64, HN = 32, H = 33;
   extern __shared__ __align__(16) float2 sm2[];
   __shared__ float red[32];
@@ -657,12 +661,15 @@ fft_z64_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ w
     ss += s.x * s.x + s.y * s.y;
     const float2 p = make_float2(s.x * t.x + s.y * t.y, s.x * t.y - s.y * t.x);
     if (SPLIT) {
-      const __nv_bfloat16 rh = __float2bfloat16_rn(p.x), ih = __float2bfloat16_rn(p.y);
-      const __nv_bfloat162 hi = __halves2bfloat162(rh, ih);
-      const __nv_bfloat162 lo = __floats2bfloat162_rn(p.x - __bfloat162float(rh), p.y - __bfloat162float(ih));
-      const size_t row = ((size_t)b * H + m2) * N + jp;
-      a1[row * a1_ws + ip] = *reinterpret_cast<const uint32_t*>(&hi);
-      a1[((size_t)a1_R + row) * a1_ws + ip] = *reinterpret_cast<const uint32_t*>(&lo);
+      if (m2 < HN) {
+        uint32_t hi, lo;
+        split_bf16x2(p.x, p.y, hi, lo);
+        const size_t row = ((size_t)b * HN + m2) * N + jp;
+        a1[row * a1_ws + ip] = hi;
+        a1[((size_t)a1_R + row) * a1_ws + ip] = lo;
+      } else {
+        p32[((size_t)b * N + jp) * N + ip] = p;  // the Nyquist plane m2 = N/2, FP32
+      }
     } else {
       base[(int64_t)ip * N * H + m2] = p;
     }
@@ -878,11 +885,11 @@ int shift_front_n(mtb_shift* h, const float* subtomos, const float* shift_zyx, c
   if (h->use_tc) {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
     fft_z_kernel<N, true><<<dim3(N, B), kT, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm,
-                                                       (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1);
+                                                       (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1, h->tc.p32);
   } else {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
     fft_z_kernel<N, false><<<dim3(N, B), kT, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm, nullptr,
-                                                        0, 0);
+                                                        0, 0, nullptr);
   }
   MTB_LAUNCH_CHECK();
   return MTB_OK;
@@ -898,11 +905,11 @@ int shift_front_64(mtb_shift* h, const float* subtomos, const float* shift_zyx, 
   if (h->use_tc) {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
     fft_z64_kernel<true><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
-                                                         (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1);
+                                                         (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1, h->tc.p32);
   } else {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
     fft_z64_kernel<false><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm, nullptr,
-                                                          0, 0);
+                                                          0, 0, nullptr);
   }
   MTB_LAUNCH_CHECK();
   return MTB_OK;
@@ -1006,11 +1013,13 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
   if (cudaGetLastError() != cudaSuccess) return fail(MTB_ERR_CUDA);
   if (shift_front(h, nullptr, nullptr, nullptr, nullptr, 0, 0) != MTB_OK) return fail(MTB_ERR_CUDA);
   if (cudaStreamSynchronize(0) != cudaSuccess) return fail(MTB_ERR_CUDA);
-  if (cfg->precision == MTB_SHIFT_BF16X3) {
+  // BF16X3 on a geometry the tensor-core kernels do not cover (box 128, or an upsampled region
+  // past their tensor/shared memory budget) runs the FP32 CUDA-core kernels instead
+  if (cfg->precision == MTB_SHIFT_BF16X3 && shift_tc_fits(N, g.U) == MTB_OK) {
     const int rc = shift_tc_prepare(&h->tc, N, g.H, g.U, cfg->upsample_factor, g.dftshift, cfg->max_batch);
     if (rc) return fail(rc);
     h->use_tc = true;
-  } else if (cfg->precision != MTB_SHIFT_FP32) {
+  } else if (cfg->precision != MTB_SHIFT_FP32 && cfg->precision != MTB_SHIFT_BF16X3) {
     return fail(MTB_ERR_ARG);
   }
   *out = h;

@@ -2,16 +2,24 @@
 //
 // The refined correlation of src/matcha/core/ShiftMatcher.py:46-91, 241-272,
 //   V[u0,u1,u2] = Re sum_{m0,m1,m2} P[m0,m1,m2] E0[u0,m0] E0[u1,m1] E2[u2,m2],
-// E[u,m] = exp(+2 pi i (u - dftshift) fftfreq(n, uf)[m]), is computed as three GEMMs whose
-// complex products are real GEMMs on interleaved (re, im) K axes:
-//   pass 1  rows (b, m2, m1),  K = (m0, re/im) = 2N,    N-tile = (u0, re/im) = 2U
-//   pass 2  rows (b, u0, m2),  K = (m1, re/im) = 2N,    N-tile = (u1, re/im) = 2U
-//   pass 3  rows (b, u0, u1),  K = (m2, re/im) = 2H -> padded to 2N, N-tile = u2 (real part)
-// Each pass's epilogue writes the next pass's A operand directly in its K-major bf16 hi/lo
-// layout (no transpose kernel), and pass 3 keeps a running argmax per subtomogram in a
-// 64-bit key (ordered value, inverted flat index), so the U^3 grid never reaches memory.
-// Operands are split A = A_hi + A_lo, B = B_hi + B_lo; A B ~ A_hi B_hi + A_lo B_hi + A_hi B_lo
-// is one GEMM over three K segments.  All device waits are bounded.
+// E[u,m] = exp(+2 pi i (u - dftshift) fftfreq(n, uf)[m]), m2 < H = N/2 + 1, is split into the
+// planes m2 < N/2 (tensor cores) and the Nyquist plane m2 = N/2 (FP32 CUDA cores):
+//   nyquist  Y[u0,u1] = sum_{m0,m1} E0[u0,m0] E0[u1,m1] P[m0,m1,N/2]        (nyq_kernel)
+//   pass 1   rows (b, m2, m1), K = (m0, re/im) = 2N, N-tile = (u0, re/im) = 2U   (X1 -> A2)
+//   pass 2   rows (b, u0, m2), K = (m1, re/im) = 2N, N-tile = (u1, re/im) = 2U   (X2)
+//   pass 3   rows (b, u0, u1), K = (m2, re/im) = N,  N-tile = u2 (real part), + Re(Y E2[u2, N/2])
+// Complex products are real GEMMs on interleaved (re, im) K axes.  Operands are split
+// A = A_hi + A_lo, B = B_hi + B_lo and A B ~ A_hi B_hi + A_lo B_hi + A_hi B_lo.
+//
+// Both kernels are persistent (one CTA per SM) with their B operands resident in shared
+// memory.  Pass 1 double-buffers its accumulator in tensor memory, so the epilogue that
+// writes the pass-2 operand A2 (K-major bf16 hi/lo) overlaps the next tile's MMAs.  Passes 2
+// and 3 are fused: a tile is G = 128 / (N/2) consecutive u0 of one subtomogram with all their
+// m2 < N/2, so its pass-2 accumulator holds complete X2[u0, u1, :] rows; the epilogue writes
+// them as the pass-3 A operand straight into shared memory (the 128-byte-swizzled K-major
+// layout the tensor core reads), 128 (u0, u1) rows at a time, and the pass-3 accumulators
+// are reduced to a running argmax key per subtomogram.  Neither X2 nor the U^3 grid reaches
+// memory.  All device waits are bounded; a wait that runs out sets err and the CTA winds down.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <math.h>
@@ -27,31 +35,36 @@ namespace {
 using namespace tc;
 
 constexpr int TM = 128, TK = 64;
-constexpr int kStages = 2;
-constexpr int kThreads = 192;
-constexpr uint32_t kTmemCols = 256;
+constexpr int kThreads = 320;        // warp 0 TMA, warp 1 MMA + TMEM, warps 2-9 epilogue
+constexpr int kEpi = 256;            // epilogue threads: two warps per 32-lane quarter of TMEM
+constexpr int A_TILE = TM * TK * 2;  // one 128 x 64 bf16 K-block
+constexpr int kMaxStages = 8;
+constexpr size_t kSmemCap = 227 * 1024;
 
-struct UParams {
-  int KB;         // 64-element K blocks of A and B
-  int KBo;        // 64-element K blocks of the output operand (passes 1, 2)
-  int R;          // rows per part of A (padded)
-  int rows;       // valid rows (B * rows per subtomogram)
-  int rpb;        // rows per subtomogram
-  int N, H, U;
-  int R_out;      // rows per part of the output operand (passes 1, 2)
-  int rpb_out;    // rows per subtomogram of the output operand
+struct Pass1 {
+  int rows;     // valid rows B * N/2 * N
+  int tiles;
+  int N, HH, U;
+  int KB;       // K blocks of A1 and E1 (2N / 64)
+  int R1, R2;   // rows per part of A1 and A2
+  int NT;       // N-tile 2U rounded to 16
+  int stages;
 };
 
-__device__ __forceinline__ uint32_t pack_bf16x2(float lo_elem, float hi_elem) {
-  // first element in the low half
-  const __nv_bfloat162 v = __floats2bfloat162_rn(lo_elem, hi_elem);
-  return *reinterpret_cast<const uint32_t*>(&v);
+struct Pass23 {
+  int B, tiles;  // tiles = B * TPB
+  int N, HH, U, G, TPB, CH;
+  int KB;        // K blocks of A2 and E1
+  int R2;
+  int NT12, NT3;
+};
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void split2(float re, float im, uint32_t& hi, uint32_t& lo) {
-  const __nv_bfloat16 rh = __float2bfloat16_rn(re), ih = __float2bfloat16_rn(im);
-  hi = pack_bf16x2(__bfloat162float(rh), __bfloat162float(ih));
-  lo = pack_bf16x2(re - __bfloat162float(rh), im - __bfloat162float(ih));
+  split_bf16x2(re, im, hi, lo);
 }
 
 __device__ __forceinline__ unsigned long long argmax_key(float v, int flat) {
@@ -60,197 +73,633 @@ __device__ __forceinline__ unsigned long long argmax_key(float v, int flat) {
   return ((unsigned long long)b << 32) | (unsigned long long)(0xFFFFFFFFu - (uint32_t)flat);
 }
 
-template <int NT>
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* out) {
-  uint32_t v[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) out[i] = __uint_as_float(v[i]);
+// Split issue / wait of a 16-column TMEM load, for software pipelining: the wait names the
+// destination registers as in-out operands, so no use of them can move above it.
+__device__ __forceinline__ void tmem_issue16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+               : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait16(uint32_t (&r)[16]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+               :
+               : "memory");
 }
 
-// MODE 1: pass 1 -> A2; MODE 2: pass 2 -> A3; MODE 3: pass 3 -> argmax keys.
-template <int NT, int MODE>
+// f(r, c) for the 16-column groups c = c0, c0 + 16, .. < c1 of this warp's lanes at TMEM
+// address base + c, with the load of the next group in flight while f runs.  c0, c1 must be
+// warp-uniform.
+template <class F>
+__device__ __forceinline__ void tmem_for_groups(uint32_t base, int c0, int c1, F&& f) {
+  uint32_t ra[16], rb[16];
+  if (c0 >= c1) return;
+  tmem_issue16(base + (uint32_t)c0, ra);
+  for (int c = c0; c < c1; c += 32) {
+    tmem_wait16(ra);
+    const bool more = c + 16 < c1;
+    if (more) tmem_issue16(base + (uint32_t)(c + 16), rb);
+    f(ra, c);
+    if (more) {
+      tmem_wait16(rb);
+      if (c + 32 < c1) tmem_issue16(base + (uint32_t)(c + 32), ra);
+      f(rb, c + 16);
+    }
+  }
+}
+
+__device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
+  return reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~uintptr_t(1023));
+}
+
+// Three-segment hi/lo MMA over one 64-wide K block (four K steps of 16).
+__device__ __forceinline__ void mma_split_kblock(uint32_t d, uint64_t a_hi, uint64_t a_lo, uint64_t b_hi,
+                                                 uint64_t b_lo, uint32_t idesc, bool first) {
+#pragma unroll
+  for (int kk = 0; kk < TK / 16; ++kk) {
+    const uint64_t o = (uint64_t)(kk * 2);
+    mma_bf16_id(d, a_hi + o, b_hi + o, idesc, (first && kk == 0) ? 0u : 1u);
+    mma_bf16_id(d, a_lo + o, b_hi + o, idesc, 1u);
+    mma_bf16_id(d, a_hi + o, b_lo + o, idesc, 1u);
+  }
+}
+
+// Epilogue helpers over NC TMEM columns already in registers.  The per-value work is
+// unconditional so it can be interleaved; only the stores are predicated.
+
+// Pass 1: columns (u0, re/im) of one A1 row -> A2 words (m1) of rows (b, u0, m2).
+template <int NC>
+__device__ __forceinline__ void epi1_group(const uint32_t* v, int cb, bool valid, int U, size_t row0, int HH,
+                                           size_t ws, int m1, size_t R2, uint32_t* __restrict__ out) {
+#pragma unroll
+  for (int t = 0; t < NC / 2; ++t) {
+    uint32_t hi, lo;
+    split2(__uint_as_float(v[2 * t]), __uint_as_float(v[2 * t + 1]), hi, lo);
+    const int u0 = cb / 2 + t;
+    const size_t row = row0 + (size_t)u0 * HH;
+    if (valid && u0 < U) {
+      out[row * ws + m1] = hi;
+      out[(R2 + row) * ws + m1] = lo;
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t sw128_word(int r, int w);
+
+// Passes 2 + 3: columns (u1, re/im) of one pass-2 row (u0_local, m2) -> word m2 of the pass-3
+// operand rows rbase + u1 that fall in this chunk.
+template <int NC>
+__device__ __forceinline__ void epi2_group(const uint32_t* v, int cb, int lo_l, int hi_l, int rbase, int m2,
+                                           uint8_t* sA3) {
+#pragma unroll
+  for (int t = 0; t < NC / 2; ++t) {
+    uint32_t hi, lo;
+    split2(__uint_as_float(v[2 * t]), __uint_as_float(v[2 * t + 1]), hi, lo);
+    const int u1 = cb / 2 + t;
+    const uint32_t off = sw128_word(rbase + u1, m2);
+    if (u1 >= lo_l && u1 < hi_l) {
+      *reinterpret_cast<uint32_t*>(sA3 + off) = hi;
+      *reinterpret_cast<uint32_t*>(sA3 + A_TILE + off) = lo;
+    }
+  }
+}
+
+__device__ __forceinline__ float fmax_nan(float a, float b) {
+  float d;
+  asm("max.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+  return d;
+}
+
+// Pass 3: running argmax over NC values u2 = cb .. cb + NC - 1 of one row (flat index
+// row_flat * U + u2).  Four independent chains keep (value, index) with a strict comparison,
+// so each keeps its first maximum; they are merged by value, then by index.  NaN is detected
+// by a NaN-propagating maximum and, when present (rare), located by a rescan
+// (torch.argmax order: NaN above everything, the first index wins ties).
+template <int NC>
+__device__ __forceinline__ void scan_group(const uint32_t* vr, int cb, int U, int row_flat, float& bv, int& bi,
+                                           bool& have) {
+  float v[NC];
+#pragma unroll
+  for (int t = 0; t < NC; ++t) v[t] = __uint_as_float(vr[t]);
+  if (cb + NC > U) {
+#pragma unroll
+    for (int t = 0; t < NC; ++t) v[t] = (cb + t < U) ? v[t] : -INFINITY;
+  }
+  float m4[4] = {v[0], v[1], v[2], v[3]};
+  int i4[4] = {0, 1, 2, 3};
+  float n4[2] = {v[0], v[1]};
+#pragma unroll
+  for (int t = 4; t < NC; ++t) {
+    const bool gt = v[t] > m4[t & 3];
+    m4[t & 3] = gt ? v[t] : m4[t & 3];
+    i4[t & 3] = gt ? t : i4[t & 3];
+  }
+#pragma unroll
+  for (int t = 2; t < NC; ++t) n4[t & 1] = fmax_nan(n4[t & 1], v[t]);
+  if (bv != bv) return;  // a NaN was found earlier: nothing later wins
+  const float nn = fmax_nan(n4[0], n4[1]);
+  if (nn != nn) {
+    int tb = 0;
+#pragma unroll
+    for (int t = NC - 1; t >= 0; --t)
+      if (v[t] != v[t]) tb = t;
+    bv = nn;
+    bi = row_flat * U + cb + tb;
+    have = true;
+    return;
+  }
+  float m = m4[0];
+  int im = i4[0];
+#pragma unroll
+  for (int c = 1; c < 4; ++c) {
+    const bool take = m4[c] > m || (m4[c] == m && i4[c] < im);
+    m = take ? m4[c] : m;
+    im = take ? i4[c] : im;
+  }
+  if (!have || m > bv) {
+    bv = m;
+    bi = row_flat * U + cb + im;
+    have = true;
+  }
+}
+
+// ------------------------------------------------------------------ pass 1
+// Rows (b, m2, m1) of A1 times E1 -> X1[u0] for the tile's rows, written as A2 rows
+// (b, u0, m2) with K (m1, re/im), bf16 hi and lo parts.
 __global__ void __launch_bounds__(kThreads, 1)
-updft_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, UParams P,
-                uint32_t* __restrict__ out, unsigned long long* __restrict__ best, int* __restrict__ err) {
-  constexpr int A_TILE = TM * TK * 2;
-  constexpr int B_TILE = NT * TK * 2;
-  constexpr int STAGE = A_TILE + B_TILE;
-  const int KB = P.KB;
-  const int KB3 = 3 * KB;  // with the hi/lo split
-  constexpr uint32_t IDESC = idesc_bf16(TM, NT);
+updft1_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, Pass1 p,
+                 uint32_t* __restrict__ out, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  __shared__ __align__(8) uint64_t full_bar[kStages];
-  __shared__ __align__(8) uint64_t empty_bar[kStages];
-  __shared__ __align__(8) uint64_t done_bar;
+  uint8_t* smem = align1024(smem_raw);
+  const int KB = p.KB, S = p.stages, NT = p.NT;
+  const int B_BLK = NT * TK * 2;
+  uint8_t* sB = smem;                    // [part][kb] B_BLK
+  uint8_t* sA = smem + 2 * KB * B_BLK;   // [stage][part] A_TILE
+  __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages];
+  __shared__ __align__(8) uint64_t accF[2], accE[2], resF;
   __shared__ uint32_t tmem_base;
   __shared__ volatile int abort_flag;
-
-  const int row0 = blockIdx.x * TM;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < S; ++s) {
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
     }
-    mbar_init(&done_bar, 1);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&accF[i], 1);
+      mbar_init(&accE[i], kEpi);
+    }
+    mbar_init(&resF, 1);
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
-                 "r"(kTmemCols));
+                 "r"(512));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
+  const uint32_t idesc = idesc_bf16(TM, NT);
 
   if (warp == 0 && lane == 0) {
-    for (int j = 0; j < KB3; ++j) {
-      const int s = j % kStages;
-      const uint32_t use = j / kStages;
-      if (j >= kStages && !mbar_wait(&empty_bar[s], (use - 1) & 1)) {
-        atomicExch(err, 11);
-        abort_flag = 1;
-        break;
+    mbar_expect_tx(&resF, (uint32_t)(2 * KB * B_BLK));
+    for (int part = 0; part < 2; ++part)
+      for (int kb = 0; kb < KB; ++kb)
+        tma_load_2d(sB + (part * KB + kb) * B_BLK, &mapB, kb * TK, part * NT, &resF);
+    int it = 0;
+    for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x) {
+      for (int kb = 0; kb < KB; ++kb, ++it) {
+        const int s = it % S;
+        const uint32_t use = it / S;
+        if (it >= S && !mbar_wait(&empty_bar[s], (use - 1) & 1)) {
+          atomicExch(err, 21);
+          abort_flag = 1;
+          break;
+        }
+        uint8_t* sa = sA + s * 2 * A_TILE;
+        mbar_expect_tx(&full_bar[s], 2 * A_TILE);
+        tma_load_2d(sa, &mapA, kb * TK, tile * TM, &full_bar[s]);
+        tma_load_2d(sa + A_TILE, &mapA, kb * TK, p.R1 + tile * TM, &full_bar[s]);
       }
-      if (abort_flag) break;
-      const int part = j / KB, kb = j - part * KB;
-      const int ap = (part == 1) ? 1 : 0, bp = (part == 2) ? 1 : 0;
-      uint8_t* sa = smem + s * STAGE;
-      mbar_expect_tx(&full_bar[s], STAGE);
-      tma_load_2d(sa, &mapA, kb * TK, ap * P.R + row0, &full_bar[s]);
-      tma_load_2d(sa + A_TILE, &mapB, kb * TK, bp * NT, &full_bar[s]);
     }
   } else if (warp == 1 && lane == 0) {
-    bool ok = true;
-    for (int j = 0; j < KB3; ++j) {
-      const int s = j % kStages;
-      const uint32_t use = j / kStages;
-      if (!mbar_wait(&full_bar[s], use & 1)) {
-        atomicExch(err, 12);
+    bool ok = mbar_wait(&resF, 0);
+    if (!ok) {
+      atomicExch(err, 22);
+      abort_flag = 1;
+    }
+    int it = 0, tl = 0;
+    for (int tile = blockIdx.x; ok && tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
+      const int buf = tl & 1;
+      if (tl >= 2 && !mbar_wait(&accE[buf], ((tl >> 1) - 1) & 1)) {
+        atomicExch(err, 23);
         abort_flag = 1;
-        ok = false;
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint8_t* sa = smem + s * STAGE;
-      const uint64_t ad = smem_desc(sa), bd = smem_desc(sa + A_TILE);
-#pragma unroll
-      for (int kk = 0; kk < TK / 16; ++kk)
-        mma_bf16_id(tmem, ad + (uint64_t)(kk * 2), bd + (uint64_t)(kk * 2), IDESC, (j > 0 || kk > 0) ? 1u : 0u);
-      mma_commit_to(&empty_bar[s]);
-    }
-    if (ok) mma_commit_to(&done_bar);
-  } else if (warp >= 2) {
-    const bool ok = mbar_wait(&done_bar, 0);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!ok) {
-      atomicExch(err, 13);
-    } else {
-      const int q = warp & 3;
-      const int g = row0 + q * 32 + lane;  // global row
-      const bool valid = g < P.rows;
-      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16);
-      const int b = valid ? g / P.rpb : 0;
-      const int rem = valid ? g - b * P.rpb : 0;
-      if (MODE == 1) {
-        // row (b, m2, m1): write A2[part][b, u0, m2][2 m1 + c]
-        const int m2 = rem / P.N, m1 = rem - m2 * P.N;
-        const size_t base_row = (size_t)b * P.rpb_out + m2;  // + u0 * H
-        const size_t ws = (size_t)P.KBo * (TK / 2);           // row stride in bf16 pairs
-#pragma unroll 1
-        for (int cb = 0; cb < NT; cb += 16) {
-          float v[16];
-          tmem_ld16<NT>(taddr + (uint32_t)cb, v);
-          if (valid) {
-#pragma unroll
-            for (int t = 0; t < 8; ++t) {
-              const int u0 = cb / 2 + t;
-              if (u0 >= P.U) break;
-              uint32_t hi, lo;
-              split2(v[2 * t], v[2 * t + 1], hi, lo);
-              const size_t row = base_row + (size_t)u0 * P.H;
-              out[row * ws + m1] = hi;
-              out[((size_t)P.R_out + row) * ws + m1] = lo;
-            }
-          }
+      const uint32_t d = tmem + (uint32_t)(buf * 256);
+      for (int kb = 0; kb < KB; ++kb, ++it) {
+        const int s = it % S;
+        const uint32_t use = it / S;
+        if (!mbar_wait(&full_bar[s], use & 1)) {
+          atomicExch(err, 24);
+          abort_flag = 1;
+          ok = false;
+          break;
         }
-      } else if (MODE == 2) {
-        // row (b, u0, m2): write A3[part][b, u0, u1][2 m2 + c]
-        const int u0 = rem / P.H, m2 = rem - u0 * P.H;
-        const size_t base_row = (size_t)b * P.rpb_out + (size_t)u0 * P.U;  // + u1
-        const size_t ws = (size_t)P.KBo * (TK / 2);
-#pragma unroll 1
-        for (int cb = 0; cb < NT; cb += 16) {
-          float v[16];
-          tmem_ld16<NT>(taddr + (uint32_t)cb, v);
-          if (valid) {
-#pragma unroll
-            for (int t = 0; t < 8; ++t) {
-              const int u1 = cb / 2 + t;
-              if (u1 >= P.U) break;
-              uint32_t hi, lo;
-              split2(v[2 * t], v[2 * t + 1], hi, lo);
-              const size_t row = base_row + u1;
-              out[row * ws + m2] = hi;
-              out[((size_t)P.R_out + row) * ws + m2] = lo;
-            }
-          }
-        }
-      } else {
-        // row (b, u0, u1): running argmax over u2 < U, flat = rem * U + u2
-        float bv = -INFINITY;
-        int bi = 0x7fffffff;
-        bool have = false;
-#pragma unroll 1
-        for (int cb = 0; cb < NT; cb += 16) {
-          float v[16];
-          tmem_ld16<NT>(taddr + (uint32_t)cb, v);
-#pragma unroll
-          for (int t = 0; t < 16; ++t) {
-            const int u2 = cb + t;
-            if (u2 < P.U) {
-              const float x = v[t];
-              const bool nan_x = isnan(x);
-              if (!have || (nan_x && !isnan(bv)) || (!isnan(bv) && x > bv)) {
-                bv = x;
-                bi = u2;
-                have = true;
-              }
-            }
-          }
-        }
-        unsigned long long key = valid ? argmax_key(bv, rem * P.U + bi) : 0ull;
-        // combine lanes of the same subtomogram before the atomic
-        const int b0 = __shfl_sync(0xffffffffu, b, 0);
-        const bool uniform = __all_sync(0xffffffffu, !valid || b == b0);
-        if (uniform) {
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            const unsigned long long k2 = __shfl_xor_sync(0xffffffffu, key, o);
-            key = k2 > key ? k2 : key;
-          }
-          if (lane == 0 && key) atomicMax(&best[b0], key);
-        } else if (valid) {
-          atomicMax(&best[b], key);
-        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint8_t* sa = sA + s * 2 * A_TILE;
+        mma_split_kblock(d, smem_desc(sa), smem_desc(sa + A_TILE), smem_desc(sB + kb * B_BLK),
+                         smem_desc(sB + (KB + kb) * B_BLK), idesc, kb == 0);
+        mma_commit_to(&empty_bar[s]);
       }
+      if (ok) mma_commit_to(&accF[buf]);
+    }
+  } else if (warp >= 2) {
+    // warp (q, h): TMEM lanes 32 q .. 32 q + 31, column half h
+    const int q = warp & 3, h = (warp - 2) >> 2;
+    const int c_mid = (NT / 2) & ~15;
+    const int c0 = h ? c_mid : 0, c1 = h ? NT : c_mid;
+    const size_t ws = (size_t)KB * (TK / 2);  // A2 row stride in bf16 pairs
+    int tl = 0;
+    for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
+      const int buf = tl & 1;
+      if (!mbar_wait(&accF[buf], (tl >> 1) & 1)) {
+        atomicExch(err, 25);
+        abort_flag = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int g = tile * TM + q * 32 + lane;
+      const bool valid = g < p.rows;
+      const int rpb = p.HH * p.N;
+      const int b = g / rpb, rem = g - (g / rpb) * rpb;
+      const int m2 = rem / p.N, m1 = rem - (rem / p.N) * p.N;
+      const size_t row0 = ((size_t)b * p.U) * p.HH + m2;  // + u0 * HH
+      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 256);
+      tmem_for_groups(taddr, c0, c1, [&](const uint32_t(&r)[16], int cb) {
+        epi1_group<16>(r, cb, valid, p.U, row0, p.HH, ws, m1, (size_t)p.R2, out);
+      });
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(&accE[buf]);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+  }
+}
+
+// ------------------------------------------------------------------ fused passes 2 + 3
+// Byte offset of 4-byte word w (K pair) of row r in a 128-row K-major tile of 64 bf16 per
+// row, 128-byte swizzle (16-byte chunk c of row r at chunk c ^ (r % 8)).
+__device__ __forceinline__ uint32_t sw128_word(int r, int w) {
+  return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((((w >> 2) ^ (r & 7))) << 4) + ((w & 3) << 2));
+}
+
+// The 128 x 16 (K) Nyquist operand and its NT3 x 16 B counterpart use the plain K-major
+// layout: 8-row x 16-byte core matrices, the two K halves 128 bytes apart (leading byte
+// offset), 8-row groups 256 bytes apart (stride byte offset).
+constexpr int kNqA = TM * 16 * 2;
+
+__device__ __forceinline__ uint32_t k16_word(int r) { return (uint32_t)((r >> 3) * 256 + (r & 7) * 16); }
+
+__device__ __forceinline__ uint64_t smem_desc_k16(const void* p) {
+  const uint64_t addr = smem_u32(p);
+  uint64_t d = 0;
+  d |= (addr >> 4) & 0x3FFFull;
+  d |= (uint64_t)(128 >> 4) << 16;  // leading byte offset: K core-matrix stride
+  d |= (uint64_t)(256 >> 4) << 32;  // stride byte offset: 8-row group stride
+  d |= (uint64_t)1 << 46;           // descriptor version for tcgen05
+  return d;                          // layout type 0: no swizzle
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_constant__ CUtensorMap mapE1,
+                  const __grid_constant__ CUtensorMap mapE3, Pass23 p, const float2* __restrict__ nyq,
+                  const uint4* __restrict__ bnq, unsigned long long* __restrict__ best, int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = align1024(smem_raw);
+  const int KB = p.KB, NT12 = p.NT12, NT3 = p.NT3;
+  const int B1 = NT12 * TK * 2, B3 = NT3 * TK * 2;
+  uint8_t* sE1 = smem;                       // [part][kb] B1
+  uint8_t* sE3 = sE1 + 2 * KB * B1;          // [part] B3
+  uint8_t* sA = sE3 + 2 * B3;                // [2 stages][part] A_TILE
+  uint8_t* sA3 = sA + 4 * A_TILE;            // [part] A_TILE
+  uint8_t* sAn = sA3 + 2 * A_TILE;           // [part] 128 x 16 Nyquist operand, no swizzle
+  uint8_t* sBn = sAn + 2 * kNqA;             // [part] NT3 x 16, no swizzle
+  __shared__ __align__(8) uint64_t full_bar[2], empty_bar[2];
+  __shared__ __align__(8) uint64_t resF, acc2F, acc2E, a3F, a3E, acc3F, acc3E;
+  __shared__ uint32_t tmem_base;
+  __shared__ volatile int abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&resF, 1);
+    mbar_init(&acc2F, 1);
+    mbar_init(&acc2E, kEpi);
+    mbar_init(&a3F, kEpi);
+    mbar_init(&a3E, 1);
+    mbar_init(&acc3F, 1);
+    mbar_init(&acc3E, kEpi);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // the pass-3 operands: K columns past N (and past the Nyquist pair) stay zero, rows not
+  // written by a chunk are ignored; the Nyquist B operand comes prepared from the host
+  for (int i = threadIdx.x; i < (2 * A_TILE + 2 * kNqA) / 16; i += blockDim.x)
+    reinterpret_cast<uint4*>(sA3)[i] = make_uint4(0u, 0u, 0u, 0u);
+  for (int i = threadIdx.x; i < 2 * NT3 * 32 / 16; i += blockDim.x) reinterpret_cast<uint4*>(sBn)[i] = bnq[i];
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  const uint32_t idesc2 = idesc_bf16(TM, NT12), idesc3 = idesc_bf16(TM, NT3);
+  const int rows_a3 = p.G * p.U;  // (u0_local, u1) rows of a tile
+
+  if (warp == 0 && lane == 0) {
+    mbar_expect_tx(&resF, (uint32_t)(2 * KB * B1 + 2 * B3));
+    for (int part = 0; part < 2; ++part) {
+      for (int kb = 0; kb < KB; ++kb) tma_load_2d(sE1 + (part * KB + kb) * B1, &mapE1, kb * TK, part * NT12, &resF);
+      tma_load_2d(sE3 + part * B3, &mapE3, 0, part * NT3, &resF);
+    }
+    int it = 0;
+    for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x) {
+      const int b = tile / p.TPB, tg = tile - (tile / p.TPB) * p.TPB;
+      const int arow = (b * p.U + tg * p.G) * p.HH;
+      for (int kb = 0; kb < KB; ++kb, ++it) {
+        const int s = it & 1;
+        const uint32_t use = it >> 1;
+        if (it >= 2 && !mbar_wait(&empty_bar[s], (use - 1) & 1)) {
+          atomicExch(err, 31);
+          abort_flag = 1;
+          break;
+        }
+        uint8_t* sa = sA + s * 2 * A_TILE;
+        mbar_expect_tx(&full_bar[s], 2 * A_TILE);
+        tma_load_2d(sa, &mapA2, kb * TK, arow, &full_bar[s]);
+        tma_load_2d(sa + A_TILE, &mapA2, kb * TK, p.R2 + arow, &full_bar[s]);
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    bool ok = mbar_wait(&resF, 0);
+    if (!ok) {
+      atomicExch(err, 32);
+      abort_flag = 1;
+    }
+    int it = 0, tl = 0, cc = 0;
+    for (int tile = blockIdx.x; ok && tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
+      // pass 2 into acc2 (columns 0 .. NT12)
+      if (tl >= 1 && !mbar_wait(&acc2E, (tl - 1) & 1)) {
+        atomicExch(err, 33);
+        abort_flag = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (int kb = 0; kb < KB; ++kb, ++it) {
+        const int s = it & 1;
+        const uint32_t use = it >> 1;
+        if (!mbar_wait(&full_bar[s], use & 1)) {
+          atomicExch(err, 34);
+          abort_flag = 1;
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint8_t* sa = sA + s * 2 * A_TILE;
+        mma_split_kblock(tmem, smem_desc(sa), smem_desc(sa + A_TILE), smem_desc(sE1 + kb * B1),
+                         smem_desc(sE1 + (KB + kb) * B1), idesc2, kb == 0);
+        mma_commit_to(&empty_bar[s]);
+      }
+      if (!ok) break;
+      mma_commit_to(&acc2F);
+      // pass 3, chunk by chunk, into acc3 (columns NT12 + j NT3)
+      for (int j = 0; j < p.CH; ++j, ++cc) {
+        if (!mbar_wait(&a3F, cc & 1)) {
+          atomicExch(err, 35);
+          abort_flag = 1;
+          ok = false;
+          break;
+        }
+        if (j == 0 && tl >= 1 && !mbar_wait(&acc3E, (tl - 1) & 1)) {
+          atomicExch(err, 36);
+          abort_flag = 1;
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t d3 = tmem + (uint32_t)(NT12 + j * NT3);
+        mma_split_kblock(d3, smem_desc(sA3), smem_desc(sA3 + A_TILE), smem_desc(sE3), smem_desc(sE3 + B3), idesc3,
+                         true);
+        // the Nyquist column m2 = N/2 as one more K step of 16
+        const uint64_t an_hi = smem_desc_k16(sAn), an_lo = smem_desc_k16(sAn + kNqA);
+        const uint64_t bn_hi = smem_desc_k16(sBn), bn_lo = smem_desc_k16(sBn + NT3 * 32);
+        mma_bf16_id(d3, an_hi, bn_hi, idesc3, 1u);
+        mma_bf16_id(d3, an_lo, bn_hi, idesc3, 1u);
+        mma_bf16_id(d3, an_hi, bn_lo, idesc3, 1u);
+        mma_commit_to(&a3E);
+      }
+      if (!ok) break;
+      mma_commit_to(&acc3F);
+    }
+  } else if (warp >= 2) {
+    // warp (q, h): TMEM lanes 32 q .. 32 q + 31, half h of the columns it needs
+    const int q = warp & 3, h = (warp - 2) >> 2;
+    const int r_lane = q * 32 + lane;            // row of the pass-2 tile: (u0_local, m2)
+    const int u0l = r_lane / p.HH, m2 = r_lane - (r_lane / p.HH) * p.HH;
+    const uint32_t lane_off = (uint32_t)(q * 32) << 16;
+    const int c3_mid = (NT3 / 2) & ~15;
+    const int c3_0 = h ? c3_mid : 0, c3_1 = h ? NT3 : c3_mid;
+    int tl = 0, cc = 0;
+    for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
+      const int b = tile / p.TPB, tg = tile - (tile / p.TPB) * p.TPB;
+      if (!mbar_wait(&acc2F, tl & 1)) {
+        atomicExch(err, 37);
+        abort_flag = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      bool ok = true;
+      for (int j = 0; j < p.CH; ++j, ++cc) {
+        // rows of chunk j: (u0_local, u1) with u0_local * U + u1 in [128 j, 128 j + 128); this
+        // lane's u1 range, the warp's union of them, and this half's share of its columns
+        const int rbase = u0l * p.U - TM * j;
+        const int lo_l = max(0, -rbase), hi_l = min(p.U, TM - rbase);
+        const int lo = __reduce_min_sync(0xffffffffu, lo_l < hi_l ? lo_l : p.U);
+        const int hi = __reduce_max_sync(0xffffffffu, lo_l < hi_l ? hi_l : 0);
+        const int cA = (2 * lo) & ~15, cB = min(NT12, (2 * hi + 15) & ~15);
+        const int cM = cA + ((((cB - cA) >> 4) + 1) >> 1 << 4);  // h = 0 takes the first half
+        const int ca = lo < hi ? (h ? cM : cA) : 0, cb_end = lo < hi ? (h ? cB : cM) : 0;
+        if (cc >= 1 && !mbar_wait(&a3E, (cc - 1) & 1)) {
+          atomicExch(err, 38);
+          abort_flag = 1;
+          ok = false;
+          break;
+        }
+        tmem_for_groups(tmem + lane_off, ca, cb_end, [&](const uint32_t(&r)[16], int cb) {
+          epi2_group<16>(r, cb, lo_l, hi_l, rbase, m2, sA3);
+        });
+        if (threadIdx.x - 64 < TM) {  // row r of the chunk: its Nyquist pair Y[u0][u1]
+          const int r = TM * j + (threadIdx.x - 64);
+          const int a = r / p.U, u1 = r - (r / p.U) * p.U;
+          const int u0 = tg * p.G + a;
+          if (r < rows_a3 && u0 < p.U) {
+            const float2 y = nyq[((size_t)b * p.U + u0) * p.U + u1];
+            uint32_t hi2, lo2;
+            split2(y.x, y.y, hi2, lo2);
+            *reinterpret_cast<uint32_t*>(sAn + k16_word(threadIdx.x - 64)) = hi2;
+            *reinterpret_cast<uint32_t*>(sAn + kNqA + k16_word(threadIdx.x - 64)) = lo2;
+          }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive(&a3F);
+      }
+      if (!ok) break;
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(&acc2E);
+      if (!mbar_wait(&acc3F, tl & 1)) {
+        atomicExch(err, 39);
+        abort_flag = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      float bv = -INFINITY;
+      int bi = 0x7fffffff;
+      bool have = false;
+      for (int j = 0; j < p.CH; ++j) {
+        const int r = TM * j + r_lane;  // (u0_local, u1) row of the tile
+        const int a = r / p.U, u1 = r - (r / p.U) * p.U;
+        const int u0 = tg * p.G + a;
+        const bool valid = r < rows_a3 && u0 < p.U;
+        const int row_flat = u0 * p.U + u1;
+        tmem_for_groups(tmem + lane_off + (uint32_t)(NT12 + j * NT3), c3_0, c3_1,
+                        [&](const uint32_t(&r)[16], int cb) {
+                          if (valid) scan_group<16>(r, cb, p.U, row_flat, bv, bi, have);
+                        });
+      }
+      // a lane visits its values in increasing flat order, so a later equal value never wins;
+      // the warp's keys all belong to subtomogram b
+      unsigned long long key = have ? argmax_key(bv, bi) : 0ull;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long k2 = __shfl_xor_sync(0xffffffffu, key, o);
+        key = k2 > key ? k2 : key;
+      }
+      if (lane == 0 && key) atomicMax(&best[b], key);
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(&acc3E);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+  }
+}
+
+// ------------------------------------------------------------------ Nyquist plane (FP32)
+// Y[u0][u1] = sum_{m1} E[u1][m1] sum_{m0} E[u0][m0] P[m1][m0], one CTA per subtomogram; each
+// thread accumulates a 4 x 4 block of outputs (rows u0 = 4 i + a, columns interleaved with
+// stride nb so that neighbouring lanes read neighbouring padded rows).
+constexpr int kNyqThreads = 512;
+
+__global__ void __launch_bounds__(kNyqThreads)
+nyq_kernel(const float2* __restrict__ p32, const float2* __restrict__ E, int N, int U, float2* __restrict__ nyq) {
+  extern __shared__ __align__(16) float2 sm[];
+  const int ld = N + 1;  // padded rows
+  float2* sP = sm;             // N x ld: [m1][m0]
+  float2* sE = sP + N * ld;    // U x ld: [u][m]
+  float2* sZ = sE + U * ld;    // U x ld: [u0][m1]
+  const int b = blockIdx.x;
+  const float2* P = p32 + (size_t)b * N * N;
+  for (int e = threadIdx.x; e < N * N; e += kNyqThreads) sP[(e / N) * ld + e % N] = P[e];
+  for (int e = threadIdx.x; e < U * N; e += kNyqThreads) sE[(e / N) * ld + e % N] = E[e];
+  __syncthreads();
+  const int nu = (U + 3) / 4;
+  // Z[u0][m1]: row blocks of u0, columns m1 = c + (N / 4) j
+  {
+    const int nc = N / 4;
+    for (int task = threadIdx.x; task < nu * nc; task += kNyqThreads) {
+      const int ib = task / nc, c = task - (task / nc) * nc;
+      float2 acc[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = make_float2(0.f, 0.f);
+      int ur[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) ur[i] = min(4 * ib + i, U - 1);
+      for (int m0 = 0; m0 < N; ++m0) {
+        float2 w[4], x[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) w[i] = sE[ur[i] * ld + m0];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) x[j] = sP[(c + nc * j) * ld + m0];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            acc[i][j].x += w[i].x * x[j].x - w[i].y * x[j].y;
+            acc[i][j].y += w[i].x * x[j].y + w[i].y * x[j].x;
+          }
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (4 * ib + i < U)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) sZ[(4 * ib + i) * ld + c + nc * j] = acc[i][j];
+    }
+  }
+  __syncthreads();
+  // Y[u0][u1]: row blocks of u0, columns u1 = c + nu j
+  float2* Y = nyq + (size_t)b * U * U;
+  for (int task = threadIdx.x; task < nu * nu; task += kNyqThreads) {
+    const int ib = task / nu, c = task - (task / nu) * nu;
+    float2 acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = make_float2(0.f, 0.f);
+    int ur[4], uc[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      ur[i] = min(4 * ib + i, U - 1);
+      uc[i] = min(c + nu * i, U - 1);
+    }
+    for (int m1 = 0; m1 < N; ++m1) {
+      float2 z[4], w[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) z[i] = sZ[ur[i] * ld + m1];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) w[j] = sE[uc[j] * ld + m1];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          acc[i][j].x += w[j].x * z[i].x - w[j].y * z[i].y;
+          acc[i][j].y += w[j].x * z[i].y + w[j].y * z[i].x;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (4 * ib + i < U && c + nu * j < U) Y[(4 * ib + i) * U + c + nu * j] = acc[i][j];
   }
 }
 
@@ -291,53 +740,86 @@ float bf2f(uint16_t h) {
   return f;
 }
 
-template <int NT, int MODE>
-int launch_pass(const ShiftTc* t, const void* mapA, const void* mapB, const UParams& P, uint32_t* out,
-                cudaStream_t st) {
-  // at least 100 KB so that no more than two CTAs (2 x 256 TMEM columns) share an SM
-  size_t smem = (size_t)kStages * (TM * TK * 2 + NT * TK * 2) + 1024;
-  if (smem < 100 * 1024) smem = 100 * 1024;
-  MTB_CUDA_TRY(cudaFuncSetAttribute(updft_tc_kernel<NT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int grid = (P.rows + TM - 1) / TM;
-  updft_tc_kernel<NT, MODE><<<grid, kThreads, smem, st>>>(*reinterpret_cast<const CUtensorMap*>(mapA),
-                                                          *reinterpret_cast<const CUtensorMap*>(mapB), P, out,
-                                                          t->best, t->err);
-  MTB_LAUNCH_CHECK();
-  return MTB_OK;
+struct Geometry {
+  int HH, NT12, NT3, KB12, G, TPB, CH, stages1;
+  size_t smem1, smem23;
+};
+
+bool geometry(int N, int U, Geometry* o) {
+  if (N != 16 && N != 32 && N != 64) return false;
+  if (U < 1 || 2 * U > 256) return false;
+  Geometry g;
+  g.HH = N / 2;
+  g.NT12 = (2 * U + 15) / 16 * 16;
+  g.NT3 = (U + 15) / 16 * 16;
+  g.KB12 = (2 * N + TK - 1) / TK;
+  g.G = TM / g.HH;
+  g.TPB = (U + g.G - 1) / g.G;
+  g.CH = (g.G * U + TM - 1) / TM;
+  if (g.NT12 + g.CH * g.NT3 > 512) return false;
+  const size_t b1 = (size_t)2 * g.KB12 * g.NT12 * TK * 2;
+  const size_t b3 = (size_t)2 * g.NT3 * TK * 2;
+  g.smem23 = 1024 + b1 + b3 + 4 * (size_t)A_TILE + 2 * (size_t)A_TILE + 2 * (size_t)kNqA + (size_t)2 * g.NT3 * 32;
+  if (g.smem23 > kSmemCap) return false;
+  g.stages1 = (int)((kSmemCap - 1024 - b1) / (2 * (size_t)A_TILE));
+  if (g.stages1 > kMaxStages) g.stages1 = kMaxStages;
+  if (g.stages1 < 2) return false;
+  g.smem1 = 1024 + b1 + (size_t)g.stages1 * 2 * A_TILE;
+  *o = g;
+  return true;
 }
 
 }  // namespace
 
+int shift_tc_fits(int N, int U) {
+  Geometry g;
+  return geometry(N, U, &g) ? MTB_OK : MTB_ERR_ARG;
+}
+
 int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, int max_batch) {
   memset(t, 0, sizeof(*t));
-  // N-tile of passes 1, 2 is round_up(2U, 16) <= 256; of pass 3 round_up(U, 16)
-  if (U < 1 || 2 * U > 256 || N < 2) return MTB_ERR_ARG;
+  Geometry ge;
+  if (!geometry(N, U, &ge)) return MTB_ERR_ARG;
   t->N = N;
   t->H = H;
+  t->HH = ge.HH;
   t->U = U;
-  t->NT12 = (2 * U + 15) / 16 * 16;
-  t->NT3 = (U + 15) / 16 * 16;
-  t->KB12 = (2 * N + TK - 1) / TK;
-  t->KB3 = (2 * H + TK - 1) / TK;
+  t->NT12 = ge.NT12;
+  t->NT3 = ge.NT3;
+  t->KB12 = ge.KB12;
+  t->G = ge.G;
+  t->TPB = ge.TPB;
+  t->CH = ge.CH;
+  t->stages1 = ge.stages1;
+  t->smem1 = ge.smem1;
+  t->smem23 = ge.smem23;
   t->Bmax = max_batch;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&t->n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return MTB_ERR_CUDA;
   auto pad = [](size_t r) { return (r + TM - 1) / TM * TM; };
-  t->R1 = (int)pad((size_t)max_batch * N * H);
-  t->R2 = (int)pad((size_t)max_batch * U * H);
-  t->R3 = (int)pad((size_t)max_batch * U * U);
-  const size_t k12 = (size_t)t->KB12 * TK, k3 = (size_t)t->KB3 * TK;
-  const size_t a1 = (size_t)2 * t->R1 * k12 * 2, a2 = (size_t)2 * t->R2 * k12 * 2, a3 = (size_t)2 * t->R3 * k3 * 2;
+  const int HH = ge.HH;
+  t->R1 = (int)pad((size_t)max_batch * HH * N);
+  // a partial last u0 group of the last subtomogram reads up to G * HH rows past the end
+  t->R2 = (int)pad((size_t)max_batch * U * HH + (size_t)ge.G * HH);
+  const size_t k12 = (size_t)t->KB12 * TK, k3 = TK;
+  const size_t a1 = (size_t)2 * t->R1 * k12 * 2, a2 = (size_t)2 * t->R2 * k12 * 2;
   if (cudaMalloc(&t->A1, a1) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->A2, a2) != cudaSuccess) return MTB_ERR_OOM;
-  if (cudaMalloc(&t->A3, a3) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->E1, (size_t)2 * t->NT12 * k12 * 2) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->E3, (size_t)2 * t->NT3 * k3 * 2) != cudaSuccess) return MTB_ERR_OOM;
+  if (cudaMalloc(&t->E, (size_t)U * N * sizeof(float2)) != cudaSuccess) return MTB_ERR_OOM;
+  if (cudaMalloc(&t->ENQ, (size_t)2 * t->NT3 * 32) != cudaSuccess) return MTB_ERR_OOM;
+  if (cudaMalloc(&t->p32, (size_t)max_batch * N * N * sizeof(float2)) != cudaSuccess) return MTB_ERR_OOM;
+  if (cudaMalloc(&t->nyq, (size_t)max_batch * U * U * sizeof(float2)) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->best, (size_t)max_batch * 8) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->err, 4) != cudaSuccess) return MTB_ERR_OOM;
-  // K columns past 2N (A1, A2) and 2H (A3) stay zero; the rest is rewritten by every call
+  // K columns past 2N of A1 and A2 stay zero; the rest is rewritten by every call
   if (cudaMemset(t->A1, 0, a1) != cudaSuccess || cudaMemset(t->A2, 0, a2) != cudaSuccess ||
-      cudaMemset(t->A3, 0, a3) != cudaSuccess || cudaMemset(t->err, 0, 4) != cudaSuccess)
+      cudaMemset(t->err, 0, 4) != cudaSuccess)
     return MTB_ERR_CUDA;
-  // B operands: E1 rows (u, re/im), K (m, re/im); E3 rows u2, K (m2, re/im) -> real part
+  // B operands: E1 rows (u, re/im), K (m, re/im); E3 rows u2, K (m2 < N/2, re/im) -> real part
   auto E = [&](int n, int u, int m, double* re, double* im) {
     const int mm = (m < (n + 1) / 2) ? m : m - n;
     const double f = (double)mm / ((double)uf * n);
@@ -346,6 +828,16 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
     *im = sin(ph);
   };
   std::vector<uint16_t> e1((size_t)2 * t->NT12 * k12, 0), e3((size_t)2 * t->NT3 * k3, 0);
+  std::vector<float2> ef((size_t)U * N);
+  // Nyquist B operand: rows u2, K = (re, im) of m2 = N/2 and 14 zeros, plain K-major layout
+  std::vector<uint16_t> enq((size_t)2 * t->NT3 * 16, 0);
+  auto put_nq = [&](int u, int k, double v) {
+    const uint16_t hi = f2bf((float)v);
+    const uint16_t lo = f2bf((float)(v - (double)bf2f(hi)));
+    const size_t at = ((size_t)(u >> 3) * 256 + (size_t)(k >> 3) * 128 + (size_t)(u & 7) * 16 + (k & 7) * 2) / 2;
+    enq[at] = hi;
+    enq[(size_t)t->NT3 * 16 + at] = lo;
+  };
   auto put = [&](std::vector<uint16_t>& dst, size_t k, int rows, int r, int kk, double v) {
     const uint16_t hi = f2bf((float)v);
     const uint16_t lo = f2bf((float)(v - (double)bf2f(hi)));
@@ -360,91 +852,86 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
       put(e1, k12, t->NT12, 2 * u + 0, 2 * m + 1, -ei);
       put(e1, k12, t->NT12, 2 * u + 1, 2 * m + 0, ei);
       put(e1, k12, t->NT12, 2 * u + 1, 2 * m + 1, er);
+      ef[(size_t)u * N + m] = make_float2((float)er, (float)ei);
     }
-  for (int u = 0; u < U; ++u)
-    for (int m = 0; m < H; ++m) {
+  for (int u = 0; u < U; ++u) {
+    for (int m = 0; m < HH; ++m) {
       double er, ei;
       E(H, u, m, &er, &ei);
       put(e3, k3, t->NT3, u, 2 * m + 0, er);
       put(e3, k3, t->NT3, u, 2 * m + 1, -ei);
     }
+    double er, ei;
+    E(H, u, HH, &er, &ei);
+    put_nq(u, 0, er);
+    put_nq(u, 1, -ei);
+  }
   if (cudaMemcpy(t->E1, e1.data(), e1.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(t->E3, e3.data(), e3.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess)
+      cudaMemcpy(t->E3, e3.data(), e3.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(t->E, ef.data(), ef.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(t->ENQ, enq.data(), enq.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess)
     return MTB_ERR_CUDA;
   int rc = make_map(t->mapA1, t->A1, k12, (uint64_t)2 * t->R1, TM);
   if (!rc) rc = make_map(t->mapA2, t->A2, k12, (uint64_t)2 * t->R2, TM);
-  if (!rc) rc = make_map(t->mapA3, t->A3, k3, (uint64_t)2 * t->R3, TM);
   if (!rc) rc = make_map(t->mapE1, t->E1, k12, (uint64_t)2 * t->NT12, t->NT12);
   if (!rc) rc = make_map(t->mapE3, t->E3, k3, (uint64_t)2 * t->NT3, t->NT3);
   return rc;
 }
 
 void shift_tc_release(ShiftTc* t) {
-  void* ptrs[] = {t->A1, t->A2, t->A3, t->E1, t->E3, t->best, t->err};
+  void* ptrs[] = {t->A1, t->A2, t->E1, t->E3, t->E, t->ENQ, t->p32, t->nyq, t->best, t->err};
   for (void* p : ptrs) if (p) cudaFree(p);
   memset(t, 0, sizeof(*t));
 }
 
-template <int MODE>
-int dispatch(const ShiftTc* t, int nt, const void* mapA, const void* mapB, const UParams& P, uint32_t* out,
-             cudaStream_t st) {
-  switch (nt) {
-    case 16: return launch_pass<16, MODE>(t, mapA, mapB, P, out, st);
-    case 32: return launch_pass<32, MODE>(t, mapA, mapB, P, out, st);
-    case 48: return launch_pass<48, MODE>(t, mapA, mapB, P, out, st);
-    case 64: return launch_pass<64, MODE>(t, mapA, mapB, P, out, st);
-    case 80: return launch_pass<80, MODE>(t, mapA, mapB, P, out, st);
-    case 96: return launch_pass<96, MODE>(t, mapA, mapB, P, out, st);
-    case 112: return launch_pass<112, MODE>(t, mapA, mapB, P, out, st);
-    case 128: return launch_pass<128, MODE>(t, mapA, mapB, P, out, st);
-    case 144: return launch_pass<144, MODE>(t, mapA, mapB, P, out, st);
-    case 160: return launch_pass<160, MODE>(t, mapA, mapB, P, out, st);
-    case 176: return launch_pass<176, MODE>(t, mapA, mapB, P, out, st);
-    case 192: return launch_pass<192, MODE>(t, mapA, mapB, P, out, st);
-    case 208: return launch_pass<208, MODE>(t, mapA, mapB, P, out, st);
-    case 224: return launch_pass<224, MODE>(t, mapA, mapB, P, out, st);
-    case 240: return launch_pass<240, MODE>(t, mapA, mapB, P, out, st);
-    case 256: return launch_pass<256, MODE>(t, mapA, mapB, P, out, st);
-    default: return MTB_ERR_ARG;
-  }
-}
-
 int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st) {
   MTB_CUDA_TRY(cudaMemsetAsync(t->best, 0, (size_t)B * 8, st));
-  const int N = t->N, H = t->H, U = t->U;
-  UParams P;
-  P.N = N;
-  P.H = H;
-  P.U = U;
-  // pass 1: rows (b, m2, m1) -> A2 rows (b, u0, m2)
-  P.KB = t->KB12;
-  P.KBo = t->KB12;
-  P.R = t->R1;
-  P.rpb = N * H;
-  P.rows = B * P.rpb;
-  P.R_out = t->R2;
-  P.rpb_out = U * H;
-  int rc = dispatch<1>(t, t->NT12, t->mapA1, t->mapE1, P, (uint32_t*)t->A2, st);
-  if (rc) return rc;
-  // pass 2: rows (b, u0, m2) -> A3 rows (b, u0, u1)
-  P.KB = t->KB12;
-  P.KBo = t->KB3;
-  P.R = t->R2;
-  P.rpb = U * H;
-  P.rows = B * P.rpb;
-  P.R_out = t->R3;
-  P.rpb_out = U * U;
-  rc = dispatch<2>(t, t->NT12, t->mapA2, t->mapE1, P, (uint32_t*)t->A3, st);
-  if (rc) return rc;
-  // pass 3: rows (b, u0, u1) -> argmax keys
-  P.KB = t->KB3;
-  P.KBo = 0;
-  P.R = t->R3;
-  P.rpb = U * U;
-  P.rows = B * P.rpb;
-  P.R_out = 0;
-  P.rpb_out = 0;
-  return dispatch<3>(t, t->NT3, t->mapA3, t->mapE3, P, nullptr, st);
+  const int N = t->N, U = t->U, HH = t->HH;
+  // Nyquist plane
+  const size_t snyq = (size_t)(N + 2 * U) * (N + 1) * sizeof(float2);
+  MTB_CUDA_TRY(cudaFuncSetAttribute(nyq_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)snyq));
+  nyq_kernel<<<B, kNyqThreads, snyq, st>>>(t->p32, t->E, N, U, t->nyq);
+  MTB_LAUNCH_CHECK();
+  // pass 1
+  Pass1 p1;
+  p1.rows = B * HH * N;
+  p1.tiles = (p1.rows + TM - 1) / TM;
+  p1.N = N;
+  p1.HH = HH;
+  p1.U = U;
+  p1.KB = t->KB12;
+  p1.R1 = t->R1;
+  p1.R2 = t->R2;
+  p1.NT = t->NT12;
+  p1.stages = t->stages1;
+  MTB_CUDA_TRY(cudaFuncSetAttribute(updft1_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem1));
+  const int g1 = p1.tiles < t->n_sm ? p1.tiles : t->n_sm;
+  updft1_tc_kernel<<<g1, kThreads, t->smem1, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA1),
+                                                   *reinterpret_cast<const CUtensorMap*>(t->mapE1), p1,
+                                                   (uint32_t*)t->A2, t->err);
+  MTB_LAUNCH_CHECK();
+  // passes 2 + 3
+  Pass23 p2;
+  p2.B = B;
+  p2.TPB = t->TPB;
+  p2.tiles = B * t->TPB;
+  p2.N = N;
+  p2.HH = HH;
+  p2.U = U;
+  p2.G = t->G;
+  p2.CH = t->CH;
+  p2.KB = t->KB12;
+  p2.R2 = t->R2;
+  p2.NT12 = t->NT12;
+  p2.NT3 = t->NT3;
+  MTB_CUDA_TRY(cudaFuncSetAttribute(updft23_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem23));
+  const int g2 = p2.tiles < t->n_sm ? p2.tiles : t->n_sm;
+  updft23_tc_kernel<<<g2, kThreads, t->smem23, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA2),
+                                                     *reinterpret_cast<const CUtensorMap*>(t->mapE1),
+                                                     *reinterpret_cast<const CUtensorMap*>(t->mapE3), p2, t->nyq,
+                                                     (const uint4*)t->ENQ, t->best, t->err);
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
 }
 
 int shift_tc_check(ShiftTc* t, cudaStream_t st) {

@@ -4,21 +4,32 @@
 #include <stdint.h>
 
 struct ShiftTc {
-  alignas(64) unsigned char mapA1[128];  // pass-1 A: rows (b, m2, m1), K (m0, re/im)
-  alignas(64) unsigned char mapA2[128];  // pass-2 A: rows (b, u0, m2), K (m1, re/im)
-  alignas(64) unsigned char mapA3[128];  // pass-3 A: rows (b, u0, u1), K (m2, re/im)
-  alignas(64) unsigned char mapE1[128];  // B of passes 1, 2: rows (u, re/im)
-  alignas(64) unsigned char mapE3[128];  // B of pass 3: rows u2
-  int N, H, U, NT12, NT3, KB12, KB3, Bmax;
-  int R1, R2, R3;                        // padded rows per hi/lo part
-  void *A1, *A2, *A3, *E1, *E3;          // bf16, [part][row][K]
+  alignas(64) unsigned char mapA1[128];  // pass-1 A: rows (b, m2 < N/2, m1), K (m0, re/im)
+  alignas(64) unsigned char mapA2[128];  // pass-2 A: rows (b, u0, m2 < N/2), K (m1, re/im)
+  alignas(64) unsigned char mapE1[128];  // B of passes 1, 2: rows (u, re/im), K (m, re/im)
+  alignas(64) unsigned char mapE3[128];  // B of pass 3: rows u2, K (m2 < N/2, re/im) -> real part
+  int N, H, HH, U, NT12, NT3, KB12, G, TPB, CH, Bmax;
+  int R1, R2;                            // padded rows per hi/lo part of A1, A2
+  int stages1;                           // pipeline stages of pass 1
+  int n_sm;
+  size_t smem1, smem23;                  // dynamic shared memory of the two kernels
+  void *A1, *A2, *E1, *E3;               // bf16, [part][row][K]
+  float2* E;                             // (U, N) exp(2 pi i (u - s) f_m), the FP32 DFT kernel
+  void* ENQ;                             // pass-3 B operand of the Nyquist column m2 = N/2, bf16
+                                         // [part][NT3 x 16] in the plain K-major layout
+  float2* p32;                           // (Bmax, N, N) product plane m2 = N/2, [m1][m0], FP32
+  float2* nyq;                           // (Bmax, U, U) its 2-D upsampled DFT
   unsigned long long* best;              // (Bmax) argmax keys: ordered value << 32 | ~flat index
   int* err;                              // nonzero after a bounded wait ran out
 };
 
+// 0 when the tensor-core path fits this geometry (box 16, 32 or 64; upsampled region
+// U <= 128; tensor memory and shared memory budgets), MTB_ERR_ARG otherwise.
+int shift_tc_fits(int N, int U);
 int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, int max_batch);
 void shift_tc_release(ShiftTc* t);
-// Passes 1-3 for B subtomograms whose pass-1 operand A1 has been written (fft_z split).
+// Nyquist plane, pass 1 and fused passes 2+3 for B subtomograms whose pass-1 operand A1 and
+// Nyquist plane p32 have been written (fft_z split).
 int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st);
 // Synchronises st; MTB_ERR_TIMEOUT if a device-side wait gave up.
 int shift_tc_check(ShiftTc* t, cudaStream_t st);

@@ -6,8 +6,11 @@
 
 namespace tc {
 
-// Bounded mbarrier waits: a wait gives up after this many try_wait polls.
-constexpr long long kSpinLimit = 1LL << 22;
+// Bounded mbarrier waits: a wait gives up after this many try_wait polls, each of which may
+// suspend the thread for up to kSuspendNs (it resumes as soon as the phase completes), so a
+// waiting warp does not spin on the issue slots the working warps need.
+constexpr long long kSpinLimit = 1LL << 16;
+constexpr uint32_t kSuspendNs = 20000;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -24,9 +27,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
       : "memory");
   return ok != 0;
 }
