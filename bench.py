@@ -243,7 +243,7 @@ def run_ours(args):
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
     tracker.copy_(ident)
     ev[0].record(st)
-    sigma, norms = step.correlator.get_sigma(vols)
+    sigma, norms = step.correlator.get_sigma_upto(vols, L_MAX)
     ev[1].record(st)
     a, b, g, sc = step.matcher.search_orientations(sigma)
     ev[2].record(st)

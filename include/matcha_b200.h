@@ -175,6 +175,13 @@ int mtb_fle_forward(mtb_fle* h, const float* vol, int B, float* coeffs, int64_t 
 int mtb_sigma(mtb_fle* h, const float* coeffs, int64_t coeff_stride, const float* tmpl, int B,
               float* sigma, int64_t sigma_stride, mtb_stream_t stream);
 
+/* mtb_sigma restricted to degrees l <= lmax_out (0 <= lmax_out <= lmax): the first
+ * dsize(lmax_out) entries of each row, the rest of the row untouched.  No counterpart in
+ * the reference, which always fills every degree of the expansion; the orientation search
+ * reads degrees up to its own Lmax only. */
+int mtb_sigma_upto(mtb_fle* h, const float* coeffs, int64_t coeff_stride, const float* tmpl, int B,
+                   int lmax_out, float* sigma, int64_t sigma_stride, mtb_stream_t stream);
+
 /* Synchronises stream and returns MTB_ERR_TIMEOUT if a bounded device-side wait of the
  * tensor-core path gave up since the handle was created (then its results are invalid). */
 int mtb_fle_status(mtb_fle* h, mtb_stream_t stream);

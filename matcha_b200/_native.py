@@ -84,6 +84,7 @@ SIGNATURES = {
     "mtb_fle_destroy": (None, [_P]),
     "mtb_fle_forward": (_I, [_P, _P, _I, _P, _I64, _P, _P]),
     "mtb_sigma": (_I, [_P, _P, _I64, _P, _I, _P, _I64, _P]),
+    "mtb_sigma_upto": (_I, [_P, _P, _I64, _P, _I, _I, _P, _I64, _P]),
     "mtb_fle_status": (_I, [_P, _P]),
     "mtb_shift_create": (_I, [ctypes.POINTER(MtbShiftConfig), ctypes.POINTER(_P)]),
     "mtb_shift_destroy": (None, [_P]),

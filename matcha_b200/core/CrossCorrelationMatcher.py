@@ -78,18 +78,53 @@ class CrossCorrelationMatcher:
             raise ValueError(f"Input batch size {num_volumes} exceeds configured batchsize {self.batchsize}.")
         if self.template_coefficients_alphas_torch is None:
             raise RuntimeError("set_template must be called before get_sigma")
-        self.sigma.zero_()
-        self.bh_norms.zero_()
+        # rows past the batch read as zero (the rows of the batch are overwritten whole)
+        if num_volumes < self.batchsize:
+            self.sigma[num_volumes:].zero_()
+            self.bh_norms[num_volumes:].zero_()
         if num_volumes == 0:
             return self.sigma, self.bh_norms
-        vol = volumes.to(device=self.device, dtype=torch.float32).contiguous()
+        self._expand(volumes)
         dev = self.device
         with torch.cuda.device(dev):
-            nat.check(self.fle._lib.mtb_fle_forward(self.fle._h, nat.ptr(vol), num_volumes, nat.ptr(self._coeffs),
-                                                  self._coeffs.stride(0), nat.ptr(self.bh_norms),
-                                                  nat.stream_ptr(dev)), "mtb_fle_forward")
             nat.check(self.fle._lib.mtb_sigma(self.fle._h, nat.ptr(self._coeffs), self._coeffs.stride(0),
                                             nat.ptr(self.template_coefficients_alphas_torch), num_volumes,
                                             nat.ptr(self.sigma), self.sigma.stride(0), nat.stream_ptr(dev)),
                     "mtb_sigma")
         return self.sigma, self.bh_norms
+
+    def _expand(self, volumes: torch.Tensor):
+        vol = volumes.to(device=self.device, dtype=torch.float32).contiguous()
+        dev = self.device
+        with torch.cuda.device(dev):
+            nat.check(self.fle._lib.mtb_fle_forward(self.fle._h, nat.ptr(vol), volumes.shape[0],
+                                                  nat.ptr(self._coeffs), self._coeffs.stride(0),
+                                                  nat.ptr(self.bh_norms), nat.stream_ptr(dev)), "mtb_fle_forward")
+
+    @torch.no_grad()
+    def get_sigma_upto(self, volumes: torch.Tensor, lmax: int):
+        """get_sigma for the degrees l <= lmax only: (sigma (n, Dsize(lmax)), bh_norms (n,)) for
+        the n given volumes, in buffers of their own (extension: the reference always fills
+        every degree of the expansion; the orientation search reads degrees <= its L_max)."""
+        num_volumes = volumes.shape[0]
+        if num_volumes > self.batchsize:
+            raise ValueError(f"Input batch size {num_volumes} exceeds configured batchsize {self.batchsize}.")
+        if self.template_coefficients_alphas_torch is None:
+            raise RuntimeError("set_template must be called before get_sigma_upto")
+        if not 0 <= lmax <= self.lmax:
+            raise ValueError(f"lmax must be in [0, {self.lmax}]")
+        n = compute_size(lmax + 1)
+        buf = getattr(self, "_sigma_upto", None)
+        if buf is None or buf.shape[1] != n:
+            buf = torch.empty((self.batchsize, n), dtype=torch.complex64, device=self.device)
+            self._sigma_upto = buf
+        if num_volumes == 0:
+            return buf[:0], self.bh_norms[:0]
+        self._expand(volumes)
+        dev = self.device
+        with torch.cuda.device(dev):
+            nat.check(self.fle._lib.mtb_sigma_upto(self.fle._h, nat.ptr(self._coeffs), self._coeffs.stride(0),
+                                                 nat.ptr(self.template_coefficients_alphas_torch), num_volumes,
+                                                 lmax, nat.ptr(buf), buf.stride(0), nat.stream_ptr(dev)),
+                      "mtb_sigma_upto")
+        return buf[:num_volumes], self.bh_norms[:num_volumes]

@@ -212,35 +212,46 @@ __global__ void expand_kernel(const float* __restrict__ C, int64_t c_ld, int B, 
 
 // ------------------------------------------------------------------ sigma
 // sigma[b][Dindex(l, m, mp)] = (-1)^(m+mp) sum_k aT[l, -mp, k] conj(aV[b][l, -m, k])
-__global__ void sigma_kernel(const float2* __restrict__ aV, int64_t v_stride, const float2* __restrict__ aT,
-                             int B, int lmax, const int* __restrict__ kpad, const int* __restrict__ koff,
-                             const int* __restrict__ kidx, float2* __restrict__ sigma, int64_t s_stride) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  const int b = blockIdx.y;
-  if (b >= B || e >= mtb_dsize(lmax)) return;
-  int l = (int)cbrtf(0.75f * (float)e);
-  while (l > 0 && mtb_dsize(l - 1) > e) --l;
-  while (mtb_dsize(l) <= e) ++l;
+// One CTA per (degree l, subtomogram b), largest degrees first.  The rows mu = -l..l of the
+// template and of the subtomogram's coefficients (K = kpad[l] radial entries each, gathered
+// through kidx) are staged in shared memory with an odd row stride; each output then reads
+// two rows there: sigma[l, m, m'] = (-1)^(m+m') sum_k T[-m', k] conj(V[-m, k]).
+__global__ void __launch_bounds__(256)
+sigma_kernel(const float2* __restrict__ aV, int64_t v_stride, const float2* __restrict__ aT, int lout,
+             const int* __restrict__ kpad, const int* __restrict__ koff, const int* __restrict__ kidx,
+             float2* __restrict__ sigma, int64_t s_stride) {
+  extern __shared__ __align__(16) float2 ssm[];
+  const int l = lout - blockIdx.x, b = blockIdx.y;
   const int w = 2 * l + 1;
-  const int loc = e - mtb_dsize(l - 1);
-  const int a = loc / w, c = loc - a * w;   // m = a - l, mp = c - l
   const int K = kpad[l];
-  // row of -mp in the table is (l - mp) = 2l - c; row of -m is 2l - a
-  const int* tT = kidx + koff[l] + (2 * l - c) * K;
-  const int* tV = kidx + koff[l] + (2 * l - a) * K;
+  const int ks = K | 1;  // odd row stride: neighbouring rows fall in different banks
+  float2* sT = ssm;
+  float2* sV = ssm + w * ks;
+  const int* tab = kidx + koff[l];
   const float2* v = aV + (int64_t)b * v_stride;
-  float re = 0.f, im = 0.f;
-  for (int k = 0; k < K; ++k) {
-    const int it = tT[k], iv = tV[k];
-    if (it < 0 || iv < 0) continue;
-    const float2 t = __ldg(&aT[it]);
-    const float2 u = __ldg(&v[iv]);
-    // t * conj(u)
-    re += t.x * u.x + t.y * u.y;
-    im += t.y * u.x - t.x * u.y;
+  for (int e = threadIdx.x; e < w * K; e += blockDim.x) {
+    const int row = e / K, k = e - (e / K) * K;
+    const int idx = __ldg(&tab[e]);
+    sT[row * ks + k] = idx >= 0 ? __ldg(&aT[idx]) : make_float2(0.f, 0.f);
+    sV[row * ks + k] = idx >= 0 ? __ldg(&v[idx]) : make_float2(0.f, 0.f);
   }
-  const float sgn = ((a + c) & 1) ? -1.f : 1.f;  // (-1)^(m+mp) = (-1)^(a+c-2l)
-  sigma[(int64_t)b * s_stride + e] = make_float2(sgn * re, sgn * im);
+  __syncthreads();
+  float2* out = sigma + (int64_t)b * s_stride + mtb_dsize(l - 1);
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    const int a = e / w, c = e - (e / w) * w;  // m = a - l, m' = c - l
+    // row of -m' is 2l - c, row of -m is 2l - a
+    const float2* tr = sT + (2 * l - c) * ks;
+    const float2* vr = sV + (2 * l - a) * ks;
+    float re = 0.f, im = 0.f;
+    for (int k = 0; k < K; ++k) {
+      const float2 t = tr[k], u = vr[k];
+      // t * conj(u)
+      re += t.x * u.x + t.y * u.y;
+      im += t.y * u.x - t.x * u.y;
+    }
+    const float sgn = ((a + c) & 1) ? -1.f : 1.f;  // (-1)^(m+mp) = (-1)^(a+c-2l)
+    out[e] = make_float2(sgn * re, sgn * im);
+  }
 }
 
 template <typename T>
@@ -271,6 +282,7 @@ struct mtb_fle {
   int* kpad;
   int* koff;
   int* kidx;
+  int kmax;      // max over degrees of kpad
   FleTc tc;
   bool use_tc;
 };
@@ -330,6 +342,7 @@ extern "C" int mtb_fle_create(const mtb_fle_config* cfg, mtb_fle** out) {
   std::vector<int> koff(L + 1);
   int kt = 0;
   for (int l = 0; l <= L; ++l) { koff[l] = kt; kt += (2 * l + 1) * cfg->kpad[l]; }
+  for (int l = 0; l <= L; ++l) h->kmax = cfg->kpad[l] > h->kmax ? cfg->kpad[l] : h->kmax;
   for (int i = 0; i < kt; ++i)
     if (cfg->kidx[i] >= cfg->ne) return fail(MTB_ERR_ARG);
 
@@ -429,22 +442,29 @@ extern "C" int mtb_fle_forward(mtb_fle* h, const float* vol, int B, float* coeff
   return MTB_OK;
 }
 
-extern "C" int mtb_sigma(mtb_fle* h, const float* coeffs, int64_t coeff_stride, const float* tmpl, int B,
-                         float* sigma, int64_t sigma_stride, mtb_stream_t stream) {
+extern "C" int mtb_sigma_upto(mtb_fle* h, const float* coeffs, int64_t coeff_stride, const float* tmpl, int B,
+                              int lmax_out, float* sigma, int64_t sigma_stride, mtb_stream_t stream) {
   MTB_ARG_CHECK(h, "null handle");
   MTB_ARG_CHECK(B >= 0, "negative batch");
+  MTB_ARG_CHECK(lmax_out >= 0 && lmax_out <= h->cfg.lmax, "lmax_out must be in [0, lmax of the expansion]");
   if (B == 0) return MTB_OK;
   MTB_ARG_CHECK(coeffs && tmpl && sigma, "null pointer");
   MTB_ARG_CHECK(coeff_stride >= h->cfg.ne, "coefficient row shorter than ne");
-  MTB_ARG_CHECK(sigma_stride >= mtb_dsize(h->cfg.lmax), "sigma row shorter than dsize(lmax)");
+  MTB_ARG_CHECK(sigma_stride >= mtb_dsize(lmax_out), "sigma row shorter than dsize(lmax_out)");
   MTB_ARG_CHECK(B <= 65535, "batch too large for one launch");
-  const int n = mtb_dsize(h->cfg.lmax);
-  dim3 g((n + 255) / 256, B);
-  sigma_kernel<<<g, 256, 0, (cudaStream_t)stream>>>(reinterpret_cast<const float2*>(coeffs), coeff_stride,
-                                                    reinterpret_cast<const float2*>(tmpl), B, h->cfg.lmax, h->kpad,
-                                                    h->koff, h->kidx, reinterpret_cast<float2*>(sigma), sigma_stride);
+  const size_t smem = (size_t)2 * (2 * lmax_out + 1) * (h->kmax | 1) * sizeof(float2);
+  MTB_CUDA_TRY(cudaFuncSetAttribute(sigma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  sigma_kernel<<<dim3(lmax_out + 1, B), 256, smem, (cudaStream_t)stream>>>(
+      reinterpret_cast<const float2*>(coeffs), coeff_stride, reinterpret_cast<const float2*>(tmpl), lmax_out,
+      h->kpad, h->koff, h->kidx, reinterpret_cast<float2*>(sigma), sigma_stride);
   MTB_LAUNCH_CHECK();
   return MTB_OK;
+}
+
+extern "C" int mtb_sigma(mtb_fle* h, const float* coeffs, int64_t coeff_stride, const float* tmpl, int B,
+                         float* sigma, int64_t sigma_stride, mtb_stream_t stream) {
+  MTB_ARG_CHECK(h, "null handle");
+  return mtb_sigma_upto(h, coeffs, coeff_stride, tmpl, B, h->cfg.lmax, sigma, sigma_stride, stream);
 }
 
 extern "C" int mtb_fle_status(mtb_fle* h, mtb_stream_t stream) {

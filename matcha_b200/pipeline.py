@@ -88,8 +88,8 @@ class AlignmentStep:
         """volumes: (B, N, N, N) input of the expansion; subtomos: (B, N, N, N) for the shift
         match; tracker: (B, 4) float64 (w, x, y, z), updated in place; shift_zyx (B, 3)."""
         B = volumes.shape[0]
-        sigma, norms = self.correlator.get_sigma(volumes)
-        a, b, g, score = self.matcher.search_orientations(sigma[:B])
+        sigma, norms = self.correlator.get_sigma_upto(volumes, self.cfg.L)
+        a, b, g, score = self.matcher.search_orientations(sigma)
         dev = self.device
         with torch.cuda.device(dev):
             nat.check(self.matcher._lib.mtb_update_rotation(nat.ptr(a), nat.ptr(b), nat.ptr(g), nat.ptr(tracker), B,

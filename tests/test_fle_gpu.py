@@ -47,6 +47,27 @@ def test_sigma_and_norms_match_oracle(cuda_device):
     np.testing.assert_allclose(cc.bh_norm_template.item(), np.linalg.norm(at), rtol=1e-5)
 
 
+def test_sigma_upto_is_the_leading_degrees_of_sigma(cuda_device):
+    from matcha_b200.core.CrossCorrelationMatcher import CrossCorrelationMatcher
+    from matcha_b200.core.wigner_index import compute_size
+
+    N1, radius = 32, 14
+    rng = np.random.default_rng(5)
+    tmpl = blob_template(rng, N1, 40, 12, (1.5, 3.0), mask_radius=14)
+    vols = torch.from_numpy(rotate_volumes_reference(np.repeat(tmpl[None], 3, 0), haar_quaternions(rng, 3)))
+    cc = CrossCorrelationMatcher(N=N1, device=cuda_device, batchsize=4, bandlimit=16, radius=radius)
+    cc.set_template(tmpl)
+    full, n_full = cc.get_sigma(vols.to(cuda_device))
+    full, n_full = full[:3].cpu().numpy(), n_full[:3].cpu().numpy()
+    for lmax in (0, 7, cc.lmax):
+        part, n_part = cc.get_sigma_upto(vols.to(cuda_device), lmax)
+        assert part.shape == (3, compute_size(lmax + 1))
+        np.testing.assert_array_equal(part.cpu().numpy(), full[:, :compute_size(lmax + 1)])
+        np.testing.assert_array_equal(n_part.cpu().numpy(), n_full)
+    with pytest.raises(ValueError):
+        cc.get_sigma_upto(vols.to(cuda_device), cc.lmax + 1)
+
+
 def test_rotation_recovery_end_to_end(cuda_device):
     """Template rotated by known rotations, expanded, correlated and searched: the
     recovered Euler angles, composed with the tracker as the reference's benchmark
