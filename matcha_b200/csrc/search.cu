@@ -43,18 +43,37 @@ __device__ __forceinline__ bool better(float v1, int i1, float v2, int i2) {
   return v1 > v2 || (v1 == v2 && i1 < i2);
 }
 
+constexpr size_t kGridSmemCap = 200 * 1024;
+
+// Dynamic shared memory of the grid kernel: sigma (l < L0), the twiddle matrix, and the
+// F, G buffers of JB beta values.
+size_t grid_smem_bytes(int L0, int K, int JB) {
+  const int n = 2 * L0 * K, P = 2 * L0 - 1;
+  return (size_t)(mtb_dsize(L0 - 1) + n * P + JB * P * P + JB * P * n) * sizeof(float2);
+}
+
+// Beta values per pass: four when they fit, else one.
+int grid_jb(int L0, int K) { return grid_smem_bytes(L0, K, 4) <= kGridSmemCap ? 4 : 1; }
+size_t grid_smem_bytes(int L0, int K) { return grid_smem_bytes(L0, K, grid_jb(L0, K)); }
+
+// SOFFT on the (n x n x n) grid (beta_j = j pi/(n-1), alpha_a = 2 pi a/n, gamma_g = 2 pi g/n)
+// for one subtomogram per CTA, kGridJB beta values per pass:
+//   F_j[m'][m] = sum_{l < L0} d^l_{m'm}(beta_j) sigma_{l m' m}
+//   G_j[m'][g] = sum_m F_j[m'][m] e^{2 pi i g m / n}
+//   f_j[a][g]  = Re sum_{m'} G_j[m'][g] e^{2 pi i a m' / n} / n^2
+// with the running top-C of every thread merged at the end.
 __global__ void __launch_bounds__(kGridThreads)
 so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
-                     const float* __restrict__ dtab, int L0, int n, int C,
+                     const float* __restrict__ dtab, int L0, int n, int C, int JB,
                      float* __restrict__ alpha, float* __restrict__ beta, float* __restrict__ gamma,
                      float* __restrict__ grid_out) {
   extern __shared__ __align__(16) float gsm[];
   const int P = 2 * L0 - 1;
   const int nk = mtb_dsize(L0 - 1);
   float2* sg = reinterpret_cast<float2*>(gsm);  // nk
-  float2* F = sg + nk;                           // P*P
-  float2* G = F + P * P;                         // P*n
-  float2* tw = G + P * n;                        // n
+  float2* TW = sg + nk;                          // n x P: e^{2 pi i g (c - L0 + 1) / n}
+  float2* F = TW + n * P;                        // JB x P x P
+  float2* G = F + JB * P * P;                    // JB x P x n
   __shared__ float mv[kGridThreads / 32];
   __shared__ int mi[kGridThreads / 32];
   __shared__ int mt[kGridThreads / 32];
@@ -64,21 +83,28 @@ so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
   const int tid = threadIdx.x;
   const float2* sig = sigma + (int64_t)b * stride;
   for (int k = tid; k < nk; k += blockDim.x) sg[k] = sig[k];
-  for (int k = tid; k < n; k += blockDim.x) {
-    double s, c;
-    sincospi(2.0 * k / n, &s, &c);
-    tw[k] = make_float2((float)c, (float)s);
+  for (int q = tid; q < n * P; q += blockDim.x) {
+    const int g = q / P, c = q - (q / P) * P;
+    int k = (g * (c - (L0 - 1))) % n;
+    if (k < 0) k += n;
+    double sn, cs;
+    sincospi(2.0 * k / n, &sn, &cs);
+    TW[q] = make_float2((float)cs, (float)sn);
   }
   float tv[kMaxCand];
   int ti[kMaxCand];
   int cnt = 0, minp = 0;
+  float minv = -INFINITY;
+  int mini = 0x7fffffff;
   const float inv_n2 = 1.f / (float)(n * n);
   __syncthreads();
-  for (int j = 0; j < n; ++j) {
-    const float* dj = dtab + (int64_t)j * nk;
-    for (int q = tid; q < P * P; q += blockDim.x) {
-      const int mp = q / P - (L0 - 1), m = q % P - (L0 - 1);
+  for (int j0 = 0; j0 < n; j0 += JB) {
+    const int jn = min(JB, n - j0);
+    for (int q = tid; q < jn * P * P; q += blockDim.x) {
+      const int jb = q / (P * P), qq = q - jb * (P * P);
+      const int mp = qq / P - (L0 - 1), m = qq % P - (L0 - 1);
       const int l0 = max(abs(mp), abs(m));
+      const float* dj = dtab + (int64_t)(j0 + jb) * nk;
       float re = 0.f, im = 0.f;
       for (int l = l0; l < L0; ++l) {
         const int idx = mtb_dsize(l - 1) + (mp + l) * (2 * l + 1) + (m + l);
@@ -89,45 +115,47 @@ so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
       F[q] = make_float2(re, im);
     }
     __syncthreads();
-    for (int q = tid; q < P * n; q += blockDim.x) {
-      const int r = q / n, gg = q % n;
+    for (int q = tid; q < jn * P * n; q += blockDim.x) {
+      const int jb = q / (P * n), qq = q - jb * (P * n);
+      const int r = qq / n, gg = qq - (qq / n) * n;
+      const float2* fr = F + jb * P * P + r * P;
+      const float2* tr = TW + gg * P;
       float re = 0.f, im = 0.f;
       for (int c = 0; c < P; ++c) {
-        const int m = c - (L0 - 1);
-        int k = (gg * m) % n;
-        if (k < 0) k += n;
-        const float2 f = F[r * P + c], t = tw[k];
+        const float2 f = fr[c], t = tr[c];
         re += f.x * t.x - f.y * t.y;
         im += f.x * t.y + f.y * t.x;
       }
       G[q] = make_float2(re, im);
     }
     __syncthreads();
-    for (int q = tid; q < n * n; q += blockDim.x) {
-      const int aa = q / n, gg = q % n;
+    for (int q = tid; q < jn * n * n; q += blockDim.x) {
+      const int jb = q / (n * n), qq = q - jb * (n * n);
+      const int aa = qq / n, gg = qq - (qq / n) * n;
+      const float2* gc = G + jb * P * n + gg;
+      const float2* ta = TW + aa * P;
       float re = 0.f;
       for (int r = 0; r < P; ++r) {
-        const int mp = r - (L0 - 1);
-        int k = (aa * mp) % n;
-        if (k < 0) k += n;
-        const float2 gv = G[r * n + gg], t = tw[k];
+        const float2 gv = gc[r * n], t = ta[r];
         re += gv.x * t.x - gv.y * t.y;
       }
       const float v = re * inv_n2;
-      const int flat = j * n * n + q;
+      const int flat = (j0 + jb) * n * n + qq;
       if (grid_out) grid_out[(int64_t)b * n * n * n + flat] = v;
-      if (cnt < C) {
-        tv[cnt] = v; ti[cnt] = flat; ++cnt;
-        if (cnt == C || !better(tv[minp], ti[minp], v, flat)) {
+      // the rejection test reads the kept set's worst entry from registers
+      if (cnt < C || better(v, flat, minv, mini)) {
+        if (cnt < C) {
+          tv[cnt] = v; ti[cnt] = flat; ++cnt;
+        } else {
+          tv[minp] = v; ti[minp] = flat;
+        }
+        if (cnt == C) {
           minp = 0;
           for (int t = 1; t < cnt; ++t)
             if (better(tv[minp], ti[minp], tv[t], ti[t])) minp = t;
+          minv = tv[minp];
+          mini = ti[minp];
         }
-      } else if (better(v, flat, tv[minp], ti[minp])) {
-        tv[minp] = v; ti[minp] = flat;
-        minp = 0;
-        for (int t = 1; t < cnt; ++t)
-          if (better(tv[minp], ti[minp], tv[t], ti[t])) minp = t;
       }
     }
     __syncthreads();
@@ -263,9 +291,8 @@ extern "C" int mtb_search_create(const mtb_search_config* cfg, mtb_search** out)
   for (int i = 0; i < cfg->n_stages; ++i)
     MTB_ARG_CHECK(cfg->stages[i] >= 0 && cfg->stages[i] <= cfg->Lmax, "stage degree out of range");
   {
-    const int n = 2 * cfg->L0 * cfg->K, P = 2 * cfg->L0 - 1;
-    const size_t gsm = (size_t)(mtb_dsize(cfg->L0 - 1) + P * P + P * n + n) * 8;
-    MTB_ARG_CHECK(gsm <= 200 * 1024, "grid search too large for shared memory (reduce L0 or K)");
+    MTB_ARG_CHECK(grid_smem_bytes(cfg->L0, cfg->K) <= kGridSmemCap,
+                  "grid search too large for shared memory (reduce L0 or K)");
   }
   mtb_search* h = new mtb_search();
   memset(h, 0, sizeof(*h));
@@ -330,12 +357,12 @@ extern "C" int mtb_so3_grid_topk(mtb_search* h, const float* sigma, int64_t sigm
   if (B == 0) return MTB_OK;
   MTB_ARG_CHECK(sigma && alpha && beta && gamma, "null pointer");
   MTB_ARG_CHECK(sigma_stride >= mtb_dsize(h->cfg.L0 - 1), "sigma row shorter than dsize(L0-1)");
-  const int L0 = h->cfg.L0, n = h->n, P = 2 * L0 - 1, nk = mtb_dsize(L0 - 1);
-  const size_t smem = (size_t)(nk + P * P + P * n + n) * sizeof(float2);
+  const int L0 = h->cfg.L0, n = h->n;
+  const size_t smem = grid_smem_bytes(L0, h->cfg.K);
   MTB_CUDA_TRY(cudaFuncSetAttribute(so3_grid_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   so3_grid_topk_kernel<<<B, kGridThreads, smem, (cudaStream_t)stream>>>(
       reinterpret_cast<const float2*>(sigma), sigma_stride, B, h->dtab, L0, n, h->cfg.candidates,
-      alpha, beta, gamma, grid);
+      grid_jb(L0, h->cfg.K), alpha, beta, gamma, grid);
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }
@@ -470,8 +497,8 @@ extern "C" int mtb_search_orientations_static(const mtb_search_config* cfg, cons
   MTB_ARG_CHECK(sigma_stride >= mtb_dsize(cfg->Lmax), "sigma row shorter than dsize(Lmax)");
   const int n = 2 * cfg->L0 * cfg->K, L0 = cfg->L0, P = 2 * L0 - 1, nk = mtb_dsize(L0 - 1);
   MTB_ARG_CHECK(cfg->candidates <= n * n * n, "more candidates than grid points");
-  const size_t gsm = (size_t)(nk + P * P + P * n + n) * sizeof(float2);
-  MTB_ARG_CHECK(gsm <= 200 * 1024, "grid search too large for shared memory (reduce L0 or K)");
+  const size_t gsm = grid_smem_bytes(L0, cfg->K);
+  MTB_ARG_CHECK(gsm <= kGridSmemCap, "grid search too large for shared memory (reduce L0 or K)");
   const int C = cfg->candidates;
   const size_t dtab_b = align256((size_t)n * nk * sizeof(float));
   const size_t ctab_b = align256((size_t)(cfg->Lmax + 1) * (cfg->Lmax + 1) * sizeof(double));
@@ -508,7 +535,7 @@ extern "C" int mtb_search_orientations_static(const mtb_search_config* cfg, cons
   if (rc) return rc;
   MTB_CUDA_TRY(cudaFuncSetAttribute(so3_grid_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
   so3_grid_topk_kernel<<<B, kGridThreads, gsm, st>>>(reinterpret_cast<const float2*>(sigma), sigma_stride, B, dtab, L0,
-                                                     n, C, ca, cb, cg, nullptr);
+                                                     n, C, grid_jb(L0, cfg->K), ca, cb, cg, nullptr);
   MTB_LAUNCH_CHECK();
   NewtonParams NP;
   NP.Lmax = cfg->Lmax;
