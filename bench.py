@@ -287,22 +287,27 @@ def run_ours(args):
         ms = float(tms.item())
         dist.barrier()
     # end-to-end through the public API with host buffers
+    # (AlignmentStep.align_host: the volumes' host-to-device copy overlaps the alignment in
+    # four pieces; the results come back to pinned host memory every step)
     host = vols.cpu().pin_memory()
-    dvol = torch.empty_like(vols)
     res_host = torch.empty((B, 8), dtype=torch.float32).pin_memory()
     res_dev = torch.empty((B, 8), device=dev, dtype=torch.float32)
     e2e_start, e2e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e2e_steps = max(1, min(args.steps, 5))
-    e2e_start.record(st)
-    for _ in range(e2e_steps):
-        dvol.copy_(host, non_blocking=True)
+
+    def e2e_step():
         tracker.copy_(ident)
-        o = step(dvol, dvol, tracker, zeros3)
+        o = step.align_host(host, tracker, zeros3, chunks=4)
         res_dev[:, 0], res_dev[:, 1], res_dev[:, 2], res_dev[:, 3] = o["alpha"], o["beta"], o["gamma"], o["rotation_score"]
         res_dev[:, 4:7] = o["shift"]
         res_dev[:, 7] = o["shift_score"]
         res_host.copy_(res_dev, non_blocking=True)
+
+    e2e_step()  # untimed: allocates the staging buffer
+    torch.cuda.synchronize()
+    e2e_steps = max(1, min(args.steps, 5))
+    e2e_start.record(st)
+    for _ in range(e2e_steps):
+        e2e_step()
     e2e_end.record(st)
     torch.cuda.synchronize()
     e2e_ms = e2e_start.elapsed_time(e2e_end) / e2e_steps

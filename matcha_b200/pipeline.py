@@ -101,3 +101,51 @@ class AlignmentStep:
                       "mtb_shift_search")
         return dict(alpha=a, beta=b, gamma=g, rotation_score=score, bh_norms=norms[:B], tracker=tracker,
                     shift=self.shift[:B], shift_score=self.shift_score[:B])
+
+    _KEYS = ("alpha", "beta", "gamma", "rotation_score", "bh_norms", "shift", "shift_score")
+
+    @torch.no_grad()
+    def align_host(self, volumes_host: torch.Tensor, tracker: torch.Tensor, shift_zyx: torch.Tensor,
+                   chunks: int = 4):
+        """One alternation for a batch held in host memory (pinned for overlap).
+
+        The batch is cut into ``chunks`` pieces: the host-to-device copy of piece k + 1 runs
+        on a side stream while piece k is aligned on the current stream, so the transfer of
+        the volumes (4 N^3 bytes each) and the alignment overlap.  tracker (B, 4) float64 and
+        shift_zyx (B, 3) are device tensors; tracker is updated in place.  Returns the
+        outputs of ``__call__`` for the whole batch, in tensors of their own."""
+        B = volumes_host.shape[0]
+        if B > self.cfg.batch:
+            raise ValueError(f"batch {B} exceeds the configured batch {self.cfg.batch}")
+        dev = self.device
+        N = self.cfg.N
+        if getattr(self, "_stage", None) is None:
+            self._stage = torch.empty((self.cfg.batch, N, N, N), device=dev, dtype=torch.float32)
+            self._copy_stream = torch.cuda.Stream(device=dev)
+            self._out = {k: torch.empty((self.cfg.batch,) + ((3,) if k == "shift" else ()), device=dev,
+                                        dtype=torch.float32) for k in self._KEYS}
+        stage, cs = self._stage, self._copy_stream
+        compute = torch.cuda.current_stream(dev)
+        cs.wait_stream(compute)  # the previous call's reads of the staging buffer come first
+        bounds = [B * k // chunks for k in range(chunks + 1)]
+        ready = []
+        with torch.cuda.stream(cs):
+            for k in range(chunks):
+                lo, hi = bounds[k], bounds[k + 1]
+                if hi > lo:
+                    stage[lo:hi].copy_(volumes_host[lo:hi], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(cs)
+                ready.append(ev)
+        for k in range(chunks):
+            lo, hi = bounds[k], bounds[k + 1]
+            compute.wait_event(ready[k])
+            if hi == lo:
+                continue
+            vols = stage[lo:hi]
+            o = self(vols, vols, tracker[lo:hi], shift_zyx[lo:hi])
+            for key in self._KEYS:
+                self._out[key][lo:hi].copy_(o[key])
+        out = {k: self._out[k][:B] for k in self._KEYS}
+        out["tracker"] = tracker
+        return out

@@ -1,0 +1,52 @@
+"""AlignmentStep: the host-input entry (pipelined copies) against the device-input step."""
+import numpy as np
+import pytest
+import torch
+
+from tests.helpers import blob_template
+
+pytestmark = pytest.mark.gpu
+
+
+def _step(dev, B):
+    from matcha_b200.pipeline import AlignmentStep, StepConfig
+
+    return AlignmentStep(StepConfig(N=16, L=12, Li=[4, 8], batch=B, radius=7, shift_search_radius=1,
+                                    shift_upsample_factor=4), dev)
+
+
+@pytest.mark.parametrize("chunks", [1, 3, 8])
+def test_align_host_matches_device_step(cuda_device, chunks):
+    B, N = 6, 16
+    rng = np.random.default_rng(11)
+    tmpl = blob_template(rng, N, 12, 5, (1.0, 2.0), mask_radius=7).astype(np.float32)
+    vols = (np.repeat(tmpl[None], B, 0) + 0.05 * rng.standard_normal((B, N, N, N))).astype(np.float32)
+    step = _step(cuda_device, B)
+    step.set_template(tmpl)
+    ident = torch.zeros((B, 4), dtype=torch.float64, device=cuda_device)
+    ident[:, 0] = 1
+    zeros3 = torch.zeros((B, 3), device=cuda_device)
+
+    t_dev = ident.clone()
+    dv = torch.from_numpy(vols).to(cuda_device)
+    ref = {k: v.clone() for k, v in step(dv, dv, t_dev, zeros3).items()}
+    torch.cuda.synchronize()
+
+    host = torch.from_numpy(vols).pin_memory()
+    for _ in range(2):  # the second call reuses the staging buffer
+        t_host = ident.clone()
+        out = step.align_host(host, t_host, zeros3, chunks=chunks)
+        torch.cuda.synchronize()
+        assert out["tracker"] is t_host
+        for k in ("alpha", "beta", "gamma", "rotation_score", "bh_norms", "shift", "shift_score"):
+            np.testing.assert_allclose(out[k].cpu().numpy(), ref[k].cpu().numpy(), rtol=1e-5, atol=1e-6,
+                                       err_msg=k)
+        np.testing.assert_allclose(t_host.cpu().numpy(), t_dev.cpu().numpy(), atol=1e-6)
+
+
+def test_align_host_rejects_oversize_batch(cuda_device):
+    step = _step(cuda_device, 2)
+    host = torch.zeros((3, 16, 16, 16)).pin_memory()
+    with pytest.raises(ValueError):
+        step.align_host(host, torch.zeros((3, 4), dtype=torch.float64, device=cuda_device),
+                        torch.zeros((3, 3), device=cuda_device))
