@@ -62,12 +62,17 @@ size_t grid_smem_bytes(int L0, int K) { return grid_smem_bytes(L0, K, grid_jb(L0
 //   G_j[m'][g] = sum_m F_j[m'][m] e^{2 pi i g m / n}
 //   f_j[a][g]  = Re sum_{m'} G_j[m'][g] e^{2 pi i a m' / n} / n^2
 // with the running top-C of every thread merged at the end.
+// L0T, NT > 0 fix L0 and n at compile time (the index arithmetic then folds to constants);
+// 0 takes them from the arguments.
+template <int L0T, int NT>
 __global__ void __launch_bounds__(kGridThreads)
 so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
-                     const float* __restrict__ dtab, int L0, int n, int C, int JB,
+                     const float* __restrict__ dtab, int L0_arg, int n_arg, int C, int JB,
                      float* __restrict__ alpha, float* __restrict__ beta, float* __restrict__ gamma,
                      float* __restrict__ grid_out) {
   extern __shared__ __align__(16) float gsm[];
+  const int L0 = L0T > 0 ? L0T : L0_arg;
+  const int n = NT > 0 ? NT : n_arg;
   const int P = 2 * L0 - 1;
   const int nk = mtb_dsize(L0 - 1);
   float2* sg = reinterpret_cast<float2*>(gsm);  // nk
@@ -106,11 +111,23 @@ so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
       const int l0 = max(abs(mp), abs(m));
       const float* dj = dtab + (int64_t)(j0 + jb) * nk;
       float re = 0.f, im = 0.f;
-      for (int l = l0; l < L0; ++l) {
-        const int idx = mtb_dsize(l - 1) + (mp + l) * (2 * l + 1) + (m + l);
-        const float d = __ldg(&dj[idx]);
-        re += d * sg[idx].x;
-        im += d * sg[idx].y;
+      if (L0T > 0) {
+#pragma unroll
+        for (int l = 0; l < L0T; ++l) {
+          if (l >= l0) {
+            const int idx = mtb_dsize(l - 1) + (mp + l) * (2 * l + 1) + (m + l);
+            const float d = __ldg(&dj[idx]);
+            re += d * sg[idx].x;
+            im += d * sg[idx].y;
+          }
+        }
+      } else {
+        for (int l = l0; l < L0; ++l) {
+          const int idx = mtb_dsize(l - 1) + (mp + l) * (2 * l + 1) + (m + l);
+          const float d = __ldg(&dj[idx]);
+          re += d * sg[idx].x;
+          im += d * sg[idx].y;
+        }
       }
       F[q] = make_float2(re, im);
     }
@@ -202,6 +219,26 @@ so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
     }
     __syncthreads();
   }
+}
+
+template <int L0T, int NT>
+int grid_launch_t(const float2* sigma, int64_t stride, int B, const float* dtab, int L0, int K, int C, float* a,
+                  float* b, float* g, float* grid, cudaStream_t st) {
+  const size_t smem = grid_smem_bytes(L0, K);
+  MTB_CUDA_TRY(cudaFuncSetAttribute(so3_grid_topk_kernel<L0T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+  so3_grid_topk_kernel<L0T, NT><<<B, kGridThreads, smem, st>>>(sigma, stride, B, dtab, L0, 2 * L0 * K, C,
+                                                               grid_jb(L0, K), a, b, g, grid);
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
+}
+
+// The grid search for L0 = 8, n = 32 (the reference's default march) with its index
+// arithmetic fixed at compile time; other grids take the general instantiation.
+int grid_launch(const float2* sigma, int64_t stride, int B, const float* dtab, int L0, int K, int C, float* a,
+                float* b, float* g, float* grid, cudaStream_t st) {
+  if (L0 == 8 && K == 2) return grid_launch_t<8, 32>(sigma, stride, B, dtab, L0, K, C, a, b, g, grid, st);
+  return grid_launch_t<0, 0>(sigma, stride, B, dtab, L0, K, C, a, b, g, grid, st);
 }
 
 __global__ void reduce_candidates_kernel(const float* __restrict__ ca, const float* __restrict__ cb,
@@ -357,14 +394,8 @@ extern "C" int mtb_so3_grid_topk(mtb_search* h, const float* sigma, int64_t sigm
   if (B == 0) return MTB_OK;
   MTB_ARG_CHECK(sigma && alpha && beta && gamma, "null pointer");
   MTB_ARG_CHECK(sigma_stride >= mtb_dsize(h->cfg.L0 - 1), "sigma row shorter than dsize(L0-1)");
-  const int L0 = h->cfg.L0, n = h->n;
-  const size_t smem = grid_smem_bytes(L0, h->cfg.K);
-  MTB_CUDA_TRY(cudaFuncSetAttribute(so3_grid_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  so3_grid_topk_kernel<<<B, kGridThreads, smem, (cudaStream_t)stream>>>(
-      reinterpret_cast<const float2*>(sigma), sigma_stride, B, h->dtab, L0, n, h->cfg.candidates,
-      grid_jb(L0, h->cfg.K), alpha, beta, gamma, grid);
-  MTB_LAUNCH_CHECK();
-  return MTB_OK;
+  return grid_launch(reinterpret_cast<const float2*>(sigma), sigma_stride, B, h->dtab, h->cfg.L0, h->cfg.K,
+                     h->cfg.candidates, alpha, beta, gamma, grid, (cudaStream_t)stream);
 }
 
 extern "C" int mtb_newton_march(mtb_search* h, const float* sigma, int64_t sigma_stride, int B,
@@ -533,10 +564,9 @@ extern "C" int mtb_search_orientations_static(const mtb_search_config* cfg, cons
   MTB_LAUNCH_CHECK();
   int rc = newton_build_coef(cfg->Lmax, coef, st);
   if (rc) return rc;
-  MTB_CUDA_TRY(cudaFuncSetAttribute(so3_grid_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
-  so3_grid_topk_kernel<<<B, kGridThreads, gsm, st>>>(reinterpret_cast<const float2*>(sigma), sigma_stride, B, dtab, L0,
-                                                     n, C, grid_jb(L0, cfg->K), ca, cb, cg, nullptr);
-  MTB_LAUNCH_CHECK();
+  rc = grid_launch(reinterpret_cast<const float2*>(sigma), sigma_stride, B, dtab, L0, cfg->K, C, ca, cb, cg, nullptr,
+                   st);
+  if (rc) return rc;
   NewtonParams NP;
   NP.Lmax = cfg->Lmax;
   NP.n_stages = cfg->n_stages;
