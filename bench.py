@@ -35,8 +35,11 @@ sys.path.insert(0, ROOT)
 N_BOX, L_MAX, LI = 64, 32, [8, 16, 24]
 SHIFT_RADIUS, UPSAMPLE = 5, 8
 METRIC = "subtomograms/s at 64^3 L=32 (one alternation: FLE+sigma, SO(3) grid, Newton march, shift)"
-KERNELS_PER_STEP = 15  # fold, gemm, expand, sigma, grid, newton, reduce, tracker, bg, rfft_x, fft_y,
-# fft_z, updft1, updft23, finalize
+KERNELS_PER_STEP = 15  # FLE fold_split, gemm_tc, expand; sigma; SO(3) grid; fold_sigma, newton_march,
+# reduce_candidates; tracker_update; shift patch_fft_xy64, fft_z64, nyq, updft1_tc, updft23_tc, finalize_tc
+# DRAM bytes (read + write) of updft23_tc_kernel per subtomogram, from an ncu capture of the same kernel
+# at 200 subtomograms (dram__bytes_read.sum + dram__bytes_write.sum divided by 200)
+UPDFT23_DRAM_BYTES_PER_SUBTOMO = 1_539_000
 
 
 def parse():
@@ -273,6 +276,7 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
+        step.shifter.profile(args.steps)  # CUDA events between the shift match's kernel groups
         torch.cuda.nvtx.range_push("timed")  # lets a profiler select the timed launches
         start.record(st)
         for _ in range(args.steps):
@@ -281,6 +285,8 @@ def run_ours(args):
         torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
     ms = start.elapsed_time(end) / args.steps
+    shift_prof, shift_calls = step.shifter.profile_read()
+    step.shifter.profile(0)
     if world > 1:
         tms = torch.tensor([ms], device=dev)
         dist.all_reduce(tms, op=dist.ReduceOp.MAX)
@@ -327,16 +333,17 @@ def run_ours(args):
     pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pp):
         peaks = json.load(open(pp))
-    # roofline of the Newton march (FP32 CUDA cores): algorithmic flops per launch,
-    # sum over stages of (15 + 2) * 8 * C * Dsize(Li) * steps + 8 * C * Dsize(Li), per subtomogram
-    from matcha_b200.core.wigner_index import dsize
-
-    C, steps_n = 10, 1
-    flop_sub = sum((15 + 2) * 8 * C * dsize(l) * steps_n + 8 * C * dsize(l) for l in LI + [L_MAX])
-    achieved = flop_sub * B / (t_march * 1e-3) / 1e12
+    # roofline of the dominant kernel, the fused passes 2+3 of the shift match's upsampled DFT
+    # (tcgen05, BF16 hi+lo split): algorithmic FLOP per subtomogram = the three split GEMM
+    # segments of pass 2 (rows U*N/2, N-tile 2U, K 2N) and pass 3 (rows U^2, U columns, K N + 2
+    # with the Nyquist pair), 2*M*N*K each; its time per launch from the events recorded
+    # around it in every timed step
+    U = int(np.ceil(UPSAMPLE * (2 * SHIFT_RADIUS + 1)))
+    flop_sub = 3 * (2 * (U * N_BOX // 2) * (2 * U) * (2 * N_BOX) + 2 * U * U * U * (N_BOX + 2))
+    t_k = shift_prof["updft_pass23"] / max(1, shift_calls)
+    achieved = flop_sub * B / (t_k * 1e-3) / 1e12 if t_k > 0 else None
     clocks = clk.summary()
-    fp32_peak = 148 * 128 * 2 * (clocks["sm_mhz"] or 1965.0) * 1e6 / 1e12
-    peak = float(peaks.get("bf16_tflops", 1590.0))
+    peak = float(peaks.get("bf16_tflops_sustained", 1400.0))
     line = {
         "metric": METRIC,
         "value": world * B / (ms * 1e-3),
@@ -356,11 +363,13 @@ def run_ours(args):
         "median_rot_err_deg": float(np.median(err)),
         "p90_rot_err_deg": float(np.percentile(err, 90)),
         "stages_ms": stages,
-        "roofline": {"kernel": "newton_march_kernel", "bound": "tensor", "achieved": achieved,
-                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "fp32_core_peak_tflops": fp32_peak, "fp32_core_frac": achieved / fp32_peak,
-                     "kernel_ms": t_march, "traffic": None,
-                     "note": "FP32 CUDA-core kernel; peak is the measured bf16 tensor figure"},
+        "roofline": {"kernel": "updft23_tc_kernel", "bound": "tensor", "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
+                     "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (kernel timed inside long steps)",
+                     "kernel_ms": t_k, "flop_per_subtomogram": flop_sub,
+                     "traffic": (UPDFT23_DRAM_BYTES_PER_SUBTOMO * B) if UPDFT23_DRAM_BYTES_PER_SUBTOMO else None,
+                     "traffic_unit": "bytes per launch"},
+        "shift_kernel_ms_per_step": {k: v / max(1, shift_calls) for k, v in shift_prof.items()},
         "e2e": {"value": world * B / (e2e_ms * 1e-3), "unit": "subtomograms/s",
                 "h2d_bytes_per_step": int(B * N_BOX ** 3 * 4), "d2h_bytes_per_step": int(B * 8 * 4)},
         "gpu_launches": KERNELS_PER_STEP * args.steps,

@@ -226,6 +226,16 @@ int mtb_shift_search(mtb_shift* h, const float* subtomos, const float* shift_zyx
  * path gave up since the handle was created (then its results are invalid). */
 int mtb_shift_status(mtb_shift* h, mtb_stream_t stream);
 
+/* Launch profile of mtb_shift_search (no counterpart in the reference; instrumentation):
+ * with n_calls > 0 every search records CUDA events on its stream between its kernel
+ * groups, in a ring of the last n_calls calls (0 switches it off).  mtb_shift_profile_read
+ * synchronises on the recorded events and returns in ms[0..5] the summed time of
+ * (patch + xy FFT, z FFT + product, Nyquist plane, upsampled-DFT pass 1, passes 2+3,
+ * finalize) over those calls and their number in *calls.  For the FP32 path the Nyquist
+ * entry spans no kernel and pass 1 / passes 2+3 are its two upsampled-DFT kernels. */
+int mtb_shift_profile(mtb_shift* h, int n_calls);
+int mtb_shift_profile_read(mtb_shift* h, float* ms, int* calls);
+
 /* Rotation bookkeeping on the device: tracker <- normalized(tracker * conj(swap_xz(q(a, b, g))))
  * as update_rotation_estimate (src/matcha/utils/rotation_ops.py:23-34), and rot (B, 9), the
  * matrix the shift match uses for the new tracker (ShiftMatcher.py:503, :913).  alpha, beta,

@@ -90,6 +90,8 @@ SIGNATURES = {
     "mtb_shift_destroy": (None, [_P]),
     "mtb_shift_set_reference": (_I, [_P, _P, _P]),
     "mtb_shift_status": (_I, [_P, _P]),
+    "mtb_shift_profile": (_I, [_P, _I]),
+    "mtb_shift_profile_read": (_I, [_P, _P, _P]),
     "mtb_shift_search": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P]),
     "mtb_update_rotation": (_I, [_P, _P, _P, _P, _I, _P, _P, _P]),
 }

@@ -150,6 +150,26 @@ class ShiftMatcher:
             with torch.cuda.device(self.device):
                 nat.check(self._lib.mtb_shift_status(self._h, nat.stream_ptr(self.device)), "mtb_shift_status")
 
+    PROFILE_STAGES = ("patch_xy_fft", "z_fft_product", "nyquist", "updft_pass1", "updft_pass23", "finalize")
+
+    def profile(self, n_calls: int):
+        """Record the device time of each kernel group of the next ``n_calls`` searches
+        (extension; 0 switches it off).  The handle must exist (after a first search)."""
+        if self._h is None:
+            raise RuntimeError("profile() needs a shift handle: run search_shifts once first")
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.mtb_shift_profile(self._h, int(n_calls)), "mtb_shift_profile")
+
+    def profile_read(self):
+        """(summed ms per kernel group as a dict, number of calls) of the recorded searches."""
+        if self._h is None:
+            return {k: 0.0 for k in self.PROFILE_STAGES}, 0
+        ms = (ctypes.c_float * len(self.PROFILE_STAGES))()
+        calls = ctypes.c_int()
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.mtb_shift_profile_read(self._h, ms, ctypes.byref(calls)), "mtb_shift_profile_read")
+        return dict(zip(self.PROFILE_STAGES, list(ms))), calls.value
+
     def _free(self):
         if self._h is not None and self._h.value:
             self._lib.mtb_shift_destroy(self._h)

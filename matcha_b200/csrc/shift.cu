@@ -863,7 +863,18 @@ struct mtb_shift {
   bool has_ref;
   ShiftTc tc;
   bool use_tc;
+  // launch profile: kProfMarks events per call in a ring of prof_cap calls
+  int prof_cap, prof_n;
+  std::vector<cudaEvent_t>* prof_ev;
 };
+
+namespace {
+constexpr int kProfMarks = 7;  // start, after xy, after z, after Nyquist, after pass 1, after passes 2+3, end
+
+void prof_mark(mtb_shift* h, int k, cudaStream_t st) {
+  if (h->prof_cap > 0) cudaEventRecord((*h->prof_ev)[(h->prof_n % h->prof_cap) * kProfMarks + k], st);
+}
+}  // namespace
 
 // The front of the pipeline for box size N: with B > 0 the patch / xy-FFT and the z-FFT +
 // product of B subtomograms (into T, or into the tensor-core operand A1); with B == 0 the
@@ -882,6 +893,7 @@ int shift_front_n(mtb_shift* h, const float* subtomos, const float* shift_zyx, c
   MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
   patch_fft_xy_kernel<N, false><<<dim3(N, B), kT, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, g, h->T, h->bg);
   MTB_LAUNCH_CHECK();
+  prof_mark(h, 1, st);
   if (h->use_tc) {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
     fft_z_kernel<N, true><<<dim3(N, B), kT, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm,
@@ -902,6 +914,7 @@ int shift_front_64(mtb_shift* h, const float* subtomos, const float* shift_zyx, 
   MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
   patch_fft_xy64_kernel<<<dim3(64, B), kT64, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, h->fill_tab, g, h->T, h->bg);
   MTB_LAUNCH_CHECK();
+  prof_mark(h, 1, st);
   if (h->use_tc) {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
     fft_z64_kernel<true><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
@@ -1028,6 +1041,7 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
 
 extern "C" void mtb_shift_destroy(mtb_shift* h) {
   if (!h) return;
+  mtb_shift_profile(h, 0);
   shift_tc_release(&h->tc);
   void* ptrs[] = {h->bgw_tab, h->fill_tab, h->what, h->refq, h->ref, h->E0, h->E1, h->E2, h->bg, h->nrm, h->T, h->X1, h->pval, h->pidx};
   for (void* p : ptrs) if (p) cudaFree(p);
@@ -1069,26 +1083,74 @@ extern "C" int mtb_shift_search(mtb_shift* h, const float* subtomos, const float
   const int N = g.N, H = g.H, U = g.U;
   MTB_CUDA_TRY(cudaMemsetAsync(h->bg, 0, (size_t)B * 4, st));
   MTB_CUDA_TRY(cudaMemsetAsync(h->nrm, 0, (size_t)B * 8, st));
+  prof_mark(h, 0, st);
   int rc = shift_front(h, subtomos, shift_zyx, rot, ctf, B, st);
   if (rc) return rc;
+  prof_mark(h, 2, st);
   if (h->use_tc) {
-    rc = shift_tc_passes(&h->tc, B, st);
+    cudaEvent_t marks[3] = {nullptr, nullptr, nullptr};
+    if (h->prof_cap > 0)
+      for (int k = 0; k < 3; ++k) marks[k] = (*h->prof_ev)[(h->prof_n % h->prof_cap) * kProfMarks + 3 + k];
+    rc = shift_tc_passes(&h->tc, B, st, marks);
     if (rc) return rc;
     finalize_tc_kernel<<<(B + 127) / 128, 128, 0, st>>>(g, B, h->tc.best, h->nrm, shift_xyz, score);
     MTB_LAUNCH_CHECK();
+    prof_mark(h, 6, st);
+    if (h->prof_cap > 0) ++h->prof_n;
     return MTB_OK;
   }
   const size_t sm1 = (size_t)(U * N + N * kColTile) * 8;
   MTB_CUDA_TRY(cudaFuncSetAttribute(updft1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+  prof_mark(h, 3, st);
   updft1_kernel<<<dim3((N * H + kColTile - 1) / kColTile, B), kT, sm1, st>>>(g, h->T, h->E0, h->X1);
   MTB_LAUNCH_CHECK();
+  prof_mark(h, 4, st);
   const size_t sm2 = (size_t)(U * N + U * H + N * H + U * H) * 8;
   MTB_ARG_CHECK(sm2 <= 220 * 1024 && sm1 <= 220 * 1024, "upsampled region too large for shared memory");
   MTB_CUDA_TRY(cudaFuncSetAttribute(updft23_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
   updft23_kernel<<<dim3(h->ngrp, B), kT, sm2, st>>>(g, h->X1, h->E1, h->E2, h->rows_per_cta, h->pval, h->pidx);
   MTB_LAUNCH_CHECK();
+  prof_mark(h, 5, st);
   finalize_kernel<<<(B + 127) / 128, 128, 0, st>>>(g, B, h->ngrp, h->pval, h->pidx, h->nrm, shift_xyz, score);
   MTB_LAUNCH_CHECK();
+  prof_mark(h, 6, st);
+  if (h->prof_cap > 0) ++h->prof_n;
+  return MTB_OK;
+}
+
+extern "C" int mtb_shift_profile(mtb_shift* h, int n_calls) {
+  MTB_ARG_CHECK(h, "null handle");
+  MTB_ARG_CHECK(n_calls >= 0 && n_calls <= 4096, "n_calls must be in [0, 4096]");
+  if (h->prof_ev) {
+    for (cudaEvent_t e : *h->prof_ev) cudaEventDestroy(e);
+    delete h->prof_ev;
+    h->prof_ev = nullptr;
+  }
+  h->prof_cap = 0;
+  h->prof_n = 0;
+  if (n_calls == 0) return MTB_OK;
+  h->prof_ev = new std::vector<cudaEvent_t>((size_t)n_calls * kProfMarks, nullptr);
+  for (auto& e : *h->prof_ev) MTB_CUDA_TRY(cudaEventCreate(&e));
+  h->prof_cap = n_calls;
+  return MTB_OK;
+}
+
+extern "C" int mtb_shift_profile_read(mtb_shift* h, float* ms, int* calls) {
+  MTB_ARG_CHECK(h && ms && calls, "null argument");
+  for (int k = 0; k < kProfMarks - 1; ++k) ms[k] = 0.f;
+  *calls = 0;
+  if (h->prof_cap == 0 || h->prof_n == 0) return MTB_OK;
+  const int n = h->prof_n < h->prof_cap ? h->prof_n : h->prof_cap;
+  for (int c = 0; c < n; ++c) {
+    cudaEvent_t* e = h->prof_ev->data() + (size_t)c * kProfMarks;
+    MTB_CUDA_TRY(cudaEventSynchronize(e[kProfMarks - 1]));
+    for (int k = 0; k < kProfMarks - 1; ++k) {
+      float t = 0.f;
+      MTB_CUDA_TRY(cudaEventElapsedTime(&t, e[k], e[k + 1]));
+      ms[k] += t;
+    }
+  }
+  *calls = n;
   return MTB_OK;
 }
 

@@ -884,7 +884,7 @@ void shift_tc_release(ShiftTc* t) {
   memset(t, 0, sizeof(*t));
 }
 
-int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st) {
+int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st, const cudaEvent_t* marks) {
   MTB_CUDA_TRY(cudaMemsetAsync(t->best, 0, (size_t)B * 8, st));
   const int N = t->N, U = t->U, HH = t->HH;
   // Nyquist plane
@@ -892,6 +892,7 @@ int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st) {
   MTB_CUDA_TRY(cudaFuncSetAttribute(nyq_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)snyq));
   nyq_kernel<<<B, kNyqThreads, snyq, st>>>(t->p32, t->E, N, U, t->nyq);
   MTB_LAUNCH_CHECK();
+  if (marks && marks[0]) cudaEventRecord(marks[0], st);
   // pass 1
   Pass1 p1;
   p1.rows = B * HH * N;
@@ -910,6 +911,7 @@ int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st) {
                                                    *reinterpret_cast<const CUtensorMap*>(t->mapE1), p1,
                                                    (uint32_t*)t->A2, t->err);
   MTB_LAUNCH_CHECK();
+  if (marks && marks[1]) cudaEventRecord(marks[1], st);
   // passes 2 + 3
   Pass23 p2;
   p2.B = B;
@@ -931,6 +933,7 @@ int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st) {
                                                      *reinterpret_cast<const CUtensorMap*>(t->mapE3), p2, t->nyq,
                                                      (const uint4*)t->ENQ, t->best, t->err);
   MTB_LAUNCH_CHECK();
+  if (marks && marks[2]) cudaEventRecord(marks[2], st);
   return MTB_OK;
 }
 

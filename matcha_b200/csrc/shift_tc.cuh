@@ -30,6 +30,7 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
 void shift_tc_release(ShiftTc* t);
 // Nyquist plane, pass 1 and fused passes 2+3 for B subtomograms whose pass-1 operand A1 and
 // Nyquist plane p32 have been written (fft_z split).
-int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st);
+// marks (or null): events recorded on st after the Nyquist kernel, pass 1 and passes 2+3.
+int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st, const cudaEvent_t* marks = nullptr);
 // Synchronises st; MTB_ERR_TIMEOUT if a device-side wait gave up.
 int shift_tc_check(ShiftTc* t, cudaStream_t st);

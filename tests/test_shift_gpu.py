@@ -71,3 +71,28 @@ def test_shift_requires_reference(cuda_device):
     with pytest.raises(RuntimeError):
         sm.search_shifts(subtomos=torch.zeros((1, 16, 16, 16), device=cuda_device), ctfs=None,
                          shift_zyx=torch.zeros((1, 3), device=cuda_device), rotation_tracker=np.array([[1.0, 0, 0, 0]]))
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3"])
+def test_shift_profile_records_kernel_groups(cuda_device, precision):
+    N, B = 32, 2
+    rng = np.random.default_rng(3)
+    tmpl = blob_template(rng, N, 30, N * 0.3, (1.5, 3.0), mask_radius=N * 0.4)
+    vols = torch.from_numpy(np.repeat(tmpl[None], B, 0)).to(cuda_device)
+    sm = _matcher(N, B, 8, 3, cuda_device, precision=precision)
+    sm.set_reference(tmpl)
+    q = np.tile([1.0, 0, 0, 0], (B, 1))
+    z = torch.zeros((B, 3), device=cuda_device)
+    first = sm.search_shifts(subtomos=vols, ctfs=None, shift_zyx=z, rotation_tracker=q)
+    sm.profile(3)
+    for _ in range(2):
+        again = sm.search_shifts(subtomos=vols, ctfs=None, shift_zyx=z, rotation_tracker=q)
+    ms, calls = sm.profile_read()
+    assert calls == 2
+    assert set(ms) == set(sm.PROFILE_STAGES)
+    assert all(v >= 0 for v in ms.values()) and ms["patch_xy_fft"] > 0 and ms["updft_pass23"] > 0
+    if precision == "bf16x3":  # the FP32 path has no Nyquist kernel: its entry is two adjacent events
+        assert ms["nyquist"] > 0
+    sm.profile(0)
+    assert sm.profile_read() == ({k: 0.0 for k in sm.PROFILE_STAGES}, 0)
+    np.testing.assert_array_equal(again[0].cpu().numpy(), first[0].cpu().numpy())
