@@ -39,7 +39,7 @@ KERNELS_PER_STEP = 15  # FLE fold_split, gemm_tc, expand; sigma; SO(3) grid; fol
 # reduce_candidates; tracker_update; shift patch_fft_xy64, fft_z64, nyq, updft1_tc, updft23_tc, finalize_tc
 # DRAM bytes (read + write) of updft23_tc_kernel per subtomogram, from an ncu capture of the same kernel
 # at 200 subtomograms (dram__bytes_read.sum + dram__bytes_write.sum divided by 200)
-UPDFT23_DRAM_BYTES_PER_SUBTOMO = 1_539_000
+UPDFT23_DRAM_BYTES_PER_SUBTOMO = 1_526_000
 
 
 def parse():

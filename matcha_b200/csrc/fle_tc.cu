@@ -72,7 +72,9 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
   __shared__ int abort_flag;
 
   const int cls = blockIdx.z;
-  const int n0 = blockIdx.x * TN, m0 = blockIdx.y * TM;
+  // M tiles vary fastest: the CTAs of one basis N-tile run together and read its B slab from
+  // L2 rather than once per M tile from DRAM
+  const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
   if (n0 >= P.ncols[cls]) return;  // uniform per CTA
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -325,7 +327,7 @@ int fle_tc_forward(FleTc* t, const float* vol, int64_t vol_stride, int B, const 
   P.ldc = t->n_cols;
   const size_t smem = (size_t)STAGES * STAGE_BYTES + 1024;
   MTB_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 gg(t->Npad / TN, (B + TM - 1) / TM, 8);
+  dim3 gg((B + TM - 1) / TM, t->Npad / TN, 8);
   gemm_tc_kernel<<<gg, kThreads, smem, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA),
                                              *reinterpret_cast<const CUtensorMap*>(t->mapB), P, C, t->err);
   MTB_LAUNCH_CHECK();

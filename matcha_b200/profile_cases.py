@@ -1,0 +1,96 @@
+"""Small, self-contained runs of each stage of the alignment path, for profilers.
+
+    python -m matcha_b200.profile_cases shift  200   # ShiftMatcher.search_shifts, 64^3, uf 8, r 5
+    python -m matcha_b200.profile_cases search 296   # Matcha.search_orientations, L 32, C 10
+    python -m matcha_b200.profile_cases fle    256   # CrossCorrelationMatcher.get_sigma, 64^3, L 32
+
+Each case builds its inputs on the device from a fixed seed (random volumes, Haar rotations,
+random shifts; a synthetic sigma with a known optimum for the search), runs the stage three
+times untimed, then ``--reps`` more times between CUDA events and prints the mean time per
+call.  A kernel profiler attached to the process sees the same launches the bench makes for
+that stage, on a batch small enough to capture quickly.
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+
+import numpy as np
+import torch
+
+
+class _Cfg(dict):
+    __getattr__ = dict.__getitem__
+
+
+def _shift(B: int, dev):
+    from .core.ShiftMatcher import ShiftMatcher
+
+    N = 64
+    cfg = _Cfg(N=N, voxel_size=1.0, num_subtomograms_per_batch=B, shift_upsample_factor=8, shift_search_radius=5,
+               do_ctf_correction=False, box_size=N)
+    sm = ShiftMatcher(cfg, dev, torch.complex64, precision="bf16x3")
+    rng = np.random.default_rng(0)
+    sm.set_reference(rng.standard_normal((N, N, N)).astype(np.float32))
+    vols = torch.randn(B, N, N, N, device=dev)
+    q = rng.standard_normal((B, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    z = torch.from_numpy(rng.uniform(-2, 2, (B, 3)).astype(np.float32)).to(dev)
+    return lambda: sm.search_shifts(subtomos=vols, ctfs=None, shift_zyx=z, rotation_tracker=q)
+
+
+def _search(B: int, dev):
+    from .core.Matcha import Matcha
+    from .core.wigner_index import compute_size
+
+    L = 32
+    rng = np.random.default_rng(0)
+    n = compute_size(L + 1)
+    sig = (rng.standard_normal((B, n)) + 1j * rng.standard_normal((B, n))).astype(np.complex64)
+    st = torch.from_numpy(sig).to(dev)
+    m = Matcha(batchsize=B, device=dev, L_max=L, matcha_config=dict(Li=[8, 16, 24, 32], candidates=10,
+                                                                   num_steps=1))
+    return lambda: m.search_orientations(st)
+
+
+def _fle(B: int, dev):
+    from .core.CrossCorrelationMatcher import CrossCorrelationMatcher
+
+    N = 64
+    cc = CrossCorrelationMatcher(N=N, device=dev, batchsize=B, bandlimit=32, radius=30, precision_mode="fast",
+                                 precision="bf16x3")
+    rng = np.random.default_rng(0)
+    cc.set_template(rng.standard_normal((N, N, N)).astype(np.float32))
+    vols = torch.randn(B, N, N, N, device=dev)
+    return lambda: cc.get_sigma_upto(vols, 32)
+
+
+CASES = {"shift": _shift, "search": _search, "fle": _fle}
+
+
+def main(argv=None) -> int:
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("case", choices=sorted(CASES))
+    p.add_argument("batch", type=int)
+    p.add_argument("--reps", type=int, default=5)
+    a = p.parse_args(argv)
+    if not torch.cuda.is_available():
+        print("a CUDA device is required", file=sys.stderr)
+        return 2
+    dev = torch.device("cuda:0")
+    run = CASES[a.case](a.batch, dev)
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.reps):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    print(f"{a.case} batch {a.batch}: {e0.elapsed_time(e1) / a.reps:.3f} ms per call")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

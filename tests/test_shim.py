@@ -30,3 +30,13 @@ def test_install_routes_reference_modules(monkeypatch):
     finally:
         shim.uninstall()
     assert "matcha.core.Matcha" not in sys.modules
+
+
+def test_profile_cases_needs_a_device(monkeypatch):
+    import torch
+
+    from matcha_b200 import profile_cases
+
+    monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
+    assert profile_cases.main(["shift", "2"]) == 2
+    assert set(profile_cases.CASES) == {"shift", "search", "fle"}
