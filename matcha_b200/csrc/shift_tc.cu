@@ -389,25 +389,26 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
   const int B1 = NT12 * TK * 2, B3 = NT3 * TK * 2;
   uint8_t* sE1 = smem;                       // [part][kb] B1
   uint8_t* sE3 = sE1 + 2 * KB * B1;          // [part] B3
-  uint8_t* sA = sE3 + 2 * B3;                // [2 stages][part] A_TILE
-  uint8_t* sA3 = sA + 4 * A_TILE;            // [part] A_TILE
-  uint8_t* sAn = sA3 + 2 * A_TILE;           // [part] 128 x 16 Nyquist operand, no swizzle
-  uint8_t* sBn = sAn + 2 * kNqA;             // [part] NT3 x 16, no swizzle
-  __shared__ __align__(8) uint64_t full_bar[2], empty_bar[2];
-  __shared__ __align__(8) uint64_t resF, acc2F, acc2E, a3F, a3E, acc3F, acc3E;
+  // [2][part] A_TILE: the two K blocks of the tile's A2 rows, then (once pass 2 has read
+  // them) the two pass-3 operand buffers of alternate chunks
+  uint8_t* sA = sE3 + 2 * B3;
+  uint8_t* sAn = sA + 4 * A_TILE;            // [2][part] 128 x 16 Nyquist operand, no swizzle
+  uint8_t* sBn = sAn + 4 * kNqA;             // [part] NT3 x 16, no swizzle
+  __shared__ __align__(8) uint64_t full_bar[2], a3F[2], a3E[2];
+  __shared__ __align__(8) uint64_t resF, regionF, acc2F, acc2E, acc3F, acc3E;
   __shared__ uint32_t tmem_base;
   __shared__ volatile int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < 2; ++s) {
       mbar_init(&full_bar[s], 1);
-      mbar_init(&empty_bar[s], 1);
+      mbar_init(&a3F[s], kEpi);
+      mbar_init(&a3E[s], 1);
     }
     mbar_init(&resF, 1);
+    mbar_init(&regionF, 1);
     mbar_init(&acc2F, 1);
     mbar_init(&acc2E, kEpi);
-    mbar_init(&a3F, kEpi);
-    mbar_init(&a3E, 1);
     mbar_init(&acc3F, 1);
     mbar_init(&acc3E, kEpi);
     abort_flag = 0;
@@ -415,8 +416,8 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
   }
   // the pass-3 operands: K columns past N (and past the Nyquist pair) stay zero, rows not
   // written by a chunk are ignored; the Nyquist B operand comes prepared from the host
-  for (int i = threadIdx.x; i < (2 * A_TILE + 2 * kNqA) / 16; i += blockDim.x)
-    reinterpret_cast<uint4*>(sA3)[i] = make_uint4(0u, 0u, 0u, 0u);
+  for (int i = threadIdx.x; i < 4 * kNqA / 16; i += blockDim.x)
+    reinterpret_cast<uint4*>(sAn)[i] = make_uint4(0u, 0u, 0u, 0u);
   for (int i = threadIdx.x; i < 2 * NT3 * 32 / 16; i += blockDim.x) reinterpret_cast<uint4*>(sBn)[i] = bnq[i];
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (warp == 1) {
@@ -437,22 +438,21 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
       for (int kb = 0; kb < KB; ++kb) tma_load_2d(sE1 + (part * KB + kb) * B1, &mapE1, kb * TK, part * NT12, &resF);
       tma_load_2d(sE3 + part * B3, &mapE3, 0, part * NT3, &resF);
     }
-    int it = 0;
-    for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x) {
+    int tl = 0;
+    for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
       const int b = tile / p.TPB, tg = tile - (tile / p.TPB) * p.TPB;
       const int arow = (b * p.U + tg * p.G) * p.HH;
-      for (int kb = 0; kb < KB; ++kb, ++it) {
-        const int s = it & 1;
-        const uint32_t use = it >> 1;
-        if (it >= 2 && !mbar_wait(&empty_bar[s], (use - 1) & 1)) {
-          atomicExch(err, 31);
-          abort_flag = 1;
-          break;
-        }
-        uint8_t* sa = sA + s * 2 * A_TILE;
-        mbar_expect_tx(&full_bar[s], 2 * A_TILE);
-        tma_load_2d(sa, &mapA2, kb * TK, arow, &full_bar[s]);
-        tma_load_2d(sa + A_TILE, &mapA2, kb * TK, p.R2 + arow, &full_bar[s]);
+      // the region is free once the previous tile's pass-3 MMAs have read their operands
+      if (tl >= 1 && !mbar_wait(&regionF, (tl - 1) & 1)) {
+        atomicExch(err, 31);
+        abort_flag = 1;
+        break;
+      }
+      for (int kb = 0; kb < KB; ++kb) {
+        uint8_t* sa = sA + kb * 2 * A_TILE;
+        mbar_expect_tx(&full_bar[kb], 2 * A_TILE);
+        tma_load_2d(sa, &mapA2, kb * TK, arow, &full_bar[kb]);
+        tma_load_2d(sa + A_TILE, &mapA2, kb * TK, p.R2 + arow, &full_bar[kb]);
       }
     }
   } else if (warp == 1 && lane == 0) {
@@ -461,7 +461,7 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
       atomicExch(err, 32);
       abort_flag = 1;
     }
-    int it = 0, tl = 0, cc = 0;
+    int tl = 0, cc = 0;
     for (int tile = blockIdx.x; ok && tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
       // pass 2 into acc2 (columns 0 .. NT12)
       if (tl >= 1 && !mbar_wait(&acc2E, (tl - 1) & 1)) {
@@ -470,26 +470,24 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      for (int kb = 0; kb < KB; ++kb, ++it) {
-        const int s = it & 1;
-        const uint32_t use = it >> 1;
-        if (!mbar_wait(&full_bar[s], use & 1)) {
+      for (int kb = 0; kb < KB; ++kb) {
+        if (!mbar_wait(&full_bar[kb], tl & 1)) {
           atomicExch(err, 34);
           abort_flag = 1;
           ok = false;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint8_t* sa = sA + s * 2 * A_TILE;
+        const uint8_t* sa = sA + kb * 2 * A_TILE;
         mma_split_kblock(tmem, smem_desc(sa), smem_desc(sa + A_TILE), smem_desc(sE1 + kb * B1),
                          smem_desc(sE1 + (KB + kb) * B1), idesc2, kb == 0);
-        mma_commit_to(&empty_bar[s]);
       }
       if (!ok) break;
       mma_commit_to(&acc2F);
       // pass 3, chunk by chunk, into acc3 (columns NT12 + j NT3)
       for (int j = 0; j < p.CH; ++j, ++cc) {
-        if (!mbar_wait(&a3F, cc & 1)) {
+        const int q3 = cc & 1;
+        if (!mbar_wait(&a3F[q3], (cc >> 1) & 1)) {
           atomicExch(err, 35);
           abort_flag = 1;
           ok = false;
@@ -503,18 +501,21 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d3 = tmem + (uint32_t)(NT12 + j * NT3);
-        mma_split_kblock(d3, smem_desc(sA3), smem_desc(sA3 + A_TILE), smem_desc(sE3), smem_desc(sE3 + B3), idesc3,
+        const uint8_t* a3 = sA + q3 * 2 * A_TILE;
+        mma_split_kblock(d3, smem_desc(a3), smem_desc(a3 + A_TILE), smem_desc(sE3), smem_desc(sE3 + B3), idesc3,
                          true);
         // the Nyquist column m2 = N/2 as one more K step of 16
-        const uint64_t an_hi = smem_desc_k16(sAn), an_lo = smem_desc_k16(sAn + kNqA);
+        const uint8_t* an = sAn + q3 * 2 * kNqA;
+        const uint64_t an_hi = smem_desc_k16(an), an_lo = smem_desc_k16(an + kNqA);
         const uint64_t bn_hi = smem_desc_k16(sBn), bn_lo = smem_desc_k16(sBn + NT3 * 32);
         mma_bf16_id(d3, an_hi, bn_hi, idesc3, 1u);
         mma_bf16_id(d3, an_lo, bn_hi, idesc3, 1u);
         mma_bf16_id(d3, an_hi, bn_lo, idesc3, 1u);
-        mma_commit_to(&a3E);
+        mma_commit_to(&a3E[q3]);
       }
       if (!ok) break;
       mma_commit_to(&acc3F);
+      mma_commit_to(&regionF);
     }
   } else if (warp >= 2) {
     // warp (q, h): TMEM lanes 32 q .. 32 q + 31, half h of the columns it needs
@@ -544,7 +545,10 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
         const int cA = (2 * lo) & ~15, cB = min(NT12, (2 * hi + 15) & ~15);
         const int cM = cA + ((((cB - cA) >> 4) + 1) >> 1 << 4);  // h = 0 takes the first half
         const int ca = lo < hi ? (h ? cM : cA) : 0, cb_end = lo < hi ? (h ? cB : cM) : 0;
-        if (cc >= 1 && !mbar_wait(&a3E, (cc - 1) & 1)) {
+        const int q3 = cc & 1;
+        uint8_t* sA3 = sA + q3 * 2 * A_TILE;
+        uint8_t* sAnq = sAn + q3 * 2 * kNqA;
+        if (cc >= 2 && !mbar_wait(&a3E[q3], ((cc >> 1) - 1) & 1)) {
           atomicExch(err, 38);
           abort_flag = 1;
           ok = false;
@@ -561,12 +565,12 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
             const float2 y = nyq[((size_t)b * p.U + u0) * p.U + u1];
             uint32_t hi2, lo2;
             split2(y.x, y.y, hi2, lo2);
-            *reinterpret_cast<uint32_t*>(sAn + k16_word(threadIdx.x - 64)) = hi2;
-            *reinterpret_cast<uint32_t*>(sAn + kNqA + k16_word(threadIdx.x - 64)) = lo2;
+            *reinterpret_cast<uint32_t*>(sAnq + k16_word(threadIdx.x - 64)) = hi2;
+            *reinterpret_cast<uint32_t*>(sAnq + kNqA + k16_word(threadIdx.x - 64)) = lo2;
           }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive(&a3F);
+        mbar_arrive(&a3F[q3]);
       }
       if (!ok) break;
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -759,7 +763,7 @@ bool geometry(int N, int U, Geometry* o) {
   if (g.NT12 + g.CH * g.NT3 > 512) return false;
   const size_t b1 = (size_t)2 * g.KB12 * g.NT12 * TK * 2;
   const size_t b3 = (size_t)2 * g.NT3 * TK * 2;
-  g.smem23 = 1024 + b1 + b3 + 4 * (size_t)A_TILE + 2 * (size_t)A_TILE + 2 * (size_t)kNqA + (size_t)2 * g.NT3 * 32;
+  g.smem23 = 1024 + b1 + b3 + 4 * (size_t)A_TILE + 4 * (size_t)kNqA + (size_t)2 * g.NT3 * 32;
   if (g.smem23 > kSmemCap) return false;
   g.stages1 = (int)((kSmemCap - 1024 - b1) / (2 * (size_t)A_TILE));
   if (g.stages1 > kMaxStages) g.stages1 = kMaxStages;
