@@ -48,8 +48,8 @@ constexpr size_t kGridSmemCap = 200 * 1024;
 // Dynamic shared memory of the grid kernel: sigma (l < L0), the twiddle matrix, and the
 // F, G buffers of JB beta values.
 size_t grid_smem_bytes(int L0, int K, int JB) {
-  const int n = 2 * L0 * K, P = 2 * L0 - 1;
-  return (size_t)(mtb_dsize(L0 - 1) + n * P + JB * P * P + JB * P * n) * sizeof(float2);
+  const int n = 2 * L0 * K, P = 2 * L0 - 1, nk = mtb_dsize(L0 - 1);
+  return (size_t)(nk + n * P + JB * P * P + JB * P * n) * sizeof(float2) + (size_t)JB * nk * sizeof(float);
 }
 
 // Beta values per pass: four when they fit, else one.
@@ -63,8 +63,9 @@ size_t grid_smem_bytes(int L0, int K) { return grid_smem_bytes(L0, K, grid_jb(L0
 //   f_j[a][g]  = Re sum_{m'} G_j[m'][g] e^{2 pi i a m' / n} / n^2
 // with the running top-C of every thread merged at the end.
 // L0T, NT > 0 fix L0 and n at compile time (the index arithmetic then folds to constants);
-// 0 takes them from the arguments.
-template <int L0T, int NT>
+// 0 takes them from the arguments.  KC >= C is the capacity of each thread's kept set, held
+// in registers (statically indexed).
+template <int L0T, int NT, int KC>
 __global__ void __launch_bounds__(kGridThreads)
 so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
                      const float* __restrict__ dtab, int L0_arg, int n_arg, int C, int JB,
@@ -79,6 +80,7 @@ so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
   float2* TW = sg + nk;                          // n x P: e^{2 pi i g (c - L0 + 1) / n}
   float2* F = TW + n * P;                        // JB x P x P
   float2* G = F + JB * P * P;                    // JB x P x n
+  float* sD = reinterpret_cast<float*>(G + JB * P * n);  // JB x nk: d^l(beta_j) of this pass
   __shared__ float mv[kGridThreads / 32];
   __shared__ int mi[kGridThreads / 32];
   __shared__ int mt[kGridThreads / 32];
@@ -96,27 +98,46 @@ so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
     sincospi(2.0 * k / n, &sn, &cs);
     TW[q] = make_float2((float)cs, (float)sn);
   }
-  float tv[kMaxCand];
-  int ti[kMaxCand];
+  float tv[KC];
+  int ti[KC];
+#pragma unroll
+  for (int t = 0; t < KC; ++t) {
+    tv[t] = -INFINITY;
+    ti[t] = 0x7fffffff;
+  }
   int cnt = 0, minp = 0;
   float minv = -INFINITY;
   int mini = 0x7fffffff;
+  // the kept set's worst entry (for a full set of C)
+  auto find_min = [&]() {
+    minp = 0;
+    minv = tv[0];
+    mini = ti[0];
+#pragma unroll
+    for (int t = 1; t < KC; ++t)
+      if (t < C && better(minv, mini, tv[t], ti[t])) {
+        minp = t;
+        minv = tv[t];
+        mini = ti[t];
+      }
+  };
   const float inv_n2 = 1.f / (float)(n * n);
-  __syncthreads();
   for (int j0 = 0; j0 < n; j0 += JB) {
     const int jn = min(JB, n - j0);
+    for (int e = tid; e < jn * nk; e += blockDim.x) sD[e] = __ldg(&dtab[(int64_t)j0 * nk + e]);
+    __syncthreads();
     for (int q = tid; q < jn * P * P; q += blockDim.x) {
       const int jb = q / (P * P), qq = q - jb * (P * P);
       const int mp = qq / P - (L0 - 1), m = qq % P - (L0 - 1);
       const int l0 = max(abs(mp), abs(m));
-      const float* dj = dtab + (int64_t)(j0 + jb) * nk;
+      const float* dj = sD + jb * nk;
       float re = 0.f, im = 0.f;
       if (L0T > 0) {
 #pragma unroll
         for (int l = 0; l < L0T; ++l) {
           if (l >= l0) {
             const int idx = mtb_dsize(l - 1) + (mp + l) * (2 * l + 1) + (m + l);
-            const float d = __ldg(&dj[idx]);
+            const float d = dj[idx];
             re += d * sg[idx].x;
             im += d * sg[idx].y;
           }
@@ -124,7 +145,7 @@ so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
       } else {
         for (int l = l0; l < L0; ++l) {
           const int idx = mtb_dsize(l - 1) + (mp + l) * (2 * l + 1) + (m + l);
-          const float d = __ldg(&dj[idx]);
+          const float d = dj[idx];
           re += d * sg[idx].x;
           im += d * sg[idx].y;
         }
@@ -161,18 +182,15 @@ so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
       if (grid_out) grid_out[(int64_t)b * n * n * n + flat] = v;
       // the rejection test reads the kept set's worst entry from registers
       if (cnt < C || better(v, flat, minv, mini)) {
-        if (cnt < C) {
-          tv[cnt] = v; ti[cnt] = flat; ++cnt;
-        } else {
-          tv[minp] = v; ti[minp] = flat;
-        }
-        if (cnt == C) {
-          minp = 0;
-          for (int t = 1; t < cnt; ++t)
-            if (better(tv[minp], ti[minp], tv[t], ti[t])) minp = t;
-          minv = tv[minp];
-          mini = ti[minp];
-        }
+        const int slot = cnt < C ? cnt : minp;
+#pragma unroll
+        for (int t = 0; t < KC; ++t)
+          if (t == slot) {
+            tv[t] = v;
+            ti[t] = flat;
+          }
+        if (cnt < C) ++cnt;
+        if (cnt == C) find_min();
       }
     }
     __syncthreads();
@@ -181,12 +199,18 @@ so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
   const int lane = tid & 31, warp = tid >> 5;
   const float bstep = (float)(M_PI / (double)(n - 1));
   const float astep = (float)(2.0 * M_PI / (double)n);
+  uint32_t live = cnt >= 32 ? 0xffffffffu : ((1u << cnt) - 1u);
   for (int c = 0; c < C; ++c) {
     int hp = -1;
     float hv = -INFINITY;
     int hi = 0x7fffffff;
-    for (int t = 0; t < cnt; ++t)
-      if (hp < 0 || better(tv[t], ti[t], hv, hi)) { hp = t; hv = tv[t]; hi = ti[t]; }
+#pragma unroll
+    for (int t = 0; t < KC; ++t)
+      if (((live >> t) & 1u) && (hp < 0 || better(tv[t], ti[t], hv, hi))) {
+        hp = t;
+        hv = tv[t];
+        hi = ti[t];
+      }
     float v = hv;
     int i = hi, who = (hp < 0) ? -1 : tid;
     for (int o = 16; o > 0; o >>= 1) {
@@ -211,23 +235,18 @@ so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
       gamma[o] = (float)gg * astep;
     }
     __syncthreads();
-    if (mt[0] == tid && hp >= 0) {
-      // remove the taken entry
-      tv[hp] = tv[cnt - 1];
-      ti[hp] = ti[cnt - 1];
-      --cnt;
-    }
+    if (mt[0] == tid && hp >= 0) live &= ~(1u << hp);  // remove the taken entry
     __syncthreads();
   }
 }
 
-template <int L0T, int NT>
+template <int L0T, int NT, int KC>
 int grid_launch_t(const float2* sigma, int64_t stride, int B, const float* dtab, int L0, int K, int C, float* a,
                   float* b, float* g, float* grid, cudaStream_t st) {
   const size_t smem = grid_smem_bytes(L0, K);
-  MTB_CUDA_TRY(cudaFuncSetAttribute(so3_grid_topk_kernel<L0T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
-  so3_grid_topk_kernel<L0T, NT><<<B, kGridThreads, smem, st>>>(sigma, stride, B, dtab, L0, 2 * L0 * K, C,
+  MTB_CUDA_TRY(cudaFuncSetAttribute(so3_grid_topk_kernel<L0T, NT, KC>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  so3_grid_topk_kernel<L0T, NT, KC><<<B, kGridThreads, smem, st>>>(sigma, stride, B, dtab, L0, 2 * L0 * K, C,
                                                                grid_jb(L0, K), a, b, g, grid);
   MTB_LAUNCH_CHECK();
   return MTB_OK;
@@ -237,8 +256,9 @@ int grid_launch_t(const float2* sigma, int64_t stride, int B, const float* dtab,
 // arithmetic fixed at compile time; other grids take the general instantiation.
 int grid_launch(const float2* sigma, int64_t stride, int B, const float* dtab, int L0, int K, int C, float* a,
                 float* b, float* g, float* grid, cudaStream_t st) {
-  if (L0 == 8 && K == 2) return grid_launch_t<8, 32>(sigma, stride, B, dtab, L0, K, C, a, b, g, grid, st);
-  return grid_launch_t<0, 0>(sigma, stride, B, dtab, L0, K, C, a, b, g, grid, st);
+  if (L0 == 8 && K == 2 && C <= 16) return grid_launch_t<8, 32, 16>(sigma, stride, B, dtab, L0, K, C, a, b, g, grid, st);
+  if (C <= 16) return grid_launch_t<0, 0, 16>(sigma, stride, B, dtab, L0, K, C, a, b, g, grid, st);
+  return grid_launch_t<0, 0, kMaxCand>(sigma, stride, B, dtab, L0, K, C, a, b, g, grid, st);
 }
 
 __global__ void reduce_candidates_kernel(const float* __restrict__ ca, const float* __restrict__ cb,
