@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--batch", type=int, default=1000)
     p.add_argument("--cpu-sample", type=int, default=2, help="subtomograms per CPU-baseline step")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-fp32", action="store_true", help="skip the plain-FP32 comparison run")
     p.add_argument("--seed", type=int, default=0)
     return p.parse_args()
 
@@ -321,7 +322,39 @@ def run_ours(args):
         t2 = torch.tensor([e2e_ms], device=dev)
         dist.all_reduce(t2, op=dist.ReduceOp.MAX)
         e2e_ms = float(t2.item())
-    # accuracy of the last step
+    # the same step with the plain FP32 kernels (the expansion GEMM and the upsampled DFT on
+    # CUDA cores instead of the BF16 hi+lo tensor-core split): the comparison the metric names
+    plain = None
+    if not args.no_fp32:
+        step32 = AlignmentStep(StepConfig(N=N_BOX, L=L_MAX, Li=LI, batch=B, shift_search_radius=SHIFT_RADIUS,
+                                          shift_upsample_factor=UPSAMPLE, precision="fp32"), dev)
+        step32.set_template(template)
+        for _ in range(2):
+            tracker.copy_(ident)
+            step32(vols, vols, tracker, zeros3)
+        n32 = max(3, args.steps // 4)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e32s, e32e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e32s.record(st)
+        for _ in range(n32):
+            tracker.copy_(ident)
+            step32(vols, vols, tracker, zeros3)
+        e32e.record(st)
+        torch.cuda.synchronize()
+        ms32 = e32s.elapsed_time(e32e) / n32
+        if world > 1:
+            t32 = torch.tensor([ms32], device=dev)
+            dist.all_reduce(t32, op=dist.ReduceOp.MAX)
+            ms32 = float(t32.item())
+        plain = {"value": world * B / (ms32 * 1e-3), "ms_per_step": ms32, "steps": n32,
+                 "chosen_speedup": ms32 / ms}
+        del step32
+    # accuracy of one more chosen-path step on the full batch (the pieces of the end-to-end
+    # runs overwrote the step's output buffers)
+    tracker.copy_(ident)
+    out = one()
     al, be, ga = (out[k].cpu().numpy() for k in ("alpha", "beta", "gamma"))
     err = rotation_error_deg(al, be, ga, q_true)
     if world > 1:
@@ -370,6 +403,7 @@ def run_ours(args):
                      "traffic": (UPDFT23_DRAM_BYTES_PER_SUBTOMO * B) if UPDFT23_DRAM_BYTES_PER_SUBTOMO else None,
                      "traffic_unit": "bytes per launch"},
         "shift_kernel_ms_per_step": {k: v / max(1, shift_calls) for k, v in shift_prof.items()},
+        "plain_fp32": plain,
         "e2e": {"value": world * B / (e2e_ms * 1e-3), "unit": "subtomograms/s",
                 "h2d_bytes_per_step": int(B * N_BOX ** 3 * 4), "d2h_bytes_per_step": int(B * 8 * 4)},
         "gpu_launches": KERNELS_PER_STEP * args.steps,
