@@ -508,23 +508,20 @@ patch_fft_xy64_kernel(const float* __restrict__ vol, const float* __restrict__ s
     s_w[ax][0][j] = (zero || iy < 0 || iy >= N) ? 0.f : 1.f - fy;
     s_w[ax][1][j] = (zero || iy + 1 < 0 || iy + 1 >= N) ? 0.f : fy;
   }
-  constexpr int P4 = N * N / 4;
-  float4* pl4 = reinterpret_cast<float4*>(P0);
-#pragma unroll 4
-  for (int e = threadIdx.x; e < 2 * P4; e += kT64) {
-    const int hi = e >= P4 ? 1 : 0;
-    const int zz = iz + hi;
-    pl4[e] = (zz >= 0 && zz < N) ? __ldg(reinterpret_cast<const float4*>(v + (int64_t)zz * N * N) + (e - hi * P4))
-                                 : make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-  __syncthreads();
-  // z: P0 <- (1 - fz) P0 + fz P1 (a zeroed plane interpolates to zero)
+  // z, on the way in: P0 <- (1 - fz) plane(iz) + fz plane(iz + 1), straight from global memory
+  // (a plane outside the box, or a zeroed plane, contributes zero)
   {
+    constexpr int P4 = N * N / 4;
     const bool zplane = (i == ps.zp[0]);
-    const float w0 = zplane ? 0.f : 1.f - fz, w1 = zplane ? 0.f : fz;
-    const float4* q1 = reinterpret_cast<const float4*>(P1);
+    const bool in0 = iz >= 0 && iz < N, in1 = iz + 1 >= 0 && iz + 1 < N;
+    const float w0 = (zplane || !in0) ? 0.f : 1.f - fz, w1 = (zplane || !in1) ? 0.f : fz;
+    const float4* g0 = reinterpret_cast<const float4*>(v + (int64_t)(in0 ? iz : 0) * N * N);
+    const float4* g1 = reinterpret_cast<const float4*>(v + (int64_t)(in1 ? iz + 1 : 0) * N * N);
+    float4* pl4 = reinterpret_cast<float4*>(P0);
+#pragma unroll 4
     for (int e = threadIdx.x; e < P4; e += kT64) {
-      const float4 a = pl4[e], c = q1[e];
+      const float4 a = in0 ? __ldg(g0 + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 c = in1 ? __ldg(g1 + e) : make_float4(0.f, 0.f, 0.f, 0.f);
       pl4[e] = make_float4(w0 * a.x + w1 * c.x, w0 * a.y + w1 * c.y, w0 * a.z + w1 * c.z, w0 * a.w + w1 * c.w);
     }
   }
@@ -576,16 +573,28 @@ patch_fft_xy64_kernel(const float* __restrict__ vol, const float* __restrict__ s
     for (int k2 = 0; k2 < 8; ++k2) line[r + 8 * k2] = w[k2];
   }
   __syncthreads();
-  // split Z = A + i B into the transforms of rows q and q + 32, columns m2 < 33
-  for (int e = threadIdx.x; e < HN * H; e += kT64) {
-    const int q = e / H, k = e - (e / H) * H;
-    const float2 zk = zb[q * kXS + k];
-    const float2 zm = zb[q * kXS + ((N - k) & (N - 1))];
-    yb[q * kYS + k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-    yb[(q + HN) * kYS + k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+  // y FFT of the columns m2 < 33, its input split on the way in: Z = A + i B holds the
+  // transforms of rows q and q + 32, so a group's rows r + 8 s' and r + 8 s' + 32 (s' < 4)
+  // come from the same two entries Z[q][m2], Z[q][-m2]
+  {
+    const int L = threadIdx.x >> 3, r = threadIdx.x & 7;
+    const int col = L < H ? L : H - 1;  // groups 33..35 shadow column 32 inside its own warp
+    float2 w[8];
+#pragma unroll
+    for (int s4 = 0; s4 < 4; ++s4) {
+      const int q = r + 8 * s4;
+      const float2 zk = zb[q * kXS + col];
+      const float2 zm = zb[q * kXS + ((N - col) & (N - 1))];
+      w[s4] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+      w[s4 + 4] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+    }
+    __syncthreads();  // zb becomes the transpose scratch
+    fft64_group(w, r, zb + L * kXS, tw);
+    if (L < H) {
+#pragma unroll
+      for (int k2 = 0; k2 < 8; ++k2) yb[(r + 8 * k2) * kYS + col] = w[k2];
+    }
   }
-  __syncthreads();
-  fft64_columns(yb, zb, tw);
   __syncthreads();
   float2* out = T + ((int64_t)b * N + ip) * N * H;
   for (int e = threadIdx.x; e < N * H; e += kT64) {
