@@ -17,8 +17,10 @@
 // and 3 are fused: a tile is G = 128 / (N/2) consecutive u0 of one subtomogram with all their
 // m2 < N/2, so its pass-2 accumulator holds complete X2[u0, u1, :] rows; the epilogue writes
 // them as the pass-3 A operand straight into shared memory (the 128-byte-swizzled K-major
-// layout the tensor core reads), 128 (u0, u1) rows at a time, and the pass-3 accumulators
-// are reduced to a running argmax key per subtomogram.  Neither X2 nor the U^3 grid reaches
+// layout the tensor core reads), 128 (u0, u1) rows at a time, into two alternating chunk
+// buffers, and the pass-3 accumulators (two alternating chunk buffers in tensor memory) are
+// reduced to a running argmax key per subtomogram by their own warps, a chunk behind the
+// warps that write the operands.  Neither X2 nor the U^3 grid reaches
 // memory.  All device waits are bounded; a wait that runs out sets err and the CTA winds down.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -37,6 +39,8 @@ using namespace tc;
 constexpr int TM = 128, TK = 64;
 constexpr int kThreads = 320;        // warp 0 TMA, warp 1 MMA + TMEM, warps 2-9 epilogue
 constexpr int kEpi = 256;            // epilogue threads: two warps per 32-lane quarter of TMEM
+constexpr int kArg = 128;            // argmax warps of the fused passes 2+3: one per quarter
+constexpr int kThreads23 = 64 + kEpi + kArg;  // warps 10-13 of updft23 take the argmax
 constexpr int A_TILE = TM * TK * 2;  // one 128 x 64 bf16 K-block
 constexpr int kMaxStages = 8;
 constexpr size_t kSmemCap = 227 * 1024;
@@ -379,7 +383,7 @@ __device__ __forceinline__ uint64_t smem_desc_k16(const void* p) {
   return d;                          // layout type 0: no swizzle
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads23, 1)
 updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_constant__ CUtensorMap mapE1,
                   const __grid_constant__ CUtensorMap mapE3, Pass23 p, const float2* __restrict__ nyq,
                   const uint4* __restrict__ bnq, unsigned long long* __restrict__ best, int* __restrict__ err) {
@@ -394,8 +398,8 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
   uint8_t* sA = sE3 + 2 * B3;
   uint8_t* sAn = sA + 4 * A_TILE;            // [2][part] 128 x 16 Nyquist operand, no swizzle
   uint8_t* sBn = sAn + 4 * kNqA;             // [part] NT3 x 16, no swizzle
-  __shared__ __align__(8) uint64_t full_bar[2], a3F[2], a3E[2];
-  __shared__ __align__(8) uint64_t resF, regionF, acc2F, acc2E, acc3F, acc3E;
+  __shared__ __align__(8) uint64_t full_bar[2], a3F[2], a3E[2], acc3F[2], acc3E[2];
+  __shared__ __align__(8) uint64_t resF, regionF, acc2F, acc2E;
   __shared__ uint32_t tmem_base;
   __shared__ volatile int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -404,13 +408,13 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
       mbar_init(&full_bar[s], 1);
       mbar_init(&a3F[s], kEpi);
       mbar_init(&a3E[s], 1);
+      mbar_init(&acc3F[s], 1);
+      mbar_init(&acc3E[s], kArg);
     }
     mbar_init(&resF, 1);
     mbar_init(&regionF, 1);
     mbar_init(&acc2F, 1);
     mbar_init(&acc2E, kEpi);
-    mbar_init(&acc3F, 1);
-    mbar_init(&acc3E, kEpi);
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -484,7 +488,8 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
       }
       if (!ok) break;
       mma_commit_to(&acc2F);
-      // pass 3, chunk by chunk, into acc3 (columns NT12 + j NT3)
+      // pass 3, chunk by chunk: the CTA's chunk cc into acc3 buffer cc & 1 (columns
+      // NT12 + (cc & 1) NT3) once the argmax warps have read chunk cc - 2 from it
       for (int j = 0; j < p.CH; ++j, ++cc) {
         const int q3 = cc & 1;
         if (!mbar_wait(&a3F[q3], (cc >> 1) & 1)) {
@@ -493,14 +498,14 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
           ok = false;
           break;
         }
-        if (j == 0 && tl >= 1 && !mbar_wait(&acc3E, (tl - 1) & 1)) {
+        if (cc >= 2 && !mbar_wait(&acc3E[q3], ((cc >> 1) - 1) & 1)) {
           atomicExch(err, 36);
           abort_flag = 1;
           ok = false;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t d3 = tmem + (uint32_t)(NT12 + j * NT3);
+        const uint32_t d3 = tmem + (uint32_t)(NT12 + q3 * NT3);
         const uint8_t* a3 = sA + q3 * 2 * A_TILE;
         mma_split_kblock(d3, smem_desc(a3), smem_desc(a3 + A_TILE), smem_desc(sE3), smem_desc(sE3 + B3), idesc3,
                          true);
@@ -512,19 +517,17 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
         mma_bf16_id(d3, an_lo, bn_hi, idesc3, 1u);
         mma_bf16_id(d3, an_hi, bn_lo, idesc3, 1u);
         mma_commit_to(&a3E[q3]);
+        mma_commit_to(&acc3F[q3]);
       }
       if (!ok) break;
-      mma_commit_to(&acc3F);
       mma_commit_to(&regionF);
     }
-  } else if (warp >= 2) {
-    // warp (q, h): TMEM lanes 32 q .. 32 q + 31, half h of the columns it needs
+  } else if (warp >= 2 && warp < 2 + kEpi / 32) {
+    // operand warps (q, h): TMEM lanes 32 q .. 32 q + 31, half h of the columns they need
     const int q = warp & 3, h = (warp - 2) >> 2;
     const int r_lane = q * 32 + lane;            // row of the pass-2 tile: (u0_local, m2)
     const int u0l = r_lane / p.HH, m2 = r_lane - (r_lane / p.HH) * p.HH;
     const uint32_t lane_off = (uint32_t)(q * 32) << 16;
-    const int c3_mid = (NT3 / 2) & ~15;
-    const int c3_0 = h ? c3_mid : 0, c3_1 = h ? NT3 : c3_mid;
     int tl = 0, cc = 0;
     for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
       const int b = tile / p.TPB, tg = tile - (tile / p.TPB) * p.TPB;
@@ -575,26 +578,42 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
       if (!ok) break;
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(&acc2E);
-      if (!mbar_wait(&acc3F, tl & 1)) {
-        atomicExch(err, 39);
-        abort_flag = 1;
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+  } else if (warp >= 2 + kEpi / 32) {
+    // argmax warps: TMEM lanes 32 q .. 32 q + 31 of each chunk's pass-3 accumulator, all
+    // columns; they run a chunk behind the operand warps
+    const int q = warp & 3;
+    const uint32_t lane_off = (uint32_t)(q * 32) << 16;
+    const int r_lane = q * 32 + lane;
+    int tl = 0, cc = 0;
+    for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
+      const int b = tile / p.TPB, tg = tile - (tile / p.TPB) * p.TPB;
       float bv = -INFINITY;
       int bi = 0x7fffffff;
       bool have = false;
-      for (int j = 0; j < p.CH; ++j) {
+      bool ok = true;
+      for (int j = 0; j < p.CH; ++j, ++cc) {
+        const int q3 = cc & 1;
+        if (!mbar_wait(&acc3F[q3], (cc >> 1) & 1)) {
+          atomicExch(err, 39);
+          abort_flag = 1;
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int r = TM * j + r_lane;  // (u0_local, u1) row of the tile
         const int a = r / p.U, u1 = r - (r / p.U) * p.U;
         const int u0 = tg * p.G + a;
         const bool valid = r < rows_a3 && u0 < p.U;
         const int row_flat = u0 * p.U + u1;
-        tmem_for_groups(tmem + lane_off + (uint32_t)(NT12 + j * NT3), c3_0, c3_1,
-                        [&](const uint32_t(&r)[16], int cb) {
-                          if (valid) scan_group<16>(r, cb, p.U, row_flat, bv, bi, have);
+        tmem_for_groups(tmem + lane_off + (uint32_t)(NT12 + q3 * NT3), 0, NT3,
+                        [&](const uint32_t(&rr)[16], int cb) {
+                          if (valid) scan_group<16>(rr, cb, p.U, row_flat, bv, bi, have);
                         });
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        mbar_arrive(&acc3E[q3]);
       }
+      if (!ok) break;
       // a lane visits its values in increasing flat order, so a later equal value never wins;
       // the warp's keys all belong to subtomogram b
       unsigned long long key = have ? argmax_key(bv, bi) : 0ull;
@@ -604,8 +623,6 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
         key = k2 > key ? k2 : key;
       }
       if (lane == 0 && key) atomicMax(&best[b], key);
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      mbar_arrive(&acc3E);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -760,7 +777,7 @@ bool geometry(int N, int U, Geometry* o) {
   g.G = TM / g.HH;
   g.TPB = (U + g.G - 1) / g.G;
   g.CH = (g.G * U + TM - 1) / TM;
-  if (g.NT12 + g.CH * g.NT3 > 512) return false;
+  if (g.NT12 + 2 * g.NT3 > 512) return false;
   const size_t b1 = (size_t)2 * g.KB12 * g.NT12 * TK * 2;
   const size_t b3 = (size_t)2 * g.NT3 * TK * 2;
   g.smem23 = 1024 + b1 + b3 + 4 * (size_t)A_TILE + 4 * (size_t)kNqA + (size_t)2 * g.NT3 * 32;
@@ -932,7 +949,7 @@ int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st, const cudaEvent_t* marks
   p2.NT3 = t->NT3;
   MTB_CUDA_TRY(cudaFuncSetAttribute(updft23_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem23));
   const int g2 = p2.tiles < t->n_sm ? p2.tiles : t->n_sm;
-  updft23_tc_kernel<<<g2, kThreads, t->smem23, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA2),
+  updft23_tc_kernel<<<g2, kThreads23, t->smem23, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA2),
                                                      *reinterpret_cast<const CUtensorMap*>(t->mapE1),
                                                      *reinterpret_cast<const CUtensorMap*>(t->mapE3), p2, t->nyq,
                                                      (const uint4*)t->ENQ, t->best, t->err);

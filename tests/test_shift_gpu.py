@@ -38,7 +38,8 @@ def test_shift_matches_reference_fixture(cuda_device):
 
 @pytest.mark.parametrize("N,uf,r,precision", [(32, 8, 3, "fp32"), (64, 8, 5, "fp32"), (32, 4, 2, "fp32"),
                                               (64, 8, 5, "bf16x3"), (32, 8, 3, "bf16x3"),
-                                              (16, 4, 1, "bf16x3"), (32, 4, 2, "bf16x3")])
+                                              (16, 4, 1, "bf16x3"), (32, 4, 2, "bf16x3"),
+                                              (32, 8, 5, "bf16x3"), (16, 8, 5, "bf16x3")])
 def test_shift_matches_oracle(cuda_device, N, uf, r, precision):
     rng = np.random.default_rng(N + uf + r)
     tmpl = blob_template(rng, N, 60, N * 0.3, (1.5, 3.0), mask_radius=N * 0.4)
@@ -96,3 +97,25 @@ def test_shift_profile_records_kernel_groups(cuda_device, precision):
     sm.profile(0)
     assert sm.profile_read() == ({k: 0.0 for k in sm.PROFILE_STAGES}, 0)
     np.testing.assert_array_equal(again[0].cpu().numpy(), first[0].cpu().numpy())
+
+
+def test_shift_tensor_path_many_tiles_per_cta(cuda_device):
+    """B = 40 at 64^3, uf 8, r 5: 840 pass-2/3 tiles, several per persistent CTA, against the
+    FP32 path (itself checked against the oracle above)."""
+    N, B = 64, 40
+    rng = np.random.default_rng(11)
+    tmpl = blob_template(rng, N, 60, N * 0.3, (1.5, 3.0), mask_radius=N * 0.4)
+    vols = torch.from_numpy(np.repeat(tmpl[None], B, 0) + 0.5 * rng.standard_normal((B, N, N, N)).astype(np.float32))
+    vols = vols.to(cuda_device)
+    q = haar_quaternions(rng, B)
+    z = torch.from_numpy(rng.uniform(-1.5, 1.5, (B, 3)).astype(np.float32)).to(cuda_device)
+    out = {}
+    for precision in ("fp32", "bf16x3"):
+        sm = _matcher(N, B, 8, 5, cuda_device, precision=precision)
+        sm.set_reference(tmpl)
+        shift, score = sm.search_shifts(subtomos=vols, ctfs=None, shift_zyx=z, rotation_tracker=q)
+        sm.status()
+        out[precision] = (shift.cpu().numpy(), score.cpu().numpy())
+    np.testing.assert_allclose(out["bf16x3"][1], out["fp32"][1], rtol=1e-4)
+    same = np.all(np.abs(out["bf16x3"][0] - out["fp32"][0]) <= 1e-6, axis=1)
+    assert same.mean() >= 0.9, same
