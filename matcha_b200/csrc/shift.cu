@@ -21,6 +21,7 @@
 // Contracting the half axis (N/2+1) last needs 51M instead of 87M complex MACs per
 // subtomogram at N=64, U=88; the separable sum is the same.
 #include <math.h>
+#include <stdio.h>
 #include <string.h>
 #include <vector>
 #include <cuda_bf16.h>
@@ -1063,8 +1064,13 @@ extern "C" int mtb_shift_status(mtb_shift* h, mtb_stream_t stream) {
     MTB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
     return MTB_OK;
   }
-  const int rc = shift_tc_check(&h->tc, (cudaStream_t)stream);
-  if (rc) mtb_set_last_error("tensor-core shift DFT: a bounded wait ran out", __FILE__, __LINE__);
+  int site = 0;
+  const int rc = shift_tc_check(&h->tc, (cudaStream_t)stream, &site);
+  if (rc == MTB_ERR_TIMEOUT) {
+    char msg[96];
+    snprintf(msg, sizeof(msg), "tensor-core shift DFT: a bounded wait ran out (wait site %d)", site);
+    mtb_set_last_error(msg, __FILE__, __LINE__);
+  }
   return rc;
 }
 

@@ -7,7 +7,8 @@
 //   nyquist  Y[u0,u1] = sum_{m0,m1} E0[u0,m0] E0[u1,m1] P[m0,m1,N/2]        (nyq_kernel)
 //   pass 1   rows (b, m2, m1), K = (m0, re/im) = 2N, N-tile = (u0, re/im) = 2U   (X1 -> A2)
 //   pass 2   rows (b, u0, m2), K = (m1, re/im) = 2N, N-tile = (u1, re/im) = 2U   (X2)
-//   pass 3   rows (b, u0, u1), K = (m2, re/im) = N,  N-tile = u2 (real part), + Re(Y E2[u2, N/2])
+//   pass 3   rows (b, u0, u1), K = (m2, re/im) = N,  N-tile = u2 (real part); + Re(Y E2[u2, N/2])
+//            added in FP32 before the argmax
 // Complex products are real GEMMs on interleaved (re, im) K axes.  Operands are split
 // A = A_hi + A_lo, B = B_hi + B_lo and A B ~ A_hi B_hi + A_lo B_hi + A_hi B_lo.
 //
@@ -15,13 +16,15 @@
 // memory.  Pass 1 double-buffers its accumulator in tensor memory, so the epilogue that
 // writes the pass-2 operand A2 (K-major bf16 hi/lo) overlaps the next tile's MMAs.  Passes 2
 // and 3 are fused: a tile is G = 128 / (N/2) consecutive u0 of one subtomogram with all their
-// m2 < N/2, so its pass-2 accumulator holds complete X2[u0, u1, :] rows; the epilogue writes
+// m2 < N/2, so its pass-2 accumulator holds complete X2[u0, u1, :] rows.  Eight warps write
 // them as the pass-3 A operand straight into shared memory (the 128-byte-swizzled K-major
-// layout the tensor core reads), 128 (u0, u1) rows at a time, into two alternating chunk
-// buffers, and the pass-3 accumulators (two alternating chunk buffers in tensor memory) are
-// reduced to a running argmax key per subtomogram by their own warps, a chunk behind the
-// warps that write the operands.  Neither X2 nor the U^3 grid reaches
-// memory.  All device waits are bounded; a wait that runs out sets err and the CTA winds down.
+// layout the tensor core reads), one chunk of N/2 consecutive u1 for all G u0 at a time, so
+// each lane has the same share of every chunk.  Eight more warps reduce each chunk's pass-3
+// accumulator (two alternating buffers in tensor memory), plus the Nyquist term in FP32, to
+// a running argmax key per subtomogram, a chunk behind the writers.  A2 K-blocks and pass-3
+// chunks take turns in a ring of two or three shared-memory slots, so the next tile's A2
+// loads while this tile's pass 3 runs.  Neither X2 nor the U^3 grid reaches memory.  All
+// device waits are bounded; a wait that runs out sets err and the CTA winds down.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <math.h>
@@ -39,8 +42,9 @@ using namespace tc;
 constexpr int TM = 128, TK = 64;
 constexpr int kThreads = 320;        // warp 0 TMA, warp 1 MMA + TMEM, warps 2-9 epilogue
 constexpr int kEpi = 256;            // epilogue threads: two warps per 32-lane quarter of TMEM
-constexpr int kArg = 128;            // argmax warps of the fused passes 2+3: one per quarter
-constexpr int kThreads23 = 64 + kEpi + kArg;  // warps 10-13 of updft23 take the argmax
+constexpr int kArg = 256;            // argmax threads of the fused passes 2+3: two warps per quarter
+constexpr int kThreads23 = 64 + kEpi + kArg;  // warps 10-17 of updft23 take the argmax
+constexpr int kMaxSlots = 3;         // operand slots of the fused passes 2+3
 constexpr int A_TILE = TM * TK * 2;  // one 128 x 64 bf16 K-block
 constexpr int kMaxStages = 8;
 constexpr size_t kSmemCap = 227 * 1024;
@@ -61,6 +65,7 @@ struct Pass23 {
   int KB;        // K blocks of A2 and E1
   int R2;
   int NT12, NT3;
+  int NB;        // operand slots (2 or 3)
 };
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
@@ -279,7 +284,7 @@ updft1_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant
         const int s = it % S;
         const uint32_t use = it / S;
         if (it >= S && !mbar_wait(&empty_bar[s], (use - 1) & 1)) {
-          atomicExch(err, 21);
+          atomicCAS(err, 0, 21);
           abort_flag = 1;
           break;
         }
@@ -292,14 +297,14 @@ updft1_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant
   } else if (warp == 1 && lane == 0) {
     bool ok = mbar_wait(&resF, 0);
     if (!ok) {
-      atomicExch(err, 22);
+      atomicCAS(err, 0, 22);
       abort_flag = 1;
     }
     int it = 0, tl = 0;
     for (int tile = blockIdx.x; ok && tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
       const int buf = tl & 1;
       if (tl >= 2 && !mbar_wait(&accE[buf], ((tl >> 1) - 1) & 1)) {
-        atomicExch(err, 23);
+        atomicCAS(err, 0, 23);
         abort_flag = 1;
         break;
       }
@@ -309,7 +314,7 @@ updft1_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant
         const int s = it % S;
         const uint32_t use = it / S;
         if (!mbar_wait(&full_bar[s], use & 1)) {
-          atomicExch(err, 24);
+          atomicCAS(err, 0, 24);
           abort_flag = 1;
           ok = false;
           break;
@@ -332,7 +337,7 @@ updft1_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant
     for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
       const int buf = tl & 1;
       if (!mbar_wait(&accF[buf], (tl >> 1) & 1)) {
-        atomicExch(err, 25);
+        atomicCAS(err, 0, 25);
         abort_flag = 1;
         break;
       }
@@ -366,63 +371,65 @@ __device__ __forceinline__ uint32_t sw128_word(int r, int w) {
   return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((((w >> 2) ^ (r & 7))) << 4) + ((w & 3) << 2));
 }
 
-// The 128 x 16 (K) Nyquist operand and its NT3 x 16 B counterpart use the plain K-major
-// layout: 8-row x 16-byte core matrices, the two K halves 128 bytes apart (leading byte
-// offset), 8-row groups 256 bytes apart (stride byte offset).
-constexpr int kNqA = TM * 16 * 2;
-
-__device__ __forceinline__ uint32_t k16_word(int r) { return (uint32_t)((r >> 3) * 256 + (r & 7) * 16); }
-
-__device__ __forceinline__ uint64_t smem_desc_k16(const void* p) {
-  const uint64_t addr = smem_u32(p);
-  uint64_t d = 0;
-  d |= (addr >> 4) & 0x3FFFull;
-  d |= (uint64_t)(128 >> 4) << 16;  // leading byte offset: K core-matrix stride
-  d |= (uint64_t)(256 >> 4) << 32;  // stride byte offset: 8-row group stride
-  d |= (uint64_t)1 << 46;           // descriptor version for tcgen05
-  return d;                          // layout type 0: no swizzle
+// Pass 3 plus the Nyquist term: running argmax over NC values u2 = cb .. cb + NC - 1 of one
+// row, each v[u2] + Re(Y E2[u2, N/2]) = v + y.x en[u2].x + y.y en[u2].y in FP32.
+template <int NC>
+__device__ __forceinline__ void scan_group_nq(const uint32_t* vr, int cb, int U, int row_flat, float2 y,
+                                              const float4* __restrict__ en2, float& bv, int& bi, bool& have) {
+  uint32_t w[NC];
+#pragma unroll
+  for (int t = 0; t < NC; t += 2) {
+    const float4 e = en2[(cb + t) >> 1];  // the same address in every lane: a broadcast
+    w[t] = __float_as_uint(fmaf(y.y, e.y, fmaf(y.x, e.x, __uint_as_float(vr[t]))));
+    w[t + 1] = __float_as_uint(fmaf(y.y, e.w, fmaf(y.x, e.z, __uint_as_float(vr[t + 1]))));
+  }
+  scan_group<NC>(w, cb, U, row_flat, bv, bi, have);
 }
 
 __global__ void __launch_bounds__(kThreads23, 1)
 updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_constant__ CUtensorMap mapE1,
                   const __grid_constant__ CUtensorMap mapE3, Pass23 p, const float2* __restrict__ nyq,
-                  const uint4* __restrict__ bnq, unsigned long long* __restrict__ best, int* __restrict__ err) {
+                  const float4* __restrict__ enq, unsigned long long* __restrict__ best, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = align1024(smem_raw);
-  const int KB = p.KB, NT12 = p.NT12, NT3 = p.NT3;
+  const int KB = p.KB, NT12 = p.NT12, NT3 = p.NT3, NB = p.NB, HH = p.HH;
   const int B1 = NT12 * TK * 2, B3 = NT3 * TK * 2;
   uint8_t* sE1 = smem;                       // [part][kb] B1
   uint8_t* sE3 = sE1 + 2 * KB * B1;          // [part] B3
-  // [2][part] A_TILE: the two K blocks of the tile's A2 rows, then (once pass 2 has read
-  // them) the two pass-3 operand buffers of alternate chunks
-  uint8_t* sA = sE3 + 2 * B3;
-  uint8_t* sAn = sA + 4 * A_TILE;            // [2][part] 128 x 16 Nyquist operand, no swizzle
-  uint8_t* sBn = sAn + 4 * kNqA;             // [part] NT3 x 16, no swizzle
-  __shared__ __align__(8) uint64_t full_bar[2], a3F[2], a3E[2], acc3F[2], acc3E[2];
-  __shared__ __align__(8) uint64_t resF, regionF, acc2F, acc2E;
+  // NB slots of two A_TILE (hi, lo), taken in turn (use n in slot n % NB): a tile's KB A2
+  // K-blocks, then its CH pass-3 operand chunks.  A slot is refilled once the MMAs that read
+  // its last contents are done; that commit goes to freeT or freeO after the kind of the next
+  // use, so the TMA thread and the operand warps each wait their own barrier, in order, never
+  // more than one phase ahead of it.
+  uint8_t* sS = sE3 + 2 * B3;
+  float4* sEn = reinterpret_cast<float4*>(sS + NB * 2 * A_TILE);  // (er, -ei) of E2[u2, N/2], pairs
+  __shared__ __align__(8) uint64_t tmaF[kMaxSlots], opF[kMaxSlots], freeT[kMaxSlots], freeO[kMaxSlots];
+  __shared__ __align__(8) uint64_t acc3F[2], acc3E[2], resF, acc2F, acc2E;
   __shared__ uint32_t tmem_base;
   __shared__ volatile int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
+    for (int s = 0; s < kMaxSlots; ++s) {
+      mbar_init(&tmaF[s], 1);
+      mbar_init(&opF[s], kEpi);
+      mbar_init(&freeT[s], 1);
+      mbar_init(&freeO[s], 1);
+    }
     for (int s = 0; s < 2; ++s) {
-      mbar_init(&full_bar[s], 1);
-      mbar_init(&a3F[s], kEpi);
-      mbar_init(&a3E[s], 1);
       mbar_init(&acc3F[s], 1);
       mbar_init(&acc3E[s], kArg);
     }
     mbar_init(&resF, 1);
-    mbar_init(&regionF, 1);
     mbar_init(&acc2F, 1);
     mbar_init(&acc2E, kEpi);
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  // the pass-3 operands: K columns past N (and past the Nyquist pair) stay zero, rows not
-  // written by a chunk are ignored; the Nyquist B operand comes prepared from the host
-  for (int i = threadIdx.x; i < 4 * kNqA / 16; i += blockDim.x)
-    reinterpret_cast<uint4*>(sAn)[i] = make_uint4(0u, 0u, 0u, 0u);
-  for (int i = threadIdx.x; i < 2 * NT3 * 32 / 16; i += blockDim.x) reinterpret_cast<uint4*>(sBn)[i] = bnq[i];
+  for (int i = threadIdx.x; i < NT3 / 2; i += blockDim.x) sEn[i] = enq[i];
+  // a chunk writes K words < N/2 of its rows; the rest must hold finite values (they meet
+  // zero K columns of E3), so the slots start zeroed
+  for (int i = threadIdx.x; i < NB * 2 * A_TILE / 16; i += blockDim.x)
+    reinterpret_cast<uint4*>(sS)[i] = make_uint4(0u, 0u, 0u, 0u);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
@@ -434,7 +441,7 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
   const uint32_t idesc2 = idesc_bf16(TM, NT12), idesc3 = idesc_bf16(TM, NT3);
-  const int rows_a3 = p.G * p.U;  // (u0_local, u1) rows of a tile
+  const int per_tile = KB + p.CH;  // slot uses per tile
 
   if (warp == 0 && lane == 0) {
     mbar_expect_tx(&resF, (uint32_t)(2 * KB * B1 + 2 * B3));
@@ -443,172 +450,164 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
       tma_load_2d(sE3 + part * B3, &mapE3, 0, part * NT3, &resF);
     }
     int tl = 0;
-    for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
+    bool ok = true;
+    uint32_t par = 0;  // bit s: phase of the next wait on freeT[s]
+    for (int tile = blockIdx.x; ok && tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
       const int b = tile / p.TPB, tg = tile - (tile / p.TPB) * p.TPB;
-      const int arow = (b * p.U + tg * p.G) * p.HH;
-      // the region is free once the previous tile's pass-3 MMAs have read their operands
-      if (tl >= 1 && !mbar_wait(&regionF, (tl - 1) & 1)) {
-        atomicExch(err, 31);
-        abort_flag = 1;
-        break;
-      }
+      const int arow = (b * p.U + tg * p.G) * HH;
       for (int kb = 0; kb < KB; ++kb) {
-        uint8_t* sa = sA + kb * 2 * A_TILE;
-        mbar_expect_tx(&full_bar[kb], 2 * A_TILE);
-        tma_load_2d(sa, &mapA2, kb * TK, arow, &full_bar[kb]);
-        tma_load_2d(sa + A_TILE, &mapA2, kb * TK, p.R2 + arow, &full_bar[kb]);
+        const int n = tl * per_tile + kb, s = n % NB;
+        if (n >= NB) {
+          if (!mbar_wait(&freeT[s], (par >> s) & 1u)) {
+            atomicCAS(err, 0, 31);
+            abort_flag = 1;
+            ok = false;
+            break;
+          }
+          par ^= 1u << s;
+        }
+        uint8_t* sa = sS + s * 2 * A_TILE;
+        mbar_expect_tx(&tmaF[s], 2 * A_TILE);
+        tma_load_2d(sa, &mapA2, kb * TK, arow, &tmaF[s]);
+        tma_load_2d(sa + A_TILE, &mapA2, kb * TK, p.R2 + arow, &tmaF[s]);
       }
     }
   } else if (warp == 1 && lane == 0) {
     bool ok = mbar_wait(&resF, 0);
     if (!ok) {
-      atomicExch(err, 32);
+      atomicCAS(err, 0, 32);
       abort_flag = 1;
     }
-    int tl = 0, cc = 0;
+    uint32_t tma_par = 0, op_par = 0;  // bit s: phase of the next wait on tmaF[s] / opF[s]
+    int tl = 0;
     for (int tile = blockIdx.x; ok && tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
-      // pass 2 into acc2 (columns 0 .. NT12)
+      // pass 2 into acc2 (columns 0 .. NT12) once the operand warps have read the last tile's
       if (tl >= 1 && !mbar_wait(&acc2E, (tl - 1) & 1)) {
-        atomicExch(err, 33);
+        atomicCAS(err, 0, 33);
         abort_flag = 1;
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       for (int kb = 0; kb < KB; ++kb) {
-        if (!mbar_wait(&full_bar[kb], tl & 1)) {
-          atomicExch(err, 34);
+        const int n = tl * per_tile + kb, s = n % NB;
+        if (!mbar_wait(&tmaF[s], (tma_par >> s) & 1u)) {
+          atomicCAS(err, 0, 34);
           abort_flag = 1;
           ok = false;
           break;
         }
+        tma_par ^= 1u << s;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint8_t* sa = sA + kb * 2 * A_TILE;
+        const uint8_t* sa = sS + s * 2 * A_TILE;
         mma_split_kblock(tmem, smem_desc(sa), smem_desc(sa + A_TILE), smem_desc(sE1 + kb * B1),
                          smem_desc(sE1 + (KB + kb) * B1), idesc2, kb == 0);
+        mma_commit_to((n + NB) % per_tile < KB ? &freeT[s] : &freeO[s]);
       }
       if (!ok) break;
       mma_commit_to(&acc2F);
       // pass 3, chunk by chunk: the CTA's chunk cc into acc3 buffer cc & 1 (columns
       // NT12 + (cc & 1) NT3) once the argmax warps have read chunk cc - 2 from it
-      for (int j = 0; j < p.CH; ++j, ++cc) {
-        const int q3 = cc & 1;
-        if (!mbar_wait(&a3F[q3], (cc >> 1) & 1)) {
-          atomicExch(err, 35);
+      for (int j = 0; j < p.CH; ++j) {
+        const int n = tl * per_tile + KB + j, s = n % NB;
+        const int cc = tl * p.CH + j, q3 = cc & 1;
+        if (!mbar_wait(&opF[s], (op_par >> s) & 1u)) {
+          atomicCAS(err, 0, 35);
           abort_flag = 1;
           ok = false;
           break;
         }
+        op_par ^= 1u << s;
         if (cc >= 2 && !mbar_wait(&acc3E[q3], ((cc >> 1) - 1) & 1)) {
-          atomicExch(err, 36);
+          atomicCAS(err, 0, 36);
           abort_flag = 1;
           ok = false;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t d3 = tmem + (uint32_t)(NT12 + q3 * NT3);
-        const uint8_t* a3 = sA + q3 * 2 * A_TILE;
-        mma_split_kblock(d3, smem_desc(a3), smem_desc(a3 + A_TILE), smem_desc(sE3), smem_desc(sE3 + B3), idesc3,
-                         true);
-        // the Nyquist column m2 = N/2 as one more K step of 16
-        const uint8_t* an = sAn + q3 * 2 * kNqA;
-        const uint64_t an_hi = smem_desc_k16(an), an_lo = smem_desc_k16(an + kNqA);
-        const uint64_t bn_hi = smem_desc_k16(sBn), bn_lo = smem_desc_k16(sBn + NT3 * 32);
-        mma_bf16_id(d3, an_hi, bn_hi, idesc3, 1u);
-        mma_bf16_id(d3, an_lo, bn_hi, idesc3, 1u);
-        mma_bf16_id(d3, an_hi, bn_lo, idesc3, 1u);
-        mma_commit_to(&a3E[q3]);
+        const uint8_t* a3 = sS + s * 2 * A_TILE;
+        mma_split_kblock(tmem + (uint32_t)(NT12 + q3 * NT3), smem_desc(a3), smem_desc(a3 + A_TILE), smem_desc(sE3),
+                         smem_desc(sE3 + B3), idesc3, true);
+        mma_commit_to((n + NB) % per_tile < KB ? &freeT[s] : &freeO[s]);
         mma_commit_to(&acc3F[q3]);
       }
-      if (!ok) break;
-      mma_commit_to(&regionF);
     }
   } else if (warp >= 2 && warp < 2 + kEpi / 32) {
-    // operand warps (q, h): TMEM lanes 32 q .. 32 q + 31, half h of the columns they need
+    // operand warps (q, h): TMEM lanes 32 q .. 32 q + 31 (rows (u0_local, m2) of acc2), half h
+    // of a chunk's columns.  Chunk j is u1 in [j HH, j HH + HH) for all G u0 of the tile:
+    // pass-3 row (u0_local, u1 - j HH), so every lane has the same share of every chunk.
     const int q = warp & 3, h = (warp - 2) >> 2;
-    const int r_lane = q * 32 + lane;            // row of the pass-2 tile: (u0_local, m2)
-    const int u0l = r_lane / p.HH, m2 = r_lane - (r_lane / p.HH) * p.HH;
+    const int r_lane = q * 32 + lane;
+    const int u0l = r_lane / HH, m2 = r_lane - (r_lane / HH) * HH;
     const uint32_t lane_off = (uint32_t)(q * 32) << 16;
-    int tl = 0, cc = 0;
+    int tl = 0;
+    uint32_t par = 0;  // bit s: phase of the next wait on freeO[s]
     for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
-      const int b = tile / p.TPB, tg = tile - (tile / p.TPB) * p.TPB;
       if (!mbar_wait(&acc2F, tl & 1)) {
-        atomicExch(err, 37);
+        atomicCAS(err, 0, 37);
         abort_flag = 1;
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       bool ok = true;
-      for (int j = 0; j < p.CH; ++j, ++cc) {
-        // rows of chunk j: (u0_local, u1) with u0_local * U + u1 in [128 j, 128 j + 128); this
-        // lane's u1 range, the warp's union of them, and this half's share of its columns
-        const int rbase = u0l * p.U - TM * j;
-        const int lo_l = max(0, -rbase), hi_l = min(p.U, TM - rbase);
-        const int lo = __reduce_min_sync(0xffffffffu, lo_l < hi_l ? lo_l : p.U);
-        const int hi = __reduce_max_sync(0xffffffffu, lo_l < hi_l ? hi_l : 0);
-        const int cA = (2 * lo) & ~15, cB = min(NT12, (2 * hi + 15) & ~15);
+      for (int j = 0; j < p.CH; ++j) {
+        const int n = tl * per_tile + KB + j, s = n % NB;
+        const int lo_l = j * HH, hi_l = min(p.U, lo_l + HH);  // this chunk's u1
+        const int cA = 2 * lo_l, cB = min(NT12, (2 * hi_l + 15) & ~15);
         const int cM = cA + ((((cB - cA) >> 4) + 1) >> 1 << 4);  // h = 0 takes the first half
-        const int ca = lo < hi ? (h ? cM : cA) : 0, cb_end = lo < hi ? (h ? cB : cM) : 0;
-        const int q3 = cc & 1;
-        uint8_t* sA3 = sA + q3 * 2 * A_TILE;
-        uint8_t* sAnq = sAn + q3 * 2 * kNqA;
-        if (cc >= 2 && !mbar_wait(&a3E[q3], ((cc >> 1) - 1) & 1)) {
-          atomicExch(err, 38);
-          abort_flag = 1;
-          ok = false;
-          break;
+        const int ca = h ? cM : cA, cb_end = h ? cB : cM;
+        uint8_t* sA3 = sS + s * 2 * A_TILE;
+        if (n >= NB) {
+          if (!mbar_wait(&freeO[s], (par >> s) & 1u)) {
+            atomicCAS(err, 0, 38);
+            abort_flag = 1;
+            ok = false;
+            break;
+          }
+          par ^= 1u << s;
         }
         tmem_for_groups(tmem + lane_off, ca, cb_end, [&](const uint32_t(&r)[16], int cb) {
-          epi2_group<16>(r, cb, lo_l, hi_l, rbase, m2, sA3);
+          epi2_group<16>(r, cb, lo_l, hi_l, (u0l - j) * HH, m2, sA3);
         });
-        if (threadIdx.x - 64 < TM) {  // row r of the chunk: its Nyquist pair Y[u0][u1]
-          const int r = TM * j + (threadIdx.x - 64);
-          const int a = r / p.U, u1 = r - (r / p.U) * p.U;
-          const int u0 = tg * p.G + a;
-          if (r < rows_a3 && u0 < p.U) {
-            const float2 y = nyq[((size_t)b * p.U + u0) * p.U + u1];
-            uint32_t hi2, lo2;
-            split2(y.x, y.y, hi2, lo2);
-            *reinterpret_cast<uint32_t*>(sAnq + k16_word(threadIdx.x - 64)) = hi2;
-            *reinterpret_cast<uint32_t*>(sAnq + kNqA + k16_word(threadIdx.x - 64)) = lo2;
-          }
-        }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive(&a3F[q3]);
+        mbar_arrive(&opF[s]);
       }
       if (!ok) break;
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(&acc2E);
     }
   } else if (warp >= 2 + kEpi / 32) {
-    // argmax warps: TMEM lanes 32 q .. 32 q + 31 of each chunk's pass-3 accumulator, all
-    // columns; they run a chunk behind the operand warps
-    const int q = warp & 3;
-    const uint32_t lane_off = (uint32_t)(q * 32) << 16;
+    // argmax warps (q, h): TMEM lanes 32 q .. 32 q + 31 of each chunk's pass-3 accumulator,
+    // half h of its columns; they run a chunk behind the operand warps
+    const int q = warp & 3, h = (warp - 2 - kEpi / 32) >> 2;
     const int r_lane = q * 32 + lane;
-    int tl = 0, cc = 0;
+    const int u0l = r_lane / HH, r1 = r_lane - (r_lane / HH) * HH;
+    const uint32_t lane_off = (uint32_t)(q * 32) << 16;
+    const int c3m = (((NT3 >> 4) + 1) >> 1) << 4;
+    const int ca = h ? c3m : 0, cb_end = h ? NT3 : c3m;
+    int tl = 0;
     for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
       const int b = tile / p.TPB, tg = tile - (tile / p.TPB) * p.TPB;
+      const int u0 = tg * p.G + u0l;
       float bv = -INFINITY;
       int bi = 0x7fffffff;
       bool have = false;
       bool ok = true;
-      for (int j = 0; j < p.CH; ++j, ++cc) {
-        const int q3 = cc & 1;
+      for (int j = 0; j < p.CH; ++j) {
+        const int cc = tl * p.CH + j, q3 = cc & 1;
+        const int u1 = j * HH + r1;
+        const bool valid = u1 < p.U && u0 < p.U;
+        const float2 y = valid ? nyq[((size_t)b * p.U + u0) * p.U + u1] : make_float2(0.f, 0.f);
         if (!mbar_wait(&acc3F[q3], (cc >> 1) & 1)) {
-          atomicExch(err, 39);
+          atomicCAS(err, 0, 39);
           abort_flag = 1;
           ok = false;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const int r = TM * j + r_lane;  // (u0_local, u1) row of the tile
-        const int a = r / p.U, u1 = r - (r / p.U) * p.U;
-        const int u0 = tg * p.G + a;
-        const bool valid = r < rows_a3 && u0 < p.U;
         const int row_flat = u0 * p.U + u1;
-        tmem_for_groups(tmem + lane_off + (uint32_t)(NT12 + q3 * NT3), 0, NT3,
+        tmem_for_groups(tmem + lane_off + (uint32_t)(NT12 + q3 * NT3), ca, cb_end,
                         [&](const uint32_t(&rr)[16], int cb) {
-                          if (valid) scan_group<16>(rr, cb, p.U, row_flat, bv, bi, have);
+                          if (valid) scan_group_nq<16>(rr, cb, p.U, row_flat, y, sEn, bv, bi, have);
                         });
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         mbar_arrive(&acc3E[q3]);
@@ -762,7 +761,7 @@ float bf2f(uint16_t h) {
 }
 
 struct Geometry {
-  int HH, NT12, NT3, KB12, G, TPB, CH, stages1;
+  int HH, NT12, NT3, KB12, G, TPB, CH, NB, stages1;
   size_t smem1, smem23;
 };
 
@@ -776,12 +775,17 @@ bool geometry(int N, int U, Geometry* o) {
   g.KB12 = (2 * N + TK - 1) / TK;
   g.G = TM / g.HH;
   g.TPB = (U + g.G - 1) / g.G;
-  g.CH = (g.G * U + TM - 1) / TM;
+  g.CH = (U + g.HH - 1) / g.HH;
   if (g.NT12 + 2 * g.NT3 > 512) return false;
   const size_t b1 = (size_t)2 * g.KB12 * g.NT12 * TK * 2;
   const size_t b3 = (size_t)2 * g.NT3 * TK * 2;
-  g.smem23 = 1024 + b1 + b3 + 4 * (size_t)A_TILE + 4 * (size_t)kNqA + (size_t)2 * g.NT3 * 32;
-  if (g.smem23 > kSmemCap) return false;
+  // three operand slots where they fit (the next tile's A2 then loads during this tile's
+  // pass 3), else two
+  for (g.NB = kMaxSlots; g.NB >= 2; --g.NB) {
+    g.smem23 = 1024 + b1 + b3 + (size_t)g.NB * 2 * A_TILE + (size_t)g.NT3 * 8;
+    if (g.smem23 <= kSmemCap) break;
+  }
+  if (g.NB < 2) return false;
   g.stages1 = (int)((kSmemCap - 1024 - b1) / (2 * (size_t)A_TILE));
   if (g.stages1 > kMaxStages) g.stages1 = kMaxStages;
   if (g.stages1 < 2) return false;
@@ -811,6 +815,7 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
   t->G = ge.G;
   t->TPB = ge.TPB;
   t->CH = ge.CH;
+  t->NB = ge.NB;
   t->stages1 = ge.stages1;
   t->smem1 = ge.smem1;
   t->smem23 = ge.smem23;
@@ -831,7 +836,7 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
   if (cudaMalloc(&t->E1, (size_t)2 * t->NT12 * k12 * 2) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->E3, (size_t)2 * t->NT3 * k3 * 2) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->E, (size_t)U * N * sizeof(float2)) != cudaSuccess) return MTB_ERR_OOM;
-  if (cudaMalloc(&t->ENQ, (size_t)2 * t->NT3 * 32) != cudaSuccess) return MTB_ERR_OOM;
+  if (cudaMalloc(&t->ENQ, (size_t)t->NT3 * sizeof(float2)) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->p32, (size_t)max_batch * N * N * sizeof(float2)) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->nyq, (size_t)max_batch * U * U * sizeof(float2)) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->best, (size_t)max_batch * 8) != cudaSuccess) return MTB_ERR_OOM;
@@ -850,15 +855,8 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
   };
   std::vector<uint16_t> e1((size_t)2 * t->NT12 * k12, 0), e3((size_t)2 * t->NT3 * k3, 0);
   std::vector<float2> ef((size_t)U * N);
-  // Nyquist B operand: rows u2, K = (re, im) of m2 = N/2 and 14 zeros, plain K-major layout
-  std::vector<uint16_t> enq((size_t)2 * t->NT3 * 16, 0);
-  auto put_nq = [&](int u, int k, double v) {
-    const uint16_t hi = f2bf((float)v);
-    const uint16_t lo = f2bf((float)(v - (double)bf2f(hi)));
-    const size_t at = ((size_t)(u >> 3) * 256 + (size_t)(k >> 3) * 128 + (size_t)(u & 7) * 16 + (k & 7) * 2) / 2;
-    enq[at] = hi;
-    enq[(size_t)t->NT3 * 16 + at] = lo;
-  };
+  // the Nyquist column's factor (re, -im) of E2[u2, N/2], FP32, zero past U
+  std::vector<float2> enq((size_t)t->NT3, make_float2(0.f, 0.f));
   auto put = [&](std::vector<uint16_t>& dst, size_t k, int rows, int r, int kk, double v) {
     const uint16_t hi = f2bf((float)v);
     const uint16_t lo = f2bf((float)(v - (double)bf2f(hi)));
@@ -884,13 +882,12 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
     }
     double er, ei;
     E(H, u, HH, &er, &ei);
-    put_nq(u, 0, er);
-    put_nq(u, 1, -ei);
+    enq[u] = make_float2((float)er, (float)-ei);
   }
   if (cudaMemcpy(t->E1, e1.data(), e1.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(t->E3, e3.data(), e3.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(t->E, ef.data(), ef.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(t->ENQ, enq.data(), enq.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess)
+      cudaMemcpy(t->ENQ, enq.data(), enq.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess)
     return MTB_ERR_CUDA;
   int rc = make_map(t->mapA1, t->A1, k12, (uint64_t)2 * t->R1, TM);
   if (!rc) rc = make_map(t->mapA2, t->A2, k12, (uint64_t)2 * t->R2, TM);
@@ -943,6 +940,7 @@ int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st, const cudaEvent_t* marks
   p2.U = U;
   p2.G = t->G;
   p2.CH = t->CH;
+  p2.NB = t->NB;
   p2.KB = t->KB12;
   p2.R2 = t->R2;
   p2.NT12 = t->NT12;
@@ -952,15 +950,16 @@ int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st, const cudaEvent_t* marks
   updft23_tc_kernel<<<g2, kThreads23, t->smem23, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA2),
                                                      *reinterpret_cast<const CUtensorMap*>(t->mapE1),
                                                      *reinterpret_cast<const CUtensorMap*>(t->mapE3), p2, t->nyq,
-                                                     (const uint4*)t->ENQ, t->best, t->err);
+                                                     (const float4*)t->ENQ, t->best, t->err);
   MTB_LAUNCH_CHECK();
   if (marks && marks[2]) cudaEventRecord(marks[2], st);
   return MTB_OK;
 }
 
-int shift_tc_check(ShiftTc* t, cudaStream_t st) {
+int shift_tc_check(ShiftTc* t, cudaStream_t st, int* site) {
   int h = 0;
   MTB_CUDA_TRY(cudaMemcpyAsync(&h, t->err, sizeof(int), cudaMemcpyDeviceToHost, st));
   MTB_CUDA_TRY(cudaStreamSynchronize(st));
+  if (site) *site = h;
   return h ? MTB_ERR_TIMEOUT : MTB_OK;
 }

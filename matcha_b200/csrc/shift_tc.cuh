@@ -8,15 +8,15 @@ struct ShiftTc {
   alignas(64) unsigned char mapA2[128];  // pass-2 A: rows (b, u0, m2 < N/2), K (m1, re/im)
   alignas(64) unsigned char mapE1[128];  // B of passes 1, 2: rows (u, re/im), K (m, re/im)
   alignas(64) unsigned char mapE3[128];  // B of pass 3: rows u2, K (m2 < N/2, re/im) -> real part
-  int N, H, HH, U, NT12, NT3, KB12, G, TPB, CH, Bmax;
+  int N, H, HH, U, NT12, NT3, KB12, G, TPB, CH, NB, Bmax;
   int R1, R2;                            // padded rows per hi/lo part of A1, A2
   int stages1;                           // pipeline stages of pass 1
   int n_sm;
   size_t smem1, smem23;                  // dynamic shared memory of the two kernels
   void *A1, *A2, *E1, *E3;               // bf16, [part][row][K]
   float2* E;                             // (U, N) exp(2 pi i (u - s) f_m), the FP32 DFT kernel
-  void* ENQ;                             // pass-3 B operand of the Nyquist column m2 = N/2, bf16
-                                         // [part][NT3 x 16] in the plain K-major layout
+  float2* ENQ;                           // (NT3) (re, -im) of E2[u2, N/2], the Nyquist column's
+                                         // pass-3 factor (zero past U)
   float2* p32;                           // (Bmax, N, N) product plane m2 = N/2, [m1][m0], FP32
   float2* nyq;                           // (Bmax, U, U) its 2-D upsampled DFT
   unsigned long long* best;              // (Bmax) argmax keys: ordered value << 32 | ~flat index
@@ -32,5 +32,6 @@ void shift_tc_release(ShiftTc* t);
 // Nyquist plane p32 have been written (fft_z split).
 // marks (or null): events recorded on st after the Nyquist kernel, pass 1 and passes 2+3.
 int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st, const cudaEvent_t* marks = nullptr);
-// Synchronises st; MTB_ERR_TIMEOUT if a device-side wait gave up.
-int shift_tc_check(ShiftTc* t, cudaStream_t st);
+// Synchronises st; MTB_ERR_TIMEOUT if a device-side wait gave up, with the code of the
+// wait that gave up first in *site (when site is not null).
+int shift_tc_check(ShiftTc* t, cudaStream_t st, int* site = nullptr);
