@@ -396,11 +396,13 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
   const int B1 = NT12 * TK * 2, B3 = NT3 * TK * 2;
   uint8_t* sE1 = smem;                       // [part][kb] B1
   uint8_t* sE3 = sE1 + 2 * KB * B1;          // [part] B3
-  // NB slots of two A_TILE (hi, lo), taken in turn (use n in slot n % NB): a tile's KB A2
-  // K-blocks, then its CH pass-3 operand chunks.  A slot is refilled once the MMAs that read
-  // its last contents are done; that commit goes to freeT or freeO after the kind of the next
-  // use, so the TMA thread and the operand warps each wait their own barrier, in order, never
-  // more than one phase ahead of it.
+  // NB slots of two A_TILE (hi, lo).  A2 K-block kb of every tile lives in slot kb; pass-3
+  // chunk j in slot chunk_slot(j), alternating between the two highest slots so that the last
+  // chunk takes the top one.  A slot that also holds an A2 K-block (kb = NB - 2 when KB = 2 and
+  // NB = 3) is last used by chunk CH - 2, so the next tile's K-block loads while chunk CH - 1
+  // is written, and slot 0 reloads as soon as pass 2 has read it.  freeT[kb] opens a K-block
+  // slot to the TMA thread once per tile; freeO[s] hands a chunk slot from one chunk to the
+  // next, so each barrier is waited in order, never more than one phase ahead.
   uint8_t* sS = sE3 + 2 * B3;
   float4* sEn = reinterpret_cast<float4*>(sS + NB * 2 * A_TILE);  // (er, -ei) of E2[u2, N/2], pairs
   __shared__ __align__(8) uint64_t tmaF[kMaxSlots], opF[kMaxSlots], freeT[kMaxSlots], freeO[kMaxSlots];
@@ -441,7 +443,10 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
   const uint32_t idesc2 = idesc_bf16(TM, NT12), idesc3 = idesc_bf16(TM, NT3);
-  const int per_tile = KB + p.CH;  // slot uses per tile
+  const int CH = p.CH;
+  // slot of chunk j; whether slot kb < KB is read by no chunk of a tile
+  auto chunk_slot = [&](int j) { return ((CH - 1 - j) & 1) ? NB - 2 : NB - 1; };
+  auto kb_chunk_free = [&](int kb) { return !(kb == NB - 1 || (kb == NB - 2 && CH >= 2)); };
 
   if (warp == 0 && lane == 0) {
     mbar_expect_tx(&resF, (uint32_t)(2 * KB * B1 + 2 * B3));
@@ -451,25 +456,20 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
     }
     int tl = 0;
     bool ok = true;
-    uint32_t par = 0;  // bit s: phase of the next wait on freeT[s]
     for (int tile = blockIdx.x; ok && tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
       const int b = tile / p.TPB, tg = tile - (tile / p.TPB) * p.TPB;
       const int arow = (b * p.U + tg * p.G) * HH;
       for (int kb = 0; kb < KB; ++kb) {
-        const int n = tl * per_tile + kb, s = n % NB;
-        if (n >= NB) {
-          if (!mbar_wait(&freeT[s], (par >> s) & 1u)) {
-            atomicCAS(err, 0, 31);
-            abort_flag = 1;
-            ok = false;
-            break;
-          }
-          par ^= 1u << s;
+        if (tl >= 1 && !mbar_wait(&freeT[kb], (tl - 1) & 1)) {
+          atomicCAS(err, 0, 31);
+          abort_flag = 1;
+          ok = false;
+          break;
         }
-        uint8_t* sa = sS + s * 2 * A_TILE;
-        mbar_expect_tx(&tmaF[s], 2 * A_TILE);
-        tma_load_2d(sa, &mapA2, kb * TK, arow, &tmaF[s]);
-        tma_load_2d(sa + A_TILE, &mapA2, kb * TK, p.R2 + arow, &tmaF[s]);
+        uint8_t* sa = sS + kb * 2 * A_TILE;
+        mbar_expect_tx(&tmaF[kb], 2 * A_TILE);
+        tma_load_2d(sa, &mapA2, kb * TK, arow, &tmaF[kb]);
+        tma_load_2d(sa + A_TILE, &mapA2, kb * TK, p.R2 + arow, &tmaF[kb]);
       }
     }
   } else if (warp == 1 && lane == 0) {
@@ -478,7 +478,7 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
       atomicCAS(err, 0, 32);
       abort_flag = 1;
     }
-    uint32_t tma_par = 0, op_par = 0;  // bit s: phase of the next wait on tmaF[s] / opF[s]
+    uint32_t op_par = 0;  // bit s: phase of the next wait on opF[s]
     int tl = 0;
     for (int tile = blockIdx.x; ok && tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
       // pass 2 into acc2 (columns 0 .. NT12) once the operand warps have read the last tile's
@@ -489,27 +489,25 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       for (int kb = 0; kb < KB; ++kb) {
-        const int n = tl * per_tile + kb, s = n % NB;
-        if (!mbar_wait(&tmaF[s], (tma_par >> s) & 1u)) {
+        if (!mbar_wait(&tmaF[kb], tl & 1)) {
           atomicCAS(err, 0, 34);
           abort_flag = 1;
           ok = false;
           break;
         }
-        tma_par ^= 1u << s;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint8_t* sa = sS + s * 2 * A_TILE;
+        const uint8_t* sa = sS + kb * 2 * A_TILE;
         mma_split_kblock(tmem, smem_desc(sa), smem_desc(sa + A_TILE), smem_desc(sE1 + kb * B1),
                          smem_desc(sE1 + (KB + kb) * B1), idesc2, kb == 0);
-        mma_commit_to((n + NB) % per_tile < KB ? &freeT[s] : &freeO[s]);
+        if (kb_chunk_free(kb)) mma_commit_to(&freeT[kb]);
       }
       if (!ok) break;
       mma_commit_to(&acc2F);
       // pass 3, chunk by chunk: the CTA's chunk cc into acc3 buffer cc & 1 (columns
       // NT12 + (cc & 1) NT3) once the argmax warps have read chunk cc - 2 from it
-      for (int j = 0; j < p.CH; ++j) {
-        const int n = tl * per_tile + KB + j, s = n % NB;
-        const int cc = tl * p.CH + j, q3 = cc & 1;
+      for (int j = 0; j < CH; ++j) {
+        const int s = chunk_slot(j);
+        const int cc = tl * CH + j, q3 = cc & 1;
         if (!mbar_wait(&opF[s], (op_par >> s) & 1u)) {
           atomicCAS(err, 0, 35);
           abort_flag = 1;
@@ -527,7 +525,8 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
         const uint8_t* a3 = sS + s * 2 * A_TILE;
         mma_split_kblock(tmem + (uint32_t)(NT12 + q3 * NT3), smem_desc(a3), smem_desc(a3 + A_TILE), smem_desc(sE3),
                          smem_desc(sE3 + B3), idesc3, true);
-        mma_commit_to((n + NB) % per_tile < KB ? &freeT[s] : &freeO[s]);
+        // a K-block slot after its last chunk of the tile goes back to the TMA thread
+        mma_commit_to(s < KB && j >= CH - 2 ? &freeT[s] : &freeO[s]);
         mma_commit_to(&acc3F[q3]);
       }
     }
@@ -549,14 +548,16 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       bool ok = true;
-      for (int j = 0; j < p.CH; ++j) {
-        const int n = tl * per_tile + KB + j, s = n % NB;
+      for (int j = 0; j < CH; ++j) {
+        const int s = chunk_slot(j);
         const int lo_l = j * HH, hi_l = min(p.U, lo_l + HH);  // this chunk's u1
         const int cA = 2 * lo_l, cB = min(NT12, (2 * hi_l + 15) & ~15);
         const int cM = cA + ((((cB - cA) >> 4) + 1) >> 1 << 4);  // h = 0 takes the first half
         const int ca = h ? cM : cA, cb_end = h ? cB : cM;
         uint8_t* sA3 = sS + s * 2 * A_TILE;
-        if (n >= NB) {
+        // the slot's last use was a chunk: this tile's j - 2, or, in a slot of its own, the
+        // previous tile's (a K-block slot's first chunk follows pass 2, waited above)
+        if (s < KB ? j >= 2 : (tl >= 1 || j >= 2)) {
           if (!mbar_wait(&freeO[s], (par >> s) & 1u)) {
             atomicCAS(err, 0, 38);
             abort_flag = 1;

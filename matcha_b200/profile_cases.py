@@ -3,6 +3,7 @@
     python -m matcha_b200.profile_cases shift  200   # ShiftMatcher.search_shifts, 64^3, uf 8, r 5
     python -m matcha_b200.profile_cases search 296   # Matcha.search_orientations, L 32, C 10
     python -m matcha_b200.profile_cases fle    256   # CrossCorrelationMatcher.get_sigma, 64^3, L 32
+    python -m matcha_b200.profile_cases shift 1000 --stages   # plus ShiftMatcher.profile per kernel group
 
 Each case builds its inputs on the device from a fixed seed (random volumes, Haar rotations,
 random shifts; a synthetic sigma with a known optimum for the search), runs the stage three
@@ -36,7 +37,9 @@ def _shift(B: int, dev):
     q = rng.standard_normal((B, 4))
     q /= np.linalg.norm(q, axis=1, keepdims=True)
     z = torch.from_numpy(rng.uniform(-2, 2, (B, 3)).astype(np.float32)).to(dev)
-    return lambda: sm.search_shifts(subtomos=vols, ctfs=None, shift_zyx=z, rotation_tracker=q)
+    run = lambda: sm.search_shifts(subtomos=vols, ctfs=None, shift_zyx=z, rotation_tracker=q)
+    run.matcher = sm
+    return run
 
 
 def _search(B: int, dev):
@@ -73,6 +76,7 @@ def main(argv=None) -> int:
     p.add_argument("case", choices=sorted(CASES))
     p.add_argument("batch", type=int)
     p.add_argument("--reps", type=int, default=5)
+    p.add_argument("--stages", action="store_true", help="shift only: time each kernel group with CUDA events")
     a = p.parse_args(argv)
     if not torch.cuda.is_available():
         print("a CUDA device is required", file=sys.stderr)
@@ -89,6 +93,15 @@ def main(argv=None) -> int:
     e1.record()
     torch.cuda.synchronize()
     print(f"{a.case} batch {a.batch}: {e0.elapsed_time(e1) / a.reps:.3f} ms per call")
+    sm = getattr(run, "matcher", None)
+    if a.stages and sm is not None:
+        sm.profile(a.reps)
+        for _ in range(a.reps):
+            run()
+        torch.cuda.synchronize()
+        ms, calls = sm.profile_read()
+        sm.profile(0)
+        print("  " + ", ".join(f"{k} {v / max(calls, 1):.3f}" for k, v in ms.items()) + " ms per call")
     return 0
 
 
