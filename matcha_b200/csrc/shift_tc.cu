@@ -153,22 +153,27 @@ __device__ __forceinline__ void epi1_group(const uint32_t* v, int cb, bool valid
   }
 }
 
-__device__ __forceinline__ uint32_t sw128_word(int r, int w);
-
 // Passes 2 + 3: columns (u1, re/im) of one pass-2 row (u0_local, m2) -> word m2 of the pass-3
-// operand rows rbase + u1 that fall in this chunk.
+// operand rows rbase + u1 that fall in this chunk (128-byte-swizzled K-major tile).  The
+// group's 8 rows r0 + t start at a multiple of 8 (rbase and cb / 2 are), so row r0 + t sits
+// t * 128 bytes into one 1024-byte swizzle atom and word m2 in 16-byte chunk (m2 / 4) ^ t: the
+// XOR with a constant is the whole per-row address arithmetic.
 template <int NC>
 __device__ __forceinline__ void epi2_group(const uint32_t* v, int cb, int lo_l, int hi_l, int rbase, int m2,
                                            uint8_t* sA3) {
+  static_assert(NC == 16, "one group is 8 rows of the pass-3 operand");
+  const int u10 = cb / 2;
+  uint8_t* base = sA3 + (((rbase + u10) >> 3) << 10) + ((m2 & 3) << 2);
+  const uint32_t cw = (uint32_t)(m2 >> 2) << 4;
+  const bool full = u10 >= lo_l && u10 + 8 <= hi_l;
 #pragma unroll
-  for (int t = 0; t < NC / 2; ++t) {
+  for (int t = 0; t < 8; ++t) {
     uint32_t hi, lo;
     split2(__uint_as_float(v[2 * t]), __uint_as_float(v[2 * t + 1]), hi, lo);
-    const int u1 = cb / 2 + t;
-    const uint32_t off = sw128_word(rbase + u1, m2);
-    if (u1 >= lo_l && u1 < hi_l) {
-      *reinterpret_cast<uint32_t*>(sA3 + off) = hi;
-      *reinterpret_cast<uint32_t*>(sA3 + A_TILE + off) = lo;
+    uint8_t* at = base + t * 128 + (cw ^ (uint32_t)(t << 4));
+    if (full || (u10 + t >= lo_l && u10 + t < hi_l)) {
+      *reinterpret_cast<uint32_t*>(at) = hi;
+      *reinterpret_cast<uint32_t*>(at + A_TILE) = lo;
     }
   }
 }
@@ -365,17 +370,13 @@ updft1_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant
 }
 
 // ------------------------------------------------------------------ fused passes 2 + 3
-// Byte offset of 4-byte word w (K pair) of row r in a 128-row K-major tile of 64 bf16 per
-// row, 128-byte swizzle (16-byte chunk c of row r at chunk c ^ (r % 8)).
-__device__ __forceinline__ uint32_t sw128_word(int r, int w) {
-  return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((((w >> 2) ^ (r & 7))) << 4) + ((w & 3) << 2));
-}
 
 // Pass 3 plus the Nyquist term: running argmax over NC values u2 = cb .. cb + NC - 1 of one
 // row, each v[u2] + Re(Y E2[u2, N/2]) = v + y.x en[u2].x + y.y en[u2].y in FP32.
 template <int NC>
 __device__ __forceinline__ void scan_group_nq(const uint32_t* vr, int cb, int U, int row_flat, float2 y,
                                               const float4* __restrict__ en2, float& bv, int& bi, bool& have) {
+  static_assert(NC == 16, "the packed scan takes groups of 16");
   uint32_t w[NC];
 #pragma unroll
   for (int t = 0; t < NC; t += 2) {
@@ -383,7 +384,35 @@ __device__ __forceinline__ void scan_group_nq(const uint32_t* vr, int cb, int U,
     w[t] = __float_as_uint(fmaf(y.y, e.y, fmaf(y.x, e.x, __uint_as_float(vr[t]))));
     w[t + 1] = __float_as_uint(fmaf(y.y, e.w, fmaf(y.x, e.z, __uint_as_float(vr[t + 1]))));
   }
-  scan_group<NC>(w, cb, U, row_flat, bv, bi, have);
+  // The position in the group rides in the low 4 mantissa bits of each value (15 - t, so the
+  // largest of equal values is the first), which lowers the compared magnitudes by at most 15
+  // units in the last place, far below the hi/lo split's own error; one NaN-propagating
+  // maximum per value then finds the group's best.  A group whose maximum is NaN (a NaN, or an
+  // infinity whose low bits were set) is rescanned exactly.
+  float m[4];
+  if (cb + NC <= U) {
+#pragma unroll
+    for (int t = 0; t < NC; ++t) {
+      const float f = __uint_as_float((w[t] & 0xFFFFFFF0u) | (uint32_t)(15 - t));
+      m[t & 3] = t < 4 ? f : fmax_nan(m[t & 3], f);
+    }
+  } else {  // the last group: columns past U take the lowest finite value
+#pragma unroll
+    for (int t = 0; t < NC; ++t) {
+      const uint32_t b = (cb + t < U) ? (w[t] & 0xFFFFFFF0u) : 0xFF7FFFF0u;
+      const float f = __uint_as_float(b | (uint32_t)(15 - t));
+      m[t & 3] = t < 4 ? f : fmax_nan(m[t & 3], f);
+    }
+  }
+  const float g = fmax_nan(fmax_nan(m[0], m[1]), fmax_nan(m[2], m[3]));
+  if (g != g) {
+    scan_group<NC>(w, cb, U, row_flat, bv, bi, have);
+    return;
+  }
+  const bool upd = g > bv;  // never once bv is NaN: nothing later wins
+  bv = upd ? g : bv;
+  bi = upd ? row_flat * U + cb + 15 - (int)(__float_as_uint(g) & 15u) : bi;
+  have = have || upd;
 }
 
 __global__ void __launch_bounds__(kThreads23, 1)
@@ -616,7 +645,8 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
       if (!ok) break;
       // a lane visits its values in increasing flat order, so a later equal value never wins;
       // the warp's keys all belong to subtomogram b
-      unsigned long long key = have ? argmax_key(bv, bi) : 0ull;
+      // (the low 4 bits of the value, position bits of the packed scan, are cleared)
+      unsigned long long key = have ? argmax_key(__uint_as_float(__float_as_uint(bv) & 0xFFFFFFF0u), bi) : 0ull;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long k2 = __shfl_xor_sync(0xffffffffu, key, o);

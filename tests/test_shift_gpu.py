@@ -119,3 +119,32 @@ def test_shift_tensor_path_many_tiles_per_cta(cuda_device):
     np.testing.assert_allclose(out["bf16x3"][1], out["fp32"][1], rtol=1e-4)
     same = np.all(np.abs(out["bf16x3"][0] - out["fp32"][0]) <= 1e-6, axis=1)
     assert same.mean() >= 0.9, same
+
+
+def test_shift_nan_subtomogram_follows_argmax_order(cuda_device):
+    """A NaN voxel makes the subtomogram's whole correlation grid NaN; argmax then takes the
+    first grid point, as torch.argmax and numpy.argmax do, on both paths.  The other
+    subtomograms of the batch are unaffected."""
+    N, B = 32, 3
+    rng = np.random.default_rng(5)
+    tmpl = blob_template(rng, N, 60, N * 0.3, (1.5, 3.0), mask_radius=N * 0.4)
+    vols = np.repeat(tmpl[None], B, 0) + 0.3 * rng.standard_normal((B, N, N, N)).astype(np.float32)
+    clean = torch.from_numpy(vols.copy()).to(cuda_device)
+    vols[1, 7, 9, 11] = np.nan
+    dirty = torch.from_numpy(vols).to(cuda_device)
+    q = haar_quaternions(rng, B)
+    z = torch.zeros((B, 3), device=cuda_device)
+    out = {}
+    for precision in ("fp32", "bf16x3"):
+        sm = _matcher(N, B, 8, 3, cuda_device, precision=precision)
+        sm.set_reference(tmpl)
+        s_d, c_d = sm.search_shifts(subtomos=dirty, ctfs=None, shift_zyx=z, rotation_tracker=q)
+        s_c, c_c = sm.search_shifts(subtomos=clean, ctfs=None, shift_zyx=z, rotation_tracker=q)
+        sm.status()
+        s_d, c_d, s_c, c_c = (t.cpu().numpy() for t in (s_d, c_d, s_c, c_c))
+        assert np.isnan(c_d[1]) and np.all(np.isfinite(c_d[[0, 2]]))
+        assert s_d[1, 0] == s_d[1, 1] == s_d[1, 2] < 0  # flat index 0: u0 = u1 = u2 = 0
+        np.testing.assert_array_equal(s_d[[0, 2]], s_c[[0, 2]])
+        np.testing.assert_allclose(c_d[[0, 2]], c_c[[0, 2]], rtol=1e-6)  # norms sum in any order
+        out[precision] = s_d[1]
+    np.testing.assert_array_equal(out["bf16x3"], out["fp32"])
