@@ -111,22 +111,29 @@ class AlignmentStep:
 
         The batch is cut into ``chunks`` pieces: the host-to-device copy of piece k + 1 runs
         on a side stream while piece k is aligned on the current stream, so the transfer of
-        the volumes (4 N^3 bytes each) and the alignment overlap.  tracker (B, 4) float64 and
-        shift_zyx (B, 3) are device tensors; tracker is updated in place.  Returns the
-        outputs of ``__call__`` for the whole batch, in tensors of their own."""
+        the volumes (4 N^3 bytes each) and the alignment overlap.  Two device staging buffers
+        alternate between calls, so the next call's first copies also overlap the end of this
+        call's alignment.  tracker (B, 4) float64 and shift_zyx (B, 3) are device tensors;
+        tracker is updated in place.  Returns the outputs of ``__call__`` for the whole batch,
+        in tensors of their own (rewritten by the next call)."""
         B = volumes_host.shape[0]
         if B > self.cfg.batch:
             raise ValueError(f"batch {B} exceeds the configured batch {self.cfg.batch}")
         dev = self.device
         N = self.cfg.N
         if getattr(self, "_stage", None) is None:
-            self._stage = torch.empty((self.cfg.batch, N, N, N), device=dev, dtype=torch.float32)
+            self._stage = [torch.empty((self.cfg.batch, N, N, N), device=dev, dtype=torch.float32)
+                           for _ in range(2)]
+            self._stage_free = [None, None]  # compute-stream events after each buffer's last reader
+            self._stage_next = 0
             self._copy_stream = torch.cuda.Stream(device=dev)
             self._out = {k: torch.empty((self.cfg.batch,) + ((3,) if k == "shift" else ()), device=dev,
                                         dtype=torch.float32) for k in self._KEYS}
-        stage, cs = self._stage, self._copy_stream
+        which = self._stage_next
+        stage, cs = self._stage[which], self._copy_stream
         compute = torch.cuda.current_stream(dev)
-        cs.wait_stream(compute)  # the previous call's reads of the staging buffer come first
+        if self._stage_free[which] is not None:
+            cs.wait_event(self._stage_free[which])  # the alignment that read this buffer is done
         bounds = [B * k // chunks for k in range(chunks + 1)]
         ready = []
         with torch.cuda.stream(cs):
@@ -146,6 +153,10 @@ class AlignmentStep:
             o = self(vols, vols, tracker[lo:hi], shift_zyx[lo:hi])
             for key in self._KEYS:
                 self._out[key][lo:hi].copy_(o[key])
+        free = torch.cuda.Event()
+        free.record(compute)
+        self._stage_free[which] = free
+        self._stage_next = which ^ 1
         out = {k: self._out[k][:B] for k in self._KEYS}
         out["tracker"] = tracker
         return out

@@ -44,6 +44,36 @@ def test_align_host_matches_device_step(cuda_device, chunks):
         np.testing.assert_allclose(t_host.cpu().numpy(), t_dev.cpu().numpy(), atol=1e-6)
 
 
+def test_align_host_back_to_back_calls(cuda_device):
+    """Three calls without a host synchronisation in between, on two different batches:
+    the third reuses the first call's staging buffer while the second may still run."""
+    B, N = 5, 16
+    rng = np.random.default_rng(12)
+    tmpl = blob_template(rng, N, 12, 5, (1.0, 2.0), mask_radius=7).astype(np.float32)
+    batches = [(np.repeat(tmpl[None], B, 0) + s * rng.standard_normal((B, N, N, N))).astype(np.float32)
+               for s in (0.05, 0.2)]
+    step = _step(cuda_device, B)
+    step.set_template(tmpl)
+    ident = torch.zeros((B, 4), dtype=torch.float64, device=cuda_device)
+    ident[:, 0] = 1
+    zeros3 = torch.zeros((B, 3), device=cuda_device)
+    keys = ("alpha", "beta", "gamma", "rotation_score", "shift", "shift_score")
+    refs = []
+    for v in batches:
+        dv = torch.from_numpy(v).to(cuda_device)
+        refs.append({k: t.clone() for k, t in step(dv, dv, ident.clone(), zeros3).items()})
+    hosts = [torch.from_numpy(v).pin_memory() for v in batches]
+    outs = []
+    for i in (0, 1, 0):
+        o = step.align_host(hosts[i], ident.clone(), zeros3, chunks=2)
+        outs.append((i, {k: o[k].clone() for k in keys}))
+    torch.cuda.synchronize()
+    for i, o in outs:
+        for k in keys:
+            np.testing.assert_allclose(o[k].cpu().numpy(), refs[i][k].cpu().numpy(), rtol=1e-5, atol=1e-6,
+                                       err_msg=k)
+
+
 def test_align_host_rejects_oversize_batch(cuda_device):
     step = _step(cuda_device, 2)
     host = torch.zeros((3, 16, 16, 16)).pin_memory()
