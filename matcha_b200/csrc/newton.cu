@@ -26,8 +26,9 @@
 //    table) is differentiated twice in b, so d', d'' ride along in registers: no neighbour
 //    rows, no shared d blocks and no barriers inside a pass.
 //
-// Each thread walks whole chains (a wedge pair from l = M' to the stage degree); chains are
-// dealt to threads in boustrophedon order so that long (small M') and short chains mix.
+// Each thread walks whole chains (a wedge pair from l = M' to the stage degree), for the two
+// candidates of its CTA at once; chains are dealt to threads in boustrophedon order so that
+// long (small M') and short chains mix.
 #include <math.h>
 #include "common.cuh"
 #include "newton.cuh"
@@ -38,13 +39,15 @@ constexpr int kNT = kNewtonThreads;
 
 enum { A_VAL = 0, A_GA, A_GB, A_GG, A_HAA, A_HAB, A_HAG, A_HBB, A_HBG, A_HGG, A_N };
 
+// Per-candidate tables of one pass (NC candidates of one subtomogram per CTA).
+template <int NC>
 struct Smem {
-  float2* ea;   // e^{i k a}, index k + Li
-  float2* eg;   // e^{i k g}, index k + Li
-  double* phc;  // cos(b/2)^k, k = 0 .. 2 Li + 2
-  double* pt;   // (-sin(b/2))^k
-  float* red;   // (threads/32) x A_N
-  float* res;   // A_N
+  float2 (*ea)[2 * kNewtonMaxL + 1];   // e^{i k a}, index k + Li
+  float2 (*eg)[2 * kNewtonMaxL + 1];   // e^{i k g}, index k + Li
+  double (*phc)[2 * kNewtonMaxL + 3];  // cos(b/2)^k, k = 0 .. 2 Li + 2
+  double (*pt)[2 * kNewtonMaxL + 3];   // (-sin(b/2))^k
+  float* red;                          // (threads/32) x NC x A_N
+  float* res;                          // NC x A_N
 };
 
 __device__ __forceinline__ double ipow(double x, int n) {
@@ -129,38 +132,47 @@ __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// One sweep over the chains of stage degree Li at (a, be, ga): value, and with DERIVS the
-// Euler gradient and Hessian, left in sm.res.  FOLDED reads the folded sigma S of this
-// subtomogram; otherwise each step folds the four images from sigma itself.
-template <bool DERIVS, bool FOLDED>
+// One sweep over the chains of stage degree Li at the NC points (a[c], be[c], ga[c]) of one
+// subtomogram's candidates: value, and with DERIVS the Euler gradient and Hessian, left in
+// sm.res[c * A_N + ..].  The candidates share each chain's loads of the folded sigma and of
+// the recurrence factors; their d, d', d'' run side by side.  FOLDED reads the folded sigma S
+// of this subtomogram; otherwise each step folds the four images from sigma itself.
+template <bool DERIVS, bool FOLDED, int NC>
 __device__ __forceinline__ void pass(const float4* __restrict__ S, const float2* __restrict__ sg,
-                                     const float4* __restrict__ coef, const double* __restrict__ Ctab, float a,
-                                     float be, float ga, int Li, const Smem sm) {
+                                     const float4* __restrict__ coef, const double* __restrict__ Ctab,
+                                     const float (&a)[NC], const float (&be)[NC], const float (&ga)[NC], int Li,
+                                     const Smem<NC> sm) {
   const int tid = threadIdx.x;
   const double two_pi = 6.283185307179586;
-  for (int r = tid; r < 2 * Li + 1; r += kNT) {
-    double t = (double)(r - Li) * (double)a;
-    t -= two_pi * rint(t / two_pi);
-    float s, c;
-    sincosf((float)t, &s, &c);
-    sm.ea[r] = make_float2(c, s);
-    t = (double)(r - Li) * (double)ga;
-    t -= two_pi * rint(t / two_pi);
-    sincosf((float)t, &s, &c);
-    sm.eg[r] = make_float2(c, s);
-  }
-  double hs, hc;
-  sincos(0.5 * (double)be, &hs, &hc);
-  for (int k = tid; k <= 2 * Li + 2; k += kNT) {
-    sm.phc[k] = ipow(hc, k);
-    sm.pt[k] = ipow(-hs, k);
-  }
-  float sb, cb;
-  sincosf(be, &sb, &cb);
-
-  float acc[A_N];
 #pragma unroll
-  for (int i = 0; i < A_N; ++i) acc[i] = 0.f;
+  for (int c = 0; c < NC; ++c) {
+    for (int r = tid; r < 2 * Li + 1; r += kNT) {
+      double t = (double)(r - Li) * (double)a[c];
+      t -= two_pi * rint(t / two_pi);
+      float s, co;
+      sincosf((float)t, &s, &co);
+      sm.ea[c][r] = make_float2(co, s);
+      t = (double)(r - Li) * (double)ga[c];
+      t -= two_pi * rint(t / two_pi);
+      sincosf((float)t, &s, &co);
+      sm.eg[c][r] = make_float2(co, s);
+    }
+    double hs, hc;
+    sincos(0.5 * (double)be[c], &hs, &hc);
+    for (int k = tid; k <= 2 * Li + 2; k += kNT) {
+      sm.phc[c][k] = ipow(hc, k);
+      sm.pt[c][k] = ipow(-hs, k);
+    }
+  }
+  float sb[NC], cb[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) sincosf(be[c], &sb[c], &cb[c]);
+
+  float acc[NC][A_N];
+#pragma unroll
+  for (int c = 0; c < NC; ++c)
+#pragma unroll
+    for (int i = 0; i < A_N; ++i) acc[c][i] = 0.f;
   __syncthreads();
 
   const int n = (Li + 1) * (Li + 1);
@@ -172,75 +184,92 @@ __device__ __forceinline__ void pass(const float4* __restrict__ S, const float2*
     wedge_pair(p, mp, m);
     // start of the chain at l = M': d = C cos^P (-sin)^Q of b/2, P = M'+M, Q = M'-M
     const int P = mp + m, Q = mp - m;
-    const double C = Ctab[p];
-    float d1 = (float)(C * sm.phc[P] * sm.pt[Q]), d0 = 0.f;
-    float e1 = 0.f, e0 = 0.f, g1 = 0.f, g0 = 0.f;
-    if (DERIVS) {
-      double fp = 0.0, fpp = -(double)(2 * P * Q + P + Q) * sm.phc[P] * sm.pt[Q];
-      if (P >= 1) fp += P * sm.phc[P - 1] * sm.pt[Q + 1];
-      if (Q >= 1) fp -= Q * sm.phc[P + 1] * sm.pt[Q - 1];
-      if (P >= 2) fpp += (double)(P * (P - 1)) * sm.phc[P - 2] * sm.pt[Q + 2];
-      if (Q >= 2) fpp += (double)(Q * (Q - 1)) * sm.phc[P + 2] * sm.pt[Q - 2];
-      e1 = (float)(0.5 * C * fp);
-      g1 = (float)(0.25 * C * fpp);
+    const double Cp = Ctab[p];
+    float d1[NC], d0[NC], e1[NC], e0[NC], g1[NC], g0[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      d1[c] = (float)(Cp * sm.phc[c][P] * sm.pt[c][Q]);
+      d0[c] = 0.f;
+      e1[c] = e0[c] = g1[c] = g0[c] = 0.f;
+      if (DERIVS) {
+        double fp = 0.0, fpp = -(double)(2 * P * Q + P + Q) * sm.phc[c][P] * sm.pt[c][Q];
+        if (P >= 1) fp += P * sm.phc[c][P - 1] * sm.pt[c][Q + 1];
+        if (Q >= 1) fp -= Q * sm.phc[c][P + 1] * sm.pt[c][Q - 1];
+        if (P >= 2) fpp += (double)(P * (P - 1)) * sm.phc[c][P - 2] * sm.pt[c][Q + 2];
+        if (Q >= 2) fpp += (double)(Q * (Q - 1)) * sm.phc[c][P + 2] * sm.pt[c][Q - 2];
+        e1[c] = (float)(0.5 * Cp * fp);
+        g1[c] = (float)(0.25 * Cp * fpp);
+      }
     }
     float4 s;
     if (FOLDED) s = __ldg(S + wedge_off(mp) + p);
     else s = fold_entry(sg, mp, mp, m);
-    float a1r = d1 * s.x, a1i = d1 * s.y, a2r = d1 * s.z, a2i = d1 * s.w;
-    float b1r = 0.f, b1i = 0.f, b2r = 0.f, b2i = 0.f, c1r = 0.f, c1i = 0.f, c2r = 0.f, c2i = 0.f;
-    if (DERIVS) {
-      b1r = e1 * s.x; b1i = e1 * s.y; b2r = e1 * s.z; b2i = e1 * s.w;
-      c1r = g1 * s.x; c1i = g1 * s.y; c2r = g1 * s.z; c2i = g1 * s.w;
+    // per candidate: A = sum d S (a1 = S1 part, a2 = S2 part), B = sum d' S, C = sum d'' S
+    float A1r[NC], A1i[NC], A2r[NC], A2i[NC];
+    float B1r[NC], B1i[NC], B2r[NC], B2i[NC], C1r[NC], C1i[NC], C2r[NC], C2i[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      A1r[c] = d1[c] * s.x; A1i[c] = d1[c] * s.y; A2r[c] = d1[c] * s.z; A2i[c] = d1[c] * s.w;
+      B1r[c] = B1i[c] = B2r[c] = B2i[c] = C1r[c] = C1i[c] = C2r[c] = C2i[c] = 0.f;
+      if (DERIVS) {
+        B1r[c] = e1[c] * s.x; B1i[c] = e1[c] * s.y; B2r[c] = e1[c] * s.z; B2i[c] = e1[c] * s.w;
+        C1r[c] = g1[c] * s.x; C1i[c] = g1[c] * s.y; C2r[c] = g1[c] * s.z; C2i[c] = g1[c] * s.w;
+      }
     }
     const float4* cp = coef + wedge_off(mp + 1) + p;
     const float4* sp = FOLDED ? S + wedge_off(mp + 1) + p : nullptr;
 #pragma unroll 2
     for (int l = mp + 1; l <= Li; ++l) {
       const float4 cf = __ldg(cp);
-      const float t = fmaf(cf.x, cb, -cf.y);
-      const float v = fmaf(t, d1, -cf.z * d0);
-      if (DERIVS) {
-        const float as = cf.x * sb;
-        const float vp = fmaf(t, e1, -fmaf(as, d1, cf.z * e0));
-        const float vpp = fmaf(t, g1, -fmaf(2.f * as, e1, fmaf(cf.x * cb, d1, cf.z * g0)));
-        e0 = e1; e1 = vp;
-        g0 = g1; g1 = vpp;
-      }
-      d0 = d1; d1 = v;
       if (FOLDED) s = __ldg(sp);
       else s = fold_entry(sg, l, mp, m);
-      a1r = fmaf(v, s.x, a1r); a1i = fmaf(v, s.y, a1i);
-      a2r = fmaf(v, s.z, a2r); a2i = fmaf(v, s.w, a2i);
-      if (DERIVS) {
-        b1r = fmaf(e1, s.x, b1r); b1i = fmaf(e1, s.y, b1i);
-        b2r = fmaf(e1, s.z, b2r); b2i = fmaf(e1, s.w, b2i);
-        c1r = fmaf(g1, s.x, c1r); c1i = fmaf(g1, s.y, c1i);
-        c2r = fmaf(g1, s.z, c2r); c2i = fmaf(g1, s.w, c2i);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float t = fmaf(cf.x, cb[c], -cf.y);
+        const float v = fmaf(t, d1[c], -cf.z * d0[c]);
+        if (DERIVS) {
+          const float as = cf.x * sb[c];
+          const float vp = fmaf(t, e1[c], -fmaf(as, d1[c], cf.z * e0[c]));
+          const float vpp = fmaf(t, g1[c], -fmaf(2.f * as, e1[c], fmaf(cf.x * cb[c], d1[c], cf.z * g0[c])));
+          e0[c] = e1[c]; e1[c] = vp;
+          g0[c] = g1[c]; g1[c] = vpp;
+        }
+        d0[c] = d1[c]; d1[c] = v;
+        A1r[c] = fmaf(v, s.x, A1r[c]); A1i[c] = fmaf(v, s.y, A1i[c]);
+        A2r[c] = fmaf(v, s.z, A2r[c]); A2i[c] = fmaf(v, s.w, A2i[c]);
+        if (DERIVS) {
+          B1r[c] = fmaf(e1[c], s.x, B1r[c]); B1i[c] = fmaf(e1[c], s.y, B1i[c]);
+          B2r[c] = fmaf(e1[c], s.z, B2r[c]); B2i[c] = fmaf(e1[c], s.w, B2i[c]);
+          C1r[c] = fmaf(g1[c], s.x, C1r[c]); C1i[c] = fmaf(g1[c], s.y, C1i[c]);
+          C2r[c] = fmaf(g1[c], s.z, C2r[c]); C2i[c] = fmaf(g1[c], s.w, C2i[c]);
+        }
       }
       cp += (l + 1) * (l + 1);
       if (FOLDED) sp += (l + 1) * (l + 1);
     }
     // phases: z1 = e^{i(M'a + Mg)}, z2 = e^{i(Ma + M'g)}
-    const float2 z1 = cmulf(sm.ea[mp + Li], sm.eg[m + Li]);
-    const float2 z2 = cmulf(sm.ea[m + Li], sm.eg[mp + Li]);
-    const float r1 = z1.x * a1r - z1.y * a1i, r2 = z2.x * a2r - z2.y * a2i;
-    acc[A_VAL] += r1 + r2;
-    if (DERIVS) {
-      const float fM = (float)mp, fm = (float)m;
-      const float j1 = z1.x * a1i + z1.y * a1r, j2 = z2.x * a2i + z2.y * a2r;
-      const float q1 = z1.x * b1r - z1.y * b1i, q2 = z2.x * b2r - z2.y * b2i;
-      const float k1 = z1.x * b1i + z1.y * b1r, k2 = z2.x * b2i + z2.y * b2r;
-      const float h1 = z1.x * c1r - z1.y * c1i, h2 = z2.x * c2r - z2.y * c2i;
-      acc[A_GA] -= fM * j1 + fm * j2;
-      acc[A_GG] -= fm * j1 + fM * j2;
-      acc[A_GB] += q1 + q2;
-      acc[A_HAA] -= fM * fM * r1 + fm * fm * r2;
-      acc[A_HGG] -= fm * fm * r1 + fM * fM * r2;
-      acc[A_HAG] -= fM * fm * (r1 + r2);
-      acc[A_HAB] -= fM * k1 + fm * k2;
-      acc[A_HBG] -= fm * k1 + fM * k2;
-      acc[A_HBB] += h1 + h2;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const float2 z1 = cmulf(sm.ea[c][mp + Li], sm.eg[c][m + Li]);
+      const float2 z2 = cmulf(sm.ea[c][m + Li], sm.eg[c][mp + Li]);
+      const float r1 = z1.x * A1r[c] - z1.y * A1i[c], r2 = z2.x * A2r[c] - z2.y * A2i[c];
+      acc[c][A_VAL] += r1 + r2;
+      if (DERIVS) {
+        const float fM = (float)mp, fm = (float)m;
+        const float j1 = z1.x * A1i[c] + z1.y * A1r[c], j2 = z2.x * A2i[c] + z2.y * A2r[c];
+        const float q1 = z1.x * B1r[c] - z1.y * B1i[c], q2 = z2.x * B2r[c] - z2.y * B2i[c];
+        const float k1 = z1.x * B1i[c] + z1.y * B1r[c], k2 = z2.x * B2i[c] + z2.y * B2r[c];
+        const float h1 = z1.x * C1r[c] - z1.y * C1i[c], h2 = z2.x * C2r[c] - z2.y * C2i[c];
+        acc[c][A_GA] -= fM * j1 + fm * j2;
+        acc[c][A_GG] -= fm * j1 + fM * j2;
+        acc[c][A_GB] += q1 + q2;
+        acc[c][A_HAA] -= fM * fM * r1 + fm * fm * r2;
+        acc[c][A_HGG] -= fm * fm * r1 + fM * fM * r2;
+        acc[c][A_HAG] -= fM * fm * (r1 + r2);
+        acc[c][A_HAB] -= fM * k1 + fm * k2;
+        acc[c][A_HBG] -= fm * k1 + fM * k2;
+        acc[c][A_HBB] += h1 + h2;
+      }
     }
   }
 
@@ -248,15 +277,20 @@ __device__ __forceinline__ void pass(const float4* __restrict__ S, const float2*
   const int lane = tid & 31, warp = tid >> 5;
   constexpr int NA = DERIVS ? A_N : 1;
 #pragma unroll
-  for (int i = 0; i < NA; ++i) {
-    const float v = warp_sum(acc[i]);
-    if (lane == 0) sm.red[warp * A_N + i] = v;
-  }
+  for (int c = 0; c < NC; ++c)
+#pragma unroll
+    for (int i = 0; i < NA; ++i) {
+      const float v = warp_sum(acc[c][i]);
+      if (lane == 0) sm.red[(warp * NC + c) * A_N + i] = v;
+    }
   __syncthreads();
-  if (tid < NA) {
-    float s = 0.f;
-    for (int q = 0; q < kNT / 32; ++q) s += sm.red[q * A_N + tid];
-    sm.res[tid] = s;
+  if (tid < NC * A_N) {
+    const int c = tid / A_N, i = tid - (tid / A_N) * A_N;
+    if (i < NA) {
+      float s2 = 0.f;
+      for (int q = 0; q < kNT / 32; ++q) s2 += sm.red[(q * NC + c) * A_N + i];
+      sm.res[c * A_N + i] = s2;
+    }
   }
   __syncthreads();
 }
@@ -290,75 +324,112 @@ __device__ bool solve3(const double H[3][3], const double g[3], double x[3]) {
   return true;
 }
 
-template <bool FOLDED>
-__global__ void __launch_bounds__(kNT, 5)
+// One CTA per NC candidates of one subtomogram (C % NC == 0).  Each candidate keeps its own
+// point, learning rate, gradient and Hessian; the passes evaluate all NC together.
+template <bool FOLDED, int NC>
+__global__ void __launch_bounds__(kNT, 4)
 newton_march_kernel(const float4* __restrict__ S, int64_t n_fold, const float2* __restrict__ sigma, int64_t stride,
                     int BC, int C, float* __restrict__ alpha, float* __restrict__ beta, float* __restrict__ gamma,
                     float* __restrict__ score, const double* __restrict__ Ctab, const float4* __restrict__ coef,
                     NewtonParams P) {
-  __shared__ float2 s_ea[2 * kNewtonMaxL + 1], s_eg[2 * kNewtonMaxL + 1];
-  __shared__ double s_phc[2 * kNewtonMaxL + 3], s_pt[2 * kNewtonMaxL + 3];
-  __shared__ float s_red[(kNT / 32) * A_N], s_res[A_N];
-  const Smem sm{s_ea, s_eg, s_phc, s_pt, s_red, s_res};
+  __shared__ float2 s_ea[NC][2 * kNewtonMaxL + 1], s_eg[NC][2 * kNewtonMaxL + 1];
+  __shared__ double s_phc[NC][2 * kNewtonMaxL + 3], s_pt[NC][2 * kNewtonMaxL + 3];
+  __shared__ float s_red[(kNT / 32) * NC * A_N], s_res[NC * A_N];
+  const Smem<NC> sm{s_ea, s_eg, s_phc, s_pt, s_red, s_res};
 
-  const int cand = blockIdx.x;
-  if (cand >= BC) return;
-  const int b = cand / C;
+  const int cand0 = blockIdx.x * NC;
+  if (cand0 >= BC) return;
+  const int b = cand0 / C;
   const float4* Sb = FOLDED ? S + (int64_t)b * n_fold : nullptr;
   const float2* sg = FOLDED ? nullptr : sigma + (int64_t)b * stride;
   const bool grad_step = (P.flags & MTB_SEARCH_GRADIENT_STEP) != 0;
   const float base_lr = grad_step ? 5e-7f : 1.f;
 
-  float a = alpha[cand], be = beta[cand], ga = gamma[cand];
-  float best = 0.f;
-  for (int s = 0; s < P.n_stages; ++s) {
-    const int Li = P.stages[s];
+  // the gradient and Hessian at each candidate's accepted point: pass results (res layout),
+  // kept in shared memory so they are not live in registers across the passes
+  __shared__ float s_gh[NC * A_N];
+  float a[NC], be[NC], ga[NC], best[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    a[c] = alpha[cand0 + c];
+    be[c] = beta[cand0 + c];
+    ga[c] = gamma[cand0 + c];
+    best[c] = 0.f;
+  }
+  for (int st = 0; st < P.n_stages; ++st) {
+    const int Li = P.stages[st];
     if (P.num_steps > 0)
-      pass<true, FOLDED>(Sb, sg, coef, Ctab, a, be, ga, Li, sm);
+      pass<true, FOLDED, NC>(Sb, sg, coef, Ctab, a, be, ga, Li, sm);
     else
-      pass<false, FOLDED>(Sb, sg, coef, Ctab, a, be, ga, Li, sm);
-    best = sm.res[A_VAL];
-    double g[3] = {sm.res[A_GA], sm.res[A_GB], sm.res[A_GG]};
-    double H[3][3] = {{sm.res[A_HAA], sm.res[A_HAB], sm.res[A_HAG]},
-                      {sm.res[A_HAB], sm.res[A_HBB], sm.res[A_HBG]},
-                      {sm.res[A_HAG], sm.res[A_HBG], sm.res[A_HGG]}};
-    float lr = base_lr;
+      pass<false, FOLDED, NC>(Sb, sg, coef, Ctab, a, be, ga, Li, sm);
+    float lr[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      best[c] = sm.res[c * A_N + A_VAL];
+      lr[c] = base_lr;
+    }
+    if (threadIdx.x < NC * A_N) s_gh[threadIdx.x] = sm.res[threadIdx.x];
+    __syncthreads();
     for (int it = 0; it < P.num_steps; ++it) {
-      double x[3] = {0.0, 0.0, 0.0};
-      if (grad_step) {
-        for (int i = 0; i < 3; ++i) x[i] = -g[i];
-      } else if (!solve3(H, g, x)) {
-        x[0] = x[1] = x[2] = 0.0;
+      float ta[NC], tb[NC], tg[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float* r = s_gh + c * A_N;
+        const double g[3] = {r[A_GA], r[A_GB], r[A_GG]};
+        const double H[3][3] = {{r[A_HAA], r[A_HAB], r[A_HAG]},
+                                {r[A_HAB], r[A_HBB], r[A_HBG]},
+                                {r[A_HAG], r[A_HBG], r[A_HGG]}};
+        double x[3] = {0.0, 0.0, 0.0};
+        if (grad_step) {
+          for (int i = 0; i < 3; ++i) x[i] = -g[i];
+        } else if (!solve3(H, g, x)) {
+          x[0] = x[1] = x[2] = 0.0;
+        }
+        ta[c] = a[c] - lr[c] * (float)x[0];
+        tb[c] = be[c] - lr[c] * (float)x[1];
+        tg[c] = ga[c] - lr[c] * (float)x[2];
       }
-      const float ta = a - lr * (float)x[0];
-      const float tb = be - lr * (float)x[1];
-      const float tg = ga - lr * (float)x[2];
       const bool last = (it == P.num_steps - 1);
       __syncthreads();  // everyone has read the previous results
       if (last)
-        pass<false, FOLDED>(Sb, sg, coef, Ctab, ta, tb, tg, Li, sm);
+        pass<false, FOLDED, NC>(Sb, sg, coef, Ctab, ta, tb, tg, Li, sm);
       else
-        pass<true, FOLDED>(Sb, sg, coef, Ctab, ta, tb, tg, Li, sm);
-      const float ev = sm.res[A_VAL];
-      if (ev > best) {
-        a = ta; be = tb; ga = tg; best = ev;
-        lr *= 1.1f;
-        if (!last) {
-          g[0] = sm.res[A_GA]; g[1] = sm.res[A_GB]; g[2] = sm.res[A_GG];
-          H[0][0] = sm.res[A_HAA]; H[0][1] = H[1][0] = sm.res[A_HAB]; H[0][2] = H[2][0] = sm.res[A_HAG];
-          H[1][1] = sm.res[A_HBB]; H[1][2] = H[2][1] = sm.res[A_HBG]; H[2][2] = sm.res[A_HGG];
+        pass<true, FOLDED, NC>(Sb, sg, coef, Ctab, ta, tb, tg, Li, sm);
+      bool took[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float ev = sm.res[c * A_N + A_VAL];
+        took[c] = ev > best[c];
+        if (took[c]) {
+          a[c] = ta[c]; be[c] = tb[c]; ga[c] = tg[c]; best[c] = ev;
+          lr[c] *= 1.1f;
+        } else {
+          lr[c] *= 0.5f;
         }
-      } else {
-        lr *= 0.5f;
+      }
+      if (!last) {
+        if (threadIdx.x < NC * A_N) {
+          const int c = threadIdx.x / A_N;
+          bool tk = false;
+#pragma unroll
+          for (int q = 0; q < NC; ++q) tk = (q == c) ? took[q] : tk;
+          if (tk) s_gh[threadIdx.x] = sm.res[threadIdx.x];
+        }
+        __syncthreads();
       }
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    alpha[cand] = a;
-    beta[cand] = be;
-    gamma[cand] = ga;
-    score[cand] = best;
+  if (threadIdx.x < NC) {
+    const int c = threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < NC; ++q)
+      if (q == c) {
+        alpha[cand0 + c] = a[q];
+        beta[cand0 + c] = be[q];
+        gamma[cand0 + c] = ga[q];
+        score[cand0 + c] = best[q];
+      }
   }
 }
 
@@ -382,12 +453,21 @@ int newton_launch(const float* sigma, int64_t stride, int B, int C, float* a, fl
   const int BC = B * C;
   const float2* sg = reinterpret_cast<const float2*>(sigma);
   const int64_t nf = newton_fold_entries(P.Lmax);
+  // two candidates of a subtomogram per CTA share its folded-sigma and recurrence-factor loads
+  const bool pair = (C % 2) == 0;
   if (fold) {
     fold_sigma_kernel<<<dim3(P.Lmax + 1, B), 256, 0, st>>>(sg, stride, nf, fold);
     MTB_LAUNCH_CHECK();
-    newton_march_kernel<true><<<BC, kNT, 0, st>>>(fold, nf, sg, stride, BC, C, a, b, g, s, Ctab, coef, P);
+    if (pair)
+      newton_march_kernel<true, 2><<<BC / 2, kNT, 0, st>>>(fold, nf, sg, stride, BC, C, a, b, g, s, Ctab, coef, P);
+    else
+      newton_march_kernel<true, 1><<<BC, kNT, 0, st>>>(fold, nf, sg, stride, BC, C, a, b, g, s, Ctab, coef, P);
   } else {
-    newton_march_kernel<false><<<BC, kNT, 0, st>>>(nullptr, nf, sg, stride, BC, C, a, b, g, s, Ctab, coef, P);
+    if (pair)
+      newton_march_kernel<false, 2><<<BC / 2, kNT, 0, st>>>(nullptr, nf, sg, stride, BC, C, a, b, g, s, Ctab, coef,
+                                                             P);
+    else
+      newton_march_kernel<false, 1><<<BC, kNT, 0, st>>>(nullptr, nf, sg, stride, BC, C, a, b, g, s, Ctab, coef, P);
   }
   MTB_LAUNCH_CHECK();
   return MTB_OK;
