@@ -407,7 +407,8 @@ constexpr size_t z_smem_bytes() {
 // by three separable linear interpolations (z, then x, then y) from the two staged planes.
 constexpr int kT64 = 288;  // 36 groups of 8: 33 lines for the (N/2+1)-column passes
 constexpr int kXS = 72;    // per-line scratch (float2): transpose slot (k1, r) at 9 k1 + r
-constexpr int kYS = 34;    // row stride (float2) of the 64 x 33 column buffers
+constexpr int kYS = 34;    // row stride (float2) of the 64 x 33 y-FFT output of the patch pass
+constexpr int kZS = 33;    // row stride (float2) of the 64 x 33 buffer of the z pass
 
 __device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -448,19 +449,23 @@ __device__ __forceinline__ void fft64_group(float2 (&v)[8], int r, float2* xs, c
   dft8(v);
 }
 
-// FFT along the rows of a 64 x 33 column buffer (element (n, col) at buf[n * kYS + col]) in
-// place, one column per group of 8 threads; xs: 36 line scratches.
+// FFT along the rows of a 64 x 33 column buffer (element (n, col) at buf[n * kZS + col], a
+// dense row stride of 33) in place, one column per group of 8 threads; xs: 36 line scratches.
+// The two groups of a half-warp take columns 8 apart (group 2 i + h: column (i & 7) + 16 (i / 8)
+// + 8 h), so their 8-byte accesses r + 8 s, (r + 8 s) * 33 + col fill the 16 bank pairs once;
+// the row-wise readers of the buffer, 16 consecutive rows per half-warp, do so too.
 __device__ __forceinline__ void fft64_columns(float2* buf, float2* xs, const float2* tw) {
   const int L = threadIdx.x >> 3, r = threadIdx.x & 7;
-  const int col = L < 33 ? L : 32;  // groups 33..35 shadow column 32 inside its own warp
+  // groups 33..35 shadow column 32 inside its own warp
+  const int col = L < 32 ? ((L >> 1) & 7) + 16 * (L >> 4) + 8 * (L & 1) : 32;
   float2 v[8];
 #pragma unroll
-  for (int s = 0; s < 8; ++s) v[s] = buf[(r + 8 * s) * kYS + col];
+  for (int s = 0; s < 8; ++s) v[s] = buf[(r + 8 * s) * kZS + col];
   fft64_group(v, r, xs + L * kXS, tw);
   __syncwarp();
   if (L < 33) {
 #pragma unroll
-    for (int k2 = 0; k2 < 8; ++k2) buf[(r + 8 * k2) * kYS + col] = v[k2];
+    for (int k2 = 0; k2 < 8; ++k2) buf[(r + 8 * k2) * kZS + col] = v[k2];
   }
 }
 
@@ -471,6 +476,12 @@ __device__ void load_twiddles64(float2* tw) {
     tw[k] = make_float2((float)c, (float)s);
   }
 }
+
+// Element (q, c) of the 32 x 64 x-FFT output of the box-64 path: row q, column c ^ f(q) with
+// f(q) = 8 (q & 1) + 2 (q / 2 & 3).  The x FFT stores rows q, q + 1 (one per group of 8
+// lanes, 8 consecutive c) and the y FFT loads columns c, c + 1 (8 rows q = r + 8 s): both fill
+// the 16 bank pairs of a half-warp's 8-byte accesses once.
+__device__ __forceinline__ int z_at(int q, int c) { return q * 64 + (c ^ (((q & 1) << 3) | ((q << 1) & 6))); }
 
 // patch_fft_xy_kernel<64, false> with the radix-8 x 8 FFTs; fill_tab[r2] is fill_weight(r2).
 __global__ void __launch_bounds__(kT64, 4)
@@ -483,10 +494,10 @@ patch_fft_xy64_kernel(const float* __restrict__ vol, const float* __restrict__ s
   __shared__ int s_c[2][2][N];      // [y/x][tap] clamped source index
   __shared__ float s_w[2][2][N];    // [y/x][tap] weight (0 for taps outside the box or zeroed)
   float2* tw = sm2;                                     // 64
-  float* P0 = reinterpret_cast<float*>(sm2 + 64);       // plane iz, then the z-interpolated plane
-  float* P1 = P0 + N * N;                               // plane iz+1, then the x-interpolated plane
+  float* P0 = reinterpret_cast<float*>(sm2 + 64);       // the z-interpolated plane
+  float2* Z = reinterpret_cast<float2*>(P0 + N * N);    // 32 x 64 x FFT output, swizzled (z_at)
   float2* yb = reinterpret_cast<float2*>(P0);           // 64 x kYS, after the patch is built
-  float2* zb = reinterpret_cast<float2*>(P1 + N * N);   // 36 x kXS: packed rows, then scratch
+  float2* zb = Z + HN * N;                              // 36 x kXS: packed rows, then scratch
   const int ip = blockIdx.x, b = blockIdx.y;
   const int i = (ip + HN) & (N - 1);
   const int di = i - HN;
@@ -527,25 +538,29 @@ patch_fft_xy64_kernel(const float* __restrict__ vol, const float* __restrict__ s
     }
   }
   __syncthreads();
-  // x: P1[yy][k] <- w0(k) P0[yy][c0(k)] + w1(k) P0[yy][c1(k)]; a thread keeps one column k
-  // (its taps in registers) and walks every fourth row
+  // x and y in one pass from the z-interpolated plane: p(j, k) = wy0(j) (wx0(k) P0[cy0][cx0] +
+  // wx1(k) P0[cy0][cx1]) + wy1(j) (..cy1..) (the x taps in registers, the y taps computed per
+  // row as the setup computes them); then background, fill weight, 1/N^3, roll, and rows j and
+  // j + 32 (rolled to j + 32 and j) packed into one complex line with one 8-byte store
   float part = 0.f;
   if (threadIdx.x < 256) {
-    const int k = threadIdx.x & (N - 1), y0r = threadIdx.x >> 6;
-    const float w0 = s_w[1][0][k], w1 = s_w[1][1][k];
-    const int c0 = s_c[1][0][k], c1 = s_c[1][1][k];
-#pragma unroll 4
-    for (int yy = y0r; yy < N; yy += 4) P1[yy * N + k] = w0 * P0[yy * N + c0] + w1 * P0[yy * N + c1];
-  }
-  __syncthreads();
-  // y, background, fill weight, 1/N^3, roll, pack rows j' and j' + 32 into one complex line
-  if (threadIdx.x < 256) {
     const int k = threadIdx.x & (N - 1), j0 = threadIdx.x >> 6;
+    const float wx0 = s_w[1][0][k], wx1 = s_w[1][1][k];
+    const int cx0 = s_c[1][0][k], cx1 = s_c[1][1][k];
     const int dk = k - HN, kp = (k + HN) & (N - 1);
     const int rk = di * di + dk * dk;
-#pragma unroll 2
-    for (int j = j0; j < N; j += 4) {
-      const float p = s_w[0][0][j] * P1[s_c[0][0][j] * N + k] + s_w[0][1][j] * P1[s_c[0][1][j] * N + k];
+    auto sample = [&](int j) -> float {
+      const float y = (float)j + ps.f[1];
+      const float y0 = floorf(y);
+      const int iy = (int)y0;
+      const float fy = y - y0;
+      const bool zero = (j == ps.zp[1]);
+      const int cy0 = min(max(iy, 0), N - 1), cy1 = min(max(iy + 1, 0), N - 1);
+      const float wy0 = (zero || iy < 0 || iy >= N) ? 0.f : 1.f - fy;
+      const float wy1 = (zero || iy + 1 < 0 || iy + 1 >= N) ? 0.f : fy;
+      const float a = wx0 * P0[cy0 * N + cx0] + wx1 * P0[cy0 * N + cx1];
+      const float c = wx0 * P0[cy1 * N + cx0] + wx1 * P0[cy1 * N + cx1];
+      const float p = wy0 * a + wy1 * c;
       const int dj = j - HN;
       const int r2 = rk + dj * dj;
       float keep = 1.f;  // 1 - W
@@ -556,12 +571,17 @@ patch_fft_xy64_kernel(const float* __restrict__ vol, const float* __restrict__ s
         part += __ldg(bgw_tab + r2) * p;
         keep = 1.f - __ldg(fill_tab + r2);
       }
-      const int jp = (j + HN) & (N - 1);
-      reinterpret_cast<float*>(zb + (jp & (HN - 1)) * kXS + kp)[jp >> 5] = keep * p * g.inv_n3;
+      return keep * p * g.inv_n3;
+    };
+#pragma unroll 2
+    for (int j = j0; j < HN; j += 4) {
+      const float lo = sample(j), hi = sample(j + HN);  // rolled to rows j + 32 and j
+      zb[j * kXS + kp] = make_float2(hi, lo);
     }
   }
   __syncthreads();
-  // x FFT of the 32 packed lines (groups 32..35 work on their own scratch lines and are dropped)
+  // x FFT of the 32 packed lines (groups 32..35 work on their own scratch lines and are
+  // dropped), out to Z
   {
     const int L = threadIdx.x >> 3, r = threadIdx.x & 7;
     float2* line = zb + L * kXS;
@@ -569,9 +589,10 @@ patch_fft_xy64_kernel(const float* __restrict__ vol, const float* __restrict__ s
 #pragma unroll
     for (int s8 = 0; s8 < 8; ++s8) w[s8] = line[r + 8 * s8];
     fft64_group(w, r, line, tw);
-    __syncwarp();
+    if (L < HN) {
 #pragma unroll
-    for (int k2 = 0; k2 < 8; ++k2) line[r + 8 * k2] = w[k2];
+      for (int k2 = 0; k2 < 8; ++k2) Z[z_at(L, r + 8 * k2)] = w[k2];
+    }
   }
   __syncthreads();
   // y FFT of the columns m2 < 33, its input split on the way in: Z = A + i B holds the
@@ -584,12 +605,12 @@ patch_fft_xy64_kernel(const float* __restrict__ vol, const float* __restrict__ s
 #pragma unroll
     for (int s4 = 0; s4 < 4; ++s4) {
       const int q = r + 8 * s4;
-      const float2 zk = zb[q * kXS + col];
-      const float2 zm = zb[q * kXS + ((N - col) & (N - 1))];
+      const float2 zk = Z[z_at(q, col)];
+      const float2 zm = Z[z_at(q, (N - col) & (N - 1))];
       w[s4] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
       w[s4 + 4] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
     }
-    __syncthreads();  // zb becomes the transpose scratch
+    __syncthreads();  // Z is read: yb may overwrite its first rows, zb is the transpose scratch
     fft64_group(w, r, zb + L * kXS, tw);
     if (L < H) {
 #pragma unroll
@@ -607,7 +628,8 @@ patch_fft_xy64_kernel(const float* __restrict__ vol, const float* __restrict__ s
 }
 
 constexpr size_t xy64_smem_bytes() {
-  return (size_t)64 * sizeof(float2) + (size_t)2 * 64 * 64 * sizeof(float) + (size_t)36 * kXS * sizeof(float2);
+  return (size_t)64 * sizeof(float2) + (size_t)64 * 64 * sizeof(float) + (size_t)32 * 64 * sizeof(float2) +
+         (size_t)36 * kXS * sizeof(float2);
 }
 
 // fft_z_kernel<64, SPLIT> with the radix-8 x 8 FFT.
@@ -620,8 +642,8 @@ fft_z64_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ w
   extern __shared__ __align__(16) float2 sm2[];
   __shared__ float red[32];
   float2* tw = sm2;              // 64
-  float2* buf = sm2 + 64;        // 64 (i') x kYS
-  float2* xs = buf + N * kYS;    // 36 x kXS
+  float2* buf = sm2 + 64;        // 64 (i') x kZS
+  float2* xs = buf + N * kZS;    // 36 x kXS
   const int jp = blockIdx.x, b = blockIdx.y;
   float2* base = T + (int64_t)b * N * N * H + (int64_t)jp * H;
   const float2* wb = what + (int64_t)jp * H;
@@ -632,7 +654,7 @@ fft_z64_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ w
     const int ip = e / H, m2 = e - (e / H) * H;
     const float2 t = base[(int64_t)ip * N * H + m2];
     const float2 w = __ldg(&wb[(int64_t)ip * N * H + m2]);
-    buf[ip * kYS + m2] = make_float2(fmaf(avg, w.x, t.x), fmaf(avg, w.y, t.y));
+    buf[ip * kZS + m2] = make_float2(fmaf(avg, w.x, t.x), fmaf(avg, w.y, t.y));
   }
   __syncthreads();
   fft64_columns(buf, xs, tw);
@@ -645,7 +667,7 @@ fft_z64_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ w
 #pragma unroll 2
   for (int e = threadIdx.x; e < N * H; e += kT64) {
     const int ip = SPLIT ? e & (N - 1) : e / H, m2 = SPLIT ? e >> 6 : e - (e / H) * H;
-    const float2 t = buf[ip * kYS + m2];
+    const float2 t = buf[ip * kZS + m2];
     const int kp = ip < HN ? ip : ip - N;
     const int jq = jp < HN ? jp : jp - N;
     const int xq = m2 < HN ? m2 : m2 - H;
@@ -693,7 +715,7 @@ fft_z64_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ w
 }
 
 constexpr size_t z64_smem_bytes() {
-  return (size_t)64 * sizeof(float2) + (size_t)64 * kYS * sizeof(float2) + (size_t)36 * kXS * sizeof(float2);
+  return (size_t)64 * sizeof(float2) + (size_t)64 * kZS * sizeof(float2) + (size_t)36 * kXS * sizeof(float2);
 }
 
 __global__ void fill_table_kernel(ShiftGeom g, int n, float* __restrict__ tab) {
