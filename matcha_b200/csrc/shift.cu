@@ -86,6 +86,14 @@ __global__ void ref_quad_kernel(const float2* __restrict__ ref, int N, float4* _
   }
 }
 
+// One 32-byte corner quad in a single 256-bit load (the quads are 32-byte aligned): half the
+// load instructions, and each sector is looked up once instead of twice.
+__device__ __forceinline__ void ldg_quad(const float4* __restrict__ p, float4& lo, float4& hi) {
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(lo.x), "=f"(lo.y), "=f"(lo.z), "=f"(lo.w), "=f"(hi.x), "=f"(hi.y), "=f"(hi.z), "=f"(hi.w)
+      : "l"(p));
+}
+
 // trilinear_c from the corner quads (same weights and summation order).
 __device__ __forceinline__ float2 trilinear_quad(const float4* __restrict__ q, int N, float z, float y, float x) {
   const float z0 = floorf(z), y0 = floorf(y), x0 = floorf(x);
@@ -95,8 +103,9 @@ __device__ __forceinline__ float2 trilinear_quad(const float4* __restrict__ q, i
   const int n1 = N + 1;
   const int64_t e0 = in ? ((int64_t)(iz + 1) * n1 + (iy + 1)) * n1 + (ix + 1) : 0;
   const int64_t e1 = e0 + (int64_t)n1 * n1;
-  const float4 a0 = __ldg(q + 2 * e0), a1 = __ldg(q + 2 * e0 + 1);
-  const float4 b0 = __ldg(q + 2 * e1), b1 = __ldg(q + 2 * e1 + 1);
+  float4 a0, a1, b0, b1;
+  ldg_quad(q + 2 * e0, a0, a1);
+  ldg_quad(q + 2 * e1, b0, b1);
   const float2 v[8] = {make_float2(a0.x, a0.y), make_float2(a0.z, a0.w), make_float2(a1.x, a1.y),
                        make_float2(a1.z, a1.w), make_float2(b0.x, b0.y), make_float2(b0.z, b0.w),
                        make_float2(b1.x, b1.y), make_float2(b1.z, b1.w)};
