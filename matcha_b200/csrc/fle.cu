@@ -237,20 +237,36 @@ sigma_kernel(const float2* __restrict__ aV, int64_t v_stride, const float2* __re
   }
   __syncthreads();
   float2* out = sigma + (int64_t)b * s_stride + mtb_dsize(l - 1);
-  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-    const int a = e / w, c = e - (e / w) * w;  // m = a - l, m' = c - l
+  // a thread: one column c (m' = c - l) and four rows a = 4 aq .. 4 aq + 3 (m = a - l); the
+  // lanes of a warp take consecutive c (odd row stride: no bank conflicts) and mostly share
+  // aq (the four row reads are broadcasts), so one template read serves four products
+  const int naq = (w + 3) >> 2;
+  for (int e = threadIdx.x; e < naq * w; e += blockDim.x) {
+    const int aq = e / w, c = e - (e / w) * w;
     // row of -m' is 2l - c, row of -m is 2l - a
     const float2* tr = sT + (2 * l - c) * ks;
-    const float2* vr = sV + (2 * l - a) * ks;
-    float re = 0.f, im = 0.f;
+    const float2* vr[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) vr[j] = sV + (2 * l - min(4 * aq + j, w - 1)) * ks;
+    float re[4] = {0.f, 0.f, 0.f, 0.f}, im[4] = {0.f, 0.f, 0.f, 0.f};
     for (int k = 0; k < K; ++k) {
-      const float2 t = tr[k], u = vr[k];
-      // t * conj(u)
-      re += t.x * u.x + t.y * u.y;
-      im += t.y * u.x - t.x * u.y;
+      const float2 t = tr[k];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float2 u = vr[j][k];
+        // t * conj(u)
+        re[j] += t.x * u.x + t.y * u.y;
+        im[j] += t.y * u.x - t.x * u.y;
+      }
     }
-    const float sgn = ((a + c) & 1) ? -1.f : 1.f;  // (-1)^(m+mp) = (-1)^(a+c-2l)
-    out[e] = make_float2(sgn * re, sgn * im);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int a = 4 * aq + j;
+      if (a < w) {
+        const float sgn = ((a + c) & 1) ? -1.f : 1.f;  // (-1)^(m+mp) = (-1)^(a+c-2l)
+        out[a * w + c] = make_float2(sgn * re[j], sgn * im[j]);
+      }
+    }
   }
 }
 
