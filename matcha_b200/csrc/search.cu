@@ -153,32 +153,44 @@ so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
       F[q] = make_float2(re, im);
     }
     __syncthreads();
-    for (int q = tid; q < jn * P * n; q += blockDim.x) {
-      const int jb = q / (P * n), qq = q - jb * (P * n);
-      const int r = qq / n, gg = qq - (qq / n) * n;
-      const float2* fr = F + jb * P * P + r * P;
-      const float2* tr = TW + gg * P;
-      float re = 0.f, im = 0.f;
-      for (int c = 0; c < P; ++c) {
-        const float2 f = fr[c], t = tr[c];
-        re += f.x * t.x - f.y * t.y;
-        im += f.x * t.y + f.y * t.x;
+    if constexpr (NT > 0) {
+      // four outputs gg = g4 + (n/4) i per thread: one F read serves four independent chains
+      constexpr int n4 = NT / 4;
+      for (int q = tid; q < jn * P * n4; q += blockDim.x) {
+        const int jb = q / (P * n4), qq = q - jb * (P * n4);
+        const int r = qq / n4, g4 = qq - (qq / n4) * n4;
+        const float2* fr = F + jb * P * P + r * P;
+        float re[4] = {0.f, 0.f, 0.f, 0.f}, im[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int c = 0; c < P; ++c) {
+          const float2 f = fr[c];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const float2 t = TW[(g4 + n4 * i) * P + c];
+            re[i] += f.x * t.x - f.y * t.y;
+            im[i] += f.x * t.y + f.y * t.x;
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) G[jb * P * n + r * n + g4 + n4 * i] = make_float2(re[i], im[i]);
       }
-      G[q] = make_float2(re, im);
+    } else {
+      for (int q = tid; q < jn * P * n; q += blockDim.x) {
+        const int jb = q / (P * n), qq = q - jb * (P * n);
+        const int r = qq / n, gg = qq - (qq / n) * n;
+        const float2* fr = F + jb * P * P + r * P;
+        const float2* tr = TW + gg * P;
+        float re = 0.f, im = 0.f;
+        for (int c = 0; c < P; ++c) {
+          const float2 f = fr[c], t = tr[c];
+          re += f.x * t.x - f.y * t.y;
+          im += f.x * t.y + f.y * t.x;
+        }
+        G[q] = make_float2(re, im);
+      }
     }
     __syncthreads();
-    for (int q = tid; q < jn * n * n; q += blockDim.x) {
-      const int jb = q / (n * n), qq = q - jb * (n * n);
-      const int aa = qq / n, gg = qq - (qq / n) * n;
-      const float2* gc = G + jb * P * n + gg;
-      const float2* ta = TW + aa * P;
-      float re = 0.f;
-      for (int r = 0; r < P; ++r) {
-        const float2 gv = gc[r * n], t = ta[r];
-        re += gv.x * t.x - gv.y * t.y;
-      }
-      const float v = re * inv_n2;
-      const int flat = (j0 + jb) * n * n + qq;
+    // offer one grid value to this thread's kept set
+    auto offer = [&](float v, int flat) {
       if (grid_out) grid_out[(int64_t)b * n * n * n + flat] = v;
       // the rejection test reads the kept set's worst entry from registers
       if (cnt < C || better(v, flat, minv, mini)) {
@@ -191,6 +203,41 @@ so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
           }
         if (cnt < C) ++cnt;
         if (cnt == C) find_min();
+      }
+    };
+    if constexpr (NT > 0) {
+      // four outputs gg = g4 + (n/4) i per thread: one twiddle read serves four chains (the
+      // kept set is a total order on (value, index), so the visiting order does not matter)
+      constexpr int n4 = NT / 4;
+      for (int q = tid; q < jn * n * n4; q += blockDim.x) {
+        const int jb = q / (n * n4), qq = q - jb * (n * n4);
+        const int aa = qq / n4, g4 = qq - (qq / n4) * n4;
+        const float2* gc = G + jb * P * n + g4;
+        const float2* ta = TW + aa * P;
+        float re[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int r = 0; r < P; ++r) {
+          const float2 t = ta[r];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const float2 gv = gc[r * n + n4 * i];
+            re[i] += gv.x * t.x - gv.y * t.y;
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) offer(re[i] * inv_n2, (j0 + jb) * n * n + aa * n + g4 + n4 * i);
+      }
+    } else {
+      for (int q = tid; q < jn * n * n; q += blockDim.x) {
+        const int jb = q / (n * n), qq = q - jb * (n * n);
+        const int aa = qq / n, gg = qq - (qq / n) * n;
+        const float2* gc = G + jb * P * n + gg;
+        const float2* ta = TW + aa * P;
+        float re = 0.f;
+        for (int r = 0; r < P; ++r) {
+          const float2 gv = gc[r * n], t = ta[r];
+          re += gv.x * t.x - gv.y * t.y;
+        }
+        offer(re * inv_n2, (j0 + jb) * n * n + qq);
       }
     }
     __syncthreads();
