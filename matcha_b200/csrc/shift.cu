@@ -325,12 +325,13 @@ constexpr size_t xy_smem_bytes() {
 // sampled on the fly, and the norms |T|^2, |S|^2 per subtomogram.  Without SPLIT P overwrites
 // T; with SPLIT the pass-1 operand of the tensor-core upsampled DFT is written instead,
 // A1[part][(b, m2, m1)][2 m0 + c] for m2 < N/2 as bf16 hi/lo pairs (a1_ws pairs per row, a1_R
-// rows per part), and the Nyquist plane m2 = N/2 in FP32 to p32[b][m1][m0].
+// rows per part), and the Nyquist plane m2 = N/2 to a1n in the same format (rows (b, m1)).
 template <int N, bool SPLIT>
 __global__ void __launch_bounds__(kT)
 fft_z_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ what, const float* __restrict__ bg,
              const float2* __restrict__ ref, const float* __restrict__ rot, const float* __restrict__ ctf,
-             float* __restrict__ nrm, uint32_t* __restrict__ a1, int a1_ws, int a1_R, float2* __restrict__ p32) {
+             float* __restrict__ nrm, uint32_t* __restrict__ a1, int a1_ws, int a1_R, uint32_t* __restrict__ a1n,
+             int a1n_R) {
   constexpr int HN = N / 2, H = N / 2 + 1;
   extern __shared__ __align__(16) float2 sm2[];
   __shared__ float red[32];
@@ -389,7 +390,12 @@ fft_z_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ wha
         a1[row * a1_ws + ip] = hi;
         a1[((size_t)a1_R + row) * a1_ws + ip] = lo;
       } else {
-        p32[((size_t)b * N + jp) * N + ip] = p;  // the Nyquist plane m2 = N/2, FP32
+        // the Nyquist plane m2 = N/2: its own pass-1 operand, rows (b, m1), K (m0, re/im)
+        uint32_t hi, lo;
+        split_bf16x2(p.x, p.y, hi, lo);
+        const size_t row = (size_t)b * N + jp;
+        a1n[row * a1_ws + ip] = hi;
+        a1n[((size_t)a1n_R + row) * a1_ws + ip] = lo;
       }
     } else {
       base[(int64_t)ip * N * H + m2] = p;
@@ -646,7 +652,8 @@ template <bool SPLIT>
 __global__ void __launch_bounds__(kT64, 4)
 fft_z64_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ what, const float* __restrict__ bg,
                const float4* __restrict__ refq, const float* __restrict__ rot, const float* __restrict__ ctf,
-               float* __restrict__ nrm, uint32_t* __restrict__ a1, int a1_ws, int a1_R, float2* __restrict__ p32) {
+               float* __restrict__ nrm, uint32_t* __restrict__ a1, int a1_ws, int a1_R, uint32_t* __restrict__ a1n,
+               int a1n_R) {
   constexpr int N = 64, HN = 32, H = 33;
   extern __shared__ __align__(16) float2 sm2[];
   __shared__ float red[32];
@@ -709,7 +716,12 @@ fft_z64_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ w
         a1[row * a1_ws + ip] = hi;
         a1[((size_t)a1_R + row) * a1_ws + ip] = lo;
       } else {
-        p32[((size_t)b * N + jp) * N + ip] = p;  // the Nyquist plane m2 = N/2, FP32
+        // the Nyquist plane m2 = N/2: its own pass-1 operand, rows (b, m1), K (m0, re/im)
+        uint32_t hi, lo;
+        split_bf16x2(p.x, p.y, hi, lo);
+        const size_t row = (size_t)b * N + jp;
+        a1n[row * a1_ws + ip] = hi;
+        a1n[((size_t)a1n_R + row) * a1_ws + ip] = lo;
       }
     } else {
       base[(int64_t)ip * N * H + m2] = p;
@@ -938,11 +950,12 @@ int shift_front_n(mtb_shift* h, const float* subtomos, const float* shift_zyx, c
   if (h->use_tc) {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
     fft_z_kernel<N, true><<<dim3(N, B), kT, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm,
-                                                       (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1, h->tc.p32);
+                                                       (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1, (uint32_t*)h->tc.A1n,
+        h->tc.R1n);
   } else {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
     fft_z_kernel<N, false><<<dim3(N, B), kT, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm, nullptr,
-                                                        0, 0, nullptr);
+                                                        0, 0, nullptr, 0);
   }
   MTB_LAUNCH_CHECK();
   return MTB_OK;
@@ -959,11 +972,12 @@ int shift_front_64(mtb_shift* h, const float* subtomos, const float* shift_zyx, 
   if (h->use_tc) {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
     fft_z64_kernel<true><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
-                                                         (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1, h->tc.p32);
+                                                         (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1, (uint32_t*)h->tc.A1n,
+        h->tc.R1n);
   } else {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
     fft_z64_kernel<false><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm, nullptr,
-                                                          0, 0, nullptr);
+                                                          0, 0, nullptr, 0);
   }
   MTB_LAUNCH_CHECK();
   return MTB_OK;

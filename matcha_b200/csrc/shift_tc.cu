@@ -4,7 +4,9 @@
 //   V[u0,u1,u2] = Re sum_{m0,m1,m2} P[m0,m1,m2] E0[u0,m0] E0[u1,m1] E2[u2,m2],
 // E[u,m] = exp(+2 pi i (u - dftshift) fftfreq(n, uf)[m]), m2 < H = N/2 + 1, is split into the
 // planes m2 < N/2 (tensor cores) and the Nyquist plane m2 = N/2 (FP32 CUDA cores):
-//   nyquist  Y[u0,u1] = sum_{m0,m1} E0[u0,m0] E0[u1,m1] P[m0,m1,N/2]        (nyq_kernel)
+//   nyquist  Y[u0,u1] = sum_{m0,m1} E0[u0,m0] E0[u1,m1] P[m0,m1,N/2]: pass 1 on the plane's own
+//            operand A1n (rows (b, m1)) into A2n (rows (b, u0)), then the pass-2 product of A2n
+//            written out as FP32 rows (the pass-1 kernel in both, with another epilogue)
 //   pass 1   rows (b, m2, m1), K = (m0, re/im) = 2N, N-tile = (u0, re/im) = 2U   (X1 -> A2)
 //   pass 2   rows (b, u0, m2), K = (m1, re/im) = 2N, N-tile = (u1, re/im) = 2U   (X2)
 //   pass 3   rows (b, u0, u1), K = (m2, re/im) = N,  N-tile = u2 (real part); + Re(Y E2[u2, N/2])
@@ -240,9 +242,10 @@ __device__ __forceinline__ void scan_group(const uint32_t* vr, int cb, int U, in
 // ------------------------------------------------------------------ pass 1
 // Rows (b, m2, m1) of A1 times E1 -> X1[u0] for the tile's rows, written as A2 rows
 // (b, u0, m2) with K (m1, re/im), bf16 hi and lo parts.
+template <bool ROWS_OUT>
 __global__ void __launch_bounds__(kThreads, 1)
 updft1_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, Pass1 p,
-                 uint32_t* __restrict__ out, int* __restrict__ err) {
+                 uint32_t* __restrict__ out, float2* __restrict__ yout, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = align1024(smem_raw);
   const int KB = p.KB, S = p.stages, NT = p.NT;
@@ -349,14 +352,26 @@ updft1_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int g = tile * TM + q * 32 + lane;
       const bool valid = g < p.rows;
-      const int rpb = p.HH * p.N;
-      const int b = g / rpb, rem = g - (g / rpb) * rpb;
-      const int m2 = rem / p.N, m1 = rem - (rem / p.N) * p.N;
-      const size_t row0 = ((size_t)b * p.U) * p.HH + m2;  // + u0 * HH
       const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 256);
-      tmem_for_groups(taddr, c0, c1, [&](const uint32_t(&r)[16], int cb) {
-        epi1_group<16>(r, cb, valid, p.U, row0, p.HH, ws, m1, (size_t)p.R2, out);
-      });
+      if (ROWS_OUT) {
+        // row g of the product as FP32 complex values, columns (u, re/im) -> yout[g][u]
+        float2* yr = yout + (size_t)g * p.U;
+        tmem_for_groups(taddr, c0, c1, [&](const uint32_t(&r)[16], int cb) {
+#pragma unroll
+          for (int t = 0; t < 8; ++t) {
+            const int u = cb / 2 + t;
+            if (valid && u < p.U) yr[u] = make_float2(__uint_as_float(r[2 * t]), __uint_as_float(r[2 * t + 1]));
+          }
+        });
+      } else {
+        const int rpb = p.HH * p.N;
+        const int b = g / rpb, rem = g - (g / rpb) * rpb;
+        const int m2 = rem / p.N, m1 = rem - (rem / p.N) * p.N;
+        const size_t row0 = ((size_t)b * p.U) * p.HH + m2;  // + u0 * HH
+        tmem_for_groups(taddr, c0, c1, [&](const uint32_t(&r)[16], int cb) {
+          epi1_group<16>(r, cb, valid, p.U, row0, p.HH, ws, m1, (size_t)p.R2, out);
+        });
+      }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(&accE[buf]);
     }
@@ -663,96 +678,6 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
   }
 }
 
-// ------------------------------------------------------------------ Nyquist plane (FP32)
-// Y[u0][u1] = sum_{m1} E[u1][m1] sum_{m0} E[u0][m0] P[m1][m0], one CTA per subtomogram; each
-// thread accumulates a 4 x 4 block of outputs (rows u0 = 4 i + a, columns interleaved with
-// stride nb so that neighbouring lanes read neighbouring padded rows).
-constexpr int kNyqThreads = 512;
-
-__global__ void __launch_bounds__(kNyqThreads)
-nyq_kernel(const float2* __restrict__ p32, const float2* __restrict__ E, int N, int U, float2* __restrict__ nyq) {
-  extern __shared__ __align__(16) float2 sm[];
-  const int ld = N + 1;  // padded rows
-  float2* sP = sm;             // N x ld: [m1][m0]
-  float2* sE = sP + N * ld;    // U x ld: [u][m]
-  float2* sZ = sE + U * ld;    // U x ld: [u0][m1]
-  const int b = blockIdx.x;
-  const float2* P = p32 + (size_t)b * N * N;
-  for (int e = threadIdx.x; e < N * N; e += kNyqThreads) sP[(e / N) * ld + e % N] = P[e];
-  for (int e = threadIdx.x; e < U * N; e += kNyqThreads) sE[(e / N) * ld + e % N] = E[e];
-  __syncthreads();
-  const int nu = (U + 3) / 4;
-  // Z[u0][m1]: row blocks of u0, columns m1 = c + (N / 4) j
-  {
-    const int nc = N / 4;
-    for (int task = threadIdx.x; task < nu * nc; task += kNyqThreads) {
-      const int ib = task / nc, c = task - (task / nc) * nc;
-      float2 acc[4][4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = make_float2(0.f, 0.f);
-      int ur[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) ur[i] = min(4 * ib + i, U - 1);
-      for (int m0 = 0; m0 < N; ++m0) {
-        float2 w[4], x[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) w[i] = sE[ur[i] * ld + m0];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) x[j] = sP[(c + nc * j) * ld + m0];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            acc[i][j].x += w[i].x * x[j].x - w[i].y * x[j].y;
-            acc[i][j].y += w[i].x * x[j].y + w[i].y * x[j].x;
-          }
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-        if (4 * ib + i < U)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) sZ[(4 * ib + i) * ld + c + nc * j] = acc[i][j];
-    }
-  }
-  __syncthreads();
-  // Y[u0][u1]: row blocks of u0, columns u1 = c + nu j
-  float2* Y = nyq + (size_t)b * U * U;
-  for (int task = threadIdx.x; task < nu * nu; task += kNyqThreads) {
-    const int ib = task / nu, c = task - (task / nu) * nu;
-    float2 acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = make_float2(0.f, 0.f);
-    int ur[4], uc[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      ur[i] = min(4 * ib + i, U - 1);
-      uc[i] = min(c + nu * i, U - 1);
-    }
-    for (int m1 = 0; m1 < N; ++m1) {
-      float2 z[4], w[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) z[i] = sZ[ur[i] * ld + m1];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) w[j] = sE[uc[j] * ld + m1];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          acc[i][j].x += w[j].x * z[i].x - w[j].y * z[i].y;
-          acc[i][j].y += w[j].x * z[i].y + w[j].y * z[i].x;
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (4 * ib + i < U && c + nu * j < U) Y[(4 * ib + i) * U + c + nu * j] = acc[i][j];
-  }
-}
 
 typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -866,9 +791,14 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
   if (cudaMalloc(&t->A2, a2) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->E1, (size_t)2 * t->NT12 * k12 * 2) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->E3, (size_t)2 * t->NT3 * k3 * 2) != cudaSuccess) return MTB_ERR_OOM;
-  if (cudaMalloc(&t->E, (size_t)U * N * sizeof(float2)) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->ENQ, (size_t)t->NT3 * sizeof(float2)) != cudaSuccess) return MTB_ERR_OOM;
-  if (cudaMalloc(&t->p32, (size_t)max_batch * N * N * sizeof(float2)) != cudaSuccess) return MTB_ERR_OOM;
+  // the Nyquist plane's operands: A1n rows (b, m1), A2n rows (b, u0), same K layout as A1, A2
+  t->R1n = (int)pad((size_t)max_batch * N);
+  t->R2n = (int)pad((size_t)max_batch * U);
+  const size_t a1n = (size_t)2 * t->R1n * k12 * 2, a2n = (size_t)2 * t->R2n * k12 * 2;
+  if (cudaMalloc(&t->A1n, a1n) != cudaSuccess) return MTB_ERR_OOM;
+  if (cudaMalloc(&t->A2n, a2n) != cudaSuccess) return MTB_ERR_OOM;
+  if (cudaMemset(t->A1n, 0, a1n) != cudaSuccess || cudaMemset(t->A2n, 0, a2n) != cudaSuccess) return MTB_ERR_CUDA;
   if (cudaMalloc(&t->nyq, (size_t)max_batch * U * U * sizeof(float2)) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->best, (size_t)max_batch * 8) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->err, 4) != cudaSuccess) return MTB_ERR_OOM;
@@ -885,7 +815,6 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
     *im = sin(ph);
   };
   std::vector<uint16_t> e1((size_t)2 * t->NT12 * k12, 0), e3((size_t)2 * t->NT3 * k3, 0);
-  std::vector<float2> ef((size_t)U * N);
   // the Nyquist column's factor (re, -im) of E2[u2, N/2], FP32, zero past U
   std::vector<float2> enq((size_t)t->NT3, make_float2(0.f, 0.f));
   auto put = [&](std::vector<uint16_t>& dst, size_t k, int rows, int r, int kk, double v) {
@@ -902,7 +831,6 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
       put(e1, k12, t->NT12, 2 * u + 0, 2 * m + 1, -ei);
       put(e1, k12, t->NT12, 2 * u + 1, 2 * m + 0, ei);
       put(e1, k12, t->NT12, 2 * u + 1, 2 * m + 1, er);
-      ef[(size_t)u * N + m] = make_float2((float)er, (float)ei);
     }
   for (int u = 0; u < U; ++u) {
     for (int m = 0; m < HH; ++m) {
@@ -917,18 +845,19 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
   }
   if (cudaMemcpy(t->E1, e1.data(), e1.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(t->E3, e3.data(), e3.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(t->E, ef.data(), ef.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(t->ENQ, enq.data(), enq.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess)
     return MTB_ERR_CUDA;
   int rc = make_map(t->mapA1, t->A1, k12, (uint64_t)2 * t->R1, TM);
   if (!rc) rc = make_map(t->mapA2, t->A2, k12, (uint64_t)2 * t->R2, TM);
   if (!rc) rc = make_map(t->mapE1, t->E1, k12, (uint64_t)2 * t->NT12, t->NT12);
   if (!rc) rc = make_map(t->mapE3, t->E3, k3, (uint64_t)2 * t->NT3, t->NT3);
+  if (!rc) rc = make_map(t->mapA1n, t->A1n, k12, (uint64_t)2 * t->R1n, TM);
+  if (!rc) rc = make_map(t->mapA2n, t->A2n, k12, (uint64_t)2 * t->R2n, TM);
   return rc;
 }
 
 void shift_tc_release(ShiftTc* t) {
-  void* ptrs[] = {t->A1, t->A2, t->E1, t->E3, t->E, t->ENQ, t->p32, t->nyq, t->best, t->err};
+  void* ptrs[] = {t->A1, t->A2, t->A1n, t->A2n, t->E1, t->E3, t->ENQ, t->nyq, t->best, t->err};
   for (void* p : ptrs) if (p) cudaFree(p);
   memset(t, 0, sizeof(*t));
 }
@@ -936,11 +865,37 @@ void shift_tc_release(ShiftTc* t) {
 int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st, const cudaEvent_t* marks) {
   MTB_CUDA_TRY(cudaMemsetAsync(t->best, 0, (size_t)B * 8, st));
   const int N = t->N, U = t->U, HH = t->HH;
-  // Nyquist plane
-  const size_t snyq = (size_t)(N + 2 * U) * (N + 1) * sizeof(float2);
-  MTB_CUDA_TRY(cudaFuncSetAttribute(nyq_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)snyq));
-  nyq_kernel<<<B, kNyqThreads, snyq, st>>>(t->p32, t->E, N, U, t->nyq);
-  MTB_LAUNCH_CHECK();
+  MTB_CUDA_TRY(cudaFuncSetAttribute(updft1_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)t->smem1));
+  MTB_CUDA_TRY(cudaFuncSetAttribute(updft1_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)t->smem1));
+  // Nyquist plane: pass 1 over its rows (b, m1) into A2n rows (b, u0), then A2n E1 -> Y
+  {
+    Pass1 pn;
+    pn.rows = B * N;
+    pn.tiles = (pn.rows + TM - 1) / TM;
+    pn.N = N;
+    pn.HH = 1;
+    pn.U = U;
+    pn.KB = t->KB12;
+    pn.R1 = t->R1n;
+    pn.R2 = t->R2n;
+    pn.NT = t->NT12;
+    pn.stages = t->stages1;
+    int gn = pn.tiles < t->n_sm ? pn.tiles : t->n_sm;
+    updft1_tc_kernel<false><<<gn, kThreads, t->smem1, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA1n),
+                                                            *reinterpret_cast<const CUtensorMap*>(t->mapE1), pn,
+                                                            (uint32_t*)t->A2n, nullptr, t->err);
+    MTB_LAUNCH_CHECK();
+    pn.rows = B * U;
+    pn.tiles = (pn.rows + TM - 1) / TM;
+    pn.R1 = t->R2n;  // the A operand is now A2n
+    gn = pn.tiles < t->n_sm ? pn.tiles : t->n_sm;
+    updft1_tc_kernel<true><<<gn, kThreads, t->smem1, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA2n),
+                                                           *reinterpret_cast<const CUtensorMap*>(t->mapE1), pn,
+                                                           nullptr, t->nyq, t->err);
+    MTB_LAUNCH_CHECK();
+  }
   if (marks && marks[0]) cudaEventRecord(marks[0], st);
   // pass 1
   Pass1 p1;
@@ -954,11 +909,10 @@ int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st, const cudaEvent_t* marks
   p1.R2 = t->R2;
   p1.NT = t->NT12;
   p1.stages = t->stages1;
-  MTB_CUDA_TRY(cudaFuncSetAttribute(updft1_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem1));
   const int g1 = p1.tiles < t->n_sm ? p1.tiles : t->n_sm;
-  updft1_tc_kernel<<<g1, kThreads, t->smem1, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA1),
-                                                   *reinterpret_cast<const CUtensorMap*>(t->mapE1), p1,
-                                                   (uint32_t*)t->A2, t->err);
+  updft1_tc_kernel<false><<<g1, kThreads, t->smem1, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA1),
+                                                          *reinterpret_cast<const CUtensorMap*>(t->mapE1), p1,
+                                                          (uint32_t*)t->A2, nullptr, t->err);
   MTB_LAUNCH_CHECK();
   if (marks && marks[1]) cudaEventRecord(marks[1], st);
   // passes 2 + 3
