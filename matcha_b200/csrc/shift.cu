@@ -508,6 +508,7 @@ patch_fft_xy64_kernel(const float* __restrict__ vol, const float* __restrict__ s
   __shared__ float red[32];
   __shared__ int s_c[2][2][N];      // [y/x][tap] clamped source index
   __shared__ float s_w[2][2][N];    // [y/x][tap] weight (0 for taps outside the box or zeroed)
+  __shared__ int4 s_ty[N];          // row j's y taps packed (c0, c1, w0, w1): one broadcast load
   float2* tw = sm2;                                     // 64
   float* P0 = reinterpret_cast<float*>(sm2 + 64);       // the z-interpolated plane
   float2* Z = reinterpret_cast<float2*>(P0 + N * N);    // 32 x 64 x FFT output, swizzled (z_at)
@@ -534,6 +535,8 @@ patch_fft_xy64_kernel(const float* __restrict__ vol, const float* __restrict__ s
     s_c[ax][1][j] = min(max(iy + 1, 0), N - 1);
     s_w[ax][0][j] = (zero || iy < 0 || iy >= N) ? 0.f : 1.f - fy;
     s_w[ax][1][j] = (zero || iy + 1 < 0 || iy + 1 >= N) ? 0.f : fy;
+    if (ax == 0)
+      s_ty[j] = make_int4(s_c[0][0][j], s_c[0][1][j], __float_as_int(s_w[0][0][j]), __float_as_int(s_w[0][1][j]));
   }
   // z, on the way in: P0 <- (1 - fz) plane(iz) + fz plane(iz + 1), straight from global memory
   // (a plane outside the box, or a zeroed plane, contributes zero)
@@ -554,9 +557,9 @@ patch_fft_xy64_kernel(const float* __restrict__ vol, const float* __restrict__ s
   }
   __syncthreads();
   // x and y in one pass from the z-interpolated plane: p(j, k) = wy0(j) (wx0(k) P0[cy0][cx0] +
-  // wx1(k) P0[cy0][cx1]) + wy1(j) (..cy1..) (the x taps in registers, the y taps computed per
-  // row as the setup computes them); then background, fill weight, 1/N^3, roll, and rows j and
-  // j + 32 (rolled to j + 32 and j) packed into one complex line with one 8-byte store
+  // wx1(k) P0[cy0][cx1]) + wy1(j) (..cy1..) (the x taps in registers, the y taps of a row one
+  // broadcast load); then background, fill weight, 1/N^3, roll, and rows j and j + 32 (rolled
+  // to j + 32 and j) packed into one complex line with one 8-byte store
   float part = 0.f;
   if (threadIdx.x < 256) {
     const int k = threadIdx.x & (N - 1), j0 = threadIdx.x >> 6;
@@ -565,14 +568,9 @@ patch_fft_xy64_kernel(const float* __restrict__ vol, const float* __restrict__ s
     const int dk = k - HN, kp = (k + HN) & (N - 1);
     const int rk = di * di + dk * dk;
     auto sample = [&](int j) -> float {
-      const float y = (float)j + ps.f[1];
-      const float y0 = floorf(y);
-      const int iy = (int)y0;
-      const float fy = y - y0;
-      const bool zero = (j == ps.zp[1]);
-      const int cy0 = min(max(iy, 0), N - 1), cy1 = min(max(iy + 1, 0), N - 1);
-      const float wy0 = (zero || iy < 0 || iy >= N) ? 0.f : 1.f - fy;
-      const float wy1 = (zero || iy + 1 < 0 || iy + 1 >= N) ? 0.f : fy;
+      const int4 ty = s_ty[j];
+      const int cy0 = ty.x, cy1 = ty.y;
+      const float wy0 = __int_as_float(ty.z), wy1 = __int_as_float(ty.w);
       const float a = wx0 * P0[cy0 * N + cx0] + wx1 * P0[cy0 * N + cx1];
       const float c = wx0 * P0[cy1 * N + cx0] + wx1 * P0[cy1 * N + cx1];
       const float p = wy0 * a + wy1 * c;
