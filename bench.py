@@ -35,8 +35,9 @@ sys.path.insert(0, ROOT)
 N_BOX, L_MAX, LI = 64, 32, [8, 16, 24]
 SHIFT_RADIUS, UPSAMPLE = 5, 8
 METRIC = "subtomograms/s at 64^3 L=32 (one alternation: FLE+sigma, SO(3) grid, Newton march, shift)"
-KERNELS_PER_STEP = 15  # FLE fold_split, gemm_tc, expand; sigma; SO(3) grid; fold_sigma, newton_march,
-# reduce_candidates; tracker_update; shift patch_fft_xy64, fft_z64, nyq, updft1_tc, updft23_tc, finalize_tc
+KERNELS_PER_STEP = 16  # FLE fold_split, gemm_tc, expand; sigma; SO(3) grid; fold_sigma, newton_march,
+# reduce_candidates; tracker_update; shift patch_fft_xy64, fft_z64, updft1_tc x2 (the Nyquist plane),
+# updft1_tc, updft23_tc, finalize_tc
 # DRAM bytes (read + write) of updft23_tc_kernel per subtomogram, from an ncu capture of the same kernel
 # at 200 subtomograms (dram__bytes_read.sum + dram__bytes_write.sum divided by 200)
 UPDFT23_DRAM_BYTES_PER_SUBTOMO = 1_526_000
