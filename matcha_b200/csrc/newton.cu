@@ -218,7 +218,7 @@ __device__ __forceinline__ void pass(const float4* __restrict__ S, const float2*
     }
     const float4* cp = coef + wedge_off(mp + 1) + p;
     const float4* sp = FOLDED ? S + wedge_off(mp + 1) + p : nullptr;
-#pragma unroll 2
+#pragma unroll 4
     for (int l = mp + 1; l <= Li; ++l) {
       const float4 cf = __ldg(cp);
       if (FOLDED) s = __ldg(sp);
