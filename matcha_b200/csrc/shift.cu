@@ -425,8 +425,10 @@ constexpr int kXS = 72;    // per-line scratch (float2): transpose slot (k1, r) 
 constexpr int kYS = 34;    // row stride (float2) of the 64 x 33 y-FFT output of the patch pass
 constexpr int kZS = 33;    // row stride (float2) of the 64 x 33 buffer of the z pass
 
-__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex add and subtract as one packed two-lane FP32 instruction each (sm_100): the same
+// IEEE results as two scalar ones (a - b is a + (-1) b with one rounding).
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
 __device__ __forceinline__ float2 c_mi(float2 a) { return make_float2(a.y, -a.x); }  // a * (-i)
 
 // 8-point forward DFT, natural order in and out (radix-2 decimation in frequency).
