@@ -395,9 +395,13 @@ __device__ __forceinline__ void scan_group_nq(const uint32_t* vr, int cb, int U,
   uint32_t w[NC];
 #pragma unroll
   for (int t = 0; t < NC; t += 2) {
-    const float4 e = en2[(cb + t) >> 1];  // the same address in every lane: a broadcast
-    w[t] = __float_as_uint(fmaf(y.y, e.y, fmaf(y.x, e.x, __uint_as_float(vr[t]))));
-    w[t + 1] = __float_as_uint(fmaf(y.y, e.w, fmaf(y.x, e.z, __uint_as_float(vr[t + 1]))));
+    // columns t, t + 1 at once: packed two-lane FMAs (sm_100), the same roundings as scalar ones
+    const float4 e = en2[(cb + t) >> 1];  // (re t, re t+1, im t, im t+1); a broadcast load
+    const float2 v2 = make_float2(__uint_as_float(vr[t]), __uint_as_float(vr[t + 1]));
+    const float2 r2 = __ffma2_rn(make_float2(y.y, y.y), make_float2(e.z, e.w),
+                                 __ffma2_rn(make_float2(y.x, y.x), make_float2(e.x, e.y), v2));
+    w[t] = __float_as_uint(r2.x);
+    w[t + 1] = __float_as_uint(r2.y);
   }
   // The position in the group rides in the low 4 mantissa bits of each value (15 - t, so the
   // largest of equal values is the first), which lowers the compared magnitudes by at most 15
@@ -448,7 +452,7 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
   // slot to the TMA thread once per tile; freeO[s] hands a chunk slot from one chunk to the
   // next, so each barrier is waited in order, never more than one phase ahead.
   uint8_t* sS = sE3 + 2 * B3;
-  float4* sEn = reinterpret_cast<float4*>(sS + NB * 2 * A_TILE);  // (er, -ei) of E2[u2, N/2], pairs
+  float4* sEn = reinterpret_cast<float4*>(sS + NB * 2 * A_TILE);  // (er, -ei) of E2[u2, N/2]: column pairs (re, re, im, im)
   __shared__ __align__(8) uint64_t tmaF[kMaxSlots], opF[kMaxSlots], freeT[kMaxSlots], freeO[kMaxSlots];
   __shared__ __align__(8) uint64_t acc3F[2], acc3E[2], resF, acc2F, acc2E;
   __shared__ uint32_t tmem_base;
@@ -471,7 +475,10 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int i = threadIdx.x; i < NT3 / 2; i += blockDim.x) sEn[i] = enq[i];
+  for (int i = threadIdx.x; i < NT3 / 2; i += blockDim.x) {  // pairs of columns, re parts first
+    const float4 e = enq[i];
+    sEn[i] = make_float4(e.x, e.z, e.y, e.w);
+  }
   // a chunk writes K words < N/2 of its rows; the rest must hold finite values (they meet
   // zero K columns of E3), so the slots start zeroed
   for (int i = threadIdx.x; i < NB * 2 * A_TILE / 16; i += blockDim.x)
