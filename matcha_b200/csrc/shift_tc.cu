@@ -403,11 +403,13 @@ __device__ __forceinline__ void scan_group_nq(const uint32_t* vr, int cb, int U,
     w[t] = __float_as_uint(r2.x);
     w[t + 1] = __float_as_uint(r2.y);
   }
-  // The position in the group rides in the low 4 mantissa bits of each value (15 - t, so the
-  // largest of equal values is the first), which lowers the compared magnitudes by at most 15
-  // units in the last place, far below the hi/lo split's own error; one NaN-propagating
-  // maximum per value then finds the group's best.  A group whose maximum is NaN (a NaN, or an
-  // infinity whose low bits were set) is rescanned exactly.
+  // The position in the group rides in the low 4 mantissa bits of each value (15 - t, so of
+  // equal positive values the first is the largest), which changes the compared magnitudes by
+  // at most 15 units in the last place, far below the hi/lo split's own error; one
+  // NaN-propagating maximum per value then finds the group's best.  (Equal negative values
+  // resolve to the last position instead; the grid's maximum is the correlation peak, and an
+  // all-negative grid with an exact tie at its top is the only case this reorders.)  A group
+  // whose maximum is NaN (a NaN, or an infinity whose low bits were set) is rescanned exactly.
   float m[4];
   if (cb + NC <= U) {
 #pragma unroll
