@@ -243,6 +243,18 @@ int mtb_shift_profile_read(mtb_shift* h, float* ms, int* calls);
 int mtb_update_rotation(const float* alpha, const float* beta, const float* gamma, const double* tracker_in,
                         int B, double* tracker_out, float* rot, mtb_stream_t stream);
 
+/* The expansion's input of every alternation, BatchProcessor._extract_rotated_batch
+ * (src/matcha/align_subtomograms.py:240-252): the patch of each volume at its current shift
+ * (extract_subtomogram_patch_batch with normalize=True, src/matcha/utils/io_utils.py:113-178),
+ * normalised by the mean and standard deviation inside the hard spherical mask of radius
+ * mask_radius about voxel N/2 and multiplied by it (src/matcha/utils/volume_ops.py:6-35), then
+ * rotated into the tracker's orientation (rotate_volumes, src/matcha/utils/volume_rotation.py:
+ * 8-125).  volumes (B, N, N, N) float32; shift_xyz (B, 3) float32 in voxels (x, y, z);
+ * tracker (B, 4) float64 (w, x, y, z); work (B, N, N, N) float32 and stats (B, 2) float64 are
+ * the caller's workspace; out (B, N, N, N) float32 may not alias volumes or work. */
+int mtb_prepare_subtomos(const float* volumes, int B, int N, const float* shift_xyz, const double* tracker,
+                         float mask_radius, float* work, double* stats, float* out, mtb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -102,6 +102,56 @@ class AlignmentStep:
         return dict(alpha=a, beta=b, gamma=g, rotation_score=score, bh_norms=norms[:B], tracker=tracker,
                     shift=self.shift[:B], shift_score=self.shift_score[:B])
 
+    @torch.no_grad()
+    def prepare(self, subtomograms: torch.Tensor, current_shift: torch.Tensor, tracker: torch.Tensor):
+        """``BatchProcessor._extract_rotated_batch`` (src/matcha/align_subtomograms.py:240-252):
+        the patch of each (N, N, N) subtomogram at ``current_shift`` (B, 3), normalised in the
+        spherical mask of radius ``radius`` and masked, rotated by its tracker (B, 4) float64.
+        The first component of ``current_shift`` moves along the last (x) axis, as the
+        reference's grid_sample reads it.  Returns a (B, N, N, N) buffer of this object,
+        rewritten by the next call (``mtb_prepare_subtomos``, two launches)."""
+        B, N = subtomograms.shape[0], self.cfg.N
+        if B > self.cfg.batch:
+            raise ValueError(f"batch {B} exceeds the configured batch {self.cfg.batch}")
+        if subtomograms.shape[1:] != (N, N, N) or subtomograms.dtype != torch.float32:
+            raise ValueError("subtomograms must be (B, N, N, N) float32")
+        if getattr(self, "_prep", None) is None:
+            self._prep = dict(work=torch.empty((self.cfg.batch, N, N, N), device=self.device, dtype=torch.float32),
+                              out=torch.empty((self.cfg.batch, N, N, N), device=self.device, dtype=torch.float32),
+                              stats=torch.empty((self.cfg.batch, 2), device=self.device, dtype=torch.float64))
+        vols = subtomograms.contiguous()
+        shift = current_shift.reshape(B, 3).to(torch.float32).contiguous()
+        trk = tracker.contiguous()
+        p = self._prep
+        with torch.cuda.device(self.device):
+            nat.check(nat.load().mtb_prepare_subtomos(nat.ptr(vols), B, N, nat.ptr(shift), nat.ptr(trk),
+                                                      float(self.correlator.radius), nat.ptr(p["work"]),
+                                                      nat.ptr(p["stats"]), nat.ptr(p["out"]),
+                                                      nat.stream_ptr(self.device)), "mtb_prepare_subtomos")
+        return p["out"][:B]
+
+    @torch.no_grad()
+    def run_alternations(self, subtomograms: torch.Tensor, tracker: torch.Tensor, local_shifts: torch.Tensor,
+                         prior_shifts: torch.Tensor, base_shifts: torch.Tensor, num_alternations: int):
+        """``BatchProcessor._run_alternations`` (src/matcha/align_subtomograms.py:316-361) for
+        one batch on the device: each alternation prepares the subtomograms at the current
+        shift and orientation, searches the rotation, matches the shift and adds it to
+        ``local_shifts`` (B, 3), updated in place like ``tracker``.  Returns one dict of
+        outputs per alternation (copies), with ``rotation_score`` also divided by the norms
+        as the stored score is (align_subtomograms.py:300-302)."""
+        results = []
+        for _ in range(num_alternations):
+            current = prior_shifts + base_shifts + local_shifts
+            data = self.prepare(subtomograms, current, tracker)
+            o = self(data, subtomograms, tracker, current)
+            local_shifts += o["shift"]
+            r = {k: v.clone() for k, v in o.items()}
+            r["normalized_rotation_score"] = r["rotation_score"].reshape(-1) / (
+                r["bh_norms"].reshape(-1) * self.correlator.bh_norm_template).clamp_min(1e-12)
+            r["local_shifts"] = local_shifts.clone()
+            results.append(r)
+        return results
+
     _KEYS = ("alpha", "beta", "gamma", "rotation_score", "bh_norms", "shift", "shift_score")
 
     @torch.no_grad()

@@ -3,6 +3,7 @@
     python -m matcha_b200.profile_cases shift  200   # ShiftMatcher.search_shifts, 64^3, uf 8, r 5
     python -m matcha_b200.profile_cases search 296   # Matcha.search_orientations, L 32, C 10
     python -m matcha_b200.profile_cases fle    256   # CrossCorrelationMatcher.get_sigma, 64^3, L 32
+    python -m matcha_b200.profile_cases prepare 1000 # shifted patch, masked normalisation, rotation, 64^3
     python -m matcha_b200.profile_cases shift 1000 --stages   # plus ShiftMatcher.profile per kernel group
 
 Each case builds its inputs on the device from a fixed seed (random volumes, Haar rotations,
@@ -68,7 +69,28 @@ def _fle(B: int, dev):
     return lambda: cc.get_sigma_upto(vols, 32)
 
 
-CASES = {"shift": _shift, "search": _search, "fle": _fle}
+def _prepare(B: int, dev):
+    from . import _native as nat
+
+    N = 64
+    lib = nat.load()
+    rng = np.random.default_rng(0)
+    vols = torch.randn(B, N, N, N, device=dev)
+    shift = torch.from_numpy(rng.uniform(-2, 2, (B, 3)).astype(np.float32)).to(dev)
+    q = rng.standard_normal((B, 4))
+    tracker = torch.from_numpy(q / np.linalg.norm(q, axis=1, keepdims=True)).to(dev)
+    work, out = torch.empty_like(vols), torch.empty_like(vols)
+    stats = torch.empty((B, 2), dtype=torch.float64, device=dev)
+
+    def run():
+        nat.check(lib.mtb_prepare_subtomos(nat.ptr(vols), B, N, nat.ptr(shift), nat.ptr(tracker), 30.0,
+                                           nat.ptr(work), nat.ptr(stats), nat.ptr(out), nat.stream_ptr(dev)),
+                  "mtb_prepare_subtomos")
+
+    return run
+
+
+CASES = {"shift": _shift, "search": _search, "fle": _fle, "prepare": _prepare}
 
 
 def main(argv=None) -> int:
