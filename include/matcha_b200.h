@@ -250,8 +250,9 @@ int mtb_update_rotation(const float* alpha, const float* beta, const float* gamm
  * mask_radius about voxel N/2 and multiplied by it (src/matcha/utils/volume_ops.py:6-35), then
  * rotated into the tracker's orientation (rotate_volumes, src/matcha/utils/volume_rotation.py:
  * 8-125).  volumes (B, N, N, N) float32; shift_xyz (B, 3) float32 in voxels (x, y, z);
- * tracker (B, 4) float64 (w, x, y, z); work (B, N, N, N) float32 and stats (B, 2) float64 are
- * the caller's workspace; out (B, N, N, N) float32 may not alias volumes or work. */
+ * tracker (B, 4) float64 (w, x, y, z); work (B, N, N, N, 2) float32 (8-byte aligned) and
+ * stats (B, 2) float64 are the caller's workspace; out (B, N, N, N) float32 may not alias
+ * volumes or work. */
 int mtb_prepare_subtomos(const float* volumes, int B, int N, const float* shift_xyz, const double* tracker,
                          float mask_radius, float* work, double* stats, float* out, mtb_stream_t stream);
 

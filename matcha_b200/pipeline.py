@@ -116,9 +116,10 @@ class AlignmentStep:
         if subtomograms.shape[1:] != (N, N, N) or subtomograms.dtype != torch.float32:
             raise ValueError("subtomograms must be (B, N, N, N) float32")
         if getattr(self, "_prep", None) is None:
-            self._prep = dict(work=torch.empty((self.cfg.batch, N, N, N), device=self.device, dtype=torch.float32),
-                              out=torch.empty((self.cfg.batch, N, N, N), device=self.device, dtype=torch.float32),
-                              stats=torch.empty((self.cfg.batch, 2), device=self.device, dtype=torch.float64))
+            Bc, dev = self.cfg.batch, self.device
+            self._prep = dict(work=torch.empty((Bc, N, N, N, 2), device=dev, dtype=torch.float32),
+                              out=torch.empty((Bc, N, N, N), device=dev, dtype=torch.float32),
+                              stats=torch.empty((Bc, 2), device=dev, dtype=torch.float64))
         vols = subtomograms.contiguous()
         shift = current_shift.reshape(B, 3).to(torch.float32).contiguous()
         trk = tracker.contiguous()

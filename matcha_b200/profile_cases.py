@@ -79,7 +79,7 @@ def _prepare(B: int, dev):
     shift = torch.from_numpy(rng.uniform(-2, 2, (B, 3)).astype(np.float32)).to(dev)
     q = rng.standard_normal((B, 4))
     tracker = torch.from_numpy(q / np.linalg.norm(q, axis=1, keepdims=True)).to(dev)
-    work, out = torch.empty_like(vols), torch.empty_like(vols)
+    work, out = torch.empty((B, N, N, N, 2), device=dev), torch.empty_like(vols)
     stats = torch.empty((B, 2), dtype=torch.float64, device=dev)
 
     def run():

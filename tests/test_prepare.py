@@ -67,7 +67,7 @@ def _prepare_gpu(vols, shifts, q, radius, device):
     v = torch.from_numpy(np.ascontiguousarray(vols, dtype=np.float32)).to(device)
     s = torch.from_numpy(np.ascontiguousarray(shifts, dtype=np.float32)).to(device)
     t = torch.from_numpy(np.ascontiguousarray(q, dtype=np.float64)).to(device)
-    work = torch.empty_like(v)
+    work = torch.empty(v.shape + (2,), dtype=torch.float32, device=device)
     stats = torch.empty((B, 2), dtype=torch.float64, device=device)
     out = torch.empty_like(v)
     with torch.cuda.device(device):
@@ -80,9 +80,10 @@ def _prepare_gpu(vols, shifts, q, radius, device):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("N,B,radius", [(16, 3, 7.0), (15, 3, 7.0), (16, 3, 9.5), (32, 4, 15.0), (64, 2, 30.0),
-                                         (64, 2, 32.0)])
+                                         (64, 2, 32.0), (80, 2, 36.0), (112, 2, 50.0)])
 def test_prepare_matches_oracle(cuda_device, N, B, radius):
-    """Even and odd boxes, masks inside the box and reaching past it (radius 9.5 of 16)."""
+    """Even and odd boxes, masks inside the box and reaching past it (radius 9.5 of 16); 112 is
+    past the box size whose plane fits the staged patch kernel's shared memory."""
     rng = np.random.default_rng(N + B + int(radius))
     vols = (rng.standard_normal((B, N, N, N)) + 3.0).astype(np.float32)  # a mean to remove
     shifts = rng.uniform(-3, 3, (B, 3)).astype(np.float32)
