@@ -243,6 +243,20 @@ int mtb_shift_profile_read(mtb_shift* h, float* ms, int* calls);
 int mtb_update_rotation(const float* alpha, const float* beta, const float* gamma, const double* tracker_in,
                         int B, double* tracker_out, float* rot, mtb_stream_t stream);
 
+/* The rotation the shift match uses for each tracker, on the device: rot (B, 9) float32, row
+ * major, the matrix of the conjugated tracker that ShiftMatcher.search_shifts builds on the host
+ * (R.from_euler('ZYZ', to_euler_angles(conj(tracker)), degrees) at src/matcha/core/
+ * ShiftMatcher.py:913, :503); tracker (B, 4) float64 (w, x, y, z), any nonzero norm. */
+int mtb_tracker_rotation(const double* tracker, int B, float* rot, mtb_stream_t stream);
+
+/* One alternation's per-particle results packed for storage, the values each row of
+ * store_alignment_parameters (src/matcha/utils/io_utils.py:181-225) takes from device tensors:
+ * out (B, 11) float64 = rotation_score, the tracker's quaternionic to_euler_angles (alpha,
+ * beta, gamma, radians), local shift (3), prior shift (3), shift_score.  rotation_score and
+ * shift_score (B,) float32; local_shift and prior_shift (B, 3) float32; tracker (B, 4) float64. */
+int mtb_pack_results(const float* rotation_score, const float* shift_score, const float* local_shift,
+                     const float* prior_shift, const double* tracker, int B, double* out, mtb_stream_t stream);
+
 /* The expansion's input of every alternation, BatchProcessor._extract_rotated_batch
  * (src/matcha/align_subtomograms.py:240-252): the patch of each volume at its current shift
  * (extract_subtomogram_patch_batch with normalize=True, src/matcha/utils/io_utils.py:113-178),

@@ -213,11 +213,21 @@ class ShiftMatcher:
         if self.reference_data_fourier is None:
             raise RuntimeError("ShiftMatcher reference is not initialized. Call `set_reference` first.")
         B = subtomos.shape[0]
-        angles = tracker_to_euler_deg(rotation_tracker)
-        if angles.shape[0] != B:
-            raise ValueError("rotation_tracker must hold one rotation per subtomogram")
-        rot = torch.from_numpy(R.from_euler("ZYZ", angles, degrees=True).as_matrix().reshape(B, 9)).to(
-            self.device, torch.float32)
+        if isinstance(rotation_tracker, torch.Tensor) and rotation_tracker.is_cuda:
+            # a tracker already on the device: its rotation is built there, with no host sync
+            trk = rotation_tracker.to(self.device, torch.float64).reshape(-1, 4).contiguous()
+            if trk.shape[0] != B:
+                raise ValueError("rotation_tracker must hold one rotation per subtomogram")
+            rot = torch.empty((B, 9), device=self.device, dtype=torch.float32)
+            with torch.cuda.device(self.device):
+                nat.check(self._lib.mtb_tracker_rotation(nat.ptr(trk), B, nat.ptr(rot), nat.stream_ptr(self.device)),
+                          "mtb_tracker_rotation")
+        else:
+            angles = tracker_to_euler_deg(rotation_tracker)
+            if angles.shape[0] != B:
+                raise ValueError("rotation_tracker must hold one rotation per subtomogram")
+            rot = torch.from_numpy(R.from_euler("ZYZ", angles, degrees=True).as_matrix().reshape(B, 9)).to(
+                self.device, torch.float32)
         vol = subtomos.to(self.device, torch.float32).contiguous()
         nat.require_cuda(vol, "subtomos")
         sz = torch.as_tensor(shift_zyx, device=self.device, dtype=torch.float32).reshape(B, 3).contiguous()

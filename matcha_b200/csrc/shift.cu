@@ -1219,6 +1219,16 @@ extern "C" int mtb_shift_profile_read(mtb_shift* h, float* ms, int* calls) {
 // rotation the shift match uses, R.from_euler('ZYZ', euler(conj(tracker))) (ShiftMatcher.py:503,
 // :913), which is the rotation matrix of conj(tracker).  FP64 quaternion arithmetic.
 namespace {
+// Rotation matrix (row major) of conj(q) for a unit quaternion q = (w, x, y, z): the matrix
+// scipy's from_euler('ZYZ', degrees) gives for the Euler angles of the conjugated tracker
+// (ShiftMatcher.py:503, :913).
+__device__ __forceinline__ void conj_rotation(double w, double x, double y, double z, float* R) {
+  const double cw = w, cx = -x, cy = -y, cz = -z;
+  R[0] = (float)(1 - 2 * (cy * cy + cz * cz)); R[1] = (float)(2 * (cx * cy - cw * cz)); R[2] = (float)(2 * (cx * cz + cw * cy));
+  R[3] = (float)(2 * (cx * cy + cw * cz)); R[4] = (float)(1 - 2 * (cx * cx + cz * cz)); R[5] = (float)(2 * (cy * cz - cw * cx));
+  R[6] = (float)(2 * (cx * cz - cw * cy)); R[7] = (float)(2 * (cy * cz + cw * cx)); R[8] = (float)(1 - 2 * (cx * cx + cy * cy));
+}
+
 __global__ void tracker_update_kernel(const float* __restrict__ alpha, const float* __restrict__ beta,
                                       const float* __restrict__ gamma, const double* __restrict__ tin, int B,
                                       double* __restrict__ tout, float* __restrict__ rot) {
@@ -1241,12 +1251,15 @@ __global__ void tracker_update_kernel(const float* __restrict__ alpha, const flo
   const double inv = 1.0 / sqrt(nw * nw + nx * nx + ny * ny + nz * nz);
   nw *= inv; nx *= inv; ny *= inv; nz *= inv;
   tout[4 * b] = nw; tout[4 * b + 1] = nx; tout[4 * b + 2] = ny; tout[4 * b + 3] = nz;
-  // rotation matrix of conj(tracker)
-  const double cw = nw, cx = -nx, cy = -ny, cz = -nz;
-  float* R = rot + 9 * b;
-  R[0] = (float)(1 - 2 * (cy * cy + cz * cz)); R[1] = (float)(2 * (cx * cy - cw * cz)); R[2] = (float)(2 * (cx * cz + cw * cy));
-  R[3] = (float)(2 * (cx * cy + cw * cz)); R[4] = (float)(1 - 2 * (cx * cx + cz * cz)); R[5] = (float)(2 * (cy * cz - cw * cx));
-  R[6] = (float)(2 * (cx * cz - cw * cy)); R[7] = (float)(2 * (cy * cz + cw * cx)); R[8] = (float)(1 - 2 * (cx * cx + cy * cy));
+  conj_rotation(nw, nx, ny, nz, rot + 9 * b);
+}
+
+__global__ void tracker_rotation_kernel(const double* __restrict__ tracker, int B, float* __restrict__ rot) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const double w = tracker[4 * b], x = tracker[4 * b + 1], y = tracker[4 * b + 2], z = tracker[4 * b + 3];
+  const double inv = 1.0 / sqrt(w * w + x * x + y * y + z * z);
+  conj_rotation(w * inv, x * inv, y * inv, z * inv, rot + 9 * b);
 }
 }  // namespace
 
@@ -1257,6 +1270,15 @@ extern "C" int mtb_update_rotation(const float* alpha, const float* beta, const 
   MTB_ARG_CHECK(alpha && beta && gamma && tracker_in && tracker_out && rot, "null pointer");
   tracker_update_kernel<<<(B + 127) / 128, 128, 0, (cudaStream_t)stream>>>(alpha, beta, gamma, tracker_in, B,
                                                                             tracker_out, rot);
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
+}
+
+extern "C" int mtb_tracker_rotation(const double* tracker, int B, float* rot, mtb_stream_t stream) {
+  MTB_ARG_CHECK(B >= 0, "negative batch");
+  if (B == 0) return MTB_OK;
+  MTB_ARG_CHECK(tracker && rot, "null pointer");
+  tracker_rotation_kernel<<<(B + 127) / 128, 128, 0, (cudaStream_t)stream>>>(tracker, B, rot);
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }
