@@ -243,6 +243,26 @@ int mtb_shift_profile_read(mtb_shift* h, float* ms, int* calls);
 int mtb_update_rotation(const float* alpha, const float* beta, const float* gamma, const double* tracker_in,
                         int B, double* tracker_out, float* rot, mtb_stream_t stream);
 
+/* Batch reader (host only): decode MRC2014 files (modes 0 int8, 1 int16, 2 float32, 6 uint16,
+ * 12 float16; either byte order; any extended header) into float32 C-order (z, y, x) voxels,
+ * as load_subtomogram_cpu / load_ctf_relion5_cpu do through mrcfile
+ * (src/matcha/utils/io_utils.py:229-253), on a pool of n_threads threads (0: one per hardware
+ * thread), the role of the reader pool of cpu_reader (src/matcha/utils/run_utils.py:430-611).
+ * mtb_read_mrc decodes paths[0..n) of shape (nz, ny, nx) each, keeping the leading
+ * [0, cz) x [0, cy) x [0, cx) box (the whole volume, or (nz/2, ny, nz/2+1) for a CTF weight
+ * file), into dst + i cz cy cx; status[i] is MTB_READ_OK or why file i was skipped.  Returns
+ * MTB_ERR_ARG for bad arguments, else MTB_OK whatever the per-file statuses. */
+#define MTB_READ_OK 0
+#define MTB_READ_OPEN 1   /* cannot open or stat the file */
+#define MTB_READ_HEADER 2 /* not an MRC header, or a mode that is not decoded */
+#define MTB_READ_SHAPE 3  /* the file's (nz, ny, nx) differs from the expected shape */
+#define MTB_READ_SHORT 4  /* the file ends before its voxels do */
+typedef struct mtb_reader mtb_reader;
+int mtb_reader_create(int n_threads, mtb_reader** out);
+int mtb_reader_destroy(mtb_reader* r);
+int mtb_read_mrc(mtb_reader* r, const char* const* paths, int n, int nz, int ny, int nx, int cz, int cy, int cx,
+                 float* dst, int* status);
+
 /* The rotation the shift match uses for each tracker, on the device: rot (B, 9) float32, row
  * major, the matrix of the conjugated tracker that ShiftMatcher.search_shifts builds on the host
  * (R.from_euler('ZYZ', to_euler_angles(conj(tracker)), degrees) at src/matcha/core/

@@ -2,7 +2,7 @@
 
     python -m matcha_b200.build [--verbose]
 
-Produces ``matcha_b200/_lib/libmatcha_b200.so`` from ``matcha_b200/csrc/*.cu`` with
+Produces ``matcha_b200/_lib/libmatcha_b200.so`` from ``matcha_b200/csrc/*.cu`` and ``*.cpp`` with
 nvcc (cross-compiles without a GPU).  The library exports the C ABI declared in
 ``include/matcha_b200.h``.
 """
@@ -29,7 +29,7 @@ def nvcc_path() -> str:
 
 
 def sources():
-    return sorted(glob.glob(os.path.join(PKG, "csrc", "*.cu")))
+    return sorted(glob.glob(os.path.join(PKG, "csrc", "*.cu")) + glob.glob(os.path.join(PKG, "csrc", "*.cpp")))
 
 
 def needs_build() -> bool:

@@ -166,7 +166,8 @@ class AlignmentStep:
         alternate between calls, so the next call's first copies also overlap the end of this
         call's alignment.  tracker (B, 4) float64 and shift_zyx (B, 3) are device tensors;
         tracker is updated in place.  Returns the outputs of ``__call__`` for the whole batch,
-        in tensors of their own (rewritten by the next call)."""
+        in tensors of their own (rewritten by the next call), and ``copies_done``, the CUDA
+        event after which ``volumes_host`` is no longer read."""
         B = volumes_host.shape[0]
         if B > self.cfg.batch:
             raise ValueError(f"batch {B} exceeds the configured batch {self.cfg.batch}")
@@ -210,4 +211,5 @@ class AlignmentStep:
         self._stage_next = which ^ 1
         out = {k: self._out[k][:B] for k in self._KEYS}
         out["tracker"] = tracker
+        out["copies_done"] = ready[-1]  # after it the host batch may be overwritten
         return out

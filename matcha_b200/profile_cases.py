@@ -4,6 +4,7 @@
     python -m matcha_b200.profile_cases search 296   # Matcha.search_orientations, L 32, C 10
     python -m matcha_b200.profile_cases fle    256   # CrossCorrelationMatcher.get_sigma, 64^3, L 32
     python -m matcha_b200.profile_cases prepare 1000 # shifted patch, masked normalisation, rotation, 64^3
+    python -m matcha_b200.profile_cases reader 1000  # MRC decode of 1000 64^3 files into pinned memory
     python -m matcha_b200.profile_cases shift 1000 --stages   # plus ShiftMatcher.profile per kernel group
 
 Each case builds its inputs on the device from a fixed seed (random volumes, Haar rotations,
@@ -90,7 +91,56 @@ def _prepare(B: int, dev):
     return run
 
 
-CASES = {"shift": _shift, "search": _search, "fle": _fle, "prepare": _prepare}
+def _reader(B: int, reps: int) -> int:
+    """Host only: writes B 64^3 float32 MRC files to a temporary directory, reads them once
+    to warm the page cache, then times ``reps`` reads of all of them into a pinned batch
+    (wall clock; the decode uses no GPU)."""
+    import os
+    import tempfile
+    import time
+
+    from .reader import MrcReader, write_mrc
+
+    N = 64
+    rng = np.random.default_rng(0)
+    with tempfile.TemporaryDirectory() as d:
+        paths = []
+        for i in range(B):
+            p = os.path.join(d, f"{i}_data.mrc")
+            write_mrc(p, rng.standard_normal((N, N, N)).astype(np.float32))
+            paths.append(p)
+        r = MrcReader(0)
+        out = torch.empty((B, N, N, N), dtype=torch.float32, pin_memory=torch.cuda.is_available())
+        st = r.read_into(paths, out, (N, N, N))
+        if st.any():
+            print("read failed", file=sys.stderr)
+            return 1
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            r.read_into(paths, out, (N, N, N))
+        dt = (time.perf_counter() - t0) / reps
+        # the reference reader's steps with numpy in place of mrcfile: a thread pool reads each
+        # file into an array of its own, torch.stack makes the batch, pin_memory copies it
+        from concurrent.futures import ThreadPoolExecutor
+
+        def one(p):
+            return torch.from_numpy(np.fromfile(p, dtype="<f4", offset=1024).reshape(N, N, N))
+
+        with ThreadPoolExecutor(max_workers=os.cpu_count()) as ex:
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                batch = torch.stack(list(ex.map(one, paths)))
+                if torch.cuda.is_available():
+                    batch = batch.pin_memory()
+            dt_np = (time.perf_counter() - t0) / reps
+    threads = os.cpu_count()
+    print(f"reader batch {B}: {dt * 1e3:.3f} ms per batch, {B / dt:.0f} files/s, "
+          f"{B * N ** 3 * 4 / dt / 1e9:.2f} GB/s ({threads} hardware threads); per-file arrays + stack"
+          f"{' + pin' if torch.cuda.is_available() else ''}: {dt_np * 1e3:.3f} ms per batch, {B / dt_np:.0f} files/s")
+    return 0
+
+
+CASES = {"shift": _shift, "search": _search, "fle": _fle, "prepare": _prepare, "reader": None}
 
 
 def main(argv=None) -> int:
@@ -100,6 +150,8 @@ def main(argv=None) -> int:
     p.add_argument("--reps", type=int, default=5)
     p.add_argument("--stages", action="store_true", help="shift only: time each kernel group with CUDA events")
     a = p.parse_args(argv)
+    if a.case == "reader":
+        return _reader(a.batch, a.reps)
     if not torch.cuda.is_available():
         print("a CUDA device is required", file=sys.stderr)
         return 2
