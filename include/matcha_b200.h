@@ -243,6 +243,15 @@ int mtb_shift_profile_read(mtb_shift* h, float* ms, int* calls);
 int mtb_update_rotation(const float* alpha, const float* beta, const float* gamma, const double* tracker_in,
                         int B, double* tracker_out, float* rot, mtb_stream_t stream);
 
+/* The shift match's Fourier reference of a template, computed on the device in FP64 as
+ * load_reference_full (src/matcha/core/ShiftMatcher.py:456-472) does in numpy: soft low-pass
+ * (apply_soft_mask, ini_high 4, edge 2), sinc^2 gridding correction, roll by -N/2, fftn
+ * (norm "forward"), fftshift, spherical frequency mask.  tmpl (N, N, N) float64; workspace
+ * (2 N^3 + 2 N) x 16 bytes, 16-byte aligned; out (N, N, N) complex64 (interleaved floats), the
+ * input of mtb_shift_set_reference.  Synchronises the stream (one-time set-up). */
+int mtb_shift_reference(const double* tmpl, int N, float voxel_size, void* workspace, float* out,
+                        mtb_stream_t stream);
+
 /* Batch reader (host only): decode MRC2014 files (modes 0 int8, 1 int16, 2 float32, 6 uint16,
  * 12 float16; either byte order; any extended header) into float32 C-order (z, y, x) voxels,
  * as load_subtomogram_cpu / load_ctf_relion5_cpu do through mrcfile

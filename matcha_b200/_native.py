@@ -95,6 +95,7 @@ SIGNATURES = {
     "mtb_shift_search": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P]),
     "mtb_update_rotation": (_I, [_P, _P, _P, _P, _I, _P, _P, _P]),
     "mtb_tracker_rotation": (_I, [_P, _I, _P, _P]),
+    "mtb_shift_reference": (_I, [_P, _I, ctypes.c_float, _P, _P, _P]),
     "mtb_reader_create": (_I, [_I, _P]),
     "mtb_reader_destroy": (_I, [_P]),
     "mtb_read_mrc": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P]),

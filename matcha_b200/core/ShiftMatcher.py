@@ -181,11 +181,21 @@ class ShiftMatcher:
             self._free()
 
     @torch.no_grad()
+    @torch.no_grad()
     def set_reference(self, template_data: np.ndarray):
-        """Precompute and cache the Fourier-domain reference (ShiftMatcher.py:805-822)."""
-        ref = load_reference_full(template_data, volume_size=self.N,
-                                  voxel_size=float(_cfg(self.config, "voxel_size", 1.0)))
-        self.reference_data_fourier = torch.from_numpy(ref).unsqueeze(0).to(self.device, dtype=self.dtype)
+        """Precompute and cache the Fourier-domain reference (ShiftMatcher.py:805-822):
+        ``load_reference_full`` on the device in FP64 (``mtb_shift_reference``)."""
+        N = self.N
+        t = torch.from_numpy(np.ascontiguousarray(template_data, dtype=np.float64)).to(self.device)
+        if tuple(t.shape) != (N, N, N):
+            raise ValueError(f"template must be ({N}, {N}, {N})")
+        ws = torch.empty((2 * (2 * N ** 3 + 2 * N),), dtype=torch.float64, device=self.device)  # 16 B each
+        ref = torch.empty((1, N, N, N), dtype=torch.complex64, device=self.device)
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.mtb_shift_reference(nat.ptr(t), N, float(_cfg(self.config, "voxel_size", 1.0)),
+                                                    nat.ptr(ws), nat.ptr(ref), nat.stream_ptr(self.device)),
+                      "mtb_shift_reference")
+        self.reference_data_fourier = ref if self.dtype == torch.complex64 else ref.to(self.dtype)
         self._ref_version += 1
 
     def get_base_shifts(self, num_subtomograms_per_batch: int, num_base_shifts: int, dtype_real: torch.dtype):

@@ -148,3 +148,19 @@ def test_shift_nan_subtomogram_follows_argmax_order(cuda_device):
         np.testing.assert_allclose(c_d[[0, 2]], c_c[[0, 2]], rtol=1e-6)  # norms sum in any order
         out[precision] = s_d[1]
     np.testing.assert_array_equal(out["bf16x3"], out["fp32"])
+
+
+@pytest.mark.parametrize("N,voxel", [(32, 1.0), (15, 1.0), (48, 1.7), (16, 0.6)])
+def test_shift_reference_on_device_matches_oracle(cuda_device, N, voxel):
+    """set_reference computes load_reference_full on the device (FP64 DFTs): odd and even boxes,
+    low-pass radii from the voxel size; the result is complex64."""
+    rng = np.random.default_rng(N)
+    tmpl = blob_template(rng, N, 30, N * 0.3, (1.0, 2.5), mask_radius=N * 0.4).astype(np.float64)
+    tmpl += 1e-3 * rng.standard_normal(tmpl.shape)  # FP64 detail below float32 resolution
+    sm = _matcher(N, 1, 4, 1, cuda_device)
+    sm.config["voxel_size"] = voxel
+    sm.set_reference(tmpl)
+    ref = OS.load_reference_full(tmpl, N, voxel)
+    got = sm.reference_data_fourier[0].cpu().numpy()
+    assert got.dtype == np.complex64
+    np.testing.assert_allclose(got, ref, atol=2e-7 * np.abs(ref).max(), rtol=0)
