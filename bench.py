@@ -125,6 +125,17 @@ def rotation_error_deg(alpha, beta, gamma, q_true):
     return np.rad2deg((tr * sw.inv()).magnitude())
 
 
+def tracker_error_deg(tracker, q_true):
+    """Angle between the true rotation and a tracker (w, x, y, z) after any number of
+    alternations: rotation_error_deg's tr * sw^-1 with sw^-1 the tracker's rotation (from the
+    identity one update gives tracker = conj(sw))."""
+    from scipy.spatial.transform import Rotation as R
+
+    t = R.from_quat(np.roll(np.asarray(tracker, dtype=np.float64), -1, axis=1))
+    tr = R.from_quat(np.roll(q_true, -1, axis=1))
+    return np.rad2deg((tr * t).magnitude())
+
+
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -352,6 +363,44 @@ def run_ours(args):
         plain = {"value": world * B / (ms32 * 1e-3), "ms_per_step": ms32, "steps": n32,
                  "chosen_speedup": ms32 / ms}
         del step32
+    # three alternations per batch, as an alignment run makes them: each prepares the batch at
+    # the current shift and orientation (patch, masked normalisation, rotation), then sigma,
+    # search, tracker update and shift match (AlignmentStep.run_alternations)
+    local3 = torch.zeros((B, 3), device=dev, dtype=torch.float32)
+
+    def three():
+        tracker.copy_(ident)
+        local3.zero_()
+        return step.run_alternations(vols, tracker, local3, zeros3, zeros3, 3)
+
+    three()
+    torch.cuda.synchronize()
+    n3 = max(2, args.steps // 4)
+    if world > 1:
+        dist.barrier()
+    e3s, e3e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e3s.record(st)
+    for _ in range(n3):
+        three()
+    e3e.record(st)
+    torch.cuda.synchronize()
+    ms3 = e3s.elapsed_time(e3e) / n3
+    ep0, ep1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ep0.record(st)
+    step.prepare(vols, zeros3, tracker)
+    ep1.record(st)
+    torch.cuda.synchronize()
+    ms_prep = ep0.elapsed_time(ep1)
+    if world > 1:
+        t3 = torch.tensor([ms3], device=dev)
+        dist.all_reduce(t3, op=dist.ReduceOp.MAX)
+        ms3 = float(t3.item())
+    # rotation error of the tracker after the third alternation (the last run's)
+    trk = tracker.cpu().numpy()
+    err3 = tracker_error_deg(trk, q_true)
+    alternations = {"value": world * B / (ms3 * 1e-3), "unit": "subtomograms/s", "alternations": 3,
+                    "ms_per_batch": ms3, "runs": n3, "prepare_ms_per_alternation": ms_prep,
+                    "median_rot_err_deg": float(np.median(err3)), "p90_rot_err_deg": float(np.percentile(err3, 90))}
     # accuracy of one more chosen-path step on the full batch (the pieces of the end-to-end
     # runs overwrote the step's output buffers)
     tracker.copy_(ident)
@@ -405,6 +454,7 @@ def run_ours(args):
                      "traffic_unit": "bytes per launch"},
         "shift_kernel_ms_per_step": {k: v / max(1, shift_calls) for k, v in shift_prof.items()},
         "plain_fp32": plain,
+        "three_alternations": alternations,
         "e2e": {"value": world * B / (e2e_ms * 1e-3), "unit": "subtomograms/s",
                 "h2d_bytes_per_step": int(B * N_BOX ** 3 * 4), "d2h_bytes_per_step": int(B * 8 * 4)},
         "gpu_launches": KERNELS_PER_STEP * args.steps,
