@@ -789,20 +789,31 @@ __device__ __forceinline__ bool better(float v1, int i1, float v2, int i2) {
   return v1 > v2 || (v1 == v2 && i1 < i2);
 }
 
+// stage_e: the twiddle tables E1, E2 are copied to shared memory; without it (large boxes or
+// upsampled regions, whose tables do not fit beside the X1 and X2 slices) they are read from
+// global memory through L1.
 __global__ void __launch_bounds__(kT)
 updft23_kernel(ShiftGeom g, const float2* __restrict__ X1, const float2* __restrict__ E1,
-               const float2* __restrict__ E2, int rows_per_cta, float* __restrict__ pval, int* __restrict__ pidx) {
+               const float2* __restrict__ E2, int rows_per_cta, int stage_e, float* __restrict__ pval,
+               int* __restrict__ pidx) {
   extern __shared__ __align__(16) float2 sm2[];
   __shared__ float rv[32];
   __shared__ int ri[32];
   const int N = g.N, H = g.H, U = g.U;
-  float2* e1 = sm2;            // U x N
-  float2* e2 = e1 + U * N;     // U x H
-  float2* x1 = e2 + U * H;     // N x H
+  const float2* e1 = E1;       // U x N
+  const float2* e2 = E2;       // U x H
+  float2* x1 = sm2;            // N x H
+  if (stage_e) {
+    float2* s1 = sm2;
+    float2* s2 = s1 + U * N;
+    for (int e = threadIdx.x; e < U * N; e += blockDim.x) s1[e] = E1[e];
+    for (int e = threadIdx.x; e < U * H; e += blockDim.x) s2[e] = E2[e];
+    e1 = s1;
+    e2 = s2;
+    x1 = s2 + U * H;
+  }
   float2* x2 = x1 + N * H;     // U x H
   const int grp = blockIdx.x, b = blockIdx.y;
-  for (int e = threadIdx.x; e < U * N; e += blockDim.x) e1[e] = E1[e];
-  for (int e = threadIdx.x; e < U * H; e += blockDim.x) e2[e] = E2[e];
   float bv = -INFINITY;
   int bi = 0x7fffffff;
   const int u0a = grp * rows_per_cta;
@@ -1165,10 +1176,13 @@ extern "C" int mtb_shift_search(mtb_shift* h, const float* subtomos, const float
   updft1_kernel<<<dim3((N * H + kColTile - 1) / kColTile, B), kT, sm1, st>>>(g, h->T, h->E0, h->X1);
   MTB_LAUNCH_CHECK();
   prof_mark(h, 4, st);
-  const size_t sm2 = (size_t)(U * N + U * H + N * H + U * H) * 8;
+  const size_t sm2_staged = (size_t)(U * N + U * H + N * H + U * H) * 8;
+  const int stage_e = sm2_staged <= 220 * 1024;
+  const size_t sm2 = stage_e ? sm2_staged : (size_t)(N * H + U * H) * 8;
   MTB_ARG_CHECK(sm2 <= 220 * 1024 && sm1 <= 220 * 1024, "upsampled region too large for shared memory");
   MTB_CUDA_TRY(cudaFuncSetAttribute(updft23_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-  updft23_kernel<<<dim3(h->ngrp, B), kT, sm2, st>>>(g, h->X1, h->E1, h->E2, h->rows_per_cta, h->pval, h->pidx);
+  updft23_kernel<<<dim3(h->ngrp, B), kT, sm2, st>>>(g, h->X1, h->E1, h->E2, h->rows_per_cta, stage_e, h->pval,
+                                                    h->pidx);
   MTB_LAUNCH_CHECK();
   prof_mark(h, 5, st);
   finalize_kernel<<<(B + 127) / 128, 128, 0, st>>>(g, B, h->ngrp, h->pval, h->pidx, h->nrm, shift_xyz, score);
