@@ -153,6 +153,22 @@ class AlignmentStep:
             results.append(r)
         return results
 
+    @torch.no_grad()
+    def capture(self, B: int, alternations: int = 0):
+        """A CUDA graph of one batch of B subtomograms, replayed with ``CapturedStep.replay()``.
+
+        alternations == 0: one alternation as ``__call__`` on prepared volumes (inputs
+        ``volumes``, ``tracker``, ``shift``); alternations >= 1: ``run_alternations`` from the
+        raw subtomograms (inputs ``volumes``, ``tracker``, ``local_shifts``, ``prior_shifts``,
+        ``base_shifts``), each alternation preparing the batch first.  Inputs are static device
+        tensors of the returned object: copy a batch into them, replay, read its outputs (also
+        static, rewritten by each replay).  The step issues no host synchronisation, so every
+        launch of the library and every torch operation of the loop is in the graph; the
+        library's handles and the step's buffers are created by two eager runs first."""
+        if not 0 < B <= self.cfg.batch:
+            raise ValueError(f"batch must be in [1, {self.cfg.batch}]")
+        return CapturedStep(self, B, alternations)
+
     _KEYS = ("alpha", "beta", "gamma", "rotation_score", "bh_norms", "shift", "shift_score")
 
     @torch.no_grad()
@@ -213,3 +229,53 @@ class AlignmentStep:
         out["tracker"] = tracker
         out["copies_done"] = ready[-1]  # after it the host batch may be overwritten
         return out
+
+
+class CapturedStep:
+    """See ``AlignmentStep.capture``."""
+
+    def __init__(self, step: AlignmentStep, B: int, alternations: int):
+        N, dev = step.cfg.N, step.device
+        self.step, self.B, self.alternations = step, B, alternations
+        self.volumes = torch.zeros((B, N, N, N), device=dev, dtype=torch.float32)
+        self.tracker = torch.zeros((B, 4), device=dev, dtype=torch.float64)
+        self.tracker[:, 0] = 1
+        self._tracker0 = self.tracker.clone()
+        z = lambda: torch.zeros((B, 3), device=dev, dtype=torch.float32)
+        if alternations == 0:
+            self.shift = z()
+        else:
+            self.local_shifts, self.prior_shifts, self.base_shifts = z(), z(), z()
+            self._local0 = z()
+        side = torch.cuda.Stream(device=dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.device(dev), torch.cuda.stream(side):
+            for _ in range(2):
+                self._restore()
+                self._run()
+        torch.cuda.current_stream(dev).wait_stream(side)
+        torch.cuda.synchronize(dev)
+        self._restore()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.device(dev), torch.cuda.graph(self.graph):
+            self.outputs = self._run()
+        torch.cuda.synchronize(dev)
+
+    def _restore(self):
+        self.tracker.copy_(self._tracker0)
+        if self.alternations:
+            self.local_shifts.copy_(self._local0)
+
+    def _run(self):
+        s = self.step
+        if self.alternations == 0:
+            return s(self.volumes, self.volumes, self.tracker, self.shift)
+        return s.run_alternations(self.volumes, self.tracker, self.local_shifts, self.prior_shifts,
+                                  self.base_shifts, self.alternations)
+
+    def replay(self):
+        """Run the captured batch on the current inputs; returns the static outputs (a dict, or
+        a list of dicts, one per alternation).  tracker (and local_shifts) are updated in place
+        as the eager calls update them."""
+        self.graph.replay()
+        return self.outputs

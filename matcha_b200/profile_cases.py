@@ -5,6 +5,7 @@
     python -m matcha_b200.profile_cases fle    256   # CrossCorrelationMatcher.get_sigma, 64^3, L 32
     python -m matcha_b200.profile_cases prepare 1000 # shifted patch, masked normalisation, rotation, 64^3
     python -m matcha_b200.profile_cases reader 1000  # MRC decode of 1000 64^3 files into pinned memory
+    python -m matcha_b200.profile_cases graph 64     # one alternation, 64^3 L 32: eager calls vs a CUDA graph
     python -m matcha_b200.profile_cases shift 1000 --stages   # plus ShiftMatcher.profile per kernel group
 
 Each case builds its inputs on the device from a fixed seed (random volumes, Haar rotations,
@@ -140,7 +141,36 @@ def _reader(B: int, reps: int) -> int:
     return 0
 
 
-CASES = {"shift": _shift, "search": _search, "fle": _fle, "prepare": _prepare, "reader": None}
+def _graph(B: int, reps: int) -> int:
+    """One alternation (AlignmentStep at 64^3, L 32) on B random volumes: eager calls against
+    the replay of its CUDA graph, CUDA events, ``reps`` calls each."""
+    from .pipeline import AlignmentStep, StepConfig
+
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(0)
+    step = AlignmentStep(StepConfig(batch=B), dev)
+    step.set_template(rng.standard_normal((64, 64, 64)).astype(np.float32))
+    cap = step.capture(B)
+    cap.volumes.copy_(torch.randn(B, 64, 64, 64, device=dev))
+    tracker = cap.tracker.clone()
+    zeros = torch.zeros((B, 3), device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times = {}
+    for name, fn in (("eager", lambda: step(cap.volumes, cap.volumes, tracker, zeros)), ("graph", cap.replay)):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        times[name] = e0.elapsed_time(e1) / reps
+    print(f"graph batch {B}: eager {times['eager']:.3f} ms, graph replay {times['graph']:.3f} ms per alternation")
+    return 0
+
+
+CASES = {"shift": _shift, "search": _search, "fle": _fle, "prepare": _prepare, "reader": None, "graph": None}
 
 
 def main(argv=None) -> int:
@@ -155,6 +185,8 @@ def main(argv=None) -> int:
     if not torch.cuda.is_available():
         print("a CUDA device is required", file=sys.stderr)
         return 2
+    if a.case == "graph":
+        return _graph(a.batch, a.reps)
     dev = torch.device("cuda:0")
     run = CASES[a.case](a.batch, dev)
     for _ in range(3):

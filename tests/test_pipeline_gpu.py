@@ -80,3 +80,39 @@ def test_align_host_rejects_oversize_batch(cuda_device):
     with pytest.raises(ValueError):
         step.align_host(host, torch.zeros((3, 4), dtype=torch.float64, device=cuda_device),
                         torch.zeros((3, 3), device=cuda_device))
+
+
+@pytest.mark.parametrize("alternations", [0, 2])
+def test_captured_step_matches_eager(cuda_device, alternations):
+    """One CUDA graph replayed on two different batches gives what the eager calls give."""
+    B, N = 4, 16
+    rng = np.random.default_rng(40 + alternations)
+    tmpl = blob_template(rng, N, 12, 5, (1.0, 2.0), mask_radius=7).astype(np.float32)
+    step = _step(cuda_device, B)
+    step.set_template(tmpl)
+    cap = step.capture(B, alternations)
+    ident = torch.zeros((B, 4), dtype=torch.float64, device=cuda_device)
+    ident[:, 0] = 1
+    zeros3 = torch.zeros((B, 3), device=cuda_device)
+    keys = ("alpha", "beta", "gamma", "rotation_score", "shift", "shift_score")
+    for trial in range(2):
+        vols = (np.repeat(tmpl[None], B, 0) + (0.05 + 0.1 * trial) * rng.standard_normal((B, N, N, N)))
+        dv = torch.from_numpy(vols.astype(np.float32)).to(cuda_device)
+        cap.volumes.copy_(dv)
+        cap.tracker.copy_(ident)
+        if alternations:
+            cap.local_shifts.zero_()
+        out = cap.replay()
+        outs = [out] if alternations == 0 else out
+        got = [{k: o[k].cpu().numpy().copy() for k in keys} for o in outs]
+        got_tracker = cap.tracker.cpu().numpy().copy()
+        t = ident.clone()
+        if alternations == 0:
+            ref = [step(dv, dv, t, zeros3)]
+        else:
+            ref = step.run_alternations(dv, t, torch.zeros_like(zeros3), zeros3, zeros3, alternations)
+        assert len(ref) == len(got)
+        for g, r in zip(got, ref):
+            for k in keys:
+                np.testing.assert_allclose(g[k], r[k].cpu().numpy(), rtol=1e-6, atol=1e-7, err_msg=k)
+        np.testing.assert_allclose(got_tracker, t.cpu().numpy(), atol=1e-12)

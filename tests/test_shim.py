@@ -39,4 +39,4 @@ def test_profile_cases_needs_a_device(monkeypatch):
 
     monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
     assert profile_cases.main(["shift", "2"]) == 2
-    assert set(profile_cases.CASES) == {"shift", "search", "fle", "prepare", "reader"}
+    assert set(profile_cases.CASES) == {"shift", "search", "fle", "prepare", "reader", "graph"}
