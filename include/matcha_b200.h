@@ -77,6 +77,16 @@ void mtb_search_destroy(mtb_search* h);
 int mtb_so3_grid_topk(mtb_search* h, const float* sigma, int64_t sigma_stride, int B,
                       float* alpha, float* beta, float* gamma, float* grid, mtb_stream_t stream);
 
+/* The alignment score f = Re sum_{l <= L} D^l(alpha, beta, gamma) sigma_l at one point per
+ * subtomogram, with its Euler gradient and Hessian: the quantities the Newton step reads
+ * (WignerDGradients.set_so3_coeffs + get_derivatives, src/matcha/core/WignerDGradients.py:
+ * 155-302), exposed for a caller's own optimiser or backward pass.  alpha, beta, gamma (B,)
+ * float32; out (B, 10) float32 = f, df/d(alpha, beta, gamma), d2f/d(aa, ab, ag, bb, bg, gg).
+ * L <= the handle's Lmax; sigma needs dsize(L) entries per row.  No workspace. */
+int mtb_score_derivatives(mtb_search* h, const float* sigma, int64_t sigma_stride, int B, int L,
+                          const float* alpha, const float* beta, const float* gamma, float* out,
+                          mtb_stream_t stream);
+
 /* Newton march over all stages for every candidate.  alpha/beta/gamma: (B, candidates)
  * float32 in/out; score: (B, candidates) float32 out (best Re sum D sigma).
  * sigma needs dsize(Lmax) entries per row.  Replaces the stage loop of

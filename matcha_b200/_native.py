@@ -78,6 +78,7 @@ SIGNATURES = {
     "mtb_search_destroy": (None, [_P]),
     "mtb_so3_grid_topk": (_I, [_P, _P, _I64, _I, _P, _P, _P, _P, _P]),
     "mtb_newton_march": (_I, [_P, _P, _I64, _I, _P, _P, _P, _P, _P]),
+    "mtb_score_derivatives": (_I, [_P, _P, _I64, _I, _I, _P, _P, _P, _P, _P]),
     "mtb_search_orientations": (_I, [_P, _P, _I64, _I, _P, _P, _P, _P, _P]),
     "mtb_search_orientations_static": (_I, [ctypes.POINTER(MtbSearchConfig), _P, _I64, _I, _P, _P, _P, _P, _P]),
     "mtb_fle_create": (_I, [ctypes.POINTER(MtbFleConfig), ctypes.POINTER(_P)]),

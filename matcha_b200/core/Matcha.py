@@ -177,6 +177,41 @@ class Matcha:
         return a, b, g, s
 
     @torch.no_grad()
+    def score_derivatives(self, sigma, alpha, beta, gamma, L: int = None):
+        """Score f = Re sum_{l <= L} D^l(alpha, beta, gamma) sigma_l at one point per row of
+        sigma, its Euler gradient (B, 3) and Hessian (B, 3, 3) (``mtb_score_derivatives``; the
+        quantities of WignerDGradients.get_derivatives, WignerDGradients.py:247-302).
+        L defaults to L_max; angles (B,) in radians."""
+        L = self.Lmax if L is None else int(L)
+        if not 0 <= L <= self.Lmax:
+            raise ValueError(f"L must be in [0, {self.Lmax}]")
+        nat.require_cuda(sigma, "sigma")
+        if sigma.ndim != 2:
+            raise ValueError("sigma must have shape (batch, Dsize)")
+        if sigma.dtype != torch.complex64:
+            sigma = sigma.to(torch.complex64)
+        if sigma.stride(1) != 1:
+            sigma = sigma.contiguous()
+        if sigma.shape[1] < dsize(L):
+            raise ValueError(f"sigma has {sigma.shape[1]} columns; dsize(L)={dsize(L)} needed")
+        B = sigma.shape[0]
+        ang = [torch.as_tensor(t, device=sigma.device).to(torch.float32).reshape(-1).contiguous()
+               for t in (alpha, beta, gamma)]
+        if any(t.shape[0] != B for t in ang):
+            raise ValueError("one (alpha, beta, gamma) per row of sigma")
+        out = torch.empty((B, 10), device=sigma.device, dtype=torch.float32)
+        with torch.cuda.device(sigma.device):
+            nat.check(self._lib.mtb_score_derivatives(self._h, nat.ptr(sigma), sigma.stride(0), B, L,
+                                                      nat.ptr(ang[0]), nat.ptr(ang[1]), nat.ptr(ang[2]),
+                                                      nat.ptr(out), nat.stream_ptr(sigma.device)),
+                      "mtb_score_derivatives")
+        h = out[:, 4:]
+        H = torch.stack([torch.stack([h[:, 0], h[:, 1], h[:, 2]], -1),
+                         torch.stack([h[:, 1], h[:, 3], h[:, 4]], -1),
+                         torch.stack([h[:, 2], h[:, 4], h[:, 5]], -1)], -2)
+        return out[:, 0], out[:, 1:4], H
+
+    @torch.no_grad()
     def search_orientations(self, sigma):
         """(alpha, beta, gamma, score), each (B,), radians (Matcha.py:369-403)."""
         sigma = self._prep_sigma(sigma)

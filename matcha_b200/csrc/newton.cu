@@ -433,7 +433,34 @@ newton_march_kernel(const float4* __restrict__ S, int64_t n_fold, const float2* 
   }
 }
 
+// The score and its Euler derivatives at one given point per subtomogram, degrees <= Li:
+// out[b] = (f, df/da, df/db, df/dg, d2f/da2, d2f/dadb, d2f/dadg, d2f/db2, d2f/dbdg, d2f/dg2),
+// the same sweep the march makes at each Newton step, read straight from sigma.
+__global__ void __launch_bounds__(kNT)
+score_derivs_kernel(const float2* __restrict__ sigma, int64_t stride, const float* __restrict__ alpha,
+                    const float* __restrict__ beta, const float* __restrict__ gamma, int Li,
+                    const double* __restrict__ Ctab, const float4* __restrict__ coef, float* __restrict__ out) {
+  __shared__ float2 s_ea[1][2 * kNewtonMaxL + 1], s_eg[1][2 * kNewtonMaxL + 1];
+  __shared__ double s_phc[1][2 * kNewtonMaxL + 3], s_pt[1][2 * kNewtonMaxL + 3];
+  __shared__ float s_red[(kNT / 32) * A_N], s_res[A_N];
+  const Smem<1> sm{s_ea, s_eg, s_phc, s_pt, s_red, s_res};
+  const int b = blockIdx.x;
+  const float a[1] = {alpha[b]}, be[1] = {beta[b]}, ga[1] = {gamma[b]};
+  pass<true, false, 1>(nullptr, sigma + (int64_t)b * stride, coef, Ctab, a, be, ga, Li, sm);
+  if (threadIdx.x < A_N) out[(int64_t)b * A_N + threadIdx.x] = sm.res[threadIdx.x];
+}
+
 }  // namespace
+
+int newton_eval_launch(const float* sigma, int64_t stride, int B, int Li, const float* alpha, const float* beta,
+                       const float* gamma, const double* Ctab, const float4* coef, float* out, cudaStream_t st) {
+  MTB_ARG_CHECK(Li >= 0 && Li <= kNewtonMaxL, "degree exceeds the Newton march limit");
+  if (B == 0) return MTB_OK;
+  score_derivs_kernel<<<B, kNT, 0, st>>>(reinterpret_cast<const float2*>(sigma), stride, alpha, beta, gamma, Li,
+                                         Ctab, coef, out);
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
+}
 
 int64_t newton_fold_entries(int Lmax) { return wedge_off(Lmax + 1); }
 

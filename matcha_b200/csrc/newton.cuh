@@ -32,6 +32,11 @@ int newton_launch(const float* sigma, int64_t stride, int B, int C, float* alpha
                   float* score, const double* Ctab, const float4* coef, float4* fold, const NewtonParams& P,
                   cudaStream_t st);
 
+// Score, Euler gradient and Hessian at one point per subtomogram (degrees <= Li <= the Lmax
+// the tables were built for): out (B, 10) float = f, g (a, b, g), H (aa, ab, ag, bb, bg, gg).
+int newton_eval_launch(const float* sigma, int64_t stride, int B, int Li, const float* alpha, const float* beta,
+                       const float* gamma, const double* Ctab, const float4* coef, float* out, cudaStream_t st);
+
 // The march that reproduces the reference's final-stage top block (flag
 // MTB_SEARCH_COMPAT_TOP_BLOCK): full d blocks in shared memory and the reference's row-shift
 // derivative stencil on the zeroed block.

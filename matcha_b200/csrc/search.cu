@@ -483,6 +483,19 @@ extern "C" int mtb_newton_march(mtb_search* h, const float* sigma, int64_t sigma
                        h->fold, P, (cudaStream_t)stream);
 }
 
+extern "C" int mtb_score_derivatives(mtb_search* h, const float* sigma, int64_t sigma_stride, int B, int L,
+                                     const float* alpha, const float* beta, const float* gamma, float* out,
+                                     mtb_stream_t stream) {
+  MTB_ARG_CHECK(h, "null handle");
+  MTB_ARG_CHECK(B >= 0, "negative batch");
+  if (B == 0) return MTB_OK;
+  MTB_ARG_CHECK(sigma && alpha && beta && gamma && out, "null pointer");
+  MTB_ARG_CHECK(L >= 0 && L <= h->cfg.Lmax, "degree must be in [0, Lmax]");
+  MTB_ARG_CHECK(sigma_stride >= mtb_dsize(L), "sigma row shorter than dsize(L)");
+  return newton_eval_launch(sigma, sigma_stride, B, L, alpha, beta, gamma, h->Ctab, h->coef, out,
+                            (cudaStream_t)stream);
+}
+
 extern "C" int mtb_search_orientations(mtb_search* h, const float* sigma, int64_t sigma_stride, int B,
                                        float* alpha, float* beta, float* gamma, float* score,
                                        mtb_stream_t stream) {
