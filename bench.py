@@ -38,9 +38,6 @@ METRIC = "subtomograms/s at 64^3 L=32 (one alternation: FLE+sigma, SO(3) grid, N
 KERNELS_PER_STEP = 16  # FLE fold_split, gemm_tc, expand; sigma; SO(3) grid; fold_sigma, newton_march,
 # reduce_candidates; tracker_update; shift patch_fft_xy64, fft_z64, updft1_tc x2 (the Nyquist plane),
 # updft1_tc, updft23_tc, finalize_tc
-# DRAM bytes (read + write) of updft23_tc_kernel per subtomogram, from an ncu capture of the same kernel
-# at 200 subtomograms (dram__bytes_read.sum + dram__bytes_write.sum divided by 200)
-UPDFT23_DRAM_BYTES_PER_SUBTOMO = 1_526_000
 
 
 def parse():
@@ -50,7 +47,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--batch", type=int, default=1000)
-    p.add_argument("--cpu-sample", type=int, default=2, help="subtomograms per CPU-baseline step")
+    p.add_argument("--cpu-sample", type=int, default=8,
+                   help="subtomograms per CPU-baseline step (also the accuracy comparison with the oracle)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp32", action="store_true", help="skip the plain-FP32 comparison run")
     p.add_argument("--seed", type=int, default=0)
@@ -86,8 +84,14 @@ def make_template(rng, N=N_BOX, n_blobs=400, window=None):
     return vol.astype(np.float32)
 
 
-def make_batch(template, rng, B, device, snr_db=0.0, max_shift=5.0):
-    """Rotated (reference rotate_volumes convention), shifted, noisy subtomograms on the device."""
+def make_batch(template, rng, B, device, snr_db=0.0, max_shift=5.0, count=None):
+    """Rotated (reference rotate_volumes convention), shifted, noisy subtomograms on ``device``.
+
+    Every random parameter of all B subtomograms is drawn first (Haar quaternions, uniform
+    shifts in voxels (z, y, x), one noise seed per subtomogram), then the first ``count``
+    (default B) volumes are synthesised, so the CPU arm can rebuild exactly the first few
+    subtomograms of the GPU arm's batch.  Noise: white Gaussian at ``snr_db`` against the
+    signal power inside the sphere of radius 0.45 N (src/matcha/example.py:93-124)."""
     import torch
     import torch.nn.functional as TF
     from scipy.spatial.transform import Rotation as R
@@ -96,7 +100,9 @@ def make_batch(template, rng, B, device, snr_db=0.0, max_shift=5.0):
     q = rng.standard_normal((B, 4))
     q /= np.linalg.norm(q, axis=1, keepdims=True)
     shifts = rng.uniform(-max_shift, max_shift, (B, 3)).astype(np.float32)
-    mats = torch.tensor(R.from_quat(np.roll(q, -1, axis=1)).as_matrix(), dtype=torch.float32, device=device)
+    seeds = rng.integers(0, 1 << 62, B)
+    n = B if count is None else min(int(count), B)
+    mats = torch.tensor(R.from_quat(np.roll(q[:n], -1, axis=1)).as_matrix(), dtype=torch.float32, device=device)
     t = torch.from_numpy(template).to(device)
     tp = TF.pad(t[None, None], (0, 1, 0, 1, 0, 1))
     lin = torch.linspace(-1, 1, N + 1, device=device)
@@ -107,12 +113,10 @@ def make_batch(template, rng, B, device, snr_db=0.0, max_shift=5.0):
     g = torch.arange(N, device=device) - N // 2
     zz, yy, xx = torch.meshgrid(g, g, g, indexing="ij")
     mask = (torch.sqrt((xx ** 2 + yy ** 2 + zz ** 2).float()) < 0.45 * N)
-    out = torch.empty((B, N, N, N), device=device, dtype=torch.float32)
-    sh = torch.from_numpy(shifts).to(device)
-    noise_gen = torch.Generator(device=device)
-    noise_gen.manual_seed(int(rng.integers(1 << 31)))
-    for s in range(0, B, 50):
-        e = min(B, s + 50)
+    out = torch.empty((n, N, N, N), device=device, dtype=torch.float32)
+    sh = torch.from_numpy(shifts[:n]).to(device)
+    for s in range(0, n, 50):
+        e = min(n, s + 50)
         rc = (mats[s:e] @ coords).permute(0, 2, 1).reshape(e - s, N + 1, N + 1, N + 1, 3)
         v = TF.grid_sample(tp.expand(e - s, -1, -1, -1, -1), rc, mode="bilinear", align_corners=True)
         v = v[:, 0, :N, :N, :N]
@@ -120,9 +124,10 @@ def make_batch(template, rng, B, device, snr_db=0.0, max_shift=5.0):
                                       + kx[None] * sh[s:e, 2, None, None, None]))
         v = torch.fft.ifftn(torch.fft.fftn(v, dim=(1, 2, 3)) * ph, dim=(1, 2, 3)).real
         power = (v[:, mask] ** 2).mean(dim=1)
-        noise = torch.randn(v.shape, device=device, generator=noise_gen) * torch.sqrt(
-            power * 10.0 ** (-snr_db / 10.0))[:, None, None, None]
-        out[s:e] = v + noise
+        noise = np.stack([np.random.default_rng(int(seeds[i])).standard_normal((N, N, N), dtype=np.float32)
+                          for i in range(s, e)])
+        out[s:e] = v + torch.from_numpy(noise).to(device) * torch.sqrt(power * 10.0 ** (-snr_db / 10.0))[:, None, None,
+                                                                                                        None]
     return out, q, shifts
 
 
@@ -211,25 +216,145 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- CPU restatement (oracle)
-def cpu_align(sample, template, vols, q_true, threads=None):
-    """Oracle pipeline on a few subtomograms; returns (seconds per subtomogram, outputs)."""
+_ORACLE_SETUP = {}  # per template: the oracle's folded basis, template coefficients, shift reference
+
+
+def cpu_align(sample, template, vols, dtype=np.float32):
+    """The oracle's alternation (FP64 expansion; orientation search in ``dtype``: float32 is the
+    reference's arithmetic, float64 the exact answer) on the first ``sample`` volumes; returns
+    (seconds per subtomogram of the alignment itself, outputs)."""
     from matcha_b200.core import fle_tables as T
-    from oracle import fle as OF
     from oracle import pipeline as OP
     from oracle import shift as OS
 
-    radius = min(N_BOX // 2, int(N_BOX // 2 * 0.95))
-    tb = T.lap_eig_ball(N_BOX, L_MAX, radius)
-    ff = OP.FoldedFLE(tb, N_BOX, float(radius))
-    a_t = ff.evaluate_t(template[None])[0]
-    ref = OS.load_reference_full(template, N_BOX, 1.0)
-    v = vols[:sample].astype(np.float64)
+    key = id(template)
+    if key not in _ORACLE_SETUP:
+        radius = min(N_BOX // 2, int(N_BOX // 2 * 0.95))
+        tb = T.lap_eig_ball(N_BOX, L_MAX, radius)
+        ff = OP.FoldedFLE(tb, N_BOX, float(radius))
+        _ORACLE_SETUP[key] = (ff, ff.evaluate_t(template[None])[0], OS.load_reference_full(template, N_BOX, 1.0))
+    ff, a_t, ref = _ORACLE_SETUP[key]
+    v = np.asarray(vols[:sample], dtype=np.float64)
     tracker = np.tile([1.0, 0, 0, 0], (sample, 1))
     t0 = time.perf_counter()
     out = OP.align_batch(ff, a_t, ref, v, v, tracker, np.zeros((sample, 3)), L_MAX, LI, uf=UPSAMPLE,
-                         shift_radius=SHIFT_RADIUS)
+                         shift_radius=SHIFT_RADIUS, dtype=dtype)
     dt = time.perf_counter() - t0
     return dt / sample, out
+
+
+def euler_dev_deg(a1, b1, g1, a2, b2, g2):
+    from scipy.spatial.transform import Rotation as R
+
+    r1 = R.from_euler("ZYZ", np.stack([a1, b1, g1], -1).astype(np.float64))
+    r2 = R.from_euler("ZYZ", np.stack([a2, b2, g2], -1).astype(np.float64))
+    return np.rad2deg((r1.inv() * r2).magnitude())
+
+
+def accuracy_vs_oracle(gpu, o32, o64, q_true, n):
+    """Per-subtomogram rotation deviation of a GPU run from the oracle on the same n inputs."""
+    ang = lambda d: [np.asarray(d[k][:n], dtype=np.float64) for k in ("alpha", "beta", "gamma")]
+    d32 = euler_dev_deg(*ang(gpu), *ang(o32))
+    d64 = euler_dev_deg(*ang(gpu), *ang(o64))
+    err = rotation_error_deg(*ang(gpu), q_true[:n])
+    return {"median_rot_err_deg": float(np.median(err)),
+            "median_dev_vs_ref_deg": float(np.median(d32)), "max_dev_vs_ref_deg": float(d32.max()),
+            "frac_within_0p05deg": float(np.mean(d32 < 0.05)),
+            "median_dev_vs_fp64_deg": float(np.median(d64)), "max_dev_vs_fp64_deg": float(d64.max()),
+            "frac_within_0p05deg_of_fp64": float(np.mean(d64 < 0.05)),
+            "shift_equal_frac": float(np.mean(np.all(np.abs(np.asarray(gpu["shift"][:n]) - o64["shift"]) < 1e-6,
+                                                     axis=1)))}
+
+
+# ---------------------------------------------------------------- roofline of every kernel of the step
+def kernel_work(B):
+    """Algorithmic work of each kernel of one alternation at 64^3, L = 32 (ne = 8252 coefficients,
+    8252 real basis columns, 15 216 octant representatives of the radius-30 ball, U = 88): FLOP
+    counted once per multiply-add pair of the exact product (a hi+lo split issues 3x as many),
+    bytes the compulsory HBM traffic of inputs and outputs.  Returns {kernel: (bound, amount)}
+    per launch of B subtomograms, amount in bytes for "hbm" and FLOP for "tensor"/"fp32"."""
+    N, H, U = N_BOX, N_BOX // 2 + 1, int(np.ceil(UPSAMPLE * (2 * SHIFT_RADIUS + 1)))
+    n_rep, n_cols, ne = 15216, 8252, 8252
+    vol = 4 * N ** 3                     # one float32 subtomogram
+    spec = 8 * N * N * H                 # (N, N, N/2+1) complex64 plane transforms
+    a1 = 2 * 2 * (N // 2) * N * 2 * N    # pass-1 operand: rows (m2 < N/2, m1), K (m0, re/im), bf16 hi and lo
+    a1n = 2 * 2 * N * 2 * N              # the Nyquist plane's pass-1 operand
+    a2 = 2 * 2 * U * (N // 2) * 2 * N    # pass-2 operand: rows (u0, m2 < N/2), K (m1, re/im), hi and lo
+    dsize = lambda L: (L + 1) * (2 * L + 1) * (2 * L + 3) // 3
+    work = {
+        "fold_split_kernel": ("hbm", vol + 2 * 2 * 8 * n_rep),
+        "gemm_tc_kernel": ("tensor", 2.0 * n_rep * n_cols),
+        "expand_kernel": ("hbm", 4 * n_cols + 8 * ne),
+        "sigma_kernel": ("hbm", 8 * ne + 8 * dsize(L_MAX)),
+        "so3_grid_topk_kernel": ("hbm", 8 * dsize(8)),
+        "fold_sigma_kernel": ("hbm", 8 * dsize(L_MAX) + 16 * sum((l + 1) ** 2 for l in range(L_MAX + 1))),
+        "tracker_update_kernel": ("hbm", 3 * 4 + 2 * 32 + 36),
+        "patch_fft_xy64_kernel": ("hbm", vol + spec),
+        "fft_z64_kernel": ("hbm", spec + a1 + a1n),
+        "updft1_tc_kernel": ("tensor", 2.0 * (N // 2 * N) * (2 * N) * (2 * U)),
+        "updft23_tc_kernel": ("tensor", 2.0 * (U * N // 2) * (2 * U) * (2 * N) + 2.0 * U * U * U * (N + 2)),
+        "finalize_tc_kernel": ("hbm", 16),
+    }
+    work["newton_march_kernel"] = ("fp32", float(sum((15 + 2) * 8 * 10 * dsize(Li) * 1 + 8 * 10 * dsize(Li)
+                                                     for Li in LI + [L_MAX])))
+    return {k: (b, a * B) for k, (b, a) in work.items()}, {"a2_bytes": a2}
+
+
+def fp32_peak_tflops(dev):
+    """FP32 CUDA-core throughput: cuBLAS SGEMM 8192^3 with TF32 off, best of 5 (CUDA events)."""
+    import torch
+
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        a = torch.randn(8192, 8192, device=dev)
+        b = torch.randn(8192, 8192, device=dev)
+        c = a @ b
+        best = None
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            c = a @ b
+            e1.record()
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1)
+            best = t if best is None else min(best, t)
+        del a, b, c
+        return 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
+def kernel_table(prof, steps, B, peaks, fp32_peak):
+    """Per kernel: ms per step, share of the step's kernel time, and roofline against the
+    measured peaks (HBM copy bandwidth, sustained bf16 tensor throughput, cuBLAS SGEMM)."""
+    work, _ = kernel_work(B)
+    total = sum(v["ms"] for v in prof.values())
+    table = {}
+    for name, v in prof.items():
+        ms = v["ms"] / steps
+        row = {"ms_per_step": ms, "launches_per_step": v["launches"] / steps, "share": v["ms"] / total if total else None}
+        base = name.split(" (")[0]
+        if base in work and v["launches"] / steps == 1:
+            bound, amount = work[base]
+            if bound == "hbm":
+                ach, peak, unit = amount / (ms * 1e-3) / 1e9, float(peaks.get("hbm_gbs", 6535.4)), "GB/s"
+            elif bound == "tensor":
+                ach, peak, unit = amount / (ms * 1e-3) / 1e12, float(peaks.get("bf16_tflops_sustained", 1401.9)), "TFLOP/s"
+            else:
+                ach, peak, unit = amount / (ms * 1e-3) / 1e12, fp32_peak, "TFLOP/s"
+            row.update(bound=bound, achieved=ach, peak=peak, unit=unit, frac=ach / peak if peak else None)
+            if DRAM_BYTES_PER_SUBTOMO.get(base):
+                row["traffic"] = DRAM_BYTES_PER_SUBTOMO[base] * B
+        table[name] = row
+    return table, total / steps
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per subtomogram of the shift kernels,
+# from one ncu capture at 200 subtomograms (profiles/shift_64_uf8_b200.md), scaled to a launch by
+# the subtomograms it processes (their traffic grows in proportion to the batch)
+DRAM_BYTES_PER_SUBTOMO = {"patch_fft_xy64_kernel": 1_910_000, "fft_z64_kernel": 2_085_000,
+                          "updft1_tc_kernel": 2_205_000, "updft23_tc_kernel": 1_525_000}
 
 
 # ---------------------------------------------------------------- our implementation
@@ -246,6 +371,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     torch.cuda.set_device(local)
     dev = torch.device(f"cuda:{local}")
+    from matcha_b200 import _native as nat
     from matcha_b200.pipeline import AlignmentStep, StepConfig
 
     rng = np.random.default_rng(args.seed)
@@ -267,32 +393,8 @@ def run_ours(args):
     for _ in range(args.warmup):
         out = one()
     torch.cuda.synchronize()
-    # per-stage breakdown (one extra untimed step)
     st = torch.cuda.current_stream()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
-    tracker.copy_(ident)
-    ev[0].record(st)
-    sigma, norms = step.correlator.get_sigma_upto(vols, L_MAX)
-    ev[1].record(st)
-    a, b, g, sc = step.matcher.search_orientations(sigma)
-    ev[2].record(st)
-    step(vols, vols, tracker, zeros3)  # full step (includes a second sigma/search)
-    ev[3].record(st)
-    torch.cuda.synchronize()
-    t_sigma = ev[0].elapsed_time(ev[1])
-    t_search = ev[1].elapsed_time(ev[2])
-    t_full = ev[2].elapsed_time(ev[3])
-    stages = {"fle_sigma_ms": t_sigma, "search_ms": t_search, "shift_ms": max(0.0, t_full - t_sigma - t_search)}
-    # per-kernel timing of the candidates for the roofline (launch stream events)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a0, b0, g0 = step.matcher._grid_search_so3fft(sigma)
-    torch.cuda.synchronize()
-    e0.record(st)
-    step.matcher.march(a0, b0, g0, sigma)
-    e1.record(st)
-    torch.cuda.synchronize()
-    t_march = e0.elapsed_time(e1)
-    # timed region
+    # timed region: every launch of the library bracketed by CUDA events on its stream
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -302,7 +404,7 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
-        step.shifter.profile(args.steps)  # CUDA events between the shift match's kernel groups
+        nat.profile_start(args.steps * (KERNELS_PER_STEP + 4))
         torch.cuda.nvtx.range_push("timed")  # lets a profiler select the timed launches
         start.record(st)
         for _ in range(args.steps):
@@ -310,9 +412,10 @@ def run_ours(args):
         end.record(st)
         torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
+        nat.profile_stop()
     ms = start.elapsed_time(end) / args.steps
-    shift_prof, shift_calls = step.shifter.profile_read()
-    step.shifter.profile(0)
+    prof, dropped = nat.profile_read()
+    launches = sum(v["launches"] for v in prof.values())
     if world > 1:
         tms = torch.tensor([ms], device=dev)
         dist.all_reduce(tms, op=dist.ReduceOp.MAX)
@@ -347,9 +450,14 @@ def run_ours(args):
         t2 = torch.tensor([e2e_ms], device=dev)
         dist.all_reduce(t2, op=dist.ReduceOp.MAX)
         e2e_ms = float(t2.item())
+    # accuracy of the chosen path on the full batch (one more step; the end-to-end runs' pieces
+    # overwrote the step's output buffers), kept for the comparison with the oracle below
+    out = one()
+    chosen = {k: out[k].cpu().numpy() for k in ("alpha", "beta", "gamma", "shift")}
     # the same step with the plain FP32 kernels (the expansion GEMM and the upsampled DFT on
     # CUDA cores instead of the BF16 hi+lo tensor-core split): the comparison the metric names
     plain = None
+    plain_out = None
     if not args.no_fp32:
         step32 = AlignmentStep(StepConfig(N=N_BOX, L=L_MAX, Li=LI, batch=B, shift_search_radius=SHIFT_RADIUS,
                                           shift_upsample_factor=UPSAMPLE, precision="fp32"), dev)
@@ -361,20 +469,24 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
+        nat.profile_start(n32 * (KERNELS_PER_STEP + 4))
         e32s, e32e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e32s.record(st)
         for _ in range(n32):
             tracker.copy_(ident)
-            step32(vols, vols, tracker, zeros3)
+            o32 = step32(vols, vols, tracker, zeros3)
         e32e.record(st)
         torch.cuda.synchronize()
+        nat.profile_stop()
+        prof32, _ = nat.profile_read()
         ms32 = e32s.elapsed_time(e32e) / n32
+        plain_out = {k: o32[k].cpu().numpy() for k in ("alpha", "beta", "gamma", "shift")}
         if world > 1:
             t32 = torch.tensor([ms32], device=dev)
             dist.all_reduce(t32, op=dist.ReduceOp.MAX)
             ms32 = float(t32.item())
         plain = {"value": world * B / (ms32 * 1e-3), "ms_per_step": ms32, "steps": n32,
-                 "chosen_speedup": ms32 / ms}
+                 "chosen_speedup": ms32 / ms, "kernels_ms_per_step": {k: v["ms"] / n32 for k, v in prof32.items()}}
         del step32
     # three alternations per batch, as an alignment run makes them: each prepares the batch at
     # the current shift and orientation (patch, masked normalisation, rotation), then sigma,
@@ -400,10 +512,11 @@ def run_ours(args):
     ms3 = e3s.elapsed_time(e3e) / n3
     ep0, ep1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ep0.record(st)
-    step.prepare(vols, zeros3, tracker)
+    for _ in range(5):
+        step.prepare(vols, zeros3, tracker)
     ep1.record(st)
     torch.cuda.synchronize()
-    ms_prep = ep0.elapsed_time(ep1)
+    ms_prep = ep0.elapsed_time(ep1) / 5
     if world > 1:
         t3 = torch.tensor([ms3], device=dev)
         dist.all_reduce(t3, op=dist.ReduceOp.MAX)
@@ -414,12 +527,8 @@ def run_ours(args):
     alternations = {"value": world * B / (ms3 * 1e-3), "unit": "subtomograms/s", "alternations": 3,
                     "ms_per_batch": ms3, "runs": n3, "prepare_ms_per_alternation": ms_prep,
                     "median_rot_err_deg": float(np.median(err3)), "p90_rot_err_deg": float(np.percentile(err3, 90))}
-    # accuracy of one more chosen-path step on the full batch (the pieces of the end-to-end
-    # runs overwrote the step's output buffers)
-    tracker.copy_(ident)
-    out = one()
-    al, be, ga = (out[k].cpu().numpy() for k in ("alpha", "beta", "gamma"))
-    err = rotation_error_deg(al, be, ga, q_true)
+    err = rotation_error_deg(chosen["alpha"], chosen["beta"], chosen["gamma"], q_true)
+    fp32_peak = fp32_peak_tflops(dev)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -429,17 +538,15 @@ def run_ours(args):
     pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pp):
         peaks = json.load(open(pp))
-    # roofline of the dominant kernel, the fused passes 2+3 of the shift match's upsampled DFT
-    # (tcgen05, BF16 hi+lo split): algorithmic FLOP per subtomogram = the three split GEMM
-    # segments of pass 2 (rows U*N/2, N-tile 2U, K 2N) and pass 3 (rows U^2, U columns, K N + 2
-    # with the Nyquist pair), 2*M*N*K each; its time per launch from the events recorded
-    # around it in every timed step
-    U = int(np.ceil(UPSAMPLE * (2 * SHIFT_RADIUS + 1)))
-    flop_sub = 3 * (2 * (U * N_BOX // 2) * (2 * U) * (2 * N_BOX) + 2 * U * U * U * (N_BOX + 2))
-    t_k = shift_prof["updft_pass23"] / max(1, shift_calls)
-    achieved = flop_sub * B / (t_k * 1e-3) / 1e12 if t_k > 0 else None
+    table, kernel_ms = kernel_table(prof, args.steps, B, peaks, fp32_peak)
+    if plain is not None:
+        plain["kernels"], _ = kernel_table({k: {"ms": v * n32, "launches": prof32[k]["launches"]}
+                                            for k, v in plain["kernels_ms_per_step"].items()}, n32, B, peaks, fp32_peak)
+        del plain["kernels_ms_per_step"]
+    top = max(table, key=lambda k: table[k]["ms_per_step"])
+    row = table[top]
+    dram = DRAM_BYTES_PER_SUBTOMO.get(top)
     clocks = clk.summary()
-    peak = float(peaks.get("bf16_tflops_sustained", 1400.0))
     line = {
         "metric": METRIC,
         "value": world * B / (ms * 1e-3),
@@ -451,36 +558,56 @@ def run_ours(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": "f32+bf16x3",
+        "precision": "expansion and upsampled-DFT GEMMs as BF16 hi+lo splits (3 MMAs, FP32 accumulation) on "
+                     "tcgen05; FP32 elsewhere; FP64 Newton 3x3 solve",
         "data": "synthetic",
         "config": {"workload": f"{B} subtomograms 64^3, L=32, march 8/16/24/32, C=10, 1 Newton step, "
                                f"shift r=5 uf=8, 0 dB", "batch_per_gpu": B, "box": N_BOX, "L": L_MAX,
                    "parallelism": f"replicas x{world}", "l2": "inputs 1.05 GB per step > 126 MB L2"},
         "median_rot_err_deg": float(np.median(err)),
         "p90_rot_err_deg": float(np.percentile(err, 90)),
-        "stages_ms": stages,
-        "roofline": {"kernel": "updft23_tc_kernel", "bound": "tensor", "achieved": achieved, "peak": peak,
-                     "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
-                     "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (kernel timed inside long steps)",
-                     "kernel_ms": t_k, "flop_per_subtomogram": flop_sub,
-                     "traffic": (UPDFT23_DRAM_BYTES_PER_SUBTOMO * B) if UPDFT23_DRAM_BYTES_PER_SUBTOMO else None,
-                     "traffic_unit": "bytes per launch"},
-        "shift_kernel_ms_per_step": {k: v / max(1, shift_calls) for k, v in shift_prof.items()},
+        "roofline": {"kernel": top, "bound": {"hbm": "hbm", "tensor": "tensor", "fp32": "fp32"}[row["bound"]],
+                     "achieved": row["achieved"], "peak": row["peak"], "unit": row["unit"], "frac": row["frac"],
+                     "peak_source": "MEASURED_PEAKS.json (hbm_gbs copy bandwidth / bf16_tflops_sustained); "
+                                    "fp32: cuBLAS SGEMM measured in this run",
+                     "kernel_ms": row["ms_per_step"],
+                     "traffic": (dram * B) if dram else None, "traffic_unit": "bytes per launch"},
+        "kernels": table,
+        "kernel_ms_per_step": kernel_ms,
+        "fp32_sgemm_tflops": fp32_peak,
         "plain_fp32": plain,
         "three_alternations": alternations,
+        "one_alternation_with_preparation": {"ms_per_step": ms + ms_prep,
+                                             "value": world * B / ((ms + ms_prep) * 1e-3)},
         "e2e": {"value": world * B / (e2e_ms * 1e-3), "unit": "subtomograms/s",
                 "h2d_bytes_per_step": int(B * N_BOX ** 3 * 4), "d2h_bytes_per_step": int(B * 8 * 4)},
-        "gpu_launches": KERNELS_PER_STEP * args.steps,
+        "gpu_launches": int(launches),
+        "profile_dropped_launches": dropped,
         "clocks": clocks,
     }
     if not args.no_cpu_baseline and world == 1:
         try:
-            import torch as _t
-
-            sec, _ = cpu_align(args.cpu_sample, template, vols[: args.cpu_sample].cpu().numpy(), q_true)
+            n = args.cpu_sample
+            sample_vols = vols[:n].cpu().numpy()
+            sec, o32 = cpu_align(n, template, sample_vols, np.float32)
+            _, o64 = cpu_align(n, template, sample_vols, np.float64)
             line["cpu_baseline"] = {"value": 1.0 / sec, "unit": "subtomograms/s", "cores": os.cpu_count(),
-                                    "kind": "port", "sample": f"{args.cpu_sample} subtomograms through the oracle "
-                                                              f"(folded exact FLE, sigma, grid, march, shift)"}
+                                    "kind": "port", "sample": f"{n} subtomograms of the batch through the oracle "
+                                                              f"(FP64 expansion, FP32 search, shift match)"}
+            acc = {"sample": n, "ref_median_rot_err_deg": float(np.median(rotation_error_deg(
+                o32["alpha"], o32["beta"], o32["gamma"], q_true[:n]))),
+                   "ref_fp64_median_rot_err_deg": float(np.median(rotation_error_deg(
+                       o64["alpha"], o64["beta"], o64["gamma"], q_true[:n]))),
+                   "ref_fp32_vs_fp64_max_deg": float(euler_dev_deg(o32["alpha"], o32["beta"], o32["gamma"],
+                                                                   o64["alpha"], o64["beta"], o64["gamma"]).max()),
+                   "chosen": accuracy_vs_oracle(chosen, o32, o64, q_true, n)}
+            if plain_out is not None:
+                acc["plain_fp32"] = accuracy_vs_oracle(plain_out, o32, o64, q_true, n)
+            line["accuracy_vs_reference"] = acc
+            line["ref_median_rot_err_deg"] = acc["ref_median_rot_err_deg"]
+            line["median_dev_vs_ref_deg"] = acc["chosen"]["median_dev_vs_ref_deg"]
+            line["frac_within_0p05deg"] = acc["chosen"]["frac_within_0p05deg"]
         except Exception as exc:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "unit": "subtomograms/s", "cores": os.cpu_count(),
                                     "kind": "port", "sample": f"failed: {exc!r}"[:200]}
@@ -488,33 +615,23 @@ def run_ours(args):
 
 
 def run_reference(args):
+    """The oracle restatement of the reference's alternation on the host cores, on the first
+    ``--cpu-sample`` subtomograms of the same batch the GPU arm aligns (same generator, same
+    seeds, built on the CPU)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    import torch
+
+    torch.set_num_threads(os.cpu_count() or 1)
     rng = np.random.default_rng(args.seed)
     template = make_template(rng)
     sample = max(1, args.cpu_sample)
-    # inputs: rotated, noisy subtomograms made on the host (no GPU on this arm)
-    from scipy.ndimage import map_coordinates
-    from scipy.spatial.transform import Rotation as R
-
-    q = rng.standard_normal((sample, 4))
-    q /= np.linalg.norm(q, axis=1, keepdims=True)
-    g = np.linspace(-1, 1, N_BOX + 1)
-    wg, hg, dg = np.meshgrid(g, g, g, indexing="ij")
-    coords = np.stack([dg.ravel(), hg.ravel(), wg.ravel()], 0)
-    vols = np.zeros((sample, N_BOX, N_BOX, N_BOX), dtype=np.float32)
-    tp = np.pad(template, ((0, 1), (0, 1), (0, 1)))
-    for i in range(sample):
-        rc = R.from_quat(np.roll(q[i], -1)).as_matrix() @ coords
-        idx = (rc + 1) / 2 * N_BOX  # align_corners=True over N+1 samples
-        v = map_coordinates(tp, [idx[2], idx[1], idx[0]], order=1, mode="constant").reshape(N_BOX + 1, N_BOX + 1,
-                                                                                              N_BOX + 1)
-        v = v[:N_BOX, :N_BOX, :N_BOX]
-        vols[i] = v + rng.standard_normal(v.shape) * np.sqrt((v ** 2).mean())
+    vols, q, _ = make_batch(template, np.random.default_rng(args.seed + 1), args.batch, "cpu", count=sample)
+    vols = vols.numpy()
     times = []
     for it in range(args.warmup + args.steps):
-        sec, _ = cpu_align(sample, template, vols, q)
+        sec, _ = cpu_align(sample, template, vols)
         if it >= args.warmup:
             times.append(sec)
     per = float(np.mean(times))
@@ -537,7 +654,8 @@ def run_reference(args):
                                f"shift r=5 uf=8, 0 dB", "batch_per_gpu": args.batch, "box": N_BOX, "L": L_MAX,
                    "parallelism": "host cores"},
         "cpu_baseline": {"value": value, "unit": "subtomograms/s", "cores": os.cpu_count(), "kind": "port",
-                         "sample": f"{sample} subtomograms per step through the oracle restatement"},
+                         "sample": f"the first {sample} subtomograms of the batch per step through the oracle "
+                                   f"restatement (FP64 expansion, FP32 search, shift match)"},
         "e2e": {"value": value, "unit": "subtomograms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -556,7 +674,7 @@ def run_highband(args):
     template = make_template(rng, N=N, n_blobs=1500, window=12)
     vols, q_true, _ = make_batch(template, np.random.default_rng(args.seed + 1), B, dev, snr_db=-5.0, max_shift=8.0)
     step = AlignmentStep(StepConfig(N=N, L=L, Li=[16, 32, 48], batch=B, shift_search_radius=8,
-                                    shift_upsample_factor=8), dev)
+                                    shift_upsample_factor=8, precision="auto"), dev)
     step.set_template(template)
     ident = torch.zeros((B, 4), device=dev, dtype=torch.float64)
     ident[:, 0] = 1
@@ -590,8 +708,9 @@ def run_highband(args):
         "value": B / (ms * 1e-3), "unit": "subtomograms/s", "ms_per_alternation": ms, "steps": n,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{B} subtomograms 128^3, L=64, march 16/32/48/64, C=10, 1 Newton step, "
-                               f"shift r=8 uf=8, -5 dB, 1500 blobs", "precision": "bf16x3 expansion, "
-                               "fp32 upsampled DFT (box 128 is outside the tensor-core shift kernels)"},
+                               f"shift r=8 uf=8, -5 dB, 1500 blobs",
+                   "precision": f"expansion {step.correlator.fle.precision}, upsampled DFT "
+                                f"{step.shifter.effective_precision}"},
         "median_rot_err_deg": float(np.median(err1)), "p90_rot_err_deg": float(np.percentile(err1, 90)),
         "three_alternations": {"ms_per_batch": ms3, "value": B / (ms3 * 1e-3),
                                "median_rot_err_deg": float(np.median(err3)),

@@ -107,9 +107,11 @@ int mtb_search_orientations(mtb_search* h, const float* sigma, int64_t sigma_str
  * cudaMalloc/cudaFree implies.  It needs no handle and calls no allocator: its tables and
  * its candidate workspace live in one file-scope device array of
  * MTB_SEARCH_STATIC_SCRATCH_BYTES, which every GPU that loads this library holds until
- * the process exits.  The first call on a device looks up that array's device address
- * (once per device, with the device current); make that first call before any stream
- * capture.  All calls share the array: calls that can overlap on the GPU (different
+ * the process exits.  Each call looks up that array's device address on the current device
+ * (cudaGetSymbolAddress, which allocates nothing); the first lookup on a device loads the
+ * library's device code there, so make the first call on a device before any stream
+ * capture.  A device reset discards the array's contents, which every call rebuilds anyway.
+ * All calls share the array: calls that can overlap on the GPU (different
  * streams, or threads without ordering between them) race with each other and must be
  * serialised by the caller.  The tables are rebuilt and every workspace entry is written
  * by each call before it is read.  Returns MTB_ERR_ARG when B x candidates (with the grid
@@ -193,8 +195,16 @@ int mtb_sigma_upto(mtb_fle* h, const float* coeffs, int64_t coeff_stride, const 
                    int lmax_out, float* sigma, int64_t sigma_stride, mtb_stream_t stream);
 
 /* Synchronises stream and returns MTB_ERR_TIMEOUT if a bounded device-side wait of the
- * tensor-core path gave up since the handle was created (then its results are invalid). */
+ * tensor-core path gave up since the last call (then the results of the forwards in between
+ * are invalid); the flag is cleared once reported, and the handle stays usable. */
 int mtb_fle_status(mtb_fle* h, mtb_stream_t stream);
+
+/* Test hook of the failure path (no counterpart in the reference): with on != 0 the
+ * tensor-core GEMM of every following forward issues no operand loads, so its MMA thread's
+ * bounded wait runs out after about 20 ms; the kernel records the error, frees its tensor
+ * memory and returns, and mtb_fle_status reports MTB_ERR_TIMEOUT.  Nothing faults or hangs.
+ * MTB_ERR_ARG on an FP32 handle. */
+int mtb_fle_inject_stall(mtb_fle* h, int on);
 
 /* ------------------------------------------------------------------------------
  * FFT shift match (RELION-style masked correlation with a local upsampled DFT).
@@ -210,11 +220,14 @@ typedef struct {
   float mask_radius;     /* box_size / (2 voxel_size), setup_utils.py:292-295; <0: N/2 */
   float cosine_width;    /* 5.0 in the reference (setup_utils.py:295)               */
   int precision;         /* MTB_SHIFT_FP32: upsampled DFT on CUDA cores; MTB_SHIFT_BF16X3:
-                            tcgen05 BF16 GEMMs with a hi+lo split (needs N % 32 == 0)  */
+                            tcgen05 BF16 GEMMs with a hi+lo split, MTB_ERR_ARG from create on a
+                            box / upsampled region the tensor-core kernels do not cover;
+                            MTB_SHIFT_AUTO: the tensor cores where they cover it, else FP32 */
 } mtb_shift_config;
 
 #define MTB_SHIFT_FP32 0
 #define MTB_SHIFT_BF16X3 1
+#define MTB_SHIFT_AUTO 2
 
 typedef struct mtb_shift mtb_shift;
 
@@ -231,6 +244,10 @@ int mtb_shift_set_reference(mtb_shift* h, const float* ref_fourier, mtb_stream_t
  * float32 or NULL.  shift_xyz (B, 3) and score (B,) float32 out. */
 int mtb_shift_search(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot,
                      const float* ctf, int B, float* shift_xyz, float* score, mtb_stream_t stream);
+
+/* The precision a handle runs the upsampled DFT in (MTB_SHIFT_FP32 or MTB_SHIFT_BF16X3):
+ * what MTB_SHIFT_AUTO resolved to.  No counterpart in the reference (a query of this build). */
+int mtb_shift_precision(const mtb_shift* h, int* precision);
 
 /* Synchronises stream; MTB_ERR_TIMEOUT if a bounded device-side wait of the tensor-core
  * path gave up since the handle was created (then its results are invalid). */
@@ -308,6 +325,21 @@ int mtb_pack_results(const float* rotation_score, const float* shift_score, cons
  * volumes or work. */
 int mtb_prepare_subtomos(const float* volumes, int B, int N, const float* shift_xyz, const double* tracker,
                          float mask_radius, float* work, double* stats, float* out, mtb_stream_t stream);
+
+/* Library-wide launch timing (no counterpart in the reference; instrumentation).
+ * mtb_profile_start(max_launches) creates 2 * max_launches CUDA events on the current device
+ * and switches recording on: from then on every hot-path kernel launch of the library is
+ * bracketed by two events on its stream, until max_launches launches have been recorded (the
+ * rest are counted as dropped).  mtb_profile_stop switches recording off and keeps what was
+ * recorded; mtb_profile_read synchronises on the recorded events and returns, per kernel name
+ * in first-launch order, the summed device time (ms) and the number of launches: names is
+ * max_entries * MTB_PROFILE_NAME_LEN bytes (NUL-terminated names), ms and launches have
+ * max_entries entries, *n_entries the kernels found and *dropped the launches not recorded.
+ * mtb_profile_start again clears the record.  Not for use during stream capture. */
+#define MTB_PROFILE_NAME_LEN 64
+int mtb_profile_start(int max_launches);
+int mtb_profile_stop(void);
+int mtb_profile_read(int max_entries, char* names, float* ms, int* launches, int* n_entries, int* dropped);
 
 #ifdef __cplusplus
 }

@@ -25,6 +25,7 @@ MTB_FLE_FP32 = 0
 MTB_FLE_BF16X3 = 1
 MTB_SHIFT_FP32 = 0
 MTB_SHIFT_BF16X3 = 1
+MTB_SHIFT_AUTO = 2
 MTB_SEARCH_COMPAT_TOP_BLOCK = 1
 MTB_SEARCH_GRADIENT_STEP = 2
 
@@ -87,10 +88,12 @@ SIGNATURES = {
     "mtb_sigma": (_I, [_P, _P, _I64, _P, _I, _P, _I64, _P]),
     "mtb_sigma_upto": (_I, [_P, _P, _I64, _P, _I, _I, _P, _I64, _P]),
     "mtb_fle_status": (_I, [_P, _P]),
+    "mtb_fle_inject_stall": (_I, [_P, _I]),
     "mtb_shift_create": (_I, [ctypes.POINTER(MtbShiftConfig), ctypes.POINTER(_P)]),
     "mtb_shift_destroy": (None, [_P]),
     "mtb_shift_set_reference": (_I, [_P, _P, _P]),
     "mtb_shift_status": (_I, [_P, _P]),
+    "mtb_shift_precision": (_I, [_P, _P]),
     "mtb_shift_profile": (_I, [_P, _I]),
     "mtb_shift_profile_read": (_I, [_P, _P, _P]),
     "mtb_shift_search": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P]),
@@ -102,7 +105,11 @@ SIGNATURES = {
     "mtb_read_mrc": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P]),
     "mtb_pack_results": (_I, [_P, _P, _P, _P, _P, _I, _P, _P]),
     "mtb_prepare_subtomos": (_I, [_P, _I, _I, _P, _P, ctypes.c_float, _P, _P, _P, _P]),
+    "mtb_profile_start": (_I, [_I]),
+    "mtb_profile_stop": (_I, []),
+    "mtb_profile_read": (_I, [_I, _P, _P, _P, _P, _P]),
 }
+MTB_PROFILE_NAME_LEN = 64
 
 
 def lib_path() -> str:
@@ -154,3 +161,29 @@ def ptr(t: torch.Tensor | None) -> int | None:
 def require_cuda(t: torch.Tensor, name: str) -> None:
     if not t.is_cuda:
         raise RuntimeError(f"{name} must be a CUDA tensor: matcha_b200 runs on the GPU only")
+
+
+def profile_start(max_launches: int) -> None:
+    """Switch on the library's launch timing (``mtb_profile_start``): every hot-path kernel
+    launch from now on is bracketed by CUDA events on its stream, up to ``max_launches``."""
+    check(load().mtb_profile_start(int(max_launches)), "mtb_profile_start")
+
+
+def profile_stop() -> None:
+    check(load().mtb_profile_stop(), "mtb_profile_stop")
+
+
+def profile_read(max_entries: int = 64) -> tuple[dict, int]:
+    """Per kernel name, in first-launch order: {"ms": summed device time, "launches": n};
+    and the number of launches that found the event pool full.  Synchronises."""
+    names = ctypes.create_string_buffer(max_entries * MTB_PROFILE_NAME_LEN)
+    ms = (ctypes.c_float * max_entries)()
+    launches = (ctypes.c_int * max_entries)()
+    n, dropped = ctypes.c_int(0), ctypes.c_int(0)
+    check(load().mtb_profile_read(max_entries, names, ms, launches, ctypes.byref(n), ctypes.byref(dropped)),
+          "mtb_profile_read")
+    out = {}
+    for k in range(n.value):
+        raw = names.raw[k * MTB_PROFILE_NAME_LEN:(k + 1) * MTB_PROFILE_NAME_LEN]
+        out[raw.split(b"\0", 1)[0].decode()] = {"ms": float(ms[k]), "launches": int(launches[k])}
+    return out, int(dropped.value)

@@ -40,21 +40,38 @@ def needs_build() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> str:
-    if not force and not needs_build():
-        return LIB
-    os.makedirs(LIB_DIR, exist_ok=True)
-    tmp = LIB + ".tmp"
-    cmd = [nvcc_path(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
-           "-I", os.path.join(ROOT, "include"), "-o", tmp, *sources(), "-lcuda"]
+def _compile(src: str, obj: str, verbose: bool):
+    cmd = [nvcc_path(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-c",
+           "-I", os.path.join(ROOT, "include"), "-o", obj, src]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    return src, res
+
+
+def build(verbose: bool = False, force: bool = False) -> str:
+    """Compile every source to an object in matcha_b200/_build (in parallel), then link."""
+    if not force and not needs_build():
+        return LIB
+    from concurrent.futures import ThreadPoolExecutor
+
+    os.makedirs(LIB_DIR, exist_ok=True)
+    obj_dir = os.path.join(PKG, "_build")
+    os.makedirs(obj_dir, exist_ok=True)
+    srcs = sources()
+    objs = [os.path.join(obj_dir, os.path.basename(s) + ".o") for s in srcs]
+    with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 1)) as ex:
+        results = list(ex.map(lambda so: _compile(so[0], so[1], verbose), zip(srcs, objs)))
+    for src, res in results:
+        if res.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {os.path.basename(src)}:\n" + res.stdout + res.stderr)
+        if verbose:
+            print(os.path.basename(src), res.stdout + res.stderr)
+    tmp = LIB + ".tmp"
+    cmd = [nvcc_path(), *ARCH, "-shared", "-o", tmp, *objs, "-lcuda"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
-    if verbose:
-        print(res.stdout + res.stderr)
+        raise RuntimeError("nvcc link failed:\n" + res.stdout + res.stderr)
     os.replace(tmp, LIB)
     return LIB
 

@@ -31,7 +31,7 @@ class CrossCorrelationMatcher:
     def __init__(self, N: int, device: torch.device, expansion_epsilon: float = 1e-4, batchsize: int = 1,
                  reduce_memory: bool = True, bandlimit: int = None, micro_batch_split: int = 2,
                  dtype=torch.float32, radius: int = None, jl_zeros_path: str = None, cs_path: str = None,
-                 precision_mode: str = "accurate", precision: str = "fp32"):
+                 precision_mode: str = "accurate", precision: str = None):
         self.N = N
         self.fle_basis_eps = expansion_epsilon
         self.batchsize = batchsize
@@ -67,8 +67,14 @@ class CrossCorrelationMatcher:
         """Expand the template (N, N, N); keeps its coefficients and norm (:117-130)."""
         t = torch.from_numpy(np.ascontiguousarray(template_data).copy()).to(dtype=torch.float32, device=self.device)
         a, norms = self.fle._forward(t.unsqueeze(0), True)
-        self.template_coefficients_alphas_torch = F.pad(a[0], (0, 1))
-        self.bh_norm_template = norms[0]
+        coeffs = F.pad(a[0], (0, 1))
+        if self.template_coefficients_alphas_torch is None:
+            self.template_coefficients_alphas_torch = coeffs
+            self.bh_norm_template = norms[0].clone()
+        else:
+            # in place: a CUDA graph captured earlier (AlignmentStep.capture) reads these addresses
+            self.template_coefficients_alphas_torch.copy_(coeffs)
+            self.bh_norm_template.copy_(norms[0])
 
     @torch.no_grad()
     def get_sigma(self, volumes: torch.Tensor):

@@ -116,7 +116,7 @@ class FLEBasis3D:
     def __init__(self, N, bandlimit, eps, maxitr=None, maxfun=None, max_l=None, mode="complex",
                  sph_harm_solver="nvidia_torch", reduce_memory=True, batchsize=1, radius=1, device="cuda",
                  dtype=torch.complex128, jl_zeros_path="jl_zeros_l=3000_k=2500.mat",
-                 cs_path="cs_l=3000_k=2500.mat", precision_mode="accurate", precision="fp32"):
+                 cs_path="cs_l=3000_k=2500.mat", precision_mode="accurate", precision=None):
         if mode not in ("complex", "real"):
             raise AssertionError("mode must be 'real' or 'complex'")
         if mode == "real":
@@ -130,6 +130,10 @@ class FLEBasis3D:
         self.dtype = dtype
         self.precision_mode = precision_mode
         self.eps = eps
+        if precision is None:
+            # the reference's "fast" mode accepts a 1e-4 transform (its NUFFT tolerance); the BF16
+            # hi+lo split GEMM is within that, the FP32 CUDA-core GEMM is the "accurate" path
+            precision = "bf16x3" if str(precision_mode).strip().lower() == "fast" else "fp32"
         if precision not in ("fp32", "bf16x3"):
             raise ValueError("precision must be 'fp32' (CUDA cores) or 'bf16x3' (tensor cores, hi+lo split)")
         self.precision = precision

@@ -1,11 +1,18 @@
 """Drop-in ``ShiftMatcher`` (src/matcha/core/ShiftMatcher.py) on the B200 kernels.
 
-``set_reference`` keeps the reference's once-per-template preparation on the host
-(``load_reference_full``: soft low-pass, gridding correction, centred FFT, spherical
-Fourier mask, FFT shift; ShiftMatcher.py:377-472) and uploads the result.
+``set_reference`` computes the reference's once-per-template preparation
+(``load_reference_full``: soft low-pass, gridding correction, centred FFT, spherical Fourier
+mask, FFT shift; ShiftMatcher.py:377-472) on the device in FP64 (``mtb_shift_reference``).
 ``search_shifts`` turns each rotation tracker into the reference's ZYZ rotation matrix
-on the host (ShiftMatcher.py:503, :913) and runs the whole per-subtomogram shift match
-in ``mtb_shift_search``.
+(ShiftMatcher.py:503, :913; on the device when the tracker is a CUDA tensor) and runs the
+whole per-subtomogram shift match in ``mtb_shift_search``.
+
+Precision of the upsampled DFT: ``precision="fp32"`` (CUDA cores), ``"bf16x3"`` (tcgen05 with
+a BF16 hi+lo split; ValueError on a box / upsampled region the tensor-core kernels do not
+cover) or ``"auto"`` (the tensor cores where they cover the geometry, FP32 elsewhere;
+``effective_precision`` says which ran).  Without the argument it comes from the config: the
+namespaced key ``b200: {precision: ...}`` if present, else the reference's ``precision_mode``
+("fast" -> "auto", "accurate" -> "fp32").
 """
 from __future__ import annotations
 
@@ -16,69 +23,6 @@ import torch
 from scipy.spatial.transform import Rotation as R
 
 from .. import _native as nat
-
-
-# ---------------------------------------------------------------- host preparation
-def apply_soft_mask(Irefs, ori_size, pixel_size, ini_high, width_fmask_edge=6.0):
-    """Cosine-edged low-pass in Fourier space (ShiftMatcher.py:377-408)."""
-    if ini_high <= 0:
-        return Irefs
-    radius = ori_size * pixel_size / ini_high - width_fmask_edge / 2.0
-    radius_p = radius + width_fmask_edge
-    out = []
-    for vol in Irefs:
-        ft = np.fft.fftshift(np.fft.fftn(vol, norm="forward"))
-        zd, yd, xd = vol.shape
-        zz, yy, xx = np.indices(vol.shape)
-        r = np.sqrt((xx - xd // 2) ** 2 + (yy - yd // 2) ** 2 + (zz - zd // 2) ** 2)
-        mask = np.ones_like(r)
-        mask[r > radius_p] = 0
-        tz = (r >= radius) & (r <= radius_p)
-        mask[tz] = 0.5 - 0.5 * np.cos(np.pi * (radius_p - r[tz]) / width_fmask_edge)
-        ft *= mask
-        out.append(np.fft.ifftn(np.fft.ifftshift(ft), norm="forward").real.astype(np.float64))
-    return out
-
-
-def gridding_correct(vol_in, ori_size, padding_factor, interpolator, r_min_nn=0):
-    """Divide by sinc^2 (trilinear) or sinc (nearest) of the radius (ShiftMatcher.py:411-439)."""
-    z, y, x = vol_in.shape
-    kk, ii, jj = np.meshgrid(np.arange(-z // 2, z // 2), np.arange(-y // 2, y // 2), np.arange(-x // 2, x // 2),
-                             indexing="ij")
-    rval = np.sqrt(kk ** 2 + ii ** 2 + jj ** 2) / (ori_size * padding_factor)
-    sinc = np.ones_like(rval)
-    nz = rval > 0
-    sinc[nz] = np.sin(np.pi * rval[nz]) / (np.pi * rval[nz])
-    if interpolator == "nearest" and r_min_nn == 0:
-        corr = sinc
-    elif interpolator == "trilinear" or (interpolator == "nearest" and r_min_nn > 0):
-        corr = sinc ** 2
-    else:
-        raise ValueError("Unrecognized interpolator: must be 'nearest' or 'trilinear'")
-    corr[corr == 0] = 1.0
-    return vol_in / corr
-
-
-def get_mask_full(shape):
-    """Spherical mask on FFT index coordinates (ShiftMatcher.py:442-453)."""
-    nz, ny, nx = shape
-    cz, cy = nz // 2, ny // 2
-    Z, Y, X = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
-    kp = np.where(Z < cz, Z, Z - nz)
-    ip = np.where(Y < cy, Y, Y - ny)
-    jp = np.where(X < cy, X, X - nx)
-    return (kp ** 2 + ip ** 2 + jp ** 2) <= nz // 2 * nz // 2
-
-
-def load_reference_full(ref, volume_size, voxel_size):
-    """Fourier-domain reference used by the shift match (ShiftMatcher.py:456-472)."""
-    ref = np.asarray(ref).astype(np.float64)
-    iref = apply_soft_mask([ref], ori_size=volume_size, pixel_size=voxel_size, ini_high=4.0, width_fmask_edge=2.0)
-    g = gridding_correct(iref[0], ori_size=volume_size, padding_factor=1.0, interpolator="trilinear")
-    h = int(volume_size // 2)
-    faux = np.fft.fftn(np.roll(g, (-h, -h, -h), axis=(0, 1, 2)), norm="forward")
-    mask = np.fft.fftshift(get_mask_full(faux.shape), axes=(0, 1, 2))
-    return np.fft.fftshift(faux, axes=(0, 1, 2)) * mask
 
 
 def tracker_to_euler_deg(rotation_tracker) -> np.ndarray:
@@ -98,13 +42,29 @@ def _cfg(config, key, default=None):
         return getattr(config, key, default)
 
 
+def resolve_precision(config) -> str:
+    """Precision of the shift match from a run config: ``b200.precision`` when the namespaced
+    key is present, else from the reference's ``precision_mode`` (setup_utils.py:6-16):
+    "fast" -> "auto", anything else -> "fp32"."""
+    ns = _cfg(config, "b200", None)
+    if ns is not None:
+        p = _cfg(ns, "precision", None)
+        if p is not None:
+            return str(p)
+    mode = str(_cfg(config, "precision_mode", "accurate")).strip().lower()
+    return "auto" if mode == "fast" else "fp32"
+
+
 class ShiftMatcher:
     """Stateful shift-search wrapper (ShiftMatcher.py:766-928)."""
 
     def __init__(self, config, device: torch.device, dtype: torch.dtype, micro_batch_size: int = None,
-                 precision: str = "fp32"):
-        if precision not in ("fp32", "bf16x3"):
-            raise ValueError("precision must be 'fp32' (CUDA cores) or 'bf16x3' (tensor cores, hi+lo split)")
+                 precision: str = None):
+        if precision is None:
+            precision = resolve_precision(config)
+        if precision not in ("fp32", "bf16x3", "auto"):
+            raise ValueError("precision must be 'fp32' (CUDA cores), 'bf16x3' (tensor cores, hi+lo split) or "
+                             "'auto' (tensor cores where the geometry allows)")
         self.precision = precision
         self.config = config
         self.device = torch.device(device)
@@ -136,13 +96,23 @@ class ShiftMatcher:
         cfg.search_radius = self.radius
         cfg.mask_radius = self.mask_radius
         cfg.cosine_width = 5.0
-        cfg.precision = nat.MTB_SHIFT_BF16X3 if self.precision == "bf16x3" else nat.MTB_SHIFT_FP32
+        cfg.precision = {"fp32": nat.MTB_SHIFT_FP32, "bf16x3": nat.MTB_SHIFT_BF16X3, "auto": nat.MTB_SHIFT_AUTO}[
+            self.precision]
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             nat.check(self._lib.mtb_shift_create(ctypes.byref(cfg), ctypes.byref(h)), "mtb_shift_create")
         self._h, self._cap = h, cfg.max_batch
         self._uploaded_version = -1
         return h
+
+    @property
+    def effective_precision(self):
+        """"bf16x3" or "fp32": what the upsampled DFT runs in (None before the first search)."""
+        if self._h is None:
+            return None
+        p = ctypes.c_int()
+        nat.check(self._lib.mtb_shift_precision(self._h, ctypes.byref(p)), "mtb_shift_precision")
+        return "bf16x3" if p.value == nat.MTB_SHIFT_BF16X3 else "fp32"
 
     def status(self):
         """Raise if a bounded device-side wait of the tensor-core path gave up (synchronises)."""
@@ -180,7 +150,6 @@ class ShiftMatcher:
         if getattr(self, "_lib", None) is not None:
             self._free()
 
-    @torch.no_grad()
     @torch.no_grad()
     def set_reference(self, template_data: np.ndarray):
         """Precompute and cache the Fourier-domain reference (ShiftMatcher.py:805-822):

@@ -26,6 +26,11 @@
 
 void mtb_set_last_error(const char* msg, const char* file, int line);
 
+// Launch timing (mtb_profile_start): an event before and one after a kernel launch on its
+// stream, a no-op while recording is off.
+void mtb_prof_begin(cudaStream_t st);
+void mtb_prof_end(cudaStream_t st, const char* kernel);
+
 __host__ __device__ inline int mtb_dsize(int L) {
   // entries of D for degrees 0..L: (L+1)(2L+1)(2L+3)/3
   return L < 0 ? 0 : (L + 1) * (2 * L + 1) * (2 * L + 3) / 3;

@@ -443,17 +443,23 @@ extern "C" int mtb_fle_forward(mtb_fle* h, const float* vol, int B, float* coeff
     if (rc) return rc;
   } else {
     dim3 fg((nr + 255) / 256, B);
+    mtb_prof_begin(st);
     fold_kernel<<<fg, 256, 0, st>>>(vol, vstride, B, nr, h->rep_img, h->A, astride);
+    mtb_prof_end(st, "fold_kernel");
     MTB_LAUNCH_CHECK();
     int maxc = 0;
     for (int k = 0; k < kClasses; ++k) maxc = h->class_cols[k] > maxc ? h->class_cols[k] : maxc;
     dim3 gg((maxc + GN - 1) / GN, (B + GM - 1) / GM, kClasses);
+    mtb_prof_begin(st);
     gemm_fp32_kernel<<<gg, 256, 0, st>>>(h->A, astride, B, nr, h->d_basis, h->d_class_cols, h->C, h->cfg.n_cols,
                                          h->d_class_off);
+    mtb_prof_end(st, "gemm_fp32_kernel");
     MTB_LAUNCH_CHECK();
   }
+  mtb_prof_begin(st);
   expand_kernel<<<B, 256, 0, st>>>(h->C, h->cfg.n_cols, B, h->cfg.ne, h->col_re, h->col_im, h->s_re, h->s_im,
                                    reinterpret_cast<float2*>(coeffs), coeff_stride, norms);
+  mtb_prof_end(st, "expand_kernel");
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }
@@ -470,9 +476,11 @@ extern "C" int mtb_sigma_upto(mtb_fle* h, const float* coeffs, int64_t coeff_str
   MTB_ARG_CHECK(B <= 65535, "batch too large for one launch");
   const size_t smem = (size_t)2 * (2 * lmax_out + 1) * (h->kmax | 1) * sizeof(float2);
   MTB_CUDA_TRY(cudaFuncSetAttribute(sigma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  mtb_prof_begin((cudaStream_t)stream);
   sigma_kernel<<<dim3(lmax_out + 1, B), 256, smem, (cudaStream_t)stream>>>(
       reinterpret_cast<const float2*>(coeffs), coeff_stride, reinterpret_cast<const float2*>(tmpl), lmax_out,
       h->kpad, h->koff, h->kidx, reinterpret_cast<float2*>(sigma), sigma_stride);
+  mtb_prof_end((cudaStream_t)stream, "sigma_kernel");
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }
@@ -481,6 +489,13 @@ extern "C" int mtb_sigma(mtb_fle* h, const float* coeffs, int64_t coeff_stride, 
                          float* sigma, int64_t sigma_stride, mtb_stream_t stream) {
   MTB_ARG_CHECK(h, "null handle");
   return mtb_sigma_upto(h, coeffs, coeff_stride, tmpl, B, h->cfg.lmax, sigma, sigma_stride, stream);
+}
+
+extern "C" int mtb_fle_inject_stall(mtb_fle* h, int on) {
+  MTB_ARG_CHECK(h, "null handle");
+  MTB_ARG_CHECK(h->use_tc, "the stall hook acts on the tensor-core path only (precision MTB_FLE_BF16X3)");
+  h->tc.stall = on ? 1 : 0;
+  return MTB_OK;
 }
 
 extern "C" int mtb_fle_status(mtb_fle* h, mtb_stream_t stream) {

@@ -5,17 +5,32 @@
 //     A B ~= A_hi B_hi + A_lo B_hi + A_hi B_lo,   A_hi = bf16(A), A_lo = bf16(A - A_hi)
 // (the dropped A_lo B_lo term is ~2^-16 relative).  The three products are one GEMM over
 // a K axis three times as long: k-block j of [0, 3 KB) selects (A_hi, B_hi), (A_lo, B_hi)
-// or (A_hi, B_lo), so every pipeline stage moves one A tile and one B tile.
+// or (A_hi, B_lo), so every pipeline stage moves one A tile and one B tile.  (Staging the
+// hi and lo tiles of both operands per K block, 96 KB, leaves room for two stages only,
+// which measured 2.2x slower: the loads are no longer hidden.)
+//
+// Accumulation: the tensor core adds each K=16 product into the FP32 accumulator with a
+// truncating alignment, an error of about one unit in the last place of the accumulator per
+// instruction.  Over the full K (15 216 octant representatives at 64^3, 2 856 instructions)
+// that biases coefficients whose terms share a sign (the low degrees of a positive-mean
+// volume) by ~2e-4 relative.  So the K axis is cut into chunks of kChunkKB blocks (240
+// instructions, ~2e-5): each chunk accumulates into one of two tensor-memory buffers, and the
+// epilogue warps add the finished buffer into running sums in registers (FP32 round-to-nearest,
+// chunks in order, so the result is deterministic) while the MMAs of the next chunk run into
+// the other buffer; C is written once at the end.  (Adding each chunk into C in global memory
+// instead measured 2.4x slower: one row per lane makes every access a 32-way scatter.)
 //
 // Layout: both operands K-major bf16, 128-byte swizzled tiles staged by TMA
 // (cp.async.bulk.tensor.2d), tile M = 128 (a batch block), N = 256 (basis columns),
-// K = 64 per stage, 4 stages.  One thread issues tcgen05.mma (kind::f16, M128 N256 K16)
-// into a 256-column FP32 accumulator in tensor memory; four warps read it back with
-// tcgen05.ld and store FP32 C.  A and B of all classes and both parts share two tensor
-// maps: rows (class * 2 + part) * Mpad + m of A, (class * 2 + part) * Npad + n of B.
+// K = 64 per stage, 4 stages of 48 KB.  One thread issues tcgen05.mma (kind::f16, M128 N256
+// K16); eight warps read the accumulators back with tcgen05.ld, two per 32-lane quarter of
+// tensor memory, each keeping 128 columns of its row.  A and B of all classes and
+// both parts share two tensor maps: rows (class * 2 + part) * Mpad + m of A,
+// (class * 2 + part) * Npad + n of B.
 //
 // Every mbarrier wait is bounded; on expiry the kernel records an error code, stops
-// issuing, and still frees its tensor memory before returning.
+// issuing, waits (bounded) for the MMAs it issued, and frees its tensor memory before
+// returning.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
@@ -33,8 +48,10 @@ constexpr int STAGES = 4;
 constexpr int A_TILE = TM * TK * 2;  // 16 KB
 constexpr int B_TILE = TN * TK * 2;  // 32 KB
 constexpr int STAGE_BYTES = A_TILE + B_TILE;
-constexpr int kThreads = 192;        // warp 0: TMA, warp 1: MMA, warps 2-5: epilogue
-constexpr uint32_t kTmemCols = 256;
+constexpr int kThreads = 320;        // warp 0: TMA, warp 1: MMA, warps 2-9: epilogue
+constexpr int kEpiThreads = 256;
+constexpr uint32_t kTmemCols = 512;  // two 256-column FP32 accumulators
+constexpr int kChunkKB = 60;         // K blocks per accumulator chunk: 60 x 4 = 240 MMAs
 
 struct TcParams {
   int Mpad, Npad, KB;   // padded batch rows per (class, part), padded columns, K blocks of 64
@@ -42,7 +59,11 @@ struct TcParams {
   int ncols[8];         // valid columns per class
   int coff[8];          // column offset of the class inside C
   int ldc;              // row stride of C (floats)
+  int stall;            // test hook: no loads are issued, and waits give up after kStallPolls
 };
+
+// Poll limit of every wait while the stall hook is on: at most kStallPolls x kSuspendNs (20 ms).
+constexpr long long kStallPolls = 1 << 10;
 
 // Instruction descriptor, kind::f16: D f32, A/B bf16, both K-major, M=128, N=256.
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
@@ -59,6 +80,10 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive_cta(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
 gemm_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcParams P,
                float* __restrict__ C, int* __restrict__ err) {
@@ -67,9 +92,9 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   __shared__ __align__(8) uint64_t full_bar[STAGES];
   __shared__ __align__(8) uint64_t empty_bar[STAGES];
-  __shared__ __align__(8) uint64_t done_bar;
+  __shared__ __align__(8) uint64_t acc_full[2], acc_empty[2], drain_bar;
   __shared__ uint32_t tmem_base;
-  __shared__ int abort_flag;
+  __shared__ volatile int abort_flag;
 
   const int cls = blockIdx.z;
   // M tiles vary fastest: the CTAs of one basis N-tile run together and read its B slab from
@@ -77,13 +102,20 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
   const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
   if (n0 >= P.ncols[cls]) return;  // uniform per CTA
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int KB3 = 3 * P.KB;  // K blocks of the three hi/lo segments
+  const int nchunks = (KB3 + kChunkKB - 1) / kChunkKB;
+  const long long polls = P.stall ? kStallPolls : kSpinLimit;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
     }
-    mbar_init(&done_bar, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], kEpiThreads);
+    }
+    mbar_init(&drain_bar, 1);
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -96,66 +128,88 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
-  const int KB3 = 3 * P.KB;
 
   if (warp == 0 && lane == 0) {
-    // ---- TMA producer
-    for (int j = 0; j < KB3; ++j) {
+    // ---- TMA producer (the stall hook issues nothing, so the MMA thread's first wait runs out)
+    for (int j = 0; j < KB3 && !abort_flag && !P.stall; ++j) {
       const int s = j % STAGES;
       const uint32_t use = j / STAGES;
-      if (j >= STAGES && !mbar_wait(&empty_bar[s], (use - 1) & 1)) {
-        atomicExch(err, 1);
+      if (j >= STAGES && !mbar_wait_n(&empty_bar[s], (use - 1) & 1, polls)) {
+        atomicCAS(err, 0, 1);
         abort_flag = 1;
         break;
       }
-      if (abort_flag) break;
       const int part = j / P.KB;           // 0: (hi, hi), 1: (lo, hi), 2: (hi, lo)
       const int kb = j - part * P.KB;
       const int apart = (part == 1) ? 1 : 0, bpart = (part == 2) ? 1 : 0;
       uint8_t* sa = smem + s * STAGE_BYTES;
-      uint8_t* sb = sa + A_TILE;
       mbar_expect_tx(&full_bar[s], STAGE_BYTES);
       tma_load_2d(sa, &mapA, kb * TK, (cls * 2 + apart) * P.Mpad + m0, &full_bar[s]);
-      tma_load_2d(sb, &mapB, kb * TK, (cls * 2 + bpart) * P.Npad + n0, &full_bar[s]);
+      tma_load_2d(sa + A_TILE, &mapB, kb * TK, (cls * 2 + bpart) * P.Npad + n0, &full_bar[s]);
     }
   } else if (warp == 1 && lane == 0) {
-    // ---- MMA issuer
+    // ---- MMA issuer: chunk c of kChunkKB K blocks into accumulator c & 1
     bool ok = true;
-    for (int j = 0; j < KB3; ++j) {
-      const int s = j % STAGES;
-      const uint32_t use = j / STAGES;
-      if (!mbar_wait(&full_bar[s], use & 1)) {
-        atomicExch(err, 2);
+    int issued = 0;
+    for (int c = 0; c < nchunks && ok; ++c) {
+      const int buf = c & 1;
+      if (c >= 2 && !mbar_wait_n(&acc_empty[buf], ((c >> 1) - 1) & 1, polls)) {
+        atomicCAS(err, 0, 4);
         abort_flag = 1;
         ok = false;
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint8_t* sa = smem + s * STAGE_BYTES;
-      const uint8_t* sb = sa + A_TILE;
-      const uint64_t ad = smem_desc(sa), bd = smem_desc(sb);
+      const uint32_t d = tmem + (uint32_t)(buf * TN);
+      const int j1 = (c + 1) * kChunkKB < KB3 ? (c + 1) * kChunkKB : KB3;
+      for (int j = c * kChunkKB; j < j1; ++j) {
+        const int s = j % STAGES;
+        const uint32_t use = j / STAGES;
+        if (abort_flag || !mbar_wait_n(&full_bar[s], use & 1, polls)) {
+          atomicCAS(err, 0, 2);
+          abort_flag = 1;
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint8_t* sa = smem + s * STAGE_BYTES;
+        const uint64_t ad = smem_desc(sa), bd = smem_desc(sa + A_TILE);
 #pragma unroll
-      for (int kk = 0; kk < TK / 16; ++kk) {
-        // 16 bf16 = 32 bytes further along K inside the swizzle atom: +2 in the >>4 address field
-        mma_bf16(tmem, ad + (uint64_t)(kk * 2), bd + (uint64_t)(kk * 2), (j > 0 || kk > 0) ? 1u : 0u);
+        for (int kk = 0; kk < TK / 16; ++kk) {
+          // 16 bf16 = 32 bytes further along K inside the swizzle atom: +2 in the >>4 address field
+          mma_bf16(d, ad + (uint64_t)(kk * 2), bd + (uint64_t)(kk * 2), (j > c * kChunkKB || kk > 0) ? 1u : 0u);
+        }
+        mma_commit(&empty_bar[s]);
+        ++issued;
       }
-      mma_commit(&empty_bar[s]);
+      if (ok) mma_commit(&acc_full[buf]);
     }
-    if (ok) mma_commit(&done_bar);
+    if (!ok && issued > 0) {
+      // let the MMAs already issued finish before the tensor memory is freed
+      mma_commit(&drain_bar);
+      mbar_wait_n(&drain_bar, 0, polls);
+    }
   } else if (warp >= 2) {
-    // ---- epilogue: TMEM lanes 32*(warp%4) .. +31 hold rows m0 + that range
-    const bool ok = mbar_wait(&done_bar, 0);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!ok) {
-      atomicExch(err, 3);
-    } else {
-      const int q = warp & 3;
-      const int row = m0 + q * 32 + lane;
-      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16);
-      float* crow = C + (int64_t)row * P.ldc + P.coff[cls];
-      const int nc = P.ncols[cls];
-#pragma unroll 1
-      for (int cb = 0; cb < TN; cb += 32) {
+    // ---- epilogue: warp w reads TMEM lanes 32*(w%4) .. +31 (rows m0 + that range), columns
+    // h*128 .. +127 with h = (w-2)/4, and keeps their running sums over the chunks
+    const int q = warp & 3, h = (warp - 2) >> 2;
+    const int row = m0 + q * 32 + lane;
+    float acc[TN / 2];
+#pragma unroll
+    for (int t = 0; t < TN / 2; ++t) acc[t] = 0.f;
+    bool done = true;
+    for (int c = 0; c < nchunks; ++c) {
+      const int buf = c & 1;
+      if (abort_flag || !mbar_wait_n(&acc_full[buf], (c >> 1) & 1, polls)) {
+        atomicCAS(err, 0, 3);
+        abort_flag = 1;
+        done = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * TN + h * (TN / 2));
+#pragma unroll
+      for (int cb = 0; cb < TN / 2; cb += 32) {
         uint32_t v[32];
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -167,13 +221,19 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
               "=r"(v[30]), "=r"(v[31])
             : "r"(taddr + (uint32_t)cb));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (row < P.M) {
-          const int nb = n0 + cb;
 #pragma unroll
-          for (int t = 0; t < 32; ++t)
-            if (nb + t < nc) crow[nb + t] = __uint_as_float(v[t]);
-        }
+        for (int t = 0; t < 32; ++t) acc[cb + t] += __uint_as_float(v[t]);
       }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive_cta(&acc_empty[buf]);
+    }
+    if (done && row < P.M) {
+      float* crow = C + (int64_t)row * P.ldc + P.coff[cls];
+      const int nc = P.ncols[cls];
+      const int nb = n0 + h * (TN / 2);
+#pragma unroll
+      for (int t = 0; t < TN / 2; ++t)
+        if (nb + t < nc) crow[nb + t] = acc[t];
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -312,8 +372,10 @@ void fle_tc_release(FleTc* t) {
 int fle_tc_forward(FleTc* t, const float* vol, int64_t vol_stride, int B, const int* rep_img, float* C,
                    cudaStream_t st) {
   dim3 fg((t->Kpad + 255) / 256, B);
+  mtb_prof_begin(st);
   fold_split_kernel<<<fg, 256, 0, st>>>(vol, vol_stride, B, t->n_rep, t->Mpad, t->Kpad, rep_img,
                                         reinterpret_cast<__nv_bfloat16*>(t->A));
+  mtb_prof_end(st, "fold_split_kernel");
   MTB_LAUNCH_CHECK();
   TcParams P;
   P.Mpad = t->Mpad;
@@ -325,11 +387,14 @@ int fle_tc_forward(FleTc* t, const float* vol, int64_t vol_stride, int B, const 
     P.coff[k] = t->coff[k];
   }
   P.ldc = t->n_cols;
+  P.stall = t->stall;
   const size_t smem = (size_t)STAGES * STAGE_BYTES + 1024;
   MTB_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 gg((B + TM - 1) / TM, t->Npad / TN, 8);
+  mtb_prof_begin(st);
   gemm_tc_kernel<<<gg, kThreads, smem, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA),
                                              *reinterpret_cast<const CUtensorMap*>(t->mapB), P, C, t->err);
+  mtb_prof_end(st, "gemm_tc_kernel");
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }
@@ -338,5 +403,6 @@ int fle_tc_check(FleTc* t, cudaStream_t st) {
   int h = 0;
   MTB_CUDA_TRY(cudaMemcpyAsync(&h, t->err, sizeof(int), cudaMemcpyDeviceToHost, st));
   MTB_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h) MTB_CUDA_TRY(cudaMemsetAsync(t->err, 0, sizeof(int), st));  // reported once
   return h ? MTB_ERR_TIMEOUT : MTB_OK;
 }

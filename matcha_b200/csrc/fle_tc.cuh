@@ -12,6 +12,7 @@ struct FleTc {
   void* A;   // (8 classes x 2 parts x Mpad, Kpad) bf16
   void* B;   // (8 classes x 2 parts x Npad, Kpad) bf16
   int* err;  // nonzero after a bounded wait ran out
+  int stall; // test hook (mtb_fle_inject_stall): the producer issues no loads, waits give up early
 };
 
 // Split the FP32 class bases into bf16 hi/lo K-major operands and build the tensor maps.
@@ -21,6 +22,6 @@ void fle_tc_release(FleTc* t);
 // Fold + split the volumes, then C (B, n_cols) = sum over classes of the split GEMMs.
 int fle_tc_forward(FleTc* t, const float* vol, int64_t vol_stride, int B, const int* rep_img, float* C,
                    cudaStream_t st);
-// Synchronises st and reports MTB_ERR_TIMEOUT if a device-side wait gave up.
+// Synchronises st and reports MTB_ERR_TIMEOUT if a device-side wait gave up (then clears it).
 int fle_tc_check(FleTc* t, cudaStream_t st);
 size_t fle_tc_a_elems(int max_batch, int n_rep);

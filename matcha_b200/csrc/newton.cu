@@ -456,8 +456,10 @@ int newton_eval_launch(const float* sigma, int64_t stride, int B, int Li, const 
                        const float* gamma, const double* Ctab, const float4* coef, float* out, cudaStream_t st) {
   MTB_ARG_CHECK(Li >= 0 && Li <= kNewtonMaxL, "degree exceeds the Newton march limit");
   if (B == 0) return MTB_OK;
+  mtb_prof_begin(st);
   score_derivs_kernel<<<B, kNT, 0, st>>>(reinterpret_cast<const float2*>(sigma), stride, alpha, beta, gamma, Li,
                                          Ctab, coef, out);
+  mtb_prof_end(st, "score_derivs_kernel");
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }
@@ -483,19 +485,24 @@ int newton_launch(const float* sigma, int64_t stride, int B, int C, float* a, fl
   // two candidates of a subtomogram per CTA share its folded-sigma and recurrence-factor loads
   const bool pair = (C % 2) == 0;
   if (fold) {
+    mtb_prof_begin(st);
     fold_sigma_kernel<<<dim3(P.Lmax + 1, B), 256, 0, st>>>(sg, stride, nf, fold);
+    mtb_prof_end(st, "fold_sigma_kernel");
     MTB_LAUNCH_CHECK();
+    mtb_prof_begin(st);
     if (pair)
       newton_march_kernel<true, 2><<<BC / 2, kNT, 0, st>>>(fold, nf, sg, stride, BC, C, a, b, g, s, Ctab, coef, P);
     else
       newton_march_kernel<true, 1><<<BC, kNT, 0, st>>>(fold, nf, sg, stride, BC, C, a, b, g, s, Ctab, coef, P);
   } else {
+    mtb_prof_begin(st);
     if (pair)
       newton_march_kernel<false, 2><<<BC / 2, kNT, 0, st>>>(nullptr, nf, sg, stride, BC, C, a, b, g, s, Ctab, coef,
                                                              P);
     else
       newton_march_kernel<false, 1><<<BC, kNT, 0, st>>>(nullptr, nf, sg, stride, BC, C, a, b, g, s, Ctab, coef, P);
   }
+  mtb_prof_end(st, "newton_march_kernel");
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }

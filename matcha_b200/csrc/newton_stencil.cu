@@ -368,7 +368,9 @@ int launch(const float2* sigma, int64_t stride, int BC, int C, float* a, float* 
            const double* Ctab, const NewtonParams& P, cudaStream_t st) {
   const size_t smem = stencil_smem_bytes(P.Lmax);
   MTB_CUDA_TRY(cudaFuncSetAttribute(newton_march_kernel<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  mtb_prof_begin(st);
   newton_march_kernel<KP><<<BC, kNT, smem, st>>>(sigma, stride, BC, C, a, b, g, s, Ctab, P);
+  mtb_prof_end(st, "newton_march_stencil_kernel");
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }

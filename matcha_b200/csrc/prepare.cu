@@ -331,17 +331,21 @@ template <int NT>
 int launch(const float* volumes, int B, int N, const float* shift_xyz, const double* tracker, int thresh, bool box,
            int skip2, int inner2, double inv_count, float2* work, double* stats, float* out, cudaStream_t st) {
   const size_t ext_smem = (size_t)N * N * sizeof(float) + (size_t)N * sizeof(Axis);
+  mtb_prof_begin(st);
   if (ext_smem <= 48 * 1024)
     extract_staged_kernel<NT><<<dim3(N, B), kPT, ext_smem, st>>>(volumes, N, shift_xyz, thresh, work, stats);
   else
     extract_kernel<NT><<<dim3(N, B), kPT, (size_t)N * sizeof(Axis), st>>>(volumes, N, shift_xyz, thresh, work,
                                                                           stats);
+  mtb_prof_end(st, "extract_kernel");
   MTB_LAUNCH_CHECK();
   const dim3 grid((N + kZW - 1) / kZW, B);
+  mtb_prof_begin(st);
   if (box)
     rotate_kernel<NT, true><<<grid, kPT, 0, st>>>(work, N, tracker, stats, inv_count, thresh, skip2, inner2, out);
   else
     rotate_kernel<NT, false><<<grid, kPT, 0, st>>>(work, N, tracker, stats, inv_count, thresh, skip2, inner2, out);
+  mtb_prof_end(st, "rotate_kernel");
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }

@@ -44,8 +44,10 @@ extern "C" int mtb_pack_results(const float* rotation_score, const float* shift_
   MTB_ARG_CHECK(B >= 0, "negative batch");
   if (B == 0) return MTB_OK;
   MTB_ARG_CHECK(rotation_score && shift_score && local_shift && prior_shift && tracker && out, "null pointer");
+  mtb_prof_begin((cudaStream_t)stream);
   pack_results_kernel<<<(B + 127) / 128, 128, 0, (cudaStream_t)stream>>>(rotation_score, shift_score, local_shift,
                                                                           prior_shift, tracker, B, out);
+  mtb_prof_end((cudaStream_t)stream, "pack_results_kernel");
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }

@@ -293,8 +293,10 @@ int grid_launch_t(const float2* sigma, int64_t stride, int B, const float* dtab,
   const size_t smem = grid_smem_bytes(L0, K);
   MTB_CUDA_TRY(cudaFuncSetAttribute(so3_grid_topk_kernel<L0T, NT, KC>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  mtb_prof_begin(st);
   so3_grid_topk_kernel<L0T, NT, KC><<<B, kGridThreads, smem, st>>>(sigma, stride, B, dtab, L0, 2 * L0 * K, C,
                                                                grid_jb(L0, K), a, b, g, grid);
+  mtb_prof_end(st, "so3_grid_topk_kernel");
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }
@@ -513,8 +515,10 @@ extern "C" int mtb_search_orientations(mtb_search* h, const float* sigma, int64_
   if (rc) return rc;
   rc = mtb_newton_march(h, sigma, sigma_stride, B, ca, cb, cg, cs, stream);
   if (rc) return rc;
+  mtb_prof_begin((cudaStream_t)stream);
   reduce_candidates_kernel<<<(B + 127) / 128, 128, 0, (cudaStream_t)stream>>>(ca, cb, cg, cs, B, C, alpha,
                                                                                beta, gamma, score);
+  mtb_prof_end((cudaStream_t)stream, "reduce_candidates_kernel");
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }
@@ -525,16 +529,10 @@ extern "C" int mtb_search_orientations(mtb_search* h, const float* sigma, int64_
 // (grid d-table, recurrence start coefficients) and the candidate workspace live in the
 // file-scope array g_search_scratch; the tables are rebuilt on the device by every call,
 // and every workspace entry is written before it is read, so nothing needs clearing.
-#include <mutex>
-
 namespace {
 
 constexpr size_t kStaticScratchBytes = (size_t)MTB_SEARCH_STATIC_SCRATCH_BYTES;
 __device__ __align__(256) unsigned char g_search_scratch[MTB_SEARCH_STATIC_SCRATCH_BYTES];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_static_mu;
-void* g_static_ptr[kMaxDevices] = {nullptr};
 
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
@@ -618,19 +616,12 @@ extern "C" int mtb_search_orientations_static(const mtb_search_config* cfg, cons
   MTB_ARG_CHECK(dtab_b + ctab_b + coef_b + cand_b <= kStaticScratchBytes,
                 "batch x candidates (or grid size) exceeds the static scratch of "
                 "MTB_SEARCH_STATIC_SCRATCH_BYTES; use mtb_search_orientations");
-  int dev = 0;
-  MTB_CUDA_TRY(cudaGetDevice(&dev));
-  MTB_ARG_CHECK(dev >= 0 && dev < kMaxDevices, "device ordinal out of range");
-  unsigned char* base = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_ptr[dev]) {
-      void* p = nullptr;
-      MTB_CUDA_TRY(cudaGetSymbolAddress(&p, g_search_scratch));
-      g_static_ptr[dev] = p;
-    }
-    base = static_cast<unsigned char*>(g_static_ptr[dev]);
-  }
+  // the array's device address in the current device's context, looked up by every call (a
+  // table lookup once the module is loaded), so a device reset or a context other than the
+  // primary one is never served a stale address
+  void* sym = nullptr;
+  MTB_CUDA_TRY(cudaGetSymbolAddress(&sym, g_search_scratch));
+  unsigned char* base = static_cast<unsigned char*>(sym);
   float* dtab = reinterpret_cast<float*>(base);
   double* Ctab = reinterpret_cast<double*>(base + dtab_b);
   float4* coef = reinterpret_cast<float4*>(base + dtab_b + ctab_b);
@@ -655,7 +646,9 @@ extern "C" int mtb_search_orientations_static(const mtb_search_config* cfg, cons
   NP.flags = cfg->flags;
   rc = newton_launch(sigma, sigma_stride, B, C, ca, cb, cg, cs, Ctab, coef, nullptr, NP, st);
   if (rc) return rc;
+  mtb_prof_begin(st);
   reduce_candidates_kernel<<<(B + 127) / 128, 128, 0, st>>>(ca, cb, cg, cs, B, C, alpha, beta, gamma, score);
+  mtb_prof_end(st, "reduce_candidates_kernel");
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }

@@ -955,18 +955,24 @@ int shift_front_n(mtb_shift* h, const float* subtomos, const float* shift_zyx, c
     return MTB_OK;
   }
   MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
+  mtb_prof_begin(st);
   patch_fft_xy_kernel<N, false><<<dim3(N, B), kT, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, g, h->T, h->bg);
+  mtb_prof_end(st, "patch_fft_xy_kernel");
   MTB_LAUNCH_CHECK();
   prof_mark(h, 1, st);
   if (h->use_tc) {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+    mtb_prof_begin(st);
     fft_z_kernel<N, true><<<dim3(N, B), kT, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm,
                                                        (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1, (uint32_t*)h->tc.A1n,
         h->tc.R1n);
+    mtb_prof_end(st, "fft_z_kernel");
   } else {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+    mtb_prof_begin(st);
     fft_z_kernel<N, false><<<dim3(N, B), kT, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm, nullptr,
                                                         0, 0, nullptr, 0);
+    mtb_prof_end(st, "fft_z_kernel");
   }
   MTB_LAUNCH_CHECK();
   return MTB_OK;
@@ -977,18 +983,24 @@ int shift_front_64(mtb_shift* h, const float* subtomos, const float* shift_zyx, 
   const ShiftGeom& g = h->g;
   const int sxy = (int)xy64_smem_bytes(), sz = (int)z64_smem_bytes();
   MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
+  mtb_prof_begin(st);
   patch_fft_xy64_kernel<<<dim3(64, B), kT64, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, h->fill_tab, g, h->T, h->bg);
+  mtb_prof_end(st, "patch_fft_xy64_kernel");
   MTB_LAUNCH_CHECK();
   prof_mark(h, 1, st);
   if (h->use_tc) {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+    mtb_prof_begin(st);
     fft_z64_kernel<true><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
                                                          (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1, (uint32_t*)h->tc.A1n,
         h->tc.R1n);
+    mtb_prof_end(st, "fft_z64_kernel");
   } else {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+    mtb_prof_begin(st);
     fft_z64_kernel<false><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm, nullptr,
                                                           0, 0, nullptr, 0);
+    mtb_prof_end(st, "fft_z64_kernel");
   }
   MTB_LAUNCH_CHECK();
   return MTB_OK;
@@ -1016,6 +1028,15 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
   MTB_ARG_CHECK(cfg->max_batch >= 1 && cfg->max_batch <= 65535, "max_batch out of range");
   MTB_ARG_CHECK(cfg->upsample_factor >= 2 && cfg->search_radius >= 0, "upsample_factor must be > 1");
   MTB_ARG_CHECK(cfg->cosine_width > 0.f, "cosine_width must be positive");
+  MTB_ARG_CHECK(cfg->precision == MTB_SHIFT_FP32 || cfg->precision == MTB_SHIFT_BF16X3 ||
+                    cfg->precision == MTB_SHIFT_AUTO,
+                "precision must be MTB_SHIFT_FP32, MTB_SHIFT_BF16X3 or MTB_SHIFT_AUTO");
+  {
+    const int U = (int)ceil((double)cfg->upsample_factor * (2 * cfg->search_radius + 1));
+    MTB_ARG_CHECK(cfg->precision != MTB_SHIFT_BF16X3 || shift_tc_fits(N, U) == MTB_OK,
+                  "MTB_SHIFT_BF16X3: the tensor-core kernels do not cover this box and upsampled region "
+                  "(MTB_SHIFT_AUTO falls back to FP32 there)");
+  }
   mtb_shift* h = new mtb_shift();
   memset(h, 0, sizeof(*h));
   h->cfg = *cfg;
@@ -1092,14 +1113,12 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
   if (cudaGetLastError() != cudaSuccess) return fail(MTB_ERR_CUDA);
   if (shift_front(h, nullptr, nullptr, nullptr, nullptr, 0, 0) != MTB_OK) return fail(MTB_ERR_CUDA);
   if (cudaStreamSynchronize(0) != cudaSuccess) return fail(MTB_ERR_CUDA);
-  // BF16X3 on a geometry the tensor-core kernels do not cover (box 128, or an upsampled region
-  // past their tensor/shared memory budget) runs the FP32 CUDA-core kernels instead
-  if (cfg->precision == MTB_SHIFT_BF16X3 && shift_tc_fits(N, g.U) == MTB_OK) {
+  // MTB_SHIFT_BF16X3 was checked to fit the tensor-core kernels above; MTB_SHIFT_AUTO uses them
+  // where they fit and the FP32 CUDA-core kernels elsewhere
+  if (cfg->precision != MTB_SHIFT_FP32 && shift_tc_fits(N, g.U) == MTB_OK) {
     const int rc = shift_tc_prepare(&h->tc, N, g.H, g.U, cfg->upsample_factor, g.dftshift, cfg->max_batch);
     if (rc) return fail(rc);
     h->use_tc = true;
-  } else if (cfg->precision != MTB_SHIFT_FP32 && cfg->precision != MTB_SHIFT_BF16X3) {
-    return fail(MTB_ERR_ARG);
   }
   *out = h;
   return MTB_OK;
@@ -1112,6 +1131,12 @@ extern "C" void mtb_shift_destroy(mtb_shift* h) {
   void* ptrs[] = {h->bgw_tab, h->fill_tab, h->what, h->refq, h->ref, h->E0, h->E1, h->E2, h->bg, h->nrm, h->T, h->X1, h->pval, h->pidx};
   for (void* p : ptrs) if (p) cudaFree(p);
   delete h;
+}
+
+extern "C" int mtb_shift_precision(const mtb_shift* h, int* precision) {
+  MTB_ARG_CHECK(h && precision, "null argument");
+  *precision = h->use_tc ? MTB_SHIFT_BF16X3 : MTB_SHIFT_FP32;
+  return MTB_OK;
 }
 
 extern "C" int mtb_shift_status(mtb_shift* h, mtb_stream_t stream) {
@@ -1164,7 +1189,9 @@ extern "C" int mtb_shift_search(mtb_shift* h, const float* subtomos, const float
       for (int k = 0; k < 3; ++k) marks[k] = (*h->prof_ev)[(h->prof_n % h->prof_cap) * kProfMarks + 3 + k];
     rc = shift_tc_passes(&h->tc, B, st, marks);
     if (rc) return rc;
+    mtb_prof_begin(st);
     finalize_tc_kernel<<<(B + 127) / 128, 128, 0, st>>>(g, B, h->tc.best, h->nrm, shift_xyz, score);
+    mtb_prof_end(st, "finalize_tc_kernel");
     MTB_LAUNCH_CHECK();
     prof_mark(h, 6, st);
     if (h->prof_cap > 0) ++h->prof_n;
@@ -1173,7 +1200,9 @@ extern "C" int mtb_shift_search(mtb_shift* h, const float* subtomos, const float
   const size_t sm1 = (size_t)(U * N + N * kColTile) * 8;
   MTB_CUDA_TRY(cudaFuncSetAttribute(updft1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
   prof_mark(h, 3, st);
+  mtb_prof_begin(st);
   updft1_kernel<<<dim3((N * H + kColTile - 1) / kColTile, B), kT, sm1, st>>>(g, h->T, h->E0, h->X1);
+  mtb_prof_end(st, "updft1_kernel");
   MTB_LAUNCH_CHECK();
   prof_mark(h, 4, st);
   const size_t sm2_staged = (size_t)(U * N + U * H + N * H + U * H) * 8;
@@ -1181,11 +1210,15 @@ extern "C" int mtb_shift_search(mtb_shift* h, const float* subtomos, const float
   const size_t sm2 = stage_e ? sm2_staged : (size_t)(N * H + U * H) * 8;
   MTB_ARG_CHECK(sm2 <= 220 * 1024 && sm1 <= 220 * 1024, "upsampled region too large for shared memory");
   MTB_CUDA_TRY(cudaFuncSetAttribute(updft23_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+  mtb_prof_begin(st);
   updft23_kernel<<<dim3(h->ngrp, B), kT, sm2, st>>>(g, h->X1, h->E1, h->E2, h->rows_per_cta, stage_e, h->pval,
                                                     h->pidx);
+  mtb_prof_end(st, "updft23_kernel");
   MTB_LAUNCH_CHECK();
   prof_mark(h, 5, st);
+  mtb_prof_begin(st);
   finalize_kernel<<<(B + 127) / 128, 128, 0, st>>>(g, B, h->ngrp, h->pval, h->pidx, h->nrm, shift_xyz, score);
+  mtb_prof_end(st, "finalize_kernel");
   MTB_LAUNCH_CHECK();
   prof_mark(h, 6, st);
   if (h->prof_cap > 0) ++h->prof_n;
@@ -1282,8 +1315,10 @@ extern "C" int mtb_update_rotation(const float* alpha, const float* beta, const 
   MTB_ARG_CHECK(B >= 0, "negative batch");
   if (B == 0) return MTB_OK;
   MTB_ARG_CHECK(alpha && beta && gamma && tracker_in && tracker_out && rot, "null pointer");
+  mtb_prof_begin((cudaStream_t)stream);
   tracker_update_kernel<<<(B + 127) / 128, 128, 0, (cudaStream_t)stream>>>(alpha, beta, gamma, tracker_in, B,
                                                                             tracker_out, rot);
+  mtb_prof_end((cudaStream_t)stream, "tracker_update_kernel");
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }
@@ -1292,7 +1327,9 @@ extern "C" int mtb_tracker_rotation(const double* tracker, int B, float* rot, mt
   MTB_ARG_CHECK(B >= 0, "negative batch");
   if (B == 0) return MTB_OK;
   MTB_ARG_CHECK(tracker && rot, "null pointer");
+  mtb_prof_begin((cudaStream_t)stream);
   tracker_rotation_kernel<<<(B + 127) / 128, 128, 0, (cudaStream_t)stream>>>(tracker, B, rot);
+  mtb_prof_end((cudaStream_t)stream, "tracker_rotation_kernel");
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }

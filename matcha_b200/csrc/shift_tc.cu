@@ -892,17 +892,21 @@ int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st, const cudaEvent_t* marks
     pn.NT = t->NT12;
     pn.stages = t->stages1;
     int gn = pn.tiles < t->n_sm ? pn.tiles : t->n_sm;
+    mtb_prof_begin(st);
     updft1_tc_kernel<false><<<gn, kThreads, t->smem1, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA1n),
                                                             *reinterpret_cast<const CUtensorMap*>(t->mapE1), pn,
                                                             (uint32_t*)t->A2n, nullptr, t->err);
+    mtb_prof_end(st, "updft1_tc_kernel (Nyquist plane, pass 1)");
     MTB_LAUNCH_CHECK();
     pn.rows = B * U;
     pn.tiles = (pn.rows + TM - 1) / TM;
     pn.R1 = t->R2n;  // the A operand is now A2n
     gn = pn.tiles < t->n_sm ? pn.tiles : t->n_sm;
+    mtb_prof_begin(st);
     updft1_tc_kernel<true><<<gn, kThreads, t->smem1, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA2n),
                                                            *reinterpret_cast<const CUtensorMap*>(t->mapE1), pn,
                                                            nullptr, t->nyq, t->err);
+    mtb_prof_end(st, "updft1_tc_kernel (Nyquist plane, pass 2)");
     MTB_LAUNCH_CHECK();
   }
   if (marks && marks[0]) cudaEventRecord(marks[0], st);
@@ -919,9 +923,11 @@ int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st, const cudaEvent_t* marks
   p1.NT = t->NT12;
   p1.stages = t->stages1;
   const int g1 = p1.tiles < t->n_sm ? p1.tiles : t->n_sm;
+  mtb_prof_begin(st);
   updft1_tc_kernel<false><<<g1, kThreads, t->smem1, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA1),
                                                           *reinterpret_cast<const CUtensorMap*>(t->mapE1), p1,
                                                           (uint32_t*)t->A2, nullptr, t->err);
+  mtb_prof_end(st, "updft1_tc_kernel");
   MTB_LAUNCH_CHECK();
   if (marks && marks[1]) cudaEventRecord(marks[1], st);
   // passes 2 + 3
@@ -941,10 +947,12 @@ int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st, const cudaEvent_t* marks
   p2.NT3 = t->NT3;
   MTB_CUDA_TRY(cudaFuncSetAttribute(updft23_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem23));
   const int g2 = p2.tiles < t->n_sm ? p2.tiles : t->n_sm;
+  mtb_prof_begin(st);
   updft23_tc_kernel<<<g2, kThreads23, t->smem23, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA2),
                                                      *reinterpret_cast<const CUtensorMap*>(t->mapE1),
                                                      *reinterpret_cast<const CUtensorMap*>(t->mapE3), p2, t->nyq,
                                                      (const float4*)t->ENQ, t->best, t->err);
+  mtb_prof_end(st, "updft23_tc_kernel");
   MTB_LAUNCH_CHECK();
   if (marks && marks[2]) cudaEventRecord(marks[2], st);
   return MTB_OK;

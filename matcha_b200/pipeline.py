@@ -36,7 +36,9 @@ class StepConfig:
     box_size: float | None = None
     voxel_size: float = 1.0
     precision: str = "bf16x3"        # dense contractions (ball expansion, upsampled DFT): "bf16x3" on
-                                     # tcgen05 with a hi+lo split, or "fp32" on CUDA cores
+                                     # tcgen05 with a hi+lo split, "fp32" on CUDA cores, or "auto":
+                                     # the expansion on tcgen05 and the upsampled DFT there where its
+                                     # kernels cover the box (ShiftMatcher.effective_precision)
 
 
 class _Cfg(dict):
@@ -54,9 +56,11 @@ class AlignmentStep:
         self.cfg = cfg
         self.device = torch.device(device)
         radius = cfg.radius if cfg.radius is not None else min(cfg.N // 2, int(cfg.N // 2 * 0.95))
+        if cfg.precision not in ("bf16x3", "fp32", "auto"):
+            raise ValueError("precision must be 'bf16x3', 'fp32' or 'auto'")
         self.correlator = CrossCorrelationMatcher(N=cfg.N, device=self.device, batchsize=cfg.batch,
                                                   bandlimit=cfg.L, radius=radius, precision_mode="fast",
-                                                  precision=cfg.precision)
+                                                  precision="fp32" if cfg.precision == "fp32" else "bf16x3")
         self.matcher = Matcha(batchsize=cfg.batch, device=self.device, L_max=cfg.L,
                               matcha_config=dict(Li=list(cfg.Li) + [cfg.L], candidates=cfg.candidates,
                                                  num_steps=cfg.num_steps, oversampling_factor_K=cfg.K))
@@ -164,7 +168,15 @@ class AlignmentStep:
         tensors of the returned object: copy a batch into them, replay, read its outputs (also
         static, rewritten by each replay).  The step issues no host synchronisation, so every
         launch of the library and every torch operation of the loop is in the graph; the
-        library's handles and the step's buffers are created by two eager runs first."""
+        library's handles and the step's buffers are created by two eager runs first.
+
+        The graph's outputs and intermediates are the step's own buffers (``shift``,
+        ``shift_score``, the matcher's and correlator's result buffers, the preparation
+        workspace): an eager call of this ``AlignmentStep``, or the replay of a second graph
+        captured from it, rewrites them.  Keep one captured graph per step and read a replay's
+        outputs before the next call.  ``set_template`` may be called between replays: the
+        template's coefficients, norm and shift reference are updated in place, at the
+        addresses the graph reads."""
         if not 0 < B <= self.cfg.batch:
             raise ValueError(f"batch must be in [1, {self.cfg.batch}]")
         return CapturedStep(self, B, alternations)

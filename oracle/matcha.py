@@ -205,8 +205,10 @@ def march_schedule(Li, Lmax):
 
 
 def optimize(alphas, betas, gammas, sigma, Li, Lmax, num_steps=1, compat_top_block=False,
-             dtype=np.float64, trace=None):
-    """One march stage (Matcha.py:239-367) with Newton steps and accept/reject (:150-205)."""
+             dtype=np.float64, trace=None, step_type="newton"):
+    """One march stage (Matcha.py:239-367) with Newton steps (or, step_type "gradient", the
+    ascent step -lr * gradient with base lr 5e-7, Matcha.py:14-15, :91, :344-345) and
+    accept/reject (:150-205)."""
     rdt = dtype
     n = W.dsize(Li)
     s = sigma[:, :n].astype(np.complex64 if dtype == np.float32 else np.complex128)
@@ -215,16 +217,19 @@ def optimize(alphas, betas, gammas, sigma, Li, Lmax, num_steps=1, compat_top_blo
     g = np.array(gammas, dtype=rdt)
     D = wigner_D_stage(a, b, g, Li, Lmax, compat_top_block, dtype)
     best = np.einsum("bcn,bn->bc", D, s).real.astype(rdt)
-    lr = np.ones(a.shape, dtype=rdt)
+    lr = np.full(a.shape, 1.0 if step_type == "newton" else 5e-7, dtype=rdt)
     for _ in range(num_steps):
         grad, H = derivatives(D.astype(np.complex128), s.astype(np.complex128), a.astype(np.float64), Li)
         step = np.zeros_like(grad)
-        for bi in range(a.shape[0]):
-            for ci in range(a.shape[1]):
-                try:
-                    step[bi, ci] = np.linalg.solve(H[bi, ci].astype(rdt), grad[bi, ci].astype(rdt))
-                except np.linalg.LinAlgError:
-                    step[bi, ci] = 0.0
+        if step_type == "gradient":
+            step = -grad
+        else:
+            for bi in range(a.shape[0]):
+                for ci in range(a.shape[1]):
+                    try:
+                        step[bi, ci] = np.linalg.solve(H[bi, ci].astype(rdt), grad[bi, ci].astype(rdt))
+                    except np.linalg.LinAlgError:
+                        step[bi, ci] = 0.0
         step = (lr[..., None] * step).astype(rdt)
         ta = (a - step[..., 0]).astype(rdt)
         tb = (b - step[..., 1]).astype(rdt)
@@ -244,8 +249,11 @@ def optimize(alphas, betas, gammas, sigma, Li, Lmax, num_steps=1, compat_top_blo
 
 
 def search_orientations(sigma, Li, Lmax, L0=None, K=2, candidates=10, num_steps=1,
-                        compat_top_block=False, dtype=np.float64, return_grid=False):
-    """Matcha.search_orientations (Matcha.py:369-403) on numpy input ``sigma`` (B, >=dsize(Lmax))."""
+                        compat_top_block=False, dtype=np.float64, return_grid=False, return_candidates=False,
+                        step_type="newton"):
+    """Matcha.search_orientations (Matcha.py:369-403) on numpy input ``sigma`` (B, >=dsize(Lmax)).
+    ``return_candidates`` appends the march's final (alpha, beta, gamma, score) of every
+    candidate, (B, C) each, before the reduction over candidates (Matcha.py:19-24)."""
     sched = march_schedule(Li, Lmax)
     if L0 is None:
         L0 = min(sched)
@@ -254,10 +262,13 @@ def search_orientations(sigma, Li, Lmax, L0=None, K=2, candidates=10, num_steps=
     n = 2 * L0 * K
     a, b, g = ids_to_angles(ids, n, dtype=dtype)
     for Li_ in sched:
-        a, b, g, best = optimize(a, b, g, sigma, Li_, Lmax, num_steps, compat_top_block, dtype)
+        a, b, g, best = optimize(a, b, g, sigma, Li_, Lmax, num_steps, compat_top_block, dtype,
+                                 step_type=step_type)
     idx = np.argmax(best, axis=-1)
     take = lambda x: np.take_along_axis(x, idx[:, None], 1)[:, 0]
     out = (take(a), take(b), take(g), take(best))
+    if return_candidates:
+        out = out + ((a, b, g, best),)
     if return_grid:
         return out, f, ids
     return out

@@ -154,8 +154,8 @@ def align_batch(fle: FoldedFLE, a_template, ref_fourier, vols, subtomos, tracker
     """One alternation for a few subtomograms: returns the same quantities as the GPU step."""
     a = fle.evaluate_t(vols)
     sigma = F.compute_sigma(fle.tables, a_template, a)
-    al, be, ga, score = M.search_orientations(sigma, list(Li) + [L], L, K=K, candidates=candidates,
-                                              num_steps=num_steps, dtype=dtype)
+    al, be, ga, score, cand = M.search_orientations(sigma, list(Li) + [L], L, K=K, candidates=candidates,
+                                                    num_steps=num_steps, dtype=dtype, return_candidates=True)
     tr = update_rotation_estimate(al.astype(np.float64), be.astype(np.float64), ga.astype(np.float64), tracker)
     ang = S.euler_zyz_deg_from_quat_conj(tr)
     shifts, scores = [], []
@@ -164,9 +164,35 @@ def align_batch(fle: FoldedFLE, a_template, ref_fourier, vols, subtomos, tracker
         shifts.append(s)
         scores.append(sc)
     return dict(alpha=al, beta=be, gamma=ga, rotation_score=score, bh_norms=np.linalg.norm(a, axis=1),
-                tracker=tr, shift=np.array(shifts), shift_score=np.array(scores))
+                tracker=tr, shift=np.array(shifts), shift_score=np.array(scores),
+                candidates=dict(zip(("alpha", "beta", "gamma", "score"), cand)))
 
 
 def rotation_matrix_of_tracker(tr):
     """Matrix the shift match uses for a tracker (ShiftMatcher.py:503, :913)."""
     return R.from_euler("ZYZ", S.euler_zyz_deg_from_quat_conj(tr), degrees=True).as_matrix()
+
+
+def run_alternations(fle: FoldedFLE, a_template, ref_fourier, subtomos, tracker, local_shifts, prior_shifts,
+                     base_shifts, L, Li, radius, num_alternations, **kw):
+    """BatchProcessor._run_alternations (src/matcha/align_subtomograms.py:316-361) for a few
+    subtomograms: each alternation prepares the batch at the current shift and orientation
+    (oracle.prepare, align_subtomograms.py:240-252), aligns it (align_batch) with the shift
+    match at the current shift, and adds the found shift to the local shifts.  Returns one
+    dict per alternation; the tracker and local shifts are not modified in place."""
+    from . import prepare as P
+
+    tr = np.asarray(tracker, dtype=np.float64).copy()
+    local = np.asarray(local_shifts, dtype=np.float64).copy()
+    outs = []
+    for _ in range(num_alternations):
+        current = (np.asarray(prior_shifts) + np.asarray(base_shifts) + local).astype(np.float32)
+        data = P.prepare(subtomos, current, tr, radius)
+        o = align_batch(fle, a_template, ref_fourier, data, np.asarray(subtomos, dtype=np.float64), tr,
+                        current.astype(np.float64), L, Li, **kw)
+        tr = o["tracker"]
+        local = local + o["shift"]
+        o["local_shifts"] = local.copy()
+        o["shift_prior"] = current
+        outs.append(o)
+    return outs

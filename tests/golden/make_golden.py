@@ -1,9 +1,8 @@
 """Generate the golden fixtures under tests/golden from the reference's own code.
 
-Run in a container that has the reference tree (default /root/reference, override
-with MATCHA_REFERENCE_ROOT):
+Run where a checkout of the reference exists, named by MATCHA_REFERENCE_ROOT:
 
-    python tests/golden/make_golden.py [wigner|grad|search|all]
+    MATCHA_REFERENCE_ROOT=<checkout> python tests/golden/make_golden.py [wigner|grad|search|shift|fle|sigma|all]
 
 What each fixture holds and which reference code produced it:
 
@@ -22,6 +21,12 @@ What each fixture holds and which reference code produced it:
   oracle: the SOFFT d-table (``spherical.Wigner(L).d``, the same small-d at
   alpha=gamma=0) and ``WignerDMatrices.D`` (pinned by ``wigner_ref.npz``); both are
   returned in float32/complex64 exactly as the reference would hold them.
+* ``fle_ref.npz``      -- ``FLEBasis3D.lap_eig_ball`` (src/matcha/core/FLEBasis3D.py:700-799) at
+  16^3/L=8, 32^3/L=16, 64^3/L=32 and 128^3/L=64, reading Bessel-zero tables written here
+  (the reference's .mat files are not in its tree), and ``create_denseB`` (:570-698) applied
+  as a = B^H f to seeded volumes (see ``gen_fle``).
+* ``sigma_ref.npz``    -- ``CrossCorrelationMatcher._precompute_indices`` + ``compute_sigma``
+  (src/matcha/core/CrossCorrelationMatcher.py:133-212) on the coefficients of ``fle_ref.npz``.
 """
 from __future__ import annotations
 
@@ -215,8 +220,173 @@ def gen_shift():
     print("shift_ref.npz", shift.numpy(), score.numpy())
 
 
+def write_bessel_tables(directory, n_l, n_k):
+    """The two tables the reference loads in lap_eig_ball (FLEBasis3D.py:726-730), absent from
+    its tree: roots_table[l, k-1] = k-th positive zero of j_l and cs[l, k-1] =
+    sqrt(2)/|j_{l+1}(root)|, for l < n_l, k <= n_k, written as .mat files."""
+    from scipy.io import savemat
+    from scipy.special import spherical_jn
+
+    from matcha_b200.core.fle_tables import BesselZeros
+
+    z = BesselZeros()
+    roots = np.zeros((n_l, n_k))
+    for l in range(n_l):
+        roots[l] = z._compute(l, n_k)
+    cs = np.sqrt(2.0) / np.abs(spherical_jn(np.arange(1, n_l + 1)[:, None], roots))
+    rp, cp = os.path.join(directory, f"jl_zeros_l={n_l}_k={n_k}.mat"), os.path.join(directory, f"cs_l={n_l}_k={n_k}.mat")
+    savemat(rp, {"roots_table": roots})
+    savemat(cp, {"cs": cs})
+    return rp, cp, roots
+
+
+class _SplShim:
+    """scipy.special with the ``sph_harm(m, l, azimuth, polar)`` call create_denseB makes
+    (FLEBasis3D.py:595,603); scipy 1.18 removed it in favour of sph_harm_y(l, m, polar, azimuth)."""
+
+    def __getattr__(self, name):
+        import scipy.special as sps
+
+        return getattr(sps, name)
+
+    @staticmethod
+    def sph_harm(m, l, p, t):
+        from scipy.special import sph_harm_y
+
+        return sph_harm_y(l, m, t, p)
+
+
+def _reference_fle_object(N, bandlimit, rp, cp):
+    """A reference FLEBasis3D whose constructor is skipped (its precomp needs cuFINUFFT and
+    torch-harmonics): the attributes lap_eig_ball and create_denseB read are set, and
+    lap_eig_ball itself is the reference's method."""
+    refharness._install_stubs()
+    F = refharness.load_module("matcha.core.FLEBasis3D")
+    F.spl = _SplShim()
+    obj = F.FLEBasis3D.__new__(F.FLEBasis3D)
+    obj.jl_zeros_path, obj.cs_path = rp, cp
+    obj.complexmode = True
+    N2 = N + (N % 2)
+    ls, ks, ms, mds, lmds, cs, ne = obj.lap_eig_ball(int(N2 ** 3 * np.pi / 6), bandlimit)
+    obj.ls, obj.ks, obj.ms, obj.mds, obj.lmds, obj.cs, obj.ne = ls, ks, ms, mds, lmds, cs, ne
+    obj.N = obj.N1 = N
+    return obj
+
+
+def _mpmath_root_check(roots, picks):
+    """Independent check of the regenerated zeros: j_l(x) = sqrt(pi/2x) J_{l+1/2}(x), so the
+    k-th zero of j_l is mpmath's k-th zero of J_{l+1/2}."""
+    import mpmath
+
+    return max(abs(float(mpmath.besseljzero(l + 0.5, k)) - roots[l, k - 1]) for l, k in picks)
+
+
+def gen_fle():
+    """fle_ref.npz: the reference's own lap_eig_ball (FLEBasis3D.py:700-799) for the shapes of
+    the alignment (16^3/L=8, 32^3/L=16, 64^3/L=32, 128^3/L=64), and its create_denseB
+    (FLEBasis3D.py:570-698) applied as the dense adjoint a = B^H f (h folded into B) to seeded
+    volumes at 16^3 (R = 8) and 32^3 (R = 16), plus the 32^3 box at radius 15 (the alignment's
+    default radius, min(N/2, int(0.95 N/2))): create_denseB on the 30^3 crop whose coordinates
+    are -15..14 (the 32^3 box's voxels outside the crop have r >= 1, where every basis function
+    is zero or j_l(lambda_lk) = 0)."""
+    sys.path.insert(0, ROOT)
+    from tests.helpers import blob_template
+
+    tmp = os.path.join("/tmp", "matcha_ref_tables")
+    os.makedirs(tmp, exist_ok=True)
+    rp, cp, roots = write_bessel_tables(tmp, 260, 260)
+    err = _mpmath_root_check(roots, [(0, 1), (0, 40), (7, 3), (31, 12), (42, 1), (100, 50), (200, 7), (259, 259)])
+    print("regenerated zeros vs mpmath: max abs err", err)
+    assert err < 1e-9
+    out = {"root_check_err": err}
+    for N, L in ((16, 8), (32, 16), (64, 32), (128, 64)):
+        obj = _reference_fle_object(N, L, rp, cp)
+        tag = f"t{N}"
+        for k in ("ls", "ks", "ms", "mds", "lmds", "cs"):
+            out[f"{tag}_{k}"] = np.asarray(getattr(obj, k))
+        out[f"{tag}_ne"] = int(obj.ne)
+        out[f"{tag}_L"] = L
+        print(f"N={N} L={L}: ne={obj.ne} lmax={int(np.max(obj.ls))}")
+    rng = np.random.default_rng(41)
+    for N, L, radius in ((16, 8, 8), (32, 16, 16), (32, 16, 15)):
+        obj = _reference_fle_object(N, L, rp, cp)
+        vols = np.stack([blob_template(rng, N, 20, N // 4, (1.0, 2.5), mask_radius=N // 2 - 2),
+                         rng.standard_normal((N, N, N))]).astype(np.float32)
+        if radius == N // 2:
+            B = obj.create_denseB()
+            a = vols.reshape(2, -1).astype(np.float64) @ np.conj(B)
+        else:
+            lo = N // 2 - radius
+            obj.N = obj.N1 = 2 * radius
+            B = obj.create_denseB()
+            crop = vols[:, lo:lo + 2 * radius, lo:lo + 2 * radius, lo:lo + 2 * radius]
+            a = crop.reshape(2, -1).astype(np.float64) @ np.conj(B)
+        tag = f"c{N}r{radius}"
+        out[f"{tag}_volumes"] = vols
+        out[f"{tag}_coeffs"] = a
+        out[f"{tag}_L"] = L
+        print(tag, a.shape, np.abs(a).max())
+        del B
+    np.savez_compressed(os.path.join(HERE, "fle_ref.npz"), **out)
+    print("fle_ref.npz")
+
+
+def gen_sigma():
+    """sigma_ref.npz: the reference's CrossCorrelationMatcher._precompute_indices and
+    compute_sigma (CrossCorrelationMatcher.py:133-212) on the 32^3 (radius 16) and 16^3
+    coefficients of fle_ref.npz, volume 0 as the template, in complex128.  The index maps
+    (idlm_list) are built from lap_eig_ball's output as precomp builds them
+    (FLEBasis3D.py:337-357); spherical.Wigner(ell).Dindex is the reference's own WignerDindex
+    (WignerDMatrices.py:969), the function it was adapted from."""
+    import torch
+
+    refharness._install_stubs()
+    wmod = refharness.load_wigner_module()
+    sph = sys.modules["spherical"]
+
+    class _Wigner:
+        def __init__(self, ell_max):
+            self.ell_max = ell_max
+
+        def Dindex(self, ell, mp, m):
+            return wmod.WignerDindex(ell, mp, m)
+
+    sph.Wigner = _Wigner
+    C = refharness.load_module("matcha.core.CrossCorrelationMatcher")
+    fx = np.load(os.path.join(HERE, "fle_ref.npz"))
+    out = {}
+    for N, radius in ((16, 8), (32, 16)):
+        tag = f"c{N}r{radius}"
+        ls, mds = fx[f"t{N}_ls"], fx[f"t{N}_mds"]
+        ne = int(fx[f"t{N}_ne"])
+        lmax = int(ls.max())
+        idlm = [[[] for _ in range(2 * lmax + 1)] for _ in range(lmax + 1)]
+        for i in range(ne):
+            idlm[ls[i]][mds[i]].append(i)
+        cc = C.CrossCorrelationMatcher.__new__(C.CrossCorrelationMatcher)
+        cc.lmax = lmax
+        cc.device = torch.device("cpu")
+        cc.dtype = torch.complex128
+        cc.fle = types.SimpleNamespace(idlm_list=idlm, ne=ne)
+        cc.alpha1_indices, cc.alpha2_indices, cc.phase_factors, cc.wigner_indices = cc._precompute_indices()
+        a = torch.from_numpy(fx[f"{tag}_coeffs"])
+        cc.template_coefficients_alphas_torch = torch.nn.functional.pad(a[0], (0, 1))
+        cc.bh_volumes_buffer = torch.zeros((a.shape[0], ne + 1), dtype=torch.complex128)
+        cc.sigma = torch.zeros((a.shape[0], wmod.WignerDsize(0, lmax, lmax)), dtype=torch.complex128)
+        cc.compute_sigma(a, 0, a.shape[0])
+        out[f"{tag}_sigma"] = cc.sigma.numpy()
+        out[f"{tag}_norms"] = torch.linalg.norm(a, dim=1).numpy()
+        print(tag, "sigma", cc.sigma.shape)
+    np.savez_compressed(os.path.join(HERE, "sigma_ref.npz"), **out)
+    print("sigma_ref.npz")
+
+
 if __name__ == "__main__":
     what = sys.argv[1] if len(sys.argv) > 1 else "all"
+    if what in ("fle", "all"):
+        gen_fle()
+    if what in ("sigma", "all"):
+        gen_sigma()
     if what in ("wigner", "all"):
         gen_wigner()
     if what in ("grad", "all"):

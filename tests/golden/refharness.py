@@ -27,7 +27,9 @@ import types
 # must be set before numba is first imported
 os.environ["NUMBA_ENABLE_CUDASIM"] = "1"
 
-REF_ROOT = os.environ.get("MATCHA_REFERENCE_ROOT", "/root/reference")
+REF_ROOT = os.environ.get("MATCHA_REFERENCE_ROOT")
+if not REF_ROOT:
+    raise RuntimeError("set MATCHA_REFERENCE_ROOT to a checkout of swing-research/Matcha to generate fixtures")
 REF_SRC = os.path.join(REF_ROOT, "src")
 
 

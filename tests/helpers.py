@@ -101,3 +101,33 @@ def alignment_error_deg(alpha, beta, gamma, quats_true):
     sw = R.from_quat(np.roll(q_wxyz, -1, axis=1))
     tr = R.from_quat(np.roll(quats_true, -1, axis=1))
     return np.rad2deg((tr * sw.inv()).magnitude())
+
+
+def make_subtomograms(template, rng, B, max_shift, snr_db=0.0, mask_radius=None):
+    """Synthetic subtomograms as the benchmark draws them, on the host: the template rotated
+    by Haar rotations (rotate_volumes_reference), shifted by uniform offsets in
+    [-max_shift, max_shift]^3 (Fourier phase ramp, (z, y, x) order), plus white Gaussian
+    noise at ``snr_db`` measured by the signal power inside the spherical mask
+    (src/matcha/example.py:93-124).  Returns (float32 volumes, quaternions, shifts)."""
+    N = template.shape[0]
+    q = haar_quaternions(rng, B)
+    shifts = rng.uniform(-max_shift, max_shift, (B, 3))
+    vols = rotate_volumes_reference(np.repeat(template[None], B, 0), q).astype(np.float64)
+    k = np.fft.fftfreq(N)
+    kz, ky, kx = np.meshgrid(k, k, k, indexing="ij")
+    g = np.arange(N) - N // 2
+    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    mask = np.sqrt(x ** 2 + y ** 2 + z ** 2) < (0.45 * N if mask_radius is None else mask_radius)
+    for i in range(B):
+        ph = np.exp(-2j * np.pi * (kz * shifts[i, 0] + ky * shifts[i, 1] + kx * shifts[i, 2]))
+        v = np.fft.ifftn(np.fft.fftn(vols[i]) * ph).real
+        power = np.mean(v[mask] ** 2)
+        vols[i] = v + rng.standard_normal(v.shape) * np.sqrt(power * 10.0 ** (-snr_db / 10.0))
+    return vols.astype(np.float32), q, shifts
+
+
+def quat_dist_deg(q1, q2):
+    """Rotation angle between (w, x, y, z) quaternions, degrees."""
+    r1 = R.from_quat(np.roll(np.asarray(q1, dtype=np.float64), -1, axis=-1))
+    r2 = R.from_quat(np.roll(np.asarray(q2, dtype=np.float64), -1, axis=-1))
+    return np.rad2deg((r1.inv() * r2).magnitude())

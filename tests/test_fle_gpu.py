@@ -124,3 +124,48 @@ def test_tensor_core_split_at_benchmark_shape(cuda_device):
     tc.status()
     rel = (torch.linalg.norm(a - b) / torch.linalg.norm(b)).item()
     assert rel < 1e-4, rel
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", 1e-5), ("bf16x3", 1e-4)])
+@pytest.mark.parametrize("tag,N1,bl,radius", [("c16r8", 16, 8, 8), ("c32r16", 32, 16, 16), ("c32r15", 32, 16, 15)])
+def test_evaluate_t_matches_reference_dense_basis(cuda_device, tag, N1, bl, radius, precision, tol):
+    """Coefficients of the volumes in tests/golden/fle_ref.npz against the reference's own
+    create_denseB adjoint (FLEBasis3D.py:570-698), at the FP32 and BF16 hi+lo tolerances."""
+    from matcha_b200.core.FLEBasis3D import FLEBasis3D
+    from tests.helpers import golden
+
+    fx = golden("fle_ref.npz")
+    vols, ref = fx[f"{tag}_volumes"], fx[f"{tag}_coeffs"]
+    fle = FLEBasis3D(N=N1, bandlimit=bl, eps=1e-4, batchsize=vols.shape[0], radius=radius, device=cuda_device,
+                     dtype=torch.complex64, precision=precision)
+    assert fle.ne == ref.shape[1]
+    a = fle.evaluate_t(torch.from_numpy(vols).to(cuda_device))
+    fle.status()
+    a = a.cpu().numpy()
+    for i in range(vols.shape[0]):
+        err = np.linalg.norm(a[i] - ref[i]) / np.linalg.norm(ref[i])
+        assert err < tol, (i, err)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3"])
+@pytest.mark.parametrize("tag,N1,bl,radius", [("c16r8", 16, 8, 8), ("c32r16", 32, 16, 16)])
+def test_sigma_matches_reference_compute_sigma(cuda_device, tag, N1, bl, radius, precision):
+    """sigma and the norms of tests/golden/sigma_ref.npz (the reference's compute_sigma,
+    CrossCorrelationMatcher.py:133-212, volume 0 as the template)."""
+    from matcha_b200.core.CrossCorrelationMatcher import CrossCorrelationMatcher
+    from tests.helpers import golden
+
+    fx, sx = golden("fle_ref.npz"), golden("sigma_ref.npz")
+    vols = fx[f"{tag}_volumes"]
+    cc = CrossCorrelationMatcher(N=N1, device=cuda_device, batchsize=2, bandlimit=bl, radius=radius,
+                                 precision=precision)
+    cc.set_template(vols[0])
+    sig, norms = cc.get_sigma(torch.from_numpy(vols).to(cuda_device))
+    ref = sx[f"{tag}_sigma"]
+    sig = sig.cpu().numpy()
+    assert sig.shape == ref.shape
+    tol = 2e-5 if precision == "fp32" else 2e-4
+    for i in range(2):
+        assert np.linalg.norm(sig[i] - ref[i]) / np.linalg.norm(ref[i]) < tol
+    np.testing.assert_allclose(norms.cpu().numpy(), sx[f"{tag}_norms"], rtol=1e-5 if precision == "fp32" else 1e-4)
+    np.testing.assert_allclose(cc.bh_norm_template.item(), sx[f"{tag}_norms"][0], rtol=1e-5 if precision == "fp32" else 1e-4)

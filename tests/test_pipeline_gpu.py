@@ -116,3 +116,28 @@ def test_captured_step_matches_eager(cuda_device, alternations):
             for k in keys:
                 np.testing.assert_allclose(g[k], r[k].cpu().numpy(), rtol=1e-6, atol=1e-7, err_msg=k)
         np.testing.assert_allclose(got_tracker, t.cpu().numpy(), atol=1e-12)
+
+
+def test_captured_step_after_set_template(cuda_device):
+    """A template changed after capture is what the next replay uses (set_template writes the
+    coefficients, the norm and the shift reference in place)."""
+    B, N = 3, 16
+    rng = np.random.default_rng(77)
+    t1 = blob_template(rng, N, 12, 5, (1.0, 2.0), mask_radius=7).astype(np.float32)
+    t2 = blob_template(rng, N, 12, 5, (1.0, 2.0), mask_radius=7).astype(np.float32)
+    step = _step(cuda_device, B)
+    step.set_template(t1)
+    cap = step.capture(B, 0)
+    step.set_template(t2)
+    ident = torch.zeros((B, 4), dtype=torch.float64, device=cuda_device)
+    ident[:, 0] = 1
+    vols = (np.repeat(t2[None], B, 0) + 0.05 * rng.standard_normal((B, N, N, N))).astype(np.float32)
+    dv = torch.from_numpy(vols).to(cuda_device)
+    cap.volumes.copy_(dv)
+    cap.tracker.copy_(ident)
+    out = cap.replay()
+    keys = ("alpha", "beta", "gamma", "rotation_score", "shift", "shift_score")
+    got = {k: out[k].cpu().numpy().copy() for k in keys}
+    ref = step(dv, dv, ident.clone(), torch.zeros((B, 3), device=cuda_device))
+    for k in keys:
+        np.testing.assert_allclose(got[k], ref[k].cpu().numpy(), rtol=1e-6, atol=1e-7, err_msg=k)

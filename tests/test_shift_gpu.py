@@ -40,7 +40,7 @@ def test_shift_matches_reference_fixture(cuda_device):
                                               (64, 8, 5, "bf16x3"), (32, 8, 3, "bf16x3"),
                                               (16, 4, 1, "bf16x3"), (32, 4, 2, "bf16x3"),
                                               (32, 8, 5, "bf16x3"), (16, 8, 5, "bf16x3"),
-                                              (128, 8, 8, "bf16x3")])
+                                              (128, 8, 8, "auto")])
 def test_shift_matches_oracle(cuda_device, N, uf, r, precision):
     rng = np.random.default_rng(N + uf + r)
     tmpl = blob_template(rng, N, 60, N * 0.3, (1.5, 3.0), mask_radius=N * 0.4)
@@ -165,3 +165,27 @@ def test_shift_reference_on_device_matches_oracle(cuda_device, N, voxel):
     got = sm.reference_data_fourier[0].cpu().numpy()
     assert got.dtype == np.complex64
     np.testing.assert_allclose(got, ref, atol=2e-7 * np.abs(ref).max(), rtol=0)
+
+
+def test_precision_selection(cuda_device):
+    """bf16x3 on a box the tensor-core kernels do not cover is an error, not a silent FP32 run;
+    "auto" says what it resolved to; without the argument the config decides (b200.precision,
+    else precision_mode "fast" -> "auto", "accurate" -> "fp32")."""
+    from matcha_b200.core.ShiftMatcher import ShiftMatcher
+
+    tmpl = np.zeros((128, 128, 128), np.float32)
+    with pytest.raises(ValueError):
+        sm = _matcher(128, 1, 8, 8, cuda_device, precision="bf16x3")
+        sm._handle(1)
+    for N, want in ((128, "fp32"), (64, "bf16x3")):
+        sm = _matcher(N, 1, 8, 5 if N == 64 else 8, cuda_device, precision="auto")
+        sm._handle(1)
+        assert sm.effective_precision == want
+    base = dict(N=64, voxel_size=1.0, num_subtomograms_per_batch=2, shift_upsample_factor=8, shift_search_radius=5,
+                do_ctf_correction=False, box_size=64)
+    for extra, want in (({"precision_mode": "fast"}, "auto"), ({"precision_mode": "accurate"}, "fp32"), ({}, "fp32"),
+                        ({"precision_mode": "fast", "b200": {"precision": "fp32"}}, "fp32"),
+                        ({"b200": {"precision": "bf16x3"}}, "bf16x3")):
+        sm = ShiftMatcher(Cfg(**base, **extra), cuda_device, torch.complex64)
+        assert sm.precision == want, (extra, sm.precision)
+    del tmpl

@@ -18,12 +18,12 @@ from tests.helpers import euler_dist_deg, synthetic_sigma
 pytestmark = pytest.mark.gpu
 
 
-def _cfg(native, Lmax, stages, L0, C, steps, B):
+def _cfg(native, Lmax, stages, L0, C, steps, B, flags=0):
     cfg = native.MtbSearchConfig()
     cfg.Lmax, cfg.n_stages, cfg.L0, cfg.K = Lmax, len(stages), L0, 2
     for i, l in enumerate(stages):
         cfg.stages[i] = l
-    cfg.candidates, cfg.num_steps, cfg.max_batch, cfg.flags = C, steps, B, 0
+    cfg.candidates, cfg.num_steps, cfg.max_batch, cfg.flags = C, steps, B, flags
     return cfg
 
 
@@ -36,15 +36,18 @@ def _run(lib, native, fn, first_arg, sig, B):
     return out.cpu().numpy()
 
 
-def test_static_search_matches_handle_search_twice(cuda_device):
+@pytest.mark.parametrize("flag", ["none", "compat_top_block", "gradient_step"])
+def test_static_search_matches_handle_search_twice(cuda_device, flag):
     from matcha_b200 import _native as native
 
     lib = native.load()
+    flags = {"none": 0, "compat_top_block": native.MTB_SEARCH_COMPAT_TOP_BLOCK,
+             "gradient_step": native.MTB_SEARCH_GRADIENT_STEP}[flag]
     B, Lmax, stages, C = 24, 16, [4, 8, 12, 16], 10
     rng = np.random.default_rng(2024)
     sig_np, _ = synthetic_sigma(rng, B, Lmax)
     sig = torch.from_numpy(sig_np).to(cuda_device)
-    cfg = _cfg(native, Lmax, stages, 4, C, 1, B)
+    cfg = _cfg(native, Lmax, stages, 4, C, 1, B, flags)
     h = ctypes.c_void_p()
     assert lib.mtb_search_create(ctypes.byref(cfg), ctypes.byref(h)) == 0, lib.mtb_last_error()
     try:
