@@ -100,6 +100,20 @@ int mtb_search_orientations(mtb_search* h, const float* sigma, int64_t sigma_str
                             float* alpha, float* beta, float* gamma, float* score,
                             mtb_stream_t stream);
 
+/* Backward of the alignment score f_b(R) = Re sum D(R_b) sigma_b (no counterpart in the
+ * reference, which differentiates only inside its Newton step, WignerDGradients.py:155-302):
+ * at the rotations (alpha, beta, gamma)_b (B,) float32 it regenerates D^l(R_b), l <= L, in
+ * FP64 (nothing is kept from a forward pass) and writes, each optional (NULL to skip):
+ *   grad_sigma (B, >= dsize(L)) complex64 = weight_b conj(D(R_b)), d f / d sigma in PyTorch's
+ *     convention for complex tensors;
+ *   grad_body (B, 3) float64 = weight_b d f_b(R_b exp(t e_k)) / dt at t = 0 (k = x, y, z), the
+ *     so(3) gradient in the body frame, from the generators of the representation applied to
+ *     sigma (no Euler-angle singularity at beta = 0 or pi; needs sigma).
+ * weight (B,) float32 or NULL (all 1). */
+int mtb_score_backward(const float* sigma, int64_t sigma_stride, int B, int L, const float* alpha, const float* beta,
+                       const float* gamma, const float* weight, float* grad_sigma, int64_t grad_stride,
+                       double* grad_body, mtb_stream_t stream);
+
 /* Allocation-free orientation search.  No counterpart in the reference: it is
  * mtb_search_orientations for callers that must not allocate device memory -- a host
  * program that hands all device memory to its own allocator or runs under a fixed
@@ -199,6 +213,18 @@ int mtb_sigma_upto(mtb_fle* h, const float* coeffs, int64_t coeff_stride, const 
  * are invalid); the flag is cleared once reported, and the handle stays usable. */
 int mtb_fle_status(mtb_fle* h, mtb_stream_t stream);
 
+/* Adjoint of the sigma contraction with respect to the template coefficients (no
+ * counterpart in the reference, which has no backward; the forward is
+ * CrossCorrelationMatcher.compute_sigma, src/matcha/core/CrossCorrelationMatcher.py:183-212):
+ * grad_tmpl[coef(l, -m, k)] = sum_b sum_m' (-1)^(m'+m) coeffs_b[coef(l, -m', k)]
+ * grad_sigma_b[l, m', m] for l <= lmax_g, zero above and in the padding entry ne.  coeffs
+ * (B, ne) complex64 (the volumes' coefficients, row stride coeff_stride), grad_sigma (B,
+ * >= dsize(lmax_g)) complex64, grad_tmpl (ne + 1) complex64 out; gradients in PyTorch's
+ * convention for complex tensors (d/dRe + i d/dIm of a real function).  One CTA per degree,
+ * the batch summed in order: deterministic. */
+int mtb_sigma_backward_template(mtb_fle* h, const float* coeffs, int64_t coeff_stride, const float* grad_sigma,
+                                int64_t grad_stride, int B, int lmax_g, float* grad_tmpl, mtb_stream_t stream);
+
 /* Test hook of the failure path (no counterpart in the reference): with on != 0 the
  * tensor-core GEMM of every following forward issues no operand loads, so its MMA thread's
  * bounded wait runs out after about 20 ms; the kernel records the error, frees its tensor
@@ -244,6 +270,20 @@ int mtb_shift_set_reference(mtb_shift* h, const float* ref_fourier, mtb_stream_t
  * float32 or NULL.  shift_xyz (B, 3) and score (B,) float32 out. */
 int mtb_shift_search(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot,
                      const float* ctf, int B, float* shift_xyz, float* score, mtb_stream_t stream);
+
+/* The shift match's correlation as a function of a continuous shift, and its gradient (no
+ * counterpart in the reference, which evaluates it only on the upsampled grid,
+ * ShiftMatcher.py:46-91, 94-282): for the same inputs as mtb_shift_search and query shifts
+ * query_xyz (B, 3) float32 in (x, y, z) voxels, score (B,) = c(s) and grad_xyz (B, 3) = dc/ds,
+ *   c(s) = Re sum_m P[m] exp(2 pi i s . f(m)) / (|T| |S|),
+ * P = conj(S) T the product of the rotated reference and the patch spectrum, f the
+ * frequencies of the (z, y, x) data axes with the half axis taken as a full period of
+ * length N/2+1 as the reference's upsampled DFT does.  On the grid s = (u - floor(U/2)) / uf
+ * c(s) is the value whose maximum mtb_shift_search returns.  Uses the handle's workspace
+ * (FP32 product whatever its precision); calls on one handle must be ordered. */
+int mtb_shift_score_grad(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot,
+                         const float* ctf, int B, const float* query_xyz, float* score, float* grad_xyz,
+                         mtb_stream_t stream);
 
 /* The precision a handle runs the upsampled DFT in (MTB_SHIFT_FP32 or MTB_SHIFT_BF16X3):
  * what MTB_SHIFT_AUTO resolved to.  No counterpart in the reference (a query of this build). */

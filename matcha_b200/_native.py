@@ -89,11 +89,14 @@ SIGNATURES = {
     "mtb_sigma_upto": (_I, [_P, _P, _I64, _P, _I, _I, _P, _I64, _P]),
     "mtb_fle_status": (_I, [_P, _P]),
     "mtb_fle_inject_stall": (_I, [_P, _I]),
+    "mtb_sigma_backward_template": (_I, [_P, _P, _I64, _P, _I64, _I, _I, _P, _P]),
+    "mtb_score_backward": (_I, [_P, _I64, _I, _I, _P, _P, _P, _P, _P, _I64, _P, _P]),
     "mtb_shift_create": (_I, [ctypes.POINTER(MtbShiftConfig), ctypes.POINTER(_P)]),
     "mtb_shift_destroy": (None, [_P]),
     "mtb_shift_set_reference": (_I, [_P, _P, _P]),
     "mtb_shift_status": (_I, [_P, _P]),
     "mtb_shift_precision": (_I, [_P, _P]),
+    "mtb_shift_score_grad": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P, _P]),
     "mtb_shift_profile": (_I, [_P, _I]),
     "mtb_shift_profile_read": (_I, [_P, _P, _P]),
     "mtb_shift_search": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P]),

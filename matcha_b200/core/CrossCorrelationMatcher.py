@@ -106,6 +106,39 @@ class CrossCorrelationMatcher:
             nat.check(self.fle._lib.mtb_fle_forward(self.fle._h, nat.ptr(vol), volumes.shape[0],
                                                   nat.ptr(self._coeffs), self._coeffs.stride(0),
                                                   nat.ptr(self.bh_norms), nat.stream_ptr(dev)), "mtb_fle_forward")
+        self._n_expanded = int(volumes.shape[0])
+
+    @torch.no_grad()
+    def expand(self, volumes: torch.Tensor):
+        """Expand a batch (b <= batchsize, N, N, N) and keep its coefficients for
+        ``sigma_from_template`` (extension: the template-independent half of get_sigma).
+        Returns the coefficients (b, ne) complex64, a view of an internal buffer."""
+        if volumes.shape[0] > self.batchsize:
+            raise ValueError(f"Input batch size {volumes.shape[0]} exceeds configured batchsize {self.batchsize}.")
+        self._expand(volumes)
+        return self._coeffs[:self._n_expanded]
+
+    @torch.no_grad()
+    def sigma_from_template(self, a_template: torch.Tensor, lmax: int):
+        """sigma (b, Dsize(lmax)) of the last expanded batch against the template coefficients
+        a_template (ne + 1,) complex64, in a tensor of its own (extension: the differentiable
+        half of get_sigma, see ``matcha_b200.autograd.template_sigma``)."""
+        n = getattr(self, "_n_expanded", None)
+        if n is None:
+            raise RuntimeError("expand (or get_sigma) must be called before sigma_from_template")
+        if not 0 <= lmax <= self.lmax:
+            raise ValueError(f"lmax must be in [0, {self.lmax}]")
+        t = a_template.to(device=self.device, dtype=torch.complex64).contiguous()
+        if t.shape != (self.fle.ne + 1,):
+            raise ValueError(f"a_template must have shape ({self.fle.ne + 1},)")
+        out = torch.empty((n, compute_size(lmax + 1)), dtype=torch.complex64, device=self.device)
+        if n == 0:
+            return out
+        with torch.cuda.device(self.device):
+            nat.check(self.fle._lib.mtb_sigma_upto(self.fle._h, nat.ptr(self._coeffs), self._coeffs.stride(0),
+                                                 nat.ptr(t), n, lmax, nat.ptr(out), out.stride(0),
+                                                 nat.stream_ptr(self.device)), "mtb_sigma_upto")
+        return out
 
     @torch.no_grad()
     def get_sigma_upto(self, volumes: torch.Tensor, lmax: int):

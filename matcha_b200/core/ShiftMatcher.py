@@ -151,6 +151,41 @@ class ShiftMatcher:
             self._free()
 
     @torch.no_grad()
+    def score_and_gradient(self, subtomos: torch.Tensor, shift_zyx: torch.Tensor, rot: torch.Tensor,
+                           query_xyz: torch.Tensor):
+        """The correlation the shift search maximises, as a function of a continuous shift, and
+        its gradient (extension, ``mtb_shift_score_grad``): for subtomograms (B, N, N, N) at the
+        prior shift_zyx (B, 3), reference rotations rot (B, 9) (row-major matrices as
+        ``mtb_tracker_rotation`` gives) and query shifts (B, 3) in (x, y, z), returns
+        (score (B,), gradient (B, 3)) float32.  On the 1/uf grid the score is the value
+        ``search_shifts`` compares."""
+        if self.reference_data_fourier is None:
+            raise RuntimeError("ShiftMatcher reference is not initialized. Call `set_reference` first.")
+        B = subtomos.shape[0]
+        vol = subtomos.to(self.device, torch.float32).contiguous()
+        nat.require_cuda(vol, "subtomos")
+        sz = torch.as_tensor(shift_zyx, device=self.device, dtype=torch.float32).reshape(B, 3).contiguous()
+        r = torch.as_tensor(rot, device=self.device, dtype=torch.float32).reshape(B, 9).contiguous()
+        q = torch.as_tensor(query_xyz, device=self.device, dtype=torch.float32).reshape(B, 3).contiguous()
+        h = self._handle(B)
+        self._upload_reference(h)
+        score = torch.empty((B,), device=self.device, dtype=torch.float32)
+        grad = torch.empty((B, 3), device=self.device, dtype=torch.float32)
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.mtb_shift_score_grad(h, nat.ptr(vol), nat.ptr(sz), nat.ptr(r), None, B, nat.ptr(q),
+                                                     nat.ptr(score), nat.ptr(grad), nat.stream_ptr(self.device)),
+                      "mtb_shift_score_grad")
+        return score, grad
+
+    def _upload_reference(self, h):
+        if self._uploaded_version != self._ref_version:
+            self._ref_dev = self.reference_data_fourier.to(torch.complex64).contiguous()
+            with torch.cuda.device(self.device):
+                nat.check(self._lib.mtb_shift_set_reference(h, nat.ptr(self._ref_dev), nat.stream_ptr(self.device)),
+                          "mtb_shift_set_reference")
+            self._uploaded_version = self._ref_version
+
+    @torch.no_grad()
     def set_reference(self, template_data: np.ndarray):
         """Precompute and cache the Fourier-domain reference (ShiftMatcher.py:805-822):
         ``load_reference_full`` on the device in FP64 (``mtb_shift_reference``)."""
@@ -216,12 +251,7 @@ class ShiftMatcher:
         out = torch.empty((B, 3), device=self.device, dtype=torch.float32)
         score = torch.empty((B,), device=self.device, dtype=torch.float32)
         h = self._handle(B)
-        if self._uploaded_version != self._ref_version:
-            self._ref_dev = self.reference_data_fourier.to(torch.complex64).contiguous()
-            with torch.cuda.device(self.device):
-                nat.check(self._lib.mtb_shift_set_reference(h, nat.ptr(self._ref_dev), nat.stream_ptr(self.device)),
-                          "mtb_shift_set_reference")
-            self._uploaded_version = self._ref_version
+        self._upload_reference(h)
         with torch.cuda.device(self.device):
             nat.check(self._lib.mtb_shift_search(h, nat.ptr(vol), nat.ptr(sz), nat.ptr(rot), nat.ptr(ctf), B,
                                                  nat.ptr(out), nat.ptr(score), nat.stream_ptr(self.device)),

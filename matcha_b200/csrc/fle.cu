@@ -491,6 +491,18 @@ extern "C" int mtb_sigma(mtb_fle* h, const float* coeffs, int64_t coeff_stride, 
   return mtb_sigma_upto(h, coeffs, coeff_stride, tmpl, B, h->cfg.lmax, sigma, sigma_stride, stream);
 }
 
+// The sigma gather tables of a handle, for the template backward (backward.cu).
+int fle_sigma_tables(const mtb_fle* h, const int** kpad, const int** koff, const int** kidx, int* lmax, int* kmax,
+                     int* ne) {
+  *kpad = h->kpad;
+  *koff = h->koff;
+  *kidx = h->kidx;
+  *lmax = h->cfg.lmax;
+  *kmax = h->kmax;
+  *ne = h->cfg.ne;
+  return MTB_OK;
+}
+
 extern "C" int mtb_fle_inject_stall(mtb_fle* h, int on) {
   MTB_ARG_CHECK(h, "null handle");
   MTB_ARG_CHECK(h->use_tc, "the stall hook acts on the tensor-core path only (precision MTB_FLE_BF16X3)");

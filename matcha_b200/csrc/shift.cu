@@ -885,6 +885,58 @@ __global__ void finalize_kernel(ShiftGeom g, int B, int ngrp, const float* __res
   score[b] = bv / den;
 }
 
+// The shift match's correlation at a continuous shift s and its gradient, from the FP32
+// product P = conj(S) T (data axes (z, y, x) = (m0, m1, m2), the last of length N/2+1):
+//   c(s) = Re sum_m P[m] exp(2 pi i s . f(m)) / (|T| |S|),  f = (fftfreq(N)[m0],
+//   fftfreq(N)[m1], fftfreq(N/2+1)[m2]),
+// the function whose values on the grid s = (u - dftshift) / uf the upsampled DFT evaluates
+// (ShiftMatcher.py:46-91, with the half axis taken as a full period as there), and
+// dc/ds_d = -2 pi sum_m f_d(m) Im(P[m] exp(2 pi i s . f(m))) / (|T| |S|).  One CTA per
+// subtomogram; s and the gradient in (x, y, z) order like the shifts the search returns.
+__device__ __forceinline__ float fftfreq_of(int m, int n) { return (float)(m <= (n - 1) / 2 ? m : m - n) / (float)n; }
+
+__global__ void __launch_bounds__(256)
+shift_score_grad_kernel(ShiftGeom g, const float2* __restrict__ P, const float* __restrict__ nrm,
+                        const float* __restrict__ s_xyz, float* __restrict__ score, float* __restrict__ grad_xyz) {
+  const int b = blockIdx.x;
+  const int N = g.N, H = g.H;
+  const int64_t per = (int64_t)N * N * H;
+  const float2* p = P + (int64_t)b * per;
+  const float sx = s_xyz[3 * b + 0], sy = s_xyz[3 * b + 1], sz = s_xyz[3 * b + 2];
+  double v = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+  for (int64_t e = threadIdx.x; e < per; e += blockDim.x) {
+    const int m0 = (int)(e / ((int64_t)N * H)), m1 = (int)((e / H) % N), m2 = (int)(e % H);
+    const float fz = fftfreq_of(m0, N), fy = fftfreq_of(m1, N), fx = fftfreq_of(m2, H);
+    float sn, cs;
+    sincospif(2.f * (sz * fz + sy * fy + sx * fx), &sn, &cs);
+    const float2 q = p[e];
+    const float re = q.x * cs - q.y * sn, im = q.x * sn + q.y * cs;
+    v += re;
+    gx += (double)(fx * im);
+    gy += (double)(fy * im);
+    gz += (double)(fz * im);
+  }
+  __shared__ double red[4][256];
+  red[0][threadIdx.x] = v;
+  red[1][threadIdx.x] = gx;
+  red[2][threadIdx.x] = gy;
+  red[3][threadIdx.x] = gz;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s)
+      for (int k = 0; k < 4; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double den = sqrt((double)nrm[2 * b]) * sqrt((double)nrm[2 * b + 1]);
+    const double tp = -2.0 * 3.14159265358979323846 / den;
+    score[b] = (float)(red[0][0] / den);
+    grad_xyz[3 * b + 0] = (float)(tp * red[1][0]);
+    grad_xyz[3 * b + 1] = (float)(tp * red[2][0]);
+    grad_xyz[3 * b + 2] = (float)(tp * red[3][0]);
+  }
+}
+
 // Tensor-core path: decode the per-subtomogram argmax key of the third pass.
 __global__ void finalize_tc_kernel(ShiftGeom g, int B, const unsigned long long* __restrict__ best,
                                    const float* __restrict__ nrm, float* __restrict__ shift_xyz,
@@ -945,7 +997,7 @@ void prof_mark(mtb_shift* h, int k, cudaStream_t st) {
 // plane transforms of the background fill weight, once per geometry, into h->what.
 template <int N>
 int shift_front_n(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
-                  int B, cudaStream_t st) {
+                  int B, cudaStream_t st, bool split) {
   const ShiftGeom& g = h->g;
   const int sxy = (int)xy_smem_bytes<N>(), sz = (int)z_smem_bytes<N>();
   if (B == 0) {
@@ -960,7 +1012,7 @@ int shift_front_n(mtb_shift* h, const float* subtomos, const float* shift_zyx, c
   mtb_prof_end(st, "patch_fft_xy_kernel");
   MTB_LAUNCH_CHECK();
   prof_mark(h, 1, st);
-  if (h->use_tc) {
+  if (split) {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
     mtb_prof_begin(st);
     fft_z_kernel<N, true><<<dim3(N, B), kT, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm,
@@ -979,7 +1031,7 @@ int shift_front_n(mtb_shift* h, const float* subtomos, const float* shift_zyx, c
 }
 
 int shift_front_64(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
-                   int B, cudaStream_t st) {
+                   int B, cudaStream_t st, bool split) {
   const ShiftGeom& g = h->g;
   const int sxy = (int)xy64_smem_bytes(), sz = (int)z64_smem_bytes();
   MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
@@ -988,7 +1040,7 @@ int shift_front_64(mtb_shift* h, const float* subtomos, const float* shift_zyx, 
   mtb_prof_end(st, "patch_fft_xy64_kernel");
   MTB_LAUNCH_CHECK();
   prof_mark(h, 1, st);
-  if (h->use_tc) {
+  if (split) {
     MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
     mtb_prof_begin(st);
     fft_z64_kernel<true><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
@@ -1006,16 +1058,17 @@ int shift_front_64(mtb_shift* h, const float* subtomos, const float* shift_zyx, 
   return MTB_OK;
 }
 
+// split: the z pass writes the tensor-core pass-1 operand (A1) instead of the FP32 product in T.
 int shift_front(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
-                int B, cudaStream_t st) {
+                int B, cudaStream_t st, bool split) {
   switch (h->g.N) {
-    case 4: return shift_front_n<4>(h, subtomos, shift_zyx, rot, ctf, B, st);
-    case 8: return shift_front_n<8>(h, subtomos, shift_zyx, rot, ctf, B, st);
-    case 16: return shift_front_n<16>(h, subtomos, shift_zyx, rot, ctf, B, st);
-    case 32: return shift_front_n<32>(h, subtomos, shift_zyx, rot, ctf, B, st);
-    case 64: return B > 0 ? shift_front_64(h, subtomos, shift_zyx, rot, ctf, B, st)
-                          : shift_front_n<64>(h, subtomos, shift_zyx, rot, ctf, B, st);
-    case 128: return shift_front_n<128>(h, subtomos, shift_zyx, rot, ctf, B, st);
+    case 4: return shift_front_n<4>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
+    case 8: return shift_front_n<8>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
+    case 16: return shift_front_n<16>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
+    case 32: return shift_front_n<32>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
+    case 64: return B > 0 ? shift_front_64(h, subtomos, shift_zyx, rot, ctf, B, st, split)
+                          : shift_front_n<64>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
+    case 128: return shift_front_n<128>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
     default: MTB_ARG_CHECK(false, "N must be a power of two in [4, 128]");
   }
 }
@@ -1111,7 +1164,7 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
     return fail(MTB_ERR_CUDA);
   fill_table_kernel<<<(r2max + 256) / 256, 256>>>(g, r2max + 1, h->fill_tab);
   if (cudaGetLastError() != cudaSuccess) return fail(MTB_ERR_CUDA);
-  if (shift_front(h, nullptr, nullptr, nullptr, nullptr, 0, 0) != MTB_OK) return fail(MTB_ERR_CUDA);
+  if (shift_front(h, nullptr, nullptr, nullptr, nullptr, 0, 0, false) != MTB_OK) return fail(MTB_ERR_CUDA);
   if (cudaStreamSynchronize(0) != cudaSuccess) return fail(MTB_ERR_CUDA);
   // MTB_SHIFT_BF16X3 was checked to fit the tensor-core kernels above; MTB_SHIFT_AUTO uses them
   // where they fit and the FP32 CUDA-core kernels elsewhere
@@ -1180,7 +1233,7 @@ extern "C" int mtb_shift_search(mtb_shift* h, const float* subtomos, const float
   MTB_CUDA_TRY(cudaMemsetAsync(h->bg, 0, (size_t)B * 4, st));
   MTB_CUDA_TRY(cudaMemsetAsync(h->nrm, 0, (size_t)B * 8, st));
   prof_mark(h, 0, st);
-  int rc = shift_front(h, subtomos, shift_zyx, rot, ctf, B, st);
+  int rc = shift_front(h, subtomos, shift_zyx, rot, ctf, B, st, h->use_tc);
   if (rc) return rc;
   prof_mark(h, 2, st);
   if (h->use_tc) {
@@ -1222,6 +1275,27 @@ extern "C" int mtb_shift_search(mtb_shift* h, const float* subtomos, const float
   MTB_LAUNCH_CHECK();
   prof_mark(h, 6, st);
   if (h->prof_cap > 0) ++h->prof_n;
+  return MTB_OK;
+}
+
+extern "C" int mtb_shift_score_grad(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot,
+                                    const float* ctf, int B, const float* query_xyz, float* score, float* grad_xyz,
+                                    mtb_stream_t stream) {
+  MTB_ARG_CHECK(h, "null handle");
+  MTB_ARG_CHECK(h->has_ref, "shift reference is not set");
+  MTB_ARG_CHECK(B >= 0 && B <= h->cfg.max_batch, "batch exceeds max_batch");
+  if (B == 0) return MTB_OK;
+  MTB_ARG_CHECK(subtomos && shift_zyx && rot && query_xyz && score && grad_xyz, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  MTB_CUDA_TRY(cudaMemsetAsync(h->bg, 0, (size_t)B * 4, st));
+  MTB_CUDA_TRY(cudaMemsetAsync(h->nrm, 0, (size_t)B * 8, st));
+  // the FP32 product in T, whatever the handle's precision
+  if (int rc = shift_front(h, subtomos, shift_zyx, rot, ctf, B, st, false)) return rc;
+  mtb_prof_begin(st);
+  shift_score_grad_kernel<<<B, 256, 0, st>>>(h->g, reinterpret_cast<const float2*>(h->T), h->nrm, query_xyz, score,
+                                             grad_xyz);
+  mtb_prof_end(st, "shift_score_grad_kernel");
+  MTB_LAUNCH_CHECK();
   return MTB_OK;
 }
 

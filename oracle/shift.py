@@ -201,3 +201,23 @@ def estimate_shift_like_relion(ref_fourier, subtomo, shift_zyx, angles_deg, uf, 
     if return_parts:
         return out, dict(rot=rot, patch=patch, sub=sub, grid=val)
     return out
+
+
+def shift_score_and_grad(ref_fourier, subtomo, shift_zyx, angles_deg, s_xyz, box_size=None, voxel_size=1.0):
+    """The correlation the upsampled DFT of local_upsampled_peak samples, as a function of a
+    continuous shift s (x, y, z): c(s) = Re sum_m prod[m] exp(2 pi i s . f(m)) / (|tgt| |src|)
+    with prod = conj(src) tgt and f = (fftfreq(N), fftfreq(N), fftfreq(N/2+1)) on the (z, y, x)
+    data axes; returns (c, dc/ds in (x, y, z))."""
+    _, parts = estimate_shift_like_relion(ref_fourier, subtomo, shift_zyx, angles_deg, 1, 0, box_size=box_size,
+                                          voxel_size=voxel_size, return_parts=True)
+    src, tgt = parts["rot"], parts["sub"]
+    prod = np.conj(src) * tgt
+    n0, n1, n2 = prod.shape
+    f0, f1, f2 = np.meshgrid(np.fft.fftfreq(n0), np.fft.fftfreq(n1), np.fft.fftfreq(n2), indexing="ij")
+    s = np.asarray(s_xyz, dtype=np.float64)
+    e = prod * np.exp(2j * np.pi * (s[2] * f0 + s[1] * f1 + s[0] * f2))
+    den = np.linalg.norm(tgt) * np.linalg.norm(src)
+    c = e.real.sum() / den
+    g = np.array([(2j * np.pi * f2 * e).real.sum(), (2j * np.pi * f1 * e).real.sum(),
+                  (2j * np.pi * f0 * e).real.sum()]) / den
+    return c, g
