@@ -1,12 +1,12 @@
 """Small, self-contained runs of each stage of the alignment path, for profilers.
 
-    python -m matcha_b200.profile_cases shift  200   # ShiftMatcher.search_shifts, 64^3, uf 8, r 5
-    python -m matcha_b200.profile_cases search 296   # Matcha.search_orientations, L 32, C 10
-    python -m matcha_b200.profile_cases fle    256   # CrossCorrelationMatcher.get_sigma, 64^3, L 32
-    python -m matcha_b200.profile_cases prepare 1000 # shifted patch, masked normalisation, rotation, 64^3
-    python -m matcha_b200.profile_cases reader 1000  # MRC decode of 1000 64^3 files into pinned memory
-    python -m matcha_b200.profile_cases graph 64     # one alternation, 64^3 L 32: eager calls vs a CUDA graph
-    python -m matcha_b200.profile_cases shift 1000 --stages   # plus ShiftMatcher.profile per kernel group
+    python bench_cases.py shift  200   # ShiftMatcher.search_shifts, 64^3, uf 8, r 5
+    python bench_cases.py search 296   # Matcha.search_orientations, L 32, C 10
+    python bench_cases.py fle    256   # CrossCorrelationMatcher.get_sigma, 64^3, L 32
+    python bench_cases.py prepare 1000 # shifted patch, masked normalisation, rotation, 64^3
+    python bench_cases.py reader 1000  # MRC decode of 1000 64^3 files into pinned memory
+    python bench_cases.py graph 64     # one alternation, 64^3 L 32: eager calls vs a CUDA graph
+    python bench_cases.py shift 1000 --stages   # plus ShiftMatcher.profile per kernel group
 
 Each case builds its inputs on the device from a fixed seed (random volumes, Haar rotations,
 random shifts; a synthetic sigma with a known optimum for the search), runs the stage three
@@ -17,7 +17,10 @@ that stage, on a batch small enough to capture quickly.
 from __future__ import annotations
 
 import argparse
+import os
 import sys
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 import numpy as np
 import torch
@@ -28,7 +31,7 @@ class _Cfg(dict):
 
 
 def _shift(B: int, dev):
-    from .core.ShiftMatcher import ShiftMatcher
+    from matcha_b200.core.ShiftMatcher import ShiftMatcher
 
     N = 64
     cfg = _Cfg(N=N, voxel_size=1.0, num_subtomograms_per_batch=B, shift_upsample_factor=8, shift_search_radius=5,
@@ -46,8 +49,8 @@ def _shift(B: int, dev):
 
 
 def _search(B: int, dev):
-    from .core.Matcha import Matcha
-    from .core.wigner_index import compute_size
+    from matcha_b200.core.Matcha import Matcha
+    from matcha_b200.core.wigner_index import compute_size
 
     L = 32
     rng = np.random.default_rng(0)
@@ -60,7 +63,7 @@ def _search(B: int, dev):
 
 
 def _fle(B: int, dev):
-    from .core.CrossCorrelationMatcher import CrossCorrelationMatcher
+    from matcha_b200.core.CrossCorrelationMatcher import CrossCorrelationMatcher
 
     N = 64
     cc = CrossCorrelationMatcher(N=N, device=dev, batchsize=B, bandlimit=32, radius=30, precision_mode="fast",
@@ -72,7 +75,7 @@ def _fle(B: int, dev):
 
 
 def _prepare(B: int, dev):
-    from . import _native as nat
+    from matcha_b200 import _native as nat
 
     N = 64
     lib = nat.load()
@@ -100,7 +103,7 @@ def _reader(B: int, reps: int) -> int:
     import tempfile
     import time
 
-    from .reader import MrcReader, write_mrc
+    from matcha_b200.reader import MrcReader, write_mrc
 
     N = 64
     rng = np.random.default_rng(0)
@@ -144,7 +147,7 @@ def _reader(B: int, reps: int) -> int:
 def _graph(B: int, reps: int) -> int:
     """One alternation (AlignmentStep at 64^3, L 32) on B random volumes: eager calls against
     the replay of its CUDA graph, CUDA events, ``reps`` calls each."""
-    from .pipeline import AlignmentStep, StepConfig
+    from matcha_b200.pipeline import AlignmentStep, StepConfig
 
     dev = torch.device("cuda:0")
     rng = np.random.default_rng(0)

@@ -249,6 +249,8 @@ typedef struct {
                             tcgen05 BF16 GEMMs with a hi+lo split, MTB_ERR_ARG from create on a
                             box / upsampled region the tensor-core kernels do not cover;
                             MTB_SHIFT_AUTO: the tensor cores where they cover it, else FP32 */
+  int tile_rows;         /* FP32 upsampled DFT: rows u0 per CTA of its passes 2+3 (0: 2), the tile
+                            shape matcha_b200.autotune chooses per box; no effect on the result */
 } mtb_shift_config;
 
 #define MTB_SHIFT_FP32 0

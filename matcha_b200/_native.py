@@ -63,7 +63,7 @@ class MtbShiftConfig(ctypes.Structure):
     _fields_ = [
         ("N", ctypes.c_int), ("max_batch", ctypes.c_int), ("upsample_factor", ctypes.c_int),
         ("search_radius", ctypes.c_int), ("mask_radius", ctypes.c_float), ("cosine_width", ctypes.c_float),
-        ("precision", ctypes.c_int),
+        ("precision", ctypes.c_int), ("tile_rows", ctypes.c_int),
     ]
 
 

@@ -59,13 +59,14 @@ class ShiftMatcher:
     """Stateful shift-search wrapper (ShiftMatcher.py:766-928)."""
 
     def __init__(self, config, device: torch.device, dtype: torch.dtype, micro_batch_size: int = None,
-                 precision: str = None):
+                 precision: str = None, tile_rows: int = 0):
         if precision is None:
             precision = resolve_precision(config)
         if precision not in ("fp32", "bf16x3", "auto"):
             raise ValueError("precision must be 'fp32' (CUDA cores), 'bf16x3' (tensor cores, hi+lo split) or "
                              "'auto' (tensor cores where the geometry allows)")
         self.precision = precision
+        self.tile_rows = int(tile_rows)  # FP32 upsampled DFT tile (0: default); matcha_b200.autotune
         self.config = config
         self.device = torch.device(device)
         self.dtype = dtype
@@ -98,6 +99,7 @@ class ShiftMatcher:
         cfg.cosine_width = 5.0
         cfg.precision = {"fp32": nat.MTB_SHIFT_FP32, "bf16x3": nat.MTB_SHIFT_BF16X3, "auto": nat.MTB_SHIFT_AUTO}[
             self.precision]
+        cfg.tile_rows = self.tile_rows
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             nat.check(self._lib.mtb_shift_create(ctypes.byref(cfg), ctypes.byref(h)), "mtb_shift_create")

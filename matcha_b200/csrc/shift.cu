@@ -168,12 +168,34 @@ __device__ __forceinline__ int brev(int k) {
   return (int)(__brev((unsigned)k) >> kShift);
 }
 
-__device__ void load_twiddles(float2* tw, int L) {
-  for (int k = threadIdx.x; k < L / 2; k += blockDim.x) {
+__device__ void load_twiddles(float2* tw, int L, int count) {
+  for (int k = threadIdx.x; k < count; k += blockDim.x) {
     double s, c;
     sincospi(-2.0 * k / L, &s, &c);
     tw[k] = make_float2((float)c, (float)s);
   }
+}
+
+__device__ void load_twiddles(float2* tw, int L) { load_twiddles(tw, L, L / 2); }
+
+// Boxes that are not powers of two (48, 80, 96) take the same kernels with the radix-2 FFTs
+// replaced by direct DFTs (O(N^2) per line, natural-order output) and the index rolls done by
+// comparison instead of a mask.
+template <int N>
+__host__ __device__ constexpr bool is_pow2() {
+  return (N & (N - 1)) == 0;
+}
+
+template <int N>
+__device__ __forceinline__ int wrap_n(int x) {  // x in [0, 2N) -> x mod N
+  if constexpr (is_pow2<N>()) return x & (N - 1);
+  return x >= N ? x - N : x;
+}
+
+// Twiddles a kernel loads: N/2 for the radix-2 FFT, N for the direct DFT.
+template <int N>
+__host__ __device__ constexpr int n_twiddles() {
+  return is_pow2<N>() ? N / 2 : N;
 }
 
 // In-place decimation-in-frequency forward FFT (e^{-2 pi i k n / N}) of `lines` sequences,
@@ -195,6 +217,46 @@ __device__ __forceinline__ void fft_dif(float2* buf, int lines, int ls, int es, 
       const float2 u = *p0, c = *p1;
       *p0 = make_float2(u.x + c.x, u.y + c.y);
       *p1 = cmul(make_float2(u.x - c.x, u.y - c.y), tw[pos * tstride]);
+    }
+    __syncthreads();
+  }
+}
+
+// Position of frequency k in a transformed line: bit-reversed after fft_dif, natural after
+// the direct DFT.
+template <int N>
+__device__ __forceinline__ int fpos(int k) {
+  if constexpr (is_pow2<N>()) return brev<N>(k);
+  return k;
+}
+
+// Forward transform of `lines` sequences in place (layout as fft_dif).  Powers of two: fft_dif
+// (scratch unused); otherwise a direct DFT through scratch (lines x N elements at the same
+// strides), tw[j] = e^{-2 pi i j / N} for j < N.  Ends with a barrier.
+template <int N>
+__device__ __forceinline__ void transform_lines(float2* buf, float2* scratch, int lines, int ls, int es,
+                                                const float2* __restrict__ tw) {
+  if constexpr (is_pow2<N>()) {
+    fft_dif<N>(buf, lines, ls, es, tw);
+  } else {
+    for (int e = threadIdx.x; e < lines * N; e += blockDim.x) {
+      const int q = e / N, t = e % N;
+      scratch[q * ls + t * es] = buf[q * ls + t * es];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < lines * N; e += blockDim.x) {
+      const int q = e / N, k = e % N;
+      const float2* src = scratch + q * ls;
+      float re = 0.f, im = 0.f;
+      int j = 0;
+      for (int n = 0; n < N; ++n) {
+        const float2 x = src[n * es], w = tw[j];
+        re += x.x * w.x - x.y * w.y;
+        im += x.x * w.y + x.y * w.x;
+        j += k;
+        if (j >= N) j -= N;
+      }
+      buf[q * ls + k * es] = make_float2(re, im);
     }
     __syncthreads();
   }
@@ -228,22 +290,26 @@ patch_fft_xy_kernel(const float* __restrict__ vol, const float* __restrict__ shi
   constexpr int HN = N / 2, H = N / 2 + 1;
   extern __shared__ __align__(16) float2 sm2[];
   __shared__ float red[32];
-  float2* tw = sm2;                                       // N/2
-  float2* zb = sm2 + HN;                                  // HN x N: rows q (re) and q + HN (im)
-  float* planes = reinterpret_cast<float*>(zb + HN * N);  // 2 x N x N input planes
+  constexpr int NTW = n_twiddles<N>();
+  // the zb region holds N x H entries (HN x N used) so that it can serve as the y
+  // transform's scratch in the direct-DFT case
+  constexpr int ZB = is_pow2<N>() ? HN * N : N * H;
+  float2* tw = sm2;                                       // NTW
+  float2* zb = sm2 + NTW;                                 // HN x N: rows q (re) and q + HN (im)
+  float* planes = reinterpret_cast<float*>(zb + ZB);      // 2 x N x N input planes
   float2* yb = reinterpret_cast<float2*>(planes);         // N x H, after the patch is built
   const int ip = blockIdx.x, b = blockIdx.y;
-  const int i = (ip + HN) & (N - 1);
+  const int i = wrap_n<N>(ip + HN);
   const int di = i - HN;
-  load_twiddles(tw, N);
+  load_twiddles(tw, N, NTW);
   auto put = [&](int jp, int kp, float val) {
-    reinterpret_cast<float*>(zb + (jp & (HN - 1)) * N + kp)[jp >= HN ? 1 : 0] = val;
+    reinterpret_cast<float*>(zb + (jp < HN ? jp : jp - HN) * N + kp)[jp >= HN ? 1 : 0] = val;
   };
   float part = 0.f;
   if (PATTERN) {
     for (int e = threadIdx.x; e < N * N; e += kT) {
       const int jp = e / N, kp = e % N;
-      const int dj = ((jp + HN) & (N - 1)) - HN, dk = ((kp + HN) & (N - 1)) - HN;
+      const int dj = wrap_n<N>(jp + HN) - HN, dk = wrap_n<N>(kp + HN) - HN;
       put(jp, kp, fill_weight(di * di + dj * dj + dk * dk, g) * g.inv_n3);
     }
   } else {
@@ -266,7 +332,7 @@ patch_fft_xy_kernel(const float* __restrict__ vol, const float* __restrict__ shi
     const bool zplane = (i == ps.zp[0]);
     for (int e = threadIdx.x; e < N * N; e += kT) {
       const int jp = e / N, kp = e % N;
-      const int j = (jp + HN) & (N - 1), k = (kp + HN) & (N - 1);
+      const int j = wrap_n<N>(jp + HN), k = wrap_n<N>(kp + HN);
       float p = 0.f;
       if (!zplane && j != ps.zp[1] && k != ps.zp[2]) {
         const float y = (float)j + ps.f[1], x = (float)k + ps.f[2];
@@ -292,21 +358,22 @@ patch_fft_xy_kernel(const float* __restrict__ vol, const float* __restrict__ shi
     }
   }
   __syncthreads();
-  fft_dif<N>(zb, HN, N, 1, tw);
+  // (the direct DFT's scratch for zb is the planes region, free once the patch is built)
+  transform_lines<N>(zb, reinterpret_cast<float2*>(planes), HN, N, 1, tw);
   // split the packed transforms: Z = A + i B with A, B the transforms of rows q and q + HN
   for (int e = threadIdx.x; e < HN * H; e += kT) {
     const int q = e / H, k = e % H;
-    const float2 zk = zb[q * N + brev<N>(k)];
-    const float2 zm = zb[q * N + brev<N>((N - k) & (N - 1))];
+    const float2 zk = zb[q * N + fpos<N>(k)];
+    const float2 zm = zb[q * N + fpos<N>(k == 0 ? 0 : N - k)];
     yb[q * H + k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
     yb[(q + HN) * H + k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
   }
   __syncthreads();
-  fft_dif<N>(yb, H, 1, H, tw);
+  transform_lines<N>(yb, zb, H, 1, H, tw);
   float2* out = T + ((int64_t)b * N + ip) * N * H;
   for (int e = threadIdx.x; e < N * H; e += kT) {
     const int jp = e / H, m2 = e % H;
-    out[e] = yb[brev<N>(jp) * H + m2];
+    out[e] = yb[fpos<N>(jp) * H + m2];
   }
   if (!PATTERN) {
     part = block_sum(part, red);
@@ -316,7 +383,8 @@ patch_fft_xy_kernel(const float* __restrict__ vol, const float* __restrict__ shi
 
 template <int N>
 constexpr size_t xy_smem_bytes() {
-  return (size_t)(N / 2 + (N / 2) * N) * sizeof(float2) + (size_t)2 * N * N * sizeof(float);
+  return (size_t)(n_twiddles<N>() + (is_pow2<N>() ? (N / 2) * N : N * (N / 2 + 1))) * sizeof(float2) +
+         (size_t)2 * N * N * sizeof(float);
 }
 
 // ------------------------------------------------------------------ FFT along z + product
@@ -333,15 +401,17 @@ fft_z_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ wha
              float* __restrict__ nrm, uint32_t* __restrict__ a1, int a1_ws, int a1_R, uint32_t* __restrict__ a1n,
              int a1n_R) {
   constexpr int HN = N / 2, H = N / 2 + 1;
+  constexpr int NTW = n_twiddles<N>();
   extern __shared__ __align__(16) float2 sm2[];
   __shared__ float red[32];
   float2* tw = sm2;
-  float2* buf = sm2 + HN;  // N (i') x H
+  float2* buf = sm2 + NTW;   // N (i') x H
+  float2* scr = buf + N * H; // the direct DFT's scratch (boxes that are not powers of two)
   const int jp = blockIdx.x, b = blockIdx.y;
   float2* base = T + (int64_t)b * N * N * H + (int64_t)jp * H;
   const float2* wb = what + (int64_t)jp * H;
   const float avg = g.wsum > 0.f ? __ldg(&bg[b]) / g.wsum : 0.f;
-  load_twiddles(tw, N);
+  load_twiddles(tw, N, NTW);
   for (int e = threadIdx.x; e < N * H; e += kT) {
     const int ip = e / H, m2 = e % H;
     const float2 t = base[(int64_t)ip * N * H + m2];
@@ -349,7 +419,7 @@ fft_z_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ wha
     buf[e] = make_float2(fmaf(avg, w.x, t.x), fmaf(avg, w.y, t.y));
   }
   __syncthreads();
-  fft_dif<N>(buf, H, 1, H, tw);
+  transform_lines<N>(buf, scr, H, 1, H, tw);
   float R[9];
 #pragma unroll
   for (int q = 0; q < 9; ++q) R[q] = __ldg(&rot[b * 9 + q]);
@@ -358,7 +428,7 @@ fft_z_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ wha
   for (int e = threadIdx.x; e < N * H; e += kT) {
     // SPLIT walks m0 fastest so the bf16 rows are written contiguously
     const int ip = SPLIT ? e % N : e / H, m2 = SPLIT ? e / N : e % H;
-    const float2 t = buf[brev<N>(ip) * H + m2];
+    const float2 t = buf[fpos<N>(ip) * H + m2];
     // mask_full on the (N, N, N/2+1) index grid (setup_utils.py:239-249)
     const int kp = ip < HN ? ip : ip - N;
     const int jq = jp < HN ? jp : jp - N;
@@ -366,7 +436,7 @@ fft_z_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ wha
     float2 s = make_float2(0.f, 0.f);
     if (kp * kp + jq * jq + xq * xq <= g.mask_r2) {
       // ifftshift over (z, y) of the slice [..., N/2:] of the rotated reference
-      const int zo = (ip + HN) & (N - 1), yo = (jp + HN) & (N - 1), xw = m2 + HN;
+      const int zo = wrap_n<N>(ip + HN), yo = wrap_n<N>(jp + HN), xw = m2 + HN;
       const float bx = (float)xw - c, by = (float)yo - c, bz = (float)zo - c;
       const float rx = R[0] * bx + R[1] * by + R[2] * bz + c;
       const float ry = R[3] * bx + R[4] * by + R[5] * bz + c;
@@ -411,7 +481,7 @@ fft_z_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ wha
 
 template <int N>
 constexpr size_t z_smem_bytes() {
-  return (size_t)(N / 2 + N * (N / 2 + 1)) * sizeof(float2);
+  return (size_t)(n_twiddles<N>() + (is_pow2<N>() ? 1 : 2) * N * (N / 2 + 1)) * sizeof(float2);
 }
 
 // ------------------------------------------------------------------ box 64: radix-8 x 8 path
@@ -1069,7 +1139,10 @@ int shift_front(mtb_shift* h, const float* subtomos, const float* shift_zyx, con
     case 64: return B > 0 ? shift_front_64(h, subtomos, shift_zyx, rot, ctf, B, st, split)
                           : shift_front_n<64>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
     case 128: return shift_front_n<128>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
-    default: MTB_ARG_CHECK(false, "N must be a power of two in [4, 128]");
+    case 48: return shift_front_n<48>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
+    case 80: return shift_front_n<80>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
+    case 96: return shift_front_n<96>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
+    default: MTB_ARG_CHECK(false, "N must be a power of two in [4, 128] or 48, 80, 96");
   }
 }
 
@@ -1077,10 +1150,12 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
   MTB_ARG_CHECK(cfg && out, "null argument");
   *out = nullptr;
   const int N = cfg->N;
-  MTB_ARG_CHECK(N >= 4 && N <= 128 && (N & (N - 1)) == 0, "N must be a power of two in [4, 128]");
+  MTB_ARG_CHECK((N >= 4 && N <= 128 && (N & (N - 1)) == 0) || N == 48 || N == 80 || N == 96,
+                "N must be a power of two in [4, 128] or 48, 80, 96");
   MTB_ARG_CHECK(cfg->max_batch >= 1 && cfg->max_batch <= 65535, "max_batch out of range");
   MTB_ARG_CHECK(cfg->upsample_factor >= 2 && cfg->search_radius >= 0, "upsample_factor must be > 1");
   MTB_ARG_CHECK(cfg->cosine_width > 0.f, "cosine_width must be positive");
+  MTB_ARG_CHECK(cfg->tile_rows >= 0 && cfg->tile_rows <= 32, "tile_rows must be in [0, 32]");
   MTB_ARG_CHECK(cfg->precision == MTB_SHIFT_FP32 || cfg->precision == MTB_SHIFT_BF16X3 ||
                     cfg->precision == MTB_SHIFT_AUTO,
                 "precision must be MTB_SHIFT_FP32, MTB_SHIFT_BF16X3 or MTB_SHIFT_AUTO");
@@ -1144,7 +1219,7 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
   std::vector<float2> e0, e2;
   kern(N, e0);
   kern(g.H, e2);
-  h->rows_per_cta = 2;
+  h->rows_per_cta = cfg->tile_rows > 0 ? cfg->tile_rows : 2;
   h->ngrp = (g.U + h->rows_per_cta - 1) / h->rows_per_cta;
   const size_t B = cfg->max_batch;
   auto fail = [&](int code) { mtb_shift_destroy(h); return code; };

@@ -35,9 +35,11 @@ class StepConfig:
     shift_search_radius: int = 5
     box_size: float | None = None
     voxel_size: float = 1.0
-    precision: str = "bf16x3"        # dense contractions (ball expansion, upsampled DFT): "bf16x3" on
-                                     # tcgen05 with a hi+lo split, "fp32" on CUDA cores, or "auto":
-                                     # the expansion on tcgen05 and the upsampled DFT there where its
+    shift_tile_rows: int = 0         # FP32 upsampled DFT tile (0: default), set by matcha_b200.autotune
+    precision: str = "auto"          # dense contractions (ball expansion, upsampled DFT): "bf16x3" on
+                                     # tcgen05 with a hi+lo split (an error where the shift kernels do
+                                     # not cover the box), "fp32" on CUDA cores, or "auto": the
+                                     # expansion on tcgen05 and the upsampled DFT there where its
                                      # kernels cover the box (ShiftMatcher.effective_precision)
 
 
@@ -68,7 +70,8 @@ class AlignmentStep:
                                          shift_upsample_factor=cfg.shift_upsample_factor,
                                          shift_search_radius=cfg.shift_search_radius, do_ctf_correction=False,
                                          box_size=cfg.box_size if cfg.box_size is not None else cfg.N),
-                                    self.device, torch.complex64, precision=cfg.precision)
+                                    self.device, torch.complex64, precision=cfg.precision,
+                                    tile_rows=cfg.shift_tile_rows)
         B = cfg.batch
         self.rot = torch.empty((B, 9), device=self.device, dtype=torch.float32)
         self.shift = torch.empty((B, 3), device=self.device, dtype=torch.float32)

@@ -40,7 +40,8 @@ def test_shift_matches_reference_fixture(cuda_device):
                                               (64, 8, 5, "bf16x3"), (32, 8, 3, "bf16x3"),
                                               (16, 4, 1, "bf16x3"), (32, 4, 2, "bf16x3"),
                                               (32, 8, 5, "bf16x3"), (16, 8, 5, "bf16x3"),
-                                              (128, 8, 8, "auto")])
+                                              (128, 8, 8, "auto"), (48, 8, 6, "fp32"), (96, 8, 6, "auto"),
+                                              (80, 4, 3, "fp32")])
 def test_shift_matches_oracle(cuda_device, N, uf, r, precision):
     rng = np.random.default_rng(N + uf + r)
     tmpl = blob_template(rng, N, 60, N * 0.3, (1.5, 3.0), mask_radius=N * 0.4)

@@ -32,10 +32,10 @@ def test_install_routes_reference_modules(monkeypatch):
     assert "matcha.core.Matcha" not in sys.modules
 
 
-def test_profile_cases_needs_a_device(monkeypatch):
+def test_bench_cases_need_a_device(monkeypatch):
     import torch
 
-    from matcha_b200 import profile_cases
+    import bench_cases as profile_cases
 
     monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
     assert profile_cases.main(["shift", "2"]) == 2
