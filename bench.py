@@ -299,11 +299,15 @@ def kernel_work(B):
         "patch_fft_xy64_kernel": ("hbm", vol + spec),
         "fft_z64_kernel": ("hbm", spec + a1 + a1n),
         "updft1_tc_kernel": ("tensor", 2.0 * (N // 2 * N) * (2 * N) * (2 * U)),
+        # the Nyquist plane m2 = N/2 as its own two small GEMMs: rows (b, m1), then rows (b, u0)
+        "updft1_tc_kernel (Nyquist plane, pass 1)": ("tensor", 2.0 * N * (2 * N) * (2 * U)),
+        "updft1_tc_kernel (Nyquist plane, pass 2)": ("tensor", 2.0 * U * (2 * N) * (2 * U)),
         "updft23_tc_kernel": ("tensor", 2.0 * (U * N // 2) * (2 * U) * (2 * N) + 2.0 * U * U * U * (N + 2)),
         "finalize_tc_kernel": ("hbm", 16),
     }
-    work["newton_march_kernel"] = ("fp32", float(sum((15 + 2) * 8 * 10 * dsize(Li) * 1 + 8 * 10 * dsize(Li)
-                                                     for Li in LI + [L_MAX])))
+    # newton_march_kernel has no entry: its folded wedge chains do far less arithmetic than the
+    # reference's 15-column bank contraction, and ncu shows it bound by issue and L2 latency
+    # (profiles/search_L32_b296.md), not by a pipe's throughput
     return {k: (b, a * B) for k, (b, a) in work.items()}, {"a2_bytes": a2}
 
 
@@ -341,7 +345,7 @@ def kernel_table(prof, steps, B, peaks, fp32_peak):
     for name, v in prof.items():
         ms = v["ms"] / steps
         row = {"ms_per_step": ms, "launches_per_step": v["launches"] / steps, "share": v["ms"] / total if total else None}
-        base = name.split(" (")[0]
+        base = name if name in work else name.split(" (")[0]
         if base in work and v["launches"] / steps == 1:
             bound, amount = work[base]
             if bound == "hbm":
@@ -351,8 +355,8 @@ def kernel_table(prof, steps, B, peaks, fp32_peak):
             else:
                 ach, peak, unit = amount / (ms * 1e-3) / 1e12, fp32_peak, "TFLOP/s"
             row.update(bound=bound, achieved=ach, peak=peak, unit=unit, frac=ach / peak if peak else None)
-            if DRAM_BYTES_PER_SUBTOMO.get(base):
-                row["traffic"] = DRAM_BYTES_PER_SUBTOMO[base] * B
+            if DRAM_BYTES_PER_SUBTOMO.get(name):
+                row["traffic"] = DRAM_BYTES_PER_SUBTOMO[name] * B
         table[name] = row
     return table, total / steps
 
@@ -542,6 +546,7 @@ def run_ours(args):
     if rank != 0:
         return
     peaks = {}
+    # (the FP32 CUDA-core peak is measured on this GPU: cuBLAS SGEMM, above)
     pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pp):
         peaks = json.load(open(pp))

@@ -75,15 +75,18 @@ def step_bytes(cfg: StepConfig, capacity: int, device) -> int:
     return free0 - free1
 
 
-def plan_capacity(cfg: StepConfig, device, budget_bytes: int = None, probe=(16, 48)) -> CapacityPlan:
+def plan_capacity(cfg: StepConfig, device, budget_bytes: int = None, probe=(128, 384),
+                  margin: float = 1.1) -> CapacityPlan:
     """The largest batch capacity of a step of ``cfg`` whose memory, with its batch of input
-    volumes, fits ``budget_bytes`` (default: 85 % of the device memory free now)."""
+    volumes, fits ``budget_bytes`` (default: 85 % of the device memory free now).  The probe
+    capacities are multiples of 128, the row tile the expansion pads its batch to, so the two
+    measurements see the same padding; ``margin`` covers the allocator's rounding."""
     device = torch.device(device)
     if budget_bytes is None:
         budget_bytes = int(0.85 * torch.cuda.mem_get_info(device)[0])
     c1, c2 = probe
     m1, m2 = step_bytes(cfg, c1, device), step_bytes(cfg, c2, device)
-    per_step = max(0, int(np.ceil((m2 - m1) / (c2 - c1))))
+    per_step = max(0, int(np.ceil(margin * (m2 - m1) / (c2 - c1))))
     fixed = max(0, m1 - per_step * c1)
     per = per_step + 4 * cfg.N ** 3  # + the batch's input volumes
     cap = int(max(0, budget_bytes - fixed) // per)
