@@ -58,7 +58,8 @@ def parse():
                         "captured graph per alternation (a reported extra, not the metric)")
     p.add_argument("--highband", action="store_true",
                    help="the high-bandlimit shape instead of the metric's: 128^3, L=64, march 16/32/48/64, "
-                        "shift r=8, -5 dB (a reported extra, not the metric; --batch defaults to 64)")
+                        "shift r=8, -5 dB (a reported extra, not the metric; --batch defaults to 512; --cpu-sample "
+                        "subtomograms, default 8, checked against the FP64 oracle)")
     return p.parse_args()
 
 
@@ -675,61 +676,140 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def highband_oracle(template, vols, L, Li, uf, radius, n, gpu_runs):
+    """The FP64 oracle on the first n subtomograms at 128^3: the streamed FP64 expansion of the
+    template and the volumes, sigma, the orientation search in FP64, and the shift match in FP64
+    at the GPU run's own orientation (so the shift's error is the shift stage's); each GPU run's
+    rotation, shift, rotation-score and shift-peak deviations from it."""
+    from matcha_b200.core import fle_tables as T
+    from oracle import fle as F
+    from oracle import matcha as M
+    from oracle import pipeline as OP
+    from oracle import shift as OS
+
+    N = template.shape[0]
+    r = min(N // 2, int(N // 2 * 0.95))
+    t0 = time.perf_counter()
+    tb = T.lap_eig_ball(N, L, r)
+    ff = OP.FoldedFLE(tb, N, float(r), dense=False)
+    v = np.asarray(vols[:n], dtype=np.float64)
+    a = ff.evaluate_t_streamed(np.concatenate([template[None].astype(np.float64), v]))
+    sigma = F.compute_sigma(tb, a[0], a[1:])
+    al, be, ga, score = M.search_orientations(sigma, list(Li) + [L], L, K=2, candidates=10, num_steps=1,
+                                              dtype=np.float64)
+    ref = OS.load_reference_full(template, N, 1.0)
+    out = {"sample": n, "seconds": None}
+    for name, g in gpu_runs.items():
+        ang = [np.asarray(g[k][:n], dtype=np.float64) for k in ("alpha", "beta", "gamma")]
+        rot = euler_dev_deg(*ang, al, be, ga)
+        tr = np.asarray(g["tracker"][:n], dtype=np.float64)
+        deg = OS.euler_zyz_deg_from_quat_conj(tr)
+        sh, pk = [], []
+        for i in range(n):
+            s_i, p_i = OS.estimate_shift_like_relion(ref, v[i], np.zeros(3), deg[i], uf, radius)
+            sh.append(s_i)
+            pk.append(p_i)
+        sh, pk = np.array(sh), np.array(pk)
+        rs = np.asarray(g["rotation_score"][:n], dtype=np.float64)
+        ss = np.asarray(g["shift_score"][:n], dtype=np.float64)
+        out[name] = {"median_rot_dev_deg": float(np.median(rot)), "max_rot_dev_deg": float(rot.max()),
+                     "max_shift_dev_px": float(np.abs(np.asarray(g["shift"][:n]) - sh).max()),
+                     "max_rotation_score_rel_dev": float(np.max(np.abs(rs - score) / np.abs(score))),
+                     "max_shift_peak_rel_dev": float(np.max(np.abs(ss - pk) / np.abs(pk)))}
+    out["seconds"] = time.perf_counter() - t0
+    return out
+
+
 def run_highband(args):
-    """One and three alternations at 128^3, L=64 (1500-blob template, -5 dB, shifts in +-8 px):
-    throughput and the tracker's rotation error, on one GPU."""
+    """Config 5: one and three alternations at 128^3, L=64 (1500-blob template, -5 dB, shifts in
+    +-8 px) on one GPU: throughput and the tracker's rotation error of the chosen precision
+    (expansion BF16 hi+lo; shift match on the tensor cores where its kernels cover the box),
+    its deviations from the plain-FP32 run over the whole batch, and both runs' deviations from
+    the FP64 oracle on a sample."""
     import torch
 
     from matcha_b200.pipeline import AlignmentStep, StepConfig
 
     dev = torch.device("cuda:0")
-    N, L, B = 128, 64, (args.batch if args.batch != 1000 else 64)
+    N, L, B = 128, 64, (args.batch if args.batch != 1000 else 512)
+    Li, uf, radius = [16, 32, 48], 8, 8
     rng = np.random.default_rng(args.seed)
     template = make_template(rng, N=N, n_blobs=1500, window=12)
     vols, q_true, _ = make_batch(template, np.random.default_rng(args.seed + 1), B, dev, snr_db=-5.0, max_shift=8.0)
-    step = AlignmentStep(StepConfig(N=N, L=L, Li=[16, 32, 48], batch=B, shift_search_radius=8,
-                                    shift_upsample_factor=8, precision="auto"), dev)
-    step.set_template(template)
     ident = torch.zeros((B, 4), device=dev, dtype=torch.float64)
     ident[:, 0] = 1
-    tracker = ident.clone()
     z3 = torch.zeros((B, 3), device=dev)
-    for _ in range(max(1, args.warmup)):
-        tracker.copy_(ident)
-        out = step(vols, vols, tracker, z3)
-    torch.cuda.synchronize()
     st = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     n = max(1, args.steps)
-    e0.record(st)
-    for _ in range(n):
-        tracker.copy_(ident)
-        out = step(vols, vols, tracker, z3)
-    e1.record(st)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / n
-    err1 = rotation_error_deg(*(out[k].cpu().numpy() for k in ("alpha", "beta", "gamma")), q_true)
-    tracker.copy_(ident)
-    local = torch.zeros((B, 3), device=dev)
-    e0.record(st)
-    step.run_alternations(vols, tracker, local, z3, z3, 3)
-    e1.record(st)
-    torch.cuda.synchronize()
-    ms3 = e0.elapsed_time(e1)
-    err3 = tracker_error_deg(tracker.cpu().numpy(), q_true)
-    print(json.dumps({
+
+    def one_precision(precision):
+        step = AlignmentStep(StepConfig(N=N, L=L, Li=Li, batch=B, shift_search_radius=radius,
+                                        shift_upsample_factor=uf, precision=precision), dev)
+        step.set_template(template)
+        tracker = ident.clone()
+        for _ in range(max(1, args.warmup)):
+            tracker.copy_(ident)
+            out = step(vols, vols, tracker, z3)
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(n):
+            tracker.copy_(ident)
+            out = step(vols, vols, tracker, z3)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / n
+        res = {k: out[k].cpu().numpy() for k in ("alpha", "beta", "gamma", "shift", "shift_score",
+                                                   "rotation_score", "tracker")}
+        prec = f"expansion {step.correlator.fle.precision}, upsampled DFT {step.shifter.effective_precision}"
+        three = None
+        if precision != "fp32":
+            tracker.copy_(ident)
+            local = torch.zeros((B, 3), device=dev)
+            e0.record(st)
+            step.run_alternations(vols, tracker, local, z3, z3, 3)
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms3 = e0.elapsed_time(e1)
+            err3 = tracker_error_deg(tracker.cpu().numpy(), q_true)
+            three = {"ms_per_batch": ms3, "value": B / (ms3 * 1e-3), "median_rot_err_deg": float(np.median(err3)),
+                     "p90_rot_err_deg": float(np.percentile(err3, 90))}
+        del step
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        return ms, res, prec, three
+
+    ms, chosen, prec, three = one_precision("auto")
+    err1 = rotation_error_deg(chosen["alpha"], chosen["beta"], chosen["gamma"], q_true)
+    line = {
         "metric": "subtomograms/s at 128^3 L=64 (one alternation), high-bandlimit shape",
         "value": B / (ms * 1e-3), "unit": "subtomograms/s", "ms_per_alternation": ms, "steps": n,
-        "dtype": "f32", "data": "synthetic",
+        "dtype": "f32+bf16x3", "data": "synthetic",
         "config": {"workload": f"{B} subtomograms 128^3, L=64, march 16/32/48/64, C=10, 1 Newton step, "
-                               f"shift r=8 uf=8, -5 dB, 1500 blobs",
-                   "precision": f"expansion {step.correlator.fle.precision}, upsampled DFT "
-                                f"{step.shifter.effective_precision}"},
+                               f"shift r=8 uf=8, -5 dB, 1500 blobs", "precision": prec},
         "median_rot_err_deg": float(np.median(err1)), "p90_rot_err_deg": float(np.percentile(err1, 90)),
-        "three_alternations": {"ms_per_batch": ms3, "value": B / (ms3 * 1e-3),
-                               "median_rot_err_deg": float(np.median(err3)),
-                               "p90_rot_err_deg": float(np.percentile(err3, 90))},
-    }))
+        "three_alternations": three,
+    }
+    runs = {"chosen": chosen}
+    if not args.no_fp32:
+        ms32, plain, prec32, _ = one_precision("fp32")
+        runs["plain_fp32"] = plain
+        ang = lambda d: [np.asarray(d[k], dtype=np.float64) for k in ("alpha", "beta", "gamma")]
+        dev_deg = euler_dev_deg(*ang(chosen), *ang(plain))
+        line["plain_fp32"] = {
+            "ms_per_alternation": ms32, "value": B / (ms32 * 1e-3), "precision": prec32,
+            "chosen_vs_plain": {
+                "median_rot_dev_deg": float(np.median(dev_deg)), "max_rot_dev_deg": float(dev_deg.max()),
+                "frac_within_0p05deg": float(np.mean(dev_deg < 0.05)),
+                "shift_equal_frac": float(np.mean(np.all(np.abs(chosen["shift"] - plain["shift"]) < 1e-6, axis=1))),
+                "max_shift_peak_rel_dev": float(np.max(np.abs(chosen["shift_score"] - plain["shift_score"])
+                                                       / np.abs(plain["shift_score"]))),
+                "median_rotation_score_rel_dev": float(np.median(np.abs(chosen["rotation_score"] - plain["rotation_score"])
+                                                                 / np.abs(plain["rotation_score"])))}}
+    if args.cpu_sample > 0 and not args.no_cpu_baseline:
+        line["vs_fp64_oracle"] = highband_oracle(template, vols[:args.cpu_sample].cpu().numpy(), L, Li, uf, radius,
+                                                 min(args.cpu_sample, B), runs)
+    print(json.dumps(line))
 
 
 def run_mixed(args):

@@ -7,6 +7,7 @@
     python bench_cases.py reader 1000  # MRC decode of 1000 64^3 files into pinned memory
     python bench_cases.py graph 64     # one alternation, 64^3 L 32: eager calls vs a CUDA graph
     python bench_cases.py shift 1000 --stages   # plus ShiftMatcher.profile per kernel group
+    python bench_cases.py shift 64 --box 128 --radius 8 --kernels   # 128^3, r 8: time per kernel
 
 Each case builds its inputs on the device from a fixed seed (random volumes, Haar rotations,
 random shifts; a synthetic sigma with a known optimum for the search), runs the stage three
@@ -30,13 +31,13 @@ class _Cfg(dict):
     __getattr__ = dict.__getitem__
 
 
-def _shift(B: int, dev):
+def _shift(B: int, dev, box=64, radius=5, precision="bf16x3"):
     from matcha_b200.core.ShiftMatcher import ShiftMatcher
 
-    N = 64
-    cfg = _Cfg(N=N, voxel_size=1.0, num_subtomograms_per_batch=B, shift_upsample_factor=8, shift_search_radius=5,
-               do_ctf_correction=False, box_size=N)
-    sm = ShiftMatcher(cfg, dev, torch.complex64, precision="bf16x3")
+    N = box
+    cfg = _Cfg(N=N, voxel_size=1.0, num_subtomograms_per_batch=B, shift_upsample_factor=8,
+               shift_search_radius=radius, do_ctf_correction=False, box_size=N)
+    sm = ShiftMatcher(cfg, dev, torch.complex64, precision=precision)
     rng = np.random.default_rng(0)
     sm.set_reference(rng.standard_normal((N, N, N)).astype(np.float32))
     vols = torch.randn(B, N, N, N, device=dev)
@@ -182,6 +183,11 @@ def main(argv=None) -> int:
     p.add_argument("batch", type=int)
     p.add_argument("--reps", type=int, default=5)
     p.add_argument("--stages", action="store_true", help="shift only: time each kernel group with CUDA events")
+    p.add_argument("--box", type=int, default=64, help="shift only: box size")
+    p.add_argument("--radius", type=int, default=5, help="shift only: search radius (voxels)")
+    p.add_argument("--precision", default="bf16x3", help="shift only: bf16x3, fp32 or auto")
+    p.add_argument("--kernels", action="store_true",
+                   help="time every kernel launch of the library with CUDA events (mtb_profile_*)")
     a = p.parse_args(argv)
     if a.case == "reader":
         return _reader(a.batch, a.reps)
@@ -191,7 +197,10 @@ def main(argv=None) -> int:
     if a.case == "graph":
         return _graph(a.batch, a.reps)
     dev = torch.device("cuda:0")
-    run = CASES[a.case](a.batch, dev)
+    if a.case == "shift":
+        run = _shift(a.batch, dev, a.box, a.radius, a.precision)
+    else:
+        run = CASES[a.case](a.batch, dev)
     for _ in range(3):
         run()
     torch.cuda.synchronize()
@@ -211,6 +220,18 @@ def main(argv=None) -> int:
         ms, calls = sm.profile_read()
         sm.profile(0)
         print("  " + ", ".join(f"{k} {v / max(calls, 1):.3f}" for k, v in ms.items()) + " ms per call")
+    if a.kernels:
+        from matcha_b200 import _native
+
+        _native.profile_start(4096)
+        for _ in range(a.reps):
+            run()
+        table, dropped = _native.profile_read()
+        _native.profile_stop()
+        for name, row in sorted(table.items(), key=lambda kv: -kv[1]["ms"]):
+            print(f"  {name}: {row['ms'] / a.reps:.3f} ms per call ({row['launches'] // a.reps} launches)")
+        if dropped:
+            print(f"  ({dropped} launches not timed: event pool full)")
     return 0
 
 

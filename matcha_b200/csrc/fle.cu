@@ -378,7 +378,10 @@ extern "C" int mtb_fle_create(const mtb_fle_config* cfg, mtb_fle** out) {
   if (!rc) rc = upload(&h->kpad, cfg->kpad, (size_t)L + 1);
   if (!rc) rc = upload(&h->koff, koff.data(), koff.size());
   if (!rc) rc = upload(&h->kidx, cfg->kidx, (size_t)kt);
-  if (!rc && cudaMalloc(&h->A, (size_t)kClasses * cfg->max_batch * nr * sizeof(float)) != cudaSuccess) rc = MTB_ERR_OOM;
+  // the FP32 fold buffer serves the CUDA-core GEMM only (the tensor-core path folds into its own bf16 operand)
+  if (!rc && cfg->precision == MTB_FLE_FP32 &&
+      cudaMalloc(&h->A, (size_t)kClasses * cfg->max_batch * nr * sizeof(float)) != cudaSuccess)
+    rc = MTB_ERR_OOM;
   if (!rc && cudaMalloc(&h->C, (size_t)cfg->max_batch * nc * sizeof(float)) != cudaSuccess) rc = MTB_ERR_OOM;
   if (rc) return fail(rc);
 
@@ -410,6 +413,13 @@ extern "C" int mtb_fle_create(const mtb_fle_config* cfg, mtb_fle** out) {
     rc = fle_tc_prepare(&h->tc, h->basis, h->class_cols, h->class_off, nr, cfg->max_batch, nc);
     if (rc) return fail(rc);
     h->use_tc = true;
+    // the FP32 basis was only the source of the hi/lo split: release it (at 128^3, L = 64 it
+    // is 33 GB, as large as the split copy)
+    for (int k = 0; k < kClasses; ++k) {
+      cudaFree(h->basis[k]);
+      h->basis[k] = nullptr;
+    }
+    if (cudaGetLastError() != cudaSuccess) return fail(MTB_ERR_CUDA);
   } else if (cfg->precision != MTB_FLE_FP32) {
     return fail(MTB_ERR_ARG);
   }

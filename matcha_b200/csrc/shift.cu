@@ -1222,14 +1222,20 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
   h->rows_per_cta = cfg->tile_rows > 0 ? cfg->tile_rows : 2;
   h->ngrp = (g.U + h->rows_per_cta - 1) / h->rows_per_cta;
   const size_t B = cfg->max_batch;
+  // MTB_SHIFT_BF16X3 was checked to fit the tensor-core kernels above; MTB_SHIFT_AUTO uses them
+  // where they fit and the FP32 CUDA-core kernels elsewhere
+  const bool want_tc = cfg->precision != MTB_SHIFT_FP32 && shift_tc_fits(N, g.U) == MTB_OK;
   auto fail = [&](int code) { mtb_shift_destroy(h); return code; };
   auto alloc = [&](void** p, size_t bytes) { return cudaMalloc(p, bytes > 0 ? bytes : 4) == cudaSuccess; };
   if (!alloc((void**)&h->bgw_tab, wtab.size() * 4) || !alloc((void**)&h->fill_tab, wtab.size() * 4) || !alloc((void**)&h->what, (size_t)N * N * g.H * 8) ||
       !alloc((void**)&h->ref, (size_t)N * N * N * 8) || !alloc((void**)&h->E0, e0.size() * 8) ||
       !alloc((void**)&h->E1, e0.size() * 8) || !alloc((void**)&h->E2, e2.size() * 8) ||
       !alloc((void**)&h->bg, B * 4) || !alloc((void**)&h->nrm, B * 8) ||
-      !alloc((void**)&h->T, B * N * N * g.H * 8) || !alloc((void**)&h->X1, B * g.U * N * g.H * 8) ||
-      !alloc((void**)&h->pval, B * h->ngrp * 4) || !alloc((void**)&h->pidx, B * h->ngrp * 4))
+      !alloc((void**)&h->T, B * N * N * g.H * 8))
+    return fail(MTB_ERR_OOM);
+  // the FP32 upsampled DFT's pass-1 output and per-group maxima (its kernels only)
+  if (!want_tc && (!alloc((void**)&h->X1, B * g.U * N * g.H * 8) || !alloc((void**)&h->pval, B * h->ngrp * 4) ||
+                   !alloc((void**)&h->pidx, B * h->ngrp * 4)))
     return fail(MTB_ERR_OOM);
   if (N == 64 && !alloc((void**)&h->refq, (size_t)(N + 2) * (N + 1) * (N + 1) * 32)) return fail(MTB_ERR_OOM);
   if (cudaMemcpy(h->bgw_tab, wtab.data(), wtab.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -1241,9 +1247,7 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
   if (cudaGetLastError() != cudaSuccess) return fail(MTB_ERR_CUDA);
   if (shift_front(h, nullptr, nullptr, nullptr, nullptr, 0, 0, false) != MTB_OK) return fail(MTB_ERR_CUDA);
   if (cudaStreamSynchronize(0) != cudaSuccess) return fail(MTB_ERR_CUDA);
-  // MTB_SHIFT_BF16X3 was checked to fit the tensor-core kernels above; MTB_SHIFT_AUTO uses them
-  // where they fit and the FP32 CUDA-core kernels elsewhere
-  if (cfg->precision != MTB_SHIFT_FP32 && shift_tc_fits(N, g.U) == MTB_OK) {
+  if (want_tc) {
     const int rc = shift_tc_prepare(&h->tc, N, g.H, g.U, cfg->upsample_factor, g.dftshift, cfg->max_batch);
     if (rc) return fail(rc);
     h->use_tc = true;

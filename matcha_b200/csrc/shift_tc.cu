@@ -49,15 +49,37 @@ constexpr int kThreads23 = 64 + kEpi + kArg;  // warps 10-17 of updft23 take the
 constexpr int kMaxSlots = 3;         // operand slots of the fused passes 2+3
 constexpr int A_TILE = TM * TK * 2;  // one 128 x 64 bf16 K-block
 constexpr int kMaxStages = 8;
-constexpr size_t kSmemCap = 227 * 1024;
+constexpr size_t kSmemCap = 227 * 1024 - 2048;  // dynamic shared memory: the opt-in limit less the
+                                                // kernels' static barriers, with room to spare
 
+// One complex DFT pass as a GEMM: rows of A (K = (m, re/im)) times E1 -> columns (u, re/im).
+// The N-tile 2U is cut into NS column parts of Us values of u (NT columns each, <= 256), one
+// part per CTA, so that E1's part stays resident in shared memory; CTAs c and c + 1 .. c + NS - 1
+// take the same row tile at the same time, so A is read from memory once.  The epilogue writes
+// the next pass's operand: input row g = b rpb + x Y + y becomes output row b SB + x SX + u SU,
+// K word y (a (re, im) bf16 pair), hi part at row, lo part at Rout + row; or, with ROWS_OUT,
+// FP32 rows (g, u).
 struct Pass1 {
-  int rows;     // valid rows B * N/2 * N
+  int rows;     // valid rows of A
   int tiles;
-  int N, HH, U;
-  int KB;       // K blocks of A1 and E1 (2N / 64)
-  int R1, R2;   // rows per part of A1 and A2
-  int NT;       // N-tile 2U rounded to 16
+  int U;
+  int KB;       // K blocks of A and E1 (2N / 64)
+  int R1;       // rows per hi/lo part of A
+  int NT;       // N-tile of one column part (2 Us rounded to 16)
+  int NS, Us;   // column parts, values of u per part
+  int stages;
+  int rpb, Y, SB, SX, SU, ws, Rout;  // operand-out epilogue (see above)
+};
+
+// The third pass on its own (boxes and upsampled regions outside the fused passes 2+3): rows
+// (b, u0 U + u1) of A3, padded to RP3 rows per subtomogram, K = (m2 < N/2, re/im), times E3 ->
+// the real grid values u2, plus the Nyquist term, reduced to a running argmax per subtomogram.
+struct Pass3 {
+  int tiles, TPB;  // tiles = B * TPB, TPB = RP3 / 128
+  int U;
+  int KB;          // K blocks of A3 and E3
+  int R3;          // rows per hi/lo part of A3
+  int NT;          // U rounded to 16
   int stages;
 };
 
@@ -138,19 +160,21 @@ __device__ __forceinline__ void mma_split_kblock(uint32_t d, uint64_t a_hi, uint
 // Epilogue helpers over NC TMEM columns already in registers.  The per-value work is
 // unconditional so it can be interleaved; only the stores are predicated.
 
-// Pass 1: columns (u0, re/im) of one A1 row -> A2 words (m1) of rows (b, u0, m2).
+// Passes 1 and 2: columns (u, re/im) of one input row -> K word y of the output rows
+// row0 + u SU, u = ubase + local column pair (local < ulim, u < U).
 template <int NC>
-__device__ __forceinline__ void epi1_group(const uint32_t* v, int cb, bool valid, int U, size_t row0, int HH,
-                                           size_t ws, int m1, size_t R2, uint32_t* __restrict__ out) {
+__device__ __forceinline__ void epi1_group(const uint32_t* v, int cb, bool valid, int ubase, int ulim, int U,
+                                           size_t row0, int SU, size_t ws, int y, size_t Rout,
+                                           uint32_t* __restrict__ out) {
 #pragma unroll
   for (int t = 0; t < NC / 2; ++t) {
     uint32_t hi, lo;
     split2(__uint_as_float(v[2 * t]), __uint_as_float(v[2 * t + 1]), hi, lo);
-    const int u0 = cb / 2 + t;
-    const size_t row = row0 + (size_t)u0 * HH;
-    if (valid && u0 < U) {
-      out[row * ws + m1] = hi;
-      out[(R2 + row) * ws + m1] = lo;
+    const int ul = cb / 2 + t, u = ubase + ul;
+    const size_t row = row0 + (size_t)u * SU;
+    if (valid && ul < ulim && u < U) {
+      out[row * ws + y] = hi;
+      out[(Rout + row) * ws + y] = lo;
     }
   }
 }
@@ -248,10 +272,12 @@ updft1_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant
                  uint32_t* __restrict__ out, float2* __restrict__ yout, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = align1024(smem_raw);
-  const int KB = p.KB, S = p.stages, NT = p.NT;
+  const int KB = p.KB, S = p.stages, NT = p.NT, NS = p.NS;
   const int B_BLK = NT * TK * 2;
   uint8_t* sB = smem;                    // [part][kb] B_BLK
   uint8_t* sA = smem + 2 * KB * B_BLK;   // [stage][part] A_TILE
+  // this CTA's column part and its walk over the row tiles (gridDim.x is a multiple of NS)
+  const int cpart = blockIdx.x % NS, t0 = blockIdx.x / NS, tstep = gridDim.x / NS;
   __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages];
   __shared__ __align__(8) uint64_t accF[2], accE[2], resF;
   __shared__ uint32_t tmem_base;
@@ -285,9 +311,9 @@ updft1_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant
     mbar_expect_tx(&resF, (uint32_t)(2 * KB * B_BLK));
     for (int part = 0; part < 2; ++part)
       for (int kb = 0; kb < KB; ++kb)
-        tma_load_2d(sB + (part * KB + kb) * B_BLK, &mapB, kb * TK, part * NT, &resF);
+        tma_load_2d(sB + (part * KB + kb) * B_BLK, &mapB, kb * TK, (part * NS + cpart) * NT, &resF);
     int it = 0;
-    for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x) {
+    for (int tile = t0; tile < p.tiles && !abort_flag; tile += tstep) {
       for (int kb = 0; kb < KB; ++kb, ++it) {
         const int s = it % S;
         const uint32_t use = it / S;
@@ -309,7 +335,7 @@ updft1_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant
       abort_flag = 1;
     }
     int it = 0, tl = 0;
-    for (int tile = blockIdx.x; ok && tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
+    for (int tile = t0; ok && tile < p.tiles && !abort_flag; tile += tstep, ++tl) {
       const int buf = tl & 1;
       if (tl >= 2 && !mbar_wait(&accE[buf], ((tl >> 1) - 1) & 1)) {
         atomicCAS(err, 0, 23);
@@ -340,9 +366,9 @@ updft1_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant
     const int q = warp & 3, h = (warp - 2) >> 2;
     const int c_mid = (NT / 2) & ~15;
     const int c0 = h ? c_mid : 0, c1 = h ? NT : c_mid;
-    const size_t ws = (size_t)KB * (TK / 2);  // A2 row stride in bf16 pairs
+    const int ubase = cpart * p.Us;
     int tl = 0;
-    for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
+    for (int tile = t0; tile < p.tiles && !abort_flag; tile += tstep, ++tl) {
       const int buf = tl & 1;
       if (!mbar_wait(&accF[buf], (tl >> 1) & 1)) {
         atomicCAS(err, 0, 25);
@@ -359,17 +385,17 @@ updft1_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant
         tmem_for_groups(taddr, c0, c1, [&](const uint32_t(&r)[16], int cb) {
 #pragma unroll
           for (int t = 0; t < 8; ++t) {
-            const int u = cb / 2 + t;
-            if (valid && u < p.U) yr[u] = make_float2(__uint_as_float(r[2 * t]), __uint_as_float(r[2 * t + 1]));
+            const int ul = cb / 2 + t, u = ubase + ul;
+            if (valid && ul < p.Us && u < p.U)
+              yr[u] = make_float2(__uint_as_float(r[2 * t]), __uint_as_float(r[2 * t + 1]));
           }
         });
       } else {
-        const int rpb = p.HH * p.N;
-        const int b = g / rpb, rem = g - (g / rpb) * rpb;
-        const int m2 = rem / p.N, m1 = rem - (rem / p.N) * p.N;
-        const size_t row0 = ((size_t)b * p.U) * p.HH + m2;  // + u0 * HH
+        const int b = g / p.rpb, rem = g - (g / p.rpb) * p.rpb;
+        const int x = rem / p.Y, y = rem - (rem / p.Y) * p.Y;
+        const size_t row0 = (size_t)b * p.SB + (size_t)x * p.SX;  // + u * SU
         tmem_for_groups(taddr, c0, c1, [&](const uint32_t(&r)[16], int cb) {
-          epi1_group<16>(r, cb, valid, p.U, row0, p.HH, ws, m1, (size_t)p.R2, out);
+          epi1_group<16>(r, cb, valid, ubase, p.Us, p.U, row0, p.SU, (size_t)p.ws, y, (size_t)p.Rout, out);
         });
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -687,6 +713,154 @@ updft23_tc_kernel(const __grid_constant__ CUtensorMap mapA2, const __grid_consta
   }
 }
 
+// ------------------------------------------------------------------ pass 3 on its own
+// Rows (b, u0 U + u1) of A3 times E3 -> grid values u2 (real part) in a double-buffered TMEM
+// accumulator; the epilogue adds the Nyquist term Re(Y[b, u0, u1] E2[u2, N/2]) in FP32 and
+// keeps a running argmax per row, reduced per warp into best[b] (every tile lies in one
+// subtomogram: its rows are padded to a multiple of 128, and pad rows are skipped).
+__global__ void __launch_bounds__(kThreads, 1)
+updft3_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, Pass3 p,
+                 const float2* __restrict__ nyq, const float4* __restrict__ enq, unsigned long long* __restrict__ best,
+                 int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = align1024(smem_raw);
+  const int KB = p.KB, S = p.stages, NT = p.NT;
+  const int B_BLK = NT * TK * 2;
+  uint8_t* sB = smem;                                          // [part][kb] B_BLK
+  uint8_t* sA = smem + 2 * KB * B_BLK;                         // [stage][part] A_TILE
+  float4* sEn = reinterpret_cast<float4*>(sA + S * 2 * A_TILE);  // NT / 2 column pairs (re, re, im, im)
+  __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages];
+  __shared__ __align__(8) uint64_t accF[2], accE[2], resF;
+  __shared__ uint32_t tmem_base;
+  __shared__ volatile int abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&accF[i], 1);
+      mbar_init(&accE[i], kEpi);
+    }
+    mbar_init(&resF, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int i = threadIdx.x; i < NT / 2; i += blockDim.x) {
+    const float4 e = enq[i];
+    sEn[i] = make_float4(e.x, e.z, e.y, e.w);
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  const uint32_t idesc = idesc_bf16(TM, NT);
+
+  if (warp == 0 && lane == 0) {
+    mbar_expect_tx(&resF, (uint32_t)(2 * KB * B_BLK));
+    for (int part = 0; part < 2; ++part)
+      for (int kb = 0; kb < KB; ++kb)
+        tma_load_2d(sB + (part * KB + kb) * B_BLK, &mapB, kb * TK, part * NT, &resF);
+    int it = 0;
+    for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x) {
+      for (int kb = 0; kb < KB; ++kb, ++it) {
+        const int s = it % S;
+        const uint32_t use = it / S;
+        if (it >= S && !mbar_wait(&empty_bar[s], (use - 1) & 1)) {
+          atomicCAS(err, 0, 41);
+          abort_flag = 1;
+          break;
+        }
+        uint8_t* sa = sA + s * 2 * A_TILE;
+        mbar_expect_tx(&full_bar[s], 2 * A_TILE);
+        tma_load_2d(sa, &mapA, kb * TK, tile * TM, &full_bar[s]);
+        tma_load_2d(sa + A_TILE, &mapA, kb * TK, p.R3 + tile * TM, &full_bar[s]);
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    bool ok = mbar_wait(&resF, 0);
+    if (!ok) {
+      atomicCAS(err, 0, 42);
+      abort_flag = 1;
+    }
+    int it = 0, tl = 0;
+    for (int tile = blockIdx.x; ok && tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
+      const int buf = tl & 1;
+      if (tl >= 2 && !mbar_wait(&accE[buf], ((tl >> 1) - 1) & 1)) {
+        atomicCAS(err, 0, 43);
+        abort_flag = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t d = tmem + (uint32_t)(buf * 256);
+      for (int kb = 0; kb < KB; ++kb, ++it) {
+        const int s = it % S;
+        const uint32_t use = it / S;
+        if (!mbar_wait(&full_bar[s], use & 1)) {
+          atomicCAS(err, 0, 44);
+          abort_flag = 1;
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint8_t* sa = sA + s * 2 * A_TILE;
+        mma_split_kblock(d, smem_desc(sa), smem_desc(sa + A_TILE), smem_desc(sB + kb * B_BLK),
+                         smem_desc(sB + (KB + kb) * B_BLK), idesc, kb == 0);
+        mma_commit_to(&empty_bar[s]);
+      }
+      if (ok) mma_commit_to(&accF[buf]);
+    }
+  } else if (warp >= 2) {
+    // warp (q, h): TMEM lanes 32 q .. 32 q + 31, column half h
+    const int q = warp & 3, h = (warp - 2) >> 2;
+    const int c_mid = (((NT >> 4) + 1) >> 1) << 4;
+    const int c0 = h ? c_mid : 0, c1 = h ? NT : c_mid;
+    const int U = p.U, UU = p.U * p.U;
+    int tl = 0;
+    for (int tile = blockIdx.x; tile < p.tiles && !abort_flag; tile += gridDim.x, ++tl) {
+      const int buf = tl & 1;
+      const int b = tile / p.TPB;
+      const int rb = (tile - b * p.TPB) * TM + q * 32 + lane;  // row in the subtomogram: u0 U + u1
+      const bool valid = rb < UU;
+      const float2 y = valid ? nyq[(size_t)b * UU + rb] : make_float2(0.f, 0.f);
+      // warp-uniform outcome: the TMEM loads and the shuffles below need the whole warp
+      if (!__all_sync(0xffffffffu, mbar_wait(&accF[buf], (tl >> 1) & 1))) {
+        if (lane == 0) atomicCAS(err, 0, 45);
+        abort_flag = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      float bv = -INFINITY;
+      int bi = 0x7fffffff;
+      bool have = false;
+      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 256);
+      tmem_for_groups(taddr, c0, c1, [&](const uint32_t(&rr)[16], int cb) {
+        if (valid) scan_group_nq<16>(rr, cb, U, rb, y, sEn, bv, bi, have);
+      });
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(&accE[buf]);
+      unsigned long long key = have ? argmax_key(__uint_as_float(__float_as_uint(bv) & 0xFFFFFFF0u), bi) : 0ull;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long k2 = __shfl_xor_sync(0xffffffffu, key, o);
+        key = k2 > key ? k2 : key;
+      }
+      if (lane == 0 && key) atomicMax(&best[b], key);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+  }
+}
 
 typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -726,31 +900,57 @@ float bf2f(uint16_t h) {
 }
 
 struct Geometry {
-  int HH, NT12, NT3, KB12, G, TPB, CH, NB, stages1;
-  size_t smem1, smem23;
+  bool fused;
+  int HH, NT12, NT3, KB12, KB3, G, TPB, CH, NB, stages1, NS, Us, RP3, stages3;
+  size_t smem1, smem23, smem3;
 };
 
 bool geometry(int N, int U, Geometry* o) {
-  if (N != 16 && N != 32 && N != 64) return false;
-  if (U < 1 || 2 * U > 256) return false;
+  if (N < 16 || N > 128 || (N & 1)) return false;
+  if (U < 1 || U > 256) return false;
   Geometry g;
   g.HH = N / 2;
-  g.NT12 = (2 * U + 15) / 16 * 16;
   g.NT3 = (U + 15) / 16 * 16;
   g.KB12 = (2 * N + TK - 1) / TK;
+  g.KB3 = (N + TK - 1) / TK;  // K of pass 3: (m2 < N/2, re/im)
+  g.fused = (N == 16 || N == 32 || N == 64) && 2 * U <= 256;
+  g.NT12 = (2 * U + 15) / 16 * 16;
   g.G = TM / g.HH;
   g.TPB = (U + g.G - 1) / g.G;
   g.CH = (U + g.HH - 1) / g.HH;
-  if (g.NT12 + 2 * g.NT3 > 512) return false;
-  const size_t b1 = (size_t)2 * g.KB12 * g.NT12 * TK * 2;
-  const size_t b3 = (size_t)2 * g.NT3 * TK * 2;
-  // three operand slots where they fit (the next tile's A2 then loads during this tile's
-  // pass 3), else two
-  for (g.NB = kMaxSlots; g.NB >= 2; --g.NB) {
-    g.smem23 = 1024 + b1 + b3 + (size_t)g.NB * 2 * A_TILE + (size_t)g.NT3 * 8;
-    if (g.smem23 <= kSmemCap) break;
+  g.NS = 1;
+  g.Us = U;
+  g.RP3 = g.stages3 = 0;
+  g.smem23 = g.smem3 = 0;
+  if (g.fused) {
+    if (g.NT12 + 2 * g.NT3 > 512) return false;
+    const size_t b1 = (size_t)2 * g.KB12 * g.NT12 * TK * 2;
+    const size_t b3 = (size_t)2 * g.NT3 * TK * 2;
+    // three operand slots where they fit (the next tile's A2 then loads during this tile's
+    // pass 3), else two
+    for (g.NB = kMaxSlots; g.NB >= 2; --g.NB) {
+      g.smem23 = 1024 + b1 + b3 + (size_t)g.NB * 2 * A_TILE + (size_t)g.NT3 * 8;
+      if (g.smem23 <= kSmemCap) break;
+    }
+    if (g.NB < 2) return false;
+  } else {
+    g.NB = 0;
+    // the fewest column parts whose E1 part leaves room for two A stages
+    for (g.NS = 1; g.NS <= 8; ++g.NS) {
+      g.Us = (U + g.NS - 1) / g.NS;
+      g.NT12 = (2 * g.Us + 15) / 16 * 16;
+      const size_t b1 = (size_t)2 * g.KB12 * g.NT12 * TK * 2;
+      if (g.NT12 <= 256 && 1024 + b1 + (size_t)2 * 2 * A_TILE <= kSmemCap) break;
+    }
+    if (g.NS > 8) return false;
+    g.RP3 = (U * U + TM - 1) / TM * TM;
+    const size_t b3 = (size_t)2 * g.KB3 * g.NT3 * TK * 2 + (size_t)g.NT3 * 8;
+    g.stages3 = (int)((kSmemCap - 1024 - b3) / (2 * (size_t)A_TILE));
+    if (g.stages3 > kMaxStages) g.stages3 = kMaxStages;
+    if (g.stages3 < 2) return false;
+    g.smem3 = 1024 + b3 + (size_t)g.stages3 * 2 * A_TILE;
   }
-  if (g.NB < 2) return false;
+  const size_t b1 = (size_t)2 * g.KB12 * g.NT12 * TK * 2;
   g.stages1 = (int)((kSmemCap - 1024 - b1) / (2 * (size_t)A_TILE));
   if (g.stages1 > kMaxStages) g.stages1 = kMaxStages;
   if (g.stages1 < 2) return false;
@@ -770,6 +970,7 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
   memset(t, 0, sizeof(*t));
   Geometry ge;
   if (!geometry(N, U, &ge)) return MTB_ERR_ARG;
+  t->fused = ge.fused;
   t->N = N;
   t->H = H;
   t->HH = ge.HH;
@@ -777,13 +978,20 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
   t->NT12 = ge.NT12;
   t->NT3 = ge.NT3;
   t->KB12 = ge.KB12;
+  t->KB3 = ge.KB3;
   t->G = ge.G;
   t->TPB = ge.TPB;
   t->CH = ge.CH;
   t->NB = ge.NB;
+  t->NS = ge.NS;
+  t->Us = ge.Us;
+  t->RP3 = ge.RP3;
+  t->TPB3 = ge.RP3 / TM;
   t->stages1 = ge.stages1;
+  t->stages3 = ge.stages3;
   t->smem1 = ge.smem1;
   t->smem23 = ge.smem23;
+  t->smem3 = ge.smem3;
   t->Bmax = max_batch;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||
@@ -792,15 +1000,24 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
   auto pad = [](size_t r) { return (r + TM - 1) / TM * TM; };
   const int HH = ge.HH;
   t->R1 = (int)pad((size_t)max_batch * HH * N);
-  // a partial last u0 group of the last subtomogram reads up to G * HH rows past the end
-  t->R2 = (int)pad((size_t)max_batch * U * HH + (size_t)ge.G * HH);
-  const size_t k12 = (size_t)t->KB12 * TK, k3 = TK;
+  // fused: a partial last u0 group of the last subtomogram reads up to G * HH rows past the end
+  t->R2 = (int)pad((size_t)max_batch * U * HH + (ge.fused ? (size_t)ge.G * HH : 0));
+  const size_t k12 = (size_t)t->KB12 * TK, k3 = (size_t)t->KB3 * TK;
   const size_t a1 = (size_t)2 * t->R1 * k12 * 2, a2 = (size_t)2 * t->R2 * k12 * 2;
   if (cudaMalloc(&t->A1, a1) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->A2, a2) != cudaSuccess) return MTB_ERR_OOM;
-  if (cudaMalloc(&t->E1, (size_t)2 * t->NT12 * k12 * 2) != cudaSuccess) return MTB_ERR_OOM;
+  const int nt1 = t->NS * t->NT12;  // E1 rows per hi/lo part
+  if (cudaMalloc(&t->E1, (size_t)2 * nt1 * k12 * 2) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->E3, (size_t)2 * t->NT3 * k3 * 2) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->ENQ, (size_t)t->NT3 * sizeof(float2)) != cudaSuccess) return MTB_ERR_OOM;
+  size_t a3 = 0;
+  if (!ge.fused) {
+    // pad rows (u0 U + u1 >= U^2) and K columns past N stay zero; the rest is rewritten by every call
+    t->R3 = (int)((size_t)max_batch * t->RP3);
+    a3 = (size_t)2 * t->R3 * k3 * 2;
+    if (cudaMalloc(&t->A3, a3) != cudaSuccess) return MTB_ERR_OOM;
+    if (cudaMemset(t->A3, 0, a3) != cudaSuccess) return MTB_ERR_CUDA;
+  }
   // the Nyquist plane's operands: A1n rows (b, m1), A2n rows (b, u0), same K layout as A1, A2
   t->R1n = (int)pad((size_t)max_batch * N);
   t->R2n = (int)pad((size_t)max_batch * U);
@@ -815,7 +1032,7 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
   if (cudaMemset(t->A1, 0, a1) != cudaSuccess || cudaMemset(t->A2, 0, a2) != cudaSuccess ||
       cudaMemset(t->err, 0, 4) != cudaSuccess)
     return MTB_ERR_CUDA;
-  // B operands: E1 rows (u, re/im), K (m, re/im); E3 rows u2, K (m2 < N/2, re/im) -> real part
+  // B operands: E1 rows (part, u local, re/im), K (m, re/im); E3 rows u2, K (m2 < N/2, re/im) -> real part
   auto E = [&](int n, int u, int m, double* re, double* im) {
     const int mm = (m < (n + 1) / 2) ? m : m - n;
     const double f = (double)mm / ((double)uf * n);
@@ -823,7 +1040,7 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
     *re = cos(ph);
     *im = sin(ph);
   };
-  std::vector<uint16_t> e1((size_t)2 * t->NT12 * k12, 0), e3((size_t)2 * t->NT3 * k3, 0);
+  std::vector<uint16_t> e1((size_t)2 * nt1 * k12, 0), e3((size_t)2 * t->NT3 * k3, 0);
   // the Nyquist column's factor (re, -im) of E2[u2, N/2], FP32, zero past U
   std::vector<float2> enq((size_t)t->NT3, make_float2(0.f, 0.f));
   auto put = [&](std::vector<uint16_t>& dst, size_t k, int rows, int r, int kk, double v) {
@@ -832,15 +1049,18 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
     dst[(size_t)r * k + kk] = hi;
     dst[((size_t)rows + r) * k + kk] = lo;
   };
-  for (int u = 0; u < U; ++u)
+  for (int u = 0; u < U; ++u) {
+    const int part = u / t->Us, ul = u - part * t->Us;
+    const int r0 = part * t->NT12 + 2 * ul;
     for (int m = 0; m < N; ++m) {
       double er, ei;
       E(N, u, m, &er, &ei);
-      put(e1, k12, t->NT12, 2 * u + 0, 2 * m + 0, er);
-      put(e1, k12, t->NT12, 2 * u + 0, 2 * m + 1, -ei);
-      put(e1, k12, t->NT12, 2 * u + 1, 2 * m + 0, ei);
-      put(e1, k12, t->NT12, 2 * u + 1, 2 * m + 1, er);
+      put(e1, k12, nt1, r0 + 0, 2 * m + 0, er);
+      put(e1, k12, nt1, r0 + 0, 2 * m + 1, -ei);
+      put(e1, k12, nt1, r0 + 1, 2 * m + 0, ei);
+      put(e1, k12, nt1, r0 + 1, 2 * m + 1, er);
     }
+  }
   for (int u = 0; u < U; ++u) {
     for (int m = 0; m < HH; ++m) {
       double er, ei;
@@ -858,18 +1078,46 @@ int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, in
     return MTB_ERR_CUDA;
   int rc = make_map(t->mapA1, t->A1, k12, (uint64_t)2 * t->R1, TM);
   if (!rc) rc = make_map(t->mapA2, t->A2, k12, (uint64_t)2 * t->R2, TM);
-  if (!rc) rc = make_map(t->mapE1, t->E1, k12, (uint64_t)2 * t->NT12, t->NT12);
+  if (!rc) rc = make_map(t->mapE1, t->E1, k12, (uint64_t)2 * nt1, t->NT12);
   if (!rc) rc = make_map(t->mapE3, t->E3, k3, (uint64_t)2 * t->NT3, t->NT3);
   if (!rc) rc = make_map(t->mapA1n, t->A1n, k12, (uint64_t)2 * t->R1n, TM);
   if (!rc) rc = make_map(t->mapA2n, t->A2n, k12, (uint64_t)2 * t->R2n, TM);
+  if (!rc && !ge.fused) rc = make_map(t->mapA3, t->A3, k3, (uint64_t)2 * t->R3, TM);
   return rc;
 }
 
 void shift_tc_release(ShiftTc* t) {
-  void* ptrs[] = {t->A1, t->A2, t->A1n, t->A2n, t->E1, t->E3, t->ENQ, t->nyq, t->best, t->err};
+  void* ptrs[] = {t->A1, t->A2, t->A3, t->A1n, t->A2n, t->E1, t->E3, t->ENQ, t->nyq, t->best, t->err};
   for (void* p : ptrs) if (p) cudaFree(p);
   memset(t, 0, sizeof(*t));
 }
+
+namespace {
+// a pass of the updft1 kernel over `rows` rows of A: the CTAs of one row tile's column parts
+// are adjacent, and the grid is a multiple of NS
+Pass1 pass1_params(const ShiftTc* t, int rows, int R1) {
+  Pass1 p;
+  p.rows = rows;
+  p.tiles = (rows + TM - 1) / TM;
+  p.U = t->U;
+  p.KB = t->KB12;
+  p.R1 = R1;
+  p.NT = t->NT12;
+  p.NS = t->NS;
+  p.Us = t->Us;
+  p.stages = t->stages1;
+  p.rpb = p.Y = 1;
+  p.SB = p.SX = p.SU = 0;
+  p.ws = t->KB12 * (TK / 2);
+  p.Rout = 0;
+  return p;
+}
+
+int pass1_grid(const ShiftTc* t, const Pass1& p) {
+  const int per = t->n_sm / p.NS > 0 ? t->n_sm / p.NS : 1;
+  return (p.tiles < per ? p.tiles : per) * p.NS;
+}
+}  // namespace
 
 int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st, const cudaEvent_t* marks) {
   MTB_CUDA_TRY(cudaMemsetAsync(t->best, 0, (size_t)B * 8, st));
@@ -878,58 +1126,76 @@ int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st, const cudaEvent_t* marks
                                     (int)t->smem1));
   MTB_CUDA_TRY(cudaFuncSetAttribute(updft1_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)t->smem1));
+  const CUtensorMap& mapE1 = *reinterpret_cast<const CUtensorMap*>(t->mapE1);
   // Nyquist plane: pass 1 over its rows (b, m1) into A2n rows (b, u0), then A2n E1 -> Y
   {
-    Pass1 pn;
-    pn.rows = B * N;
-    pn.tiles = (pn.rows + TM - 1) / TM;
-    pn.N = N;
-    pn.HH = 1;
-    pn.U = U;
-    pn.KB = t->KB12;
-    pn.R1 = t->R1n;
-    pn.R2 = t->R2n;
-    pn.NT = t->NT12;
-    pn.stages = t->stages1;
-    int gn = pn.tiles < t->n_sm ? pn.tiles : t->n_sm;
+    Pass1 pn = pass1_params(t, B * N, t->R1n);
+    pn.rpb = N;  // row (b, m1) -> A2n row b U + u0, word m1
+    pn.Y = N;
+    pn.SB = U;
+    pn.SU = 1;
+    pn.Rout = t->R2n;
     mtb_prof_begin(st);
-    updft1_tc_kernel<false><<<gn, kThreads, t->smem1, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA1n),
-                                                            *reinterpret_cast<const CUtensorMap*>(t->mapE1), pn,
-                                                            (uint32_t*)t->A2n, nullptr, t->err);
+    updft1_tc_kernel<false><<<pass1_grid(t, pn), kThreads, t->smem1, st>>>(
+        *reinterpret_cast<const CUtensorMap*>(t->mapA1n), mapE1, pn, (uint32_t*)t->A2n, nullptr, t->err);
     mtb_prof_end(st, "updft1_tc_kernel (Nyquist plane, pass 1)");
     MTB_LAUNCH_CHECK();
-    pn.rows = B * U;
-    pn.tiles = (pn.rows + TM - 1) / TM;
-    pn.R1 = t->R2n;  // the A operand is now A2n
-    gn = pn.tiles < t->n_sm ? pn.tiles : t->n_sm;
+    Pass1 py = pass1_params(t, B * U, t->R2n);  // the A operand is now A2n
     mtb_prof_begin(st);
-    updft1_tc_kernel<true><<<gn, kThreads, t->smem1, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA2n),
-                                                           *reinterpret_cast<const CUtensorMap*>(t->mapE1), pn,
-                                                           nullptr, t->nyq, t->err);
+    updft1_tc_kernel<true><<<pass1_grid(t, py), kThreads, t->smem1, st>>>(
+        *reinterpret_cast<const CUtensorMap*>(t->mapA2n), mapE1, py, nullptr, t->nyq, t->err);
     mtb_prof_end(st, "updft1_tc_kernel (Nyquist plane, pass 2)");
     MTB_LAUNCH_CHECK();
   }
   if (marks && marks[0]) cudaEventRecord(marks[0], st);
-  // pass 1
-  Pass1 p1;
-  p1.rows = B * HH * N;
-  p1.tiles = (p1.rows + TM - 1) / TM;
-  p1.N = N;
-  p1.HH = HH;
-  p1.U = U;
-  p1.KB = t->KB12;
-  p1.R1 = t->R1;
-  p1.R2 = t->R2;
-  p1.NT = t->NT12;
-  p1.stages = t->stages1;
-  const int g1 = p1.tiles < t->n_sm ? p1.tiles : t->n_sm;
+  // pass 1: row (b, m2, m1) -> A2 row (b U + u0) HH + m2, word m1
+  Pass1 p1 = pass1_params(t, B * HH * N, t->R1);
+  p1.rpb = HH * N;
+  p1.Y = N;
+  p1.SB = U * HH;
+  p1.SX = 1;
+  p1.SU = HH;
+  p1.Rout = t->R2;
   mtb_prof_begin(st);
-  updft1_tc_kernel<false><<<g1, kThreads, t->smem1, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA1),
-                                                          *reinterpret_cast<const CUtensorMap*>(t->mapE1), p1,
-                                                          (uint32_t*)t->A2, nullptr, t->err);
+  updft1_tc_kernel<false><<<pass1_grid(t, p1), kThreads, t->smem1, st>>>(
+      *reinterpret_cast<const CUtensorMap*>(t->mapA1), mapE1, p1, (uint32_t*)t->A2, nullptr, t->err);
   mtb_prof_end(st, "updft1_tc_kernel");
   MTB_LAUNCH_CHECK();
   if (marks && marks[1]) cudaEventRecord(marks[1], st);
+  if (!t->fused) {
+    // pass 2: row (b, u0, m2) -> A3 row b RP3 + u0 U + u1, word m2
+    Pass1 p2 = pass1_params(t, B * U * HH, t->R2);
+    p2.rpb = U * HH;
+    p2.Y = HH;
+    p2.SB = t->RP3;
+    p2.SX = U;
+    p2.SU = 1;
+    p2.ws = t->KB3 * (TK / 2);
+    p2.Rout = t->R3;
+    mtb_prof_begin(st);
+    updft1_tc_kernel<false><<<pass1_grid(t, p2), kThreads, t->smem1, st>>>(
+        *reinterpret_cast<const CUtensorMap*>(t->mapA2), mapE1, p2, (uint32_t*)t->A3, nullptr, t->err);
+    mtb_prof_end(st, "updft1_tc_kernel (pass 2)");
+    MTB_LAUNCH_CHECK();
+    Pass3 p3;
+    p3.TPB = t->TPB3;
+    p3.tiles = B * t->TPB3;
+    p3.U = U;
+    p3.KB = t->KB3;
+    p3.R3 = t->R3;
+    p3.NT = t->NT3;
+    p3.stages = t->stages3;
+    MTB_CUDA_TRY(cudaFuncSetAttribute(updft3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem3));
+    const int g3 = p3.tiles < t->n_sm ? p3.tiles : t->n_sm;
+    mtb_prof_begin(st);
+    updft3_tc_kernel<<<g3, kThreads, t->smem3, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA3),
+                                                     *reinterpret_cast<const CUtensorMap*>(t->mapE3), p3, t->nyq,
+                                                     (const float4*)t->ENQ, t->best, t->err);
+    mtb_prof_end(st, "updft3_tc_kernel");
+    MTB_LAUNCH_CHECK();
+    if (marks && marks[2]) cudaEventRecord(marks[2], st);
+    return MTB_OK;
+  }
   // passes 2 + 3
   Pass23 p2;
   p2.B = B;
@@ -948,8 +1214,7 @@ int shift_tc_passes(ShiftTc* t, int B, cudaStream_t st, const cudaEvent_t* marks
   MTB_CUDA_TRY(cudaFuncSetAttribute(updft23_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem23));
   const int g2 = p2.tiles < t->n_sm ? p2.tiles : t->n_sm;
   mtb_prof_begin(st);
-  updft23_tc_kernel<<<g2, kThreads23, t->smem23, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA2),
-                                                     *reinterpret_cast<const CUtensorMap*>(t->mapE1),
+  updft23_tc_kernel<<<g2, kThreads23, t->smem23, st>>>(*reinterpret_cast<const CUtensorMap*>(t->mapA2), mapE1,
                                                      *reinterpret_cast<const CUtensorMap*>(t->mapE3), p2, t->nyq,
                                                      (const float4*)t->ENQ, t->best, t->err);
   mtb_prof_end(st, "updft23_tc_kernel");

@@ -24,7 +24,9 @@ from . import shift as S
 class FoldedFLE:
     """a = h B^H f through the octant folding; exact to float64 rounding."""
 
-    def __init__(self, tables, N1: int, radius: float):
+    def __init__(self, tables, N1: int, radius: float, dense: bool = True):
+        """``dense=False`` skips the basis columns (n_rep x ne complex: 66 GB at 128^3, L = 64);
+        only ``evaluate_t_streamed`` is available then."""
         self.tables = tables
         N = N1 + (N1 % 2)
         R_ = N // 2
@@ -50,8 +52,14 @@ class FoldedFLE:
         r = np.sqrt((reps ** 2).sum(1)) / radius
         th = np.arctan2(np.sqrt(reps[:, 0] ** 2 + reps[:, 1] ** 2), reps[:, 2])
         ph = np.arctan2(reps[:, 1], reps[:, 0])
+        self.r, self.th, self.ph = r, th, ph
         tb = tables
         self.pos = np.nonzero(tb.ms >= 0)[0]
+        self.partner = {}
+        for i in range(tb.ne):
+            self.partner[(int(tb.ls[i]), int(tb.ks[i]), int(tb.ms[i]))] = i
+        if not dense:
+            return
         cols = np.zeros((reps.shape[0], self.pos.size), dtype=np.complex128)
         ylm = _sph_harm_table(tb.lmax, th, ph)
         radial = {}
@@ -66,9 +74,6 @@ class FoldedFLE:
         l = tb.ls[self.pos]
         self.par_re = np.stack([(-1.0) ** m, np.ones_like(m, dtype=float), (-1.0) ** (l + m)], 1)
         self.par_im = np.stack([-(-1.0) ** m, -np.ones_like(m, dtype=float), (-1.0) ** (l + m)], 1)
-        self.partner = {}
-        for i in range(tb.ne):
-            self.partner[(int(tb.ls[i]), int(tb.ks[i]), int(tb.ms[i]))] = i
 
     def _channel(self, vols, par):
         """sum over images of f(image) * prod over flipped axes of par -> (b, n_rep) per column class."""
@@ -101,6 +106,70 @@ class FoldedFLE:
             im[:, sel] = A @ self.cols[:, sel].imag
         a = np.zeros((b, tb.ne), dtype=np.complex128)
         a[:, self.pos] = re + 1j * im
+        for i in range(tb.ne):
+            m = int(tb.ms[i])
+            if m < 0:
+                j = self.partner[(int(tb.ls[i]), int(tb.ks[i]), -m)]
+                a[:, i] = (-1.0) ** m * np.conj(a[:, j])
+        return a
+
+
+    def evaluate_t_streamed(self, vols):
+        """``evaluate_t`` one degree at a time, holding no basis: the associated Legendre
+        functions advance in l by the same normalised recurrences as ``_sph_harm_table`` (all
+        orders m <= l of degrees l - 1 and l - 2 kept), the radial functions of degree l are
+        made for that degree only, and each (l, m) contracts the 8 sign-image channels with
+        its Re / Im parity.  Same float64 sums as the dense form, in another order."""
+        vols = np.asarray(vols, dtype=np.float64)
+        b = vols.shape[0]
+        tb = self.tables
+        keys = [(sx, sy, sz) for sx in (1.0, -1.0) for sy in (1.0, -1.0) for sz in (1.0, -1.0)]
+        ch = self._channel(vols, keys)
+        x = np.cos(self.th)
+        sn = np.sqrt(np.maximum(0.0, 1.0 - x * x))
+        lmax = int(tb.lmax)
+        # per degree: its coefficient indices with m >= 0, grouped by k
+        by_l = {}
+        for i in self.pos:
+            by_l.setdefault(int(tb.ls[i]), []).append(int(i))
+        a = np.zeros((b, tb.ne), dtype=np.complex128)
+        p1 = {}  # P_{l-1}^m
+        p2 = {}  # P_{l-2}^m
+        for l in range(lmax + 1):
+            cur = {}
+            for m in range(l + 1):
+                if m == l:
+                    cur[m] = (np.full_like(x, 1.0 / np.sqrt(4 * np.pi)) if l == 0
+                              else -np.sqrt((2 * m + 1) / (2 * m)) * sn * p1[m - 1])
+                elif m == l - 1:
+                    cur[m] = np.sqrt(2 * m + 3) * x * p1[m]
+                else:
+                    aa = np.sqrt((4 * l * l - 1) / (l * l - m * m))
+                    bb = np.sqrt(((l - 1) ** 2 - m * m) / (4 * (l - 1) ** 2 - 1))
+                    cur[m] = aa * (x * p1[m] - bb * p2[m])
+            p2, p1 = p1, cur
+            idx = by_l.get(l, [])
+            if not idx:
+                continue
+            ks = sorted({int(tb.ks[i]) for i in idx})
+            radial = {}
+            for k in ks:
+                i0 = next(i for i in idx if int(tb.ks[i]) == k)
+                radial[k] = tb.h * tb.cs[i0] * spherical_jn(l, tb.lmds[i0] * self.r)
+            Rk = np.stack([radial[k] for k in ks], 0)  # (n_k, n_rep)
+            for m in range(l + 1):
+                cols = [self.partner[(l, k, m)] for k in ks if (l, k, m) in self.partner]
+                kk = [j for j, k in enumerate(ks) if (l, k, m) in self.partner]
+                if not cols:
+                    continue
+                yc = cur[m] * np.exp(-1j * m * self.ph)  # conj(Y_l^m)
+                sre = (-1.0) ** m
+                slm = (-1.0) ** (l + m)
+                key_re = (sre, 1.0, slm)
+                key_im = (-sre, -1.0, slm)
+                re = (ch[key_re] * yc.real) @ Rk[kk].T
+                im = (ch[key_im] * yc.imag) @ Rk[kk].T
+                a[:, cols] = re + 1j * im
         for i in range(tb.ne):
             m = int(tb.ms[i])
             if m < 0:

@@ -62,3 +62,16 @@ def test_oracle_sigma_equals_reference_compute_sigma(fx, tag, N, L, radius):
     assert sig.shape == ref.shape
     assert np.abs(sig - ref).max() < 1e-12 * np.abs(ref).max()
     np.testing.assert_allclose(np.linalg.norm(a, axis=1), sx[f"{tag}_norms"], rtol=1e-14)
+
+
+@pytest.mark.parametrize("tag,N,L,radius", [("c16r8", 16, 8, 8), ("c32r16", 32, 16, 16), ("c32r15", 32, 16, 15)])
+def test_streamed_oracle_adjoint_equals_reference_dense_basis(fx, tag, N, L, radius):
+    """The basis-free form the 128^3, L = 64 accuracy check uses (one degree at a time, no
+    n_rep x ne matrix) gives the reference's dense adjoint too."""
+    from oracle import pipeline as OP
+
+    tb = T.lap_eig_ball(N, L, radius)
+    ff = OP.FoldedFLE(tb, N, float(radius), dense=False)
+    ref = fx[f"{tag}_coeffs"]
+    a = ff.evaluate_t_streamed(fx[f"{tag}_volumes"])
+    assert np.abs(a - ref).max() < 1e-10 * np.abs(ref).max()

@@ -41,7 +41,12 @@ def test_shift_matches_reference_fixture(cuda_device):
                                               (16, 4, 1, "bf16x3"), (32, 4, 2, "bf16x3"),
                                               (32, 8, 5, "bf16x3"), (16, 8, 5, "bf16x3"),
                                               (128, 8, 8, "auto"), (48, 8, 6, "fp32"), (96, 8, 6, "auto"),
-                                              (80, 4, 3, "fp32")])
+                                              (80, 4, 3, "fp32"),
+                                              # the unfused tensor-core passes: boxes outside the fused
+                                              # kernels, and U > 128 (two column parts of the N-tile)
+                                              (128, 8, 8, "bf16x3"), (96, 8, 6, "bf16x3"), (48, 8, 6, "bf16x3"),
+                                              (80, 4, 3, "bf16x3"), (64, 8, 8, "bf16x3"), (32, 8, 9, "bf16x3"),
+                                              (128, 8, 8, "fp32")])
 def test_shift_matches_oracle(cuda_device, N, uf, r, precision):
     rng = np.random.default_rng(N + uf + r)
     tmpl = blob_template(rng, N, 60, N * 0.3, (1.5, 3.0), mask_radius=N * 0.4)
@@ -123,6 +128,31 @@ def test_shift_tensor_path_many_tiles_per_cta(cuda_device):
     assert same.mean() >= 0.9, same
 
 
+@pytest.mark.parametrize("N,uf,r,B", [(128, 8, 8, 12), (96, 8, 6, 40)])
+def test_shift_unfused_tensor_path_many_tiles(cuda_device, N, uf, r, B):
+    """The unfused tensor-core passes over many row tiles per persistent CTA (at 128^3, r 8: two
+    column parts per tile and 145 pass-3 tiles per subtomogram) against the FP32 path, itself
+    checked against the oracle above."""
+    rng = np.random.default_rng(N + B)
+    tmpl = blob_template(rng, N, 80, N * 0.3, (1.5, 3.0), mask_radius=N * 0.4)
+    vols = torch.from_numpy(np.repeat(tmpl[None], B, 0) + 0.5 * rng.standard_normal((B, N, N, N)).astype(np.float32))
+    vols = vols.to(cuda_device)
+    q = haar_quaternions(rng, B)
+    z = torch.from_numpy(rng.uniform(-1.5, 1.5, (B, 3)).astype(np.float32)).to(cuda_device)
+    out = {}
+    for precision in ("fp32", "bf16x3"):
+        sm = _matcher(N, B, uf, r, cuda_device, precision=precision)
+        sm.set_reference(tmpl)
+        shift, score = sm.search_shifts(subtomos=vols, ctfs=None, shift_zyx=z, rotation_tracker=q)
+        sm.status()
+        assert sm.effective_precision == precision
+        out[precision] = (shift.cpu().numpy(), score.cpu().numpy())
+        del sm
+    np.testing.assert_allclose(out["bf16x3"][1], out["fp32"][1], rtol=1e-4)
+    same = np.all(np.abs(out["bf16x3"][0] - out["fp32"][0]) <= 1e-6, axis=1)
+    assert same.mean() >= 0.9, same
+
+
 def test_shift_nan_subtomogram_follows_argmax_order(cuda_device):
     """A NaN voxel makes the subtomogram's whole correlation grid NaN; argmax then takes the
     first grid point, as torch.argmax and numpy.argmax do, on both paths.  The other
@@ -174,12 +204,11 @@ def test_precision_selection(cuda_device):
     else precision_mode "fast" -> "auto", "accurate" -> "fp32")."""
     from matcha_b200.core.ShiftMatcher import ShiftMatcher
 
-    tmpl = np.zeros((128, 128, 128), np.float32)
     with pytest.raises(ValueError):
-        sm = _matcher(128, 1, 8, 8, cuda_device, precision="bf16x3")
+        sm = _matcher(8, 1, 4, 1, cuda_device, precision="bf16x3")
         sm._handle(1)
-    for N, want in ((128, "fp32"), (64, "bf16x3")):
-        sm = _matcher(N, 1, 8, 5 if N == 64 else 8, cuda_device, precision="auto")
+    for N, want in ((8, "fp32"), (64, "bf16x3"), (128, "bf16x3"), (96, "bf16x3")):
+        sm = _matcher(N, 1, 8 if N > 8 else 4, {8: 1, 64: 5, 128: 8, 96: 6}[N], cuda_device, precision="auto")
         sm._handle(1)
         assert sm.effective_precision == want
     base = dict(N=64, voxel_size=1.0, num_subtomograms_per_batch=2, shift_upsample_factor=8, shift_search_radius=5,
@@ -189,4 +218,3 @@ def test_precision_selection(cuda_device):
                         ({"b200": {"precision": "bf16x3"}}, "bf16x3")):
         sm = ShiftMatcher(Cfg(**base, **extra), cuda_device, torch.complex64)
         assert sm.precision == want, (extra, sm.precision)
-    del tmpl
