@@ -761,6 +761,15 @@ def run_highband(args):
         ms = e0.elapsed_time(e1) / n
         res = {k: out[k].cpu().numpy() for k in ("alpha", "beta", "gamma", "shift", "shift_score",
                                                    "rotation_score", "tracker")}
+        # one more alternation with every library launch timed (CUDA events; not the number above)
+        from matcha_b200 import _native as nat
+
+        tracker.copy_(ident)
+        nat.profile_start(256)
+        step(vols, vols, tracker, z3)
+        nat.profile_stop()
+        prof, _ = nat.profile_read()
+        res["kernel_ms"] = {k: round(v["ms"], 3) for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])}
         prec = f"expansion {step.correlator.fle.precision}, upsampled DFT {step.shifter.effective_precision}"
         three = None
         if precision != "fp32":
@@ -788,11 +797,12 @@ def run_highband(args):
         "config": {"workload": f"{B} subtomograms 128^3, L=64, march 16/32/48/64, C=10, 1 Newton step, "
                                f"shift r=8 uf=8, -5 dB, 1500 blobs", "precision": prec},
         "median_rot_err_deg": float(np.median(err1)), "p90_rot_err_deg": float(np.percentile(err1, 90)),
-        "three_alternations": three,
+        "three_alternations": three, "kernel_ms_per_alternation": chosen.pop("kernel_ms"),
     }
     runs = {"chosen": chosen}
     if not args.no_fp32:
         ms32, plain, prec32, _ = one_precision("fp32")
+        plain.pop("kernel_ms")
         runs["plain_fp32"] = plain
         ang = lambda d: [np.asarray(d[k], dtype=np.float64) for k in ("alpha", "beta", "gamma")]
         dev_deg = euler_dev_deg(*ang(chosen), *ang(plain))

@@ -809,6 +809,327 @@ constexpr size_t z64_smem_bytes() {
   return (size_t)64 * sizeof(float2) + (size_t)64 * kZS * sizeof(float2) + (size_t)36 * kXS * sizeof(float2);
 }
 
+// ------------------------------------------------------------------ box 128: radix-16 x 8 path
+// The box-64 design at N = 128: a 128-point line is x[r + 8 s] (thread r of a group of 8,
+// register s < 16); a 16-point DFT in registers (two 8-point DFTs and the W16 butterflies), the
+// twiddles W128^(r k1), one transpose through the group's scratch, and two 8-point DFTs (for
+// k1 = r and r + 8) leave X[r + 8 s] in thread r again.  36 groups take the 64 packed x lines
+// and the 65 y / z columns in two rounds.  The x-FFT output overlays the z-interpolated plane
+// once every sample is in registers, so a CTA holds about 113 KB and two fit on an SM.
+constexpr int kT128 = 288;   // 36 groups of 8
+constexpr int kG128 = 36;
+constexpr int kXS128 = 152;  // per-group scratch (float2): slot (k1, r) at 9 k1 + r; 152 = 8 (mod 16)
+                             // puts the two groups of a half-warp on disjoint bank pairs
+constexpr int kZS128 = 65;   // row stride (float2) of the 128 x 65 buffer of the z pass
+
+// 16-point forward DFT, natural order in and out: the even and odd halves by dft8, then the
+// radix-2 butterflies with W16^k.
+__device__ __forceinline__ void dft16(float2 (&v)[16]) {
+  float2 e[8], o[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    e[i] = v[2 * i];
+    o[i] = v[2 * i + 1];
+  }
+  dft8(e);
+  dft8(o);
+  // W16^k = (cos(pi k / 8), -sin(pi k / 8))
+  const float c1 = 0.92387953251128674f, s1 = 0.38268343236508977f, c2 = 0.70710678118654752f;
+  const float2 w16[8] = {make_float2(1.f, 0.f),  make_float2(c1, -s1),  make_float2(c2, -c2), make_float2(s1, -c1),
+                         make_float2(0.f, -1.f), make_float2(-s1, -c1), make_float2(-c2, -c2), make_float2(-c1, -s1)};
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const float2 t = k == 0 ? o[0] : (k == 4 ? c_mi(o[4]) : cmul(o[k], w16[k]));
+    v[k] = c_add(e[k], t);
+    v[k + 8] = c_sub(e[k], t);
+  }
+}
+
+// 128-point forward FFT of one line by its 8 threads (r = lane % 8): v[s] = x[r + 8 s] on
+// entry and v[s] = X[r + 8 s] on exit.  xs is the group's scratch (kXS128 float2); tw[m] = W128^m.
+__device__ __forceinline__ void fft128_group(float2 (&v)[16], int r, float2* xs, const float2* tw) {
+  dft16(v);  // V_r[k1] = sum_s x[r + 8 s] W16^(s k1)
+#pragma unroll
+  for (int k1 = 1; k1 < 16; ++k1) v[k1] = cmul(v[k1], tw[r * k1]);
+  __syncwarp();
+#pragma unroll
+  for (int k1 = 0; k1 < 16; ++k1) xs[9 * k1 + r] = v[k1];
+  __syncwarp();
+  float2 a[8], b[8];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    a[t] = xs[9 * r + t];        // V_t[r]
+    b[t] = xs[9 * (r + 8) + t];  // V_t[r + 8]
+  }
+  dft8(a);  // X[r + 16 k2]
+  dft8(b);  // X[r + 8 + 16 k2]
+#pragma unroll
+  for (int k2 = 0; k2 < 8; ++k2) {
+    v[2 * k2] = a[k2];
+    v[2 * k2 + 1] = b[k2];
+  }
+}
+
+__device__ void load_twiddles128(float2* tw) {
+  for (int k = threadIdx.x; k < 128; k += blockDim.x) {
+    double s, c;
+    sincospi(-2.0 * k / 128, &s, &c);
+    tw[k] = make_float2((float)c, (float)s);
+  }
+}
+
+// Element (q, c) of the 64 x 128 x-FFT output: the box-64 swizzle (c ^ f(q), f(q) = 8 (q & 1)
+// + 2 (q / 2 & 3)), so that the x FFT's row stores and the y FFT's column loads of a
+// half-warp fill the 16 bank pairs once.
+__device__ __forceinline__ int z_at128(int q, int c) { return q * 128 + (c ^ (((q & 1) << 3) | ((q << 1) & 6))); }
+
+// Column of round idx (group L + 36 round): 0 .. 63 in an order that puts the two groups of
+// a half-warp 8 columns apart, then the Nyquist column 64; idx > 64 shadows column 64.
+__device__ __forceinline__ int col128(int idx) {
+  return idx < 64 ? ((idx >> 1) & 7) + 16 * (idx >> 4) + 8 * (idx & 1) : 64;
+}
+
+// patch_fft_xy_kernel<128, false> with the radix-16 x 8 FFTs; fill_tab[r2] is fill_weight(r2).
+__global__ void __launch_bounds__(kT128, 2)
+patch_fft_xy128_kernel(const float* __restrict__ vol, const float* __restrict__ shift_zyx,
+                       const float* __restrict__ bgw_tab, const float* __restrict__ fill_tab, ShiftGeom g,
+                       float2* __restrict__ T, float* __restrict__ bg) {
+  constexpr int N = 128, HN = 64, H = 65;
+  extern __shared__ __align__(16) float2 sm2[];
+  __shared__ float red[32];
+  __shared__ int s_cx[2][N];        // [tap] clamped source column
+  __shared__ float s_wx[2][N];      // [tap] weight (0 for taps outside the box or zeroed)
+  __shared__ int4 s_ty[N];          // row j's y taps packed (c0, c1, w0, w1)
+  float2* tw = sm2;                                     // 128
+  float* P0 = reinterpret_cast<float*>(sm2 + 128);      // the z-interpolated plane (128 x 128)
+  float2* Z = reinterpret_cast<float2*>(P0);            // then the 64 x 128 x-FFT output (z_at128)
+  float2* xs = reinterpret_cast<float2*>(P0 + N * N);   // 36 x kXS128 group scratch
+  const int ip = blockIdx.x, b = blockIdx.y;
+  const int i = (ip + HN) & (N - 1);
+  const int di = i - HN;
+  const float* v = vol + (int64_t)b * N * N * N;
+  const PatchShift ps = patch_shift(shift_zyx, b, N);
+  const float z = (float)i + ps.f[0];
+  const float z0 = floorf(z);
+  const int iz = (int)z0;
+  const float fz = z - z0;
+  load_twiddles128(tw);
+  if (threadIdx.x < 2 * N) {
+    const int ax = threadIdx.x / N, j = threadIdx.x % N;  // ax 0: y (index j), 1: x (index k)
+    const float y = (float)j + ps.f[1 + ax];
+    const float y0 = floorf(y);
+    const int iy = (int)y0;
+    const float fy = y - y0;
+    const bool zero = (j == ps.zp[1 + ax]);
+    const int c0 = min(max(iy, 0), N - 1), c1 = min(max(iy + 1, 0), N - 1);
+    const float w0 = (zero || iy < 0 || iy >= N) ? 0.f : 1.f - fy;
+    const float w1 = (zero || iy + 1 < 0 || iy + 1 >= N) ? 0.f : fy;
+    if (ax == 0) {
+      s_ty[j] = make_int4(c0, c1, __float_as_int(w0), __float_as_int(w1));
+    } else {
+      s_cx[0][j] = c0;
+      s_cx[1][j] = c1;
+      s_wx[0][j] = w0;
+      s_wx[1][j] = w1;
+    }
+  }
+  {
+    constexpr int P4 = N * N / 4;
+    const bool zplane = (i == ps.zp[0]);
+    const bool in0 = iz >= 0 && iz < N, in1 = iz + 1 >= 0 && iz + 1 < N;
+    const float w0 = (zplane || !in0) ? 0.f : 1.f - fz, w1 = (zplane || !in1) ? 0.f : fz;
+    const float4* g0 = reinterpret_cast<const float4*>(v + (int64_t)(in0 ? iz : 0) * N * N);
+    const float4* g1 = reinterpret_cast<const float4*>(v + (int64_t)(in1 ? iz + 1 : 0) * N * N);
+    float4* pl4 = reinterpret_cast<float4*>(P0);
+#pragma unroll 4
+    for (int e = threadIdx.x; e < P4; e += kT128) {
+      const float4 a = in0 ? __ldg(g0 + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 c = in1 ? __ldg(g1 + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+      pl4[e] = make_float4(w0 * a.x + w1 * c.x, w0 * a.y + w1 * c.y, w0 * a.z + w1 * c.z, w0 * a.w + w1 * c.w);
+    }
+  }
+  __syncthreads();
+  const int L = threadIdx.x >> 3, r = threadIdx.x & 7;
+  float part = 0.f;
+  auto sample = [&](int j, int k) -> float {
+    const int4 ty = s_ty[j];
+    const int cy0 = ty.x, cy1 = ty.y;
+    const float wy0 = __int_as_float(ty.z), wy1 = __int_as_float(ty.w);
+    const float wx0 = s_wx[0][k], wx1 = s_wx[1][k];
+    const int cx0 = s_cx[0][k], cx1 = s_cx[1][k];
+    const float a = wx0 * P0[cy0 * N + cx0] + wx1 * P0[cy0 * N + cx1];
+    const float c = wx0 * P0[cy1 * N + cx0] + wx1 * P0[cy1 * N + cx1];
+    const float p = wy0 * a + wy1 * c;
+    const int dj = j - HN, dk = k - HN;
+    const int r2 = di * di + dj * dj + dk * dk;
+    float keep = 1.f;  // 1 - W
+    if (r2 > g.r2_outer) {
+      part += p;
+      keep = 0.f;
+    } else if (r2 >= g.r2_inner) {
+      part += __ldg(bgw_tab + r2) * p;
+      keep = 1.f - __ldg(fill_tab + r2);
+    }
+    return keep * p * g.inv_n3;
+  };
+  // x FFT: packed line q (rolled rows q and q + 64 as real and imaginary parts) of group L in
+  // rounds q = L and L + 36; all samples are taken before the plane is overwritten by Z
+  float2 w0[16], w1[16];
+  const bool second = L + kG128 < HN;  // warp-uniform (groups 28..35 are warps 7 and 8)
+#pragma unroll
+  for (int s8 = 0; s8 < 16; ++s8) {
+    const int kp = r + 8 * s8, k = (kp + HN) & (N - 1);
+    w0[s8] = make_float2(sample(L + HN, k), sample(L, k));
+    if (second) w1[s8] = make_float2(sample(L + kG128 + HN, k), sample(L + kG128, k));
+  }
+  __syncthreads();  // the plane is read: Z may overwrite it
+  float2* gx = xs + L * kXS128;
+  fft128_group(w0, r, gx, tw);
+#pragma unroll
+  for (int k2 = 0; k2 < 16; ++k2) Z[z_at128(L, r + 8 * k2)] = w0[k2];
+  if (second) {
+    fft128_group(w1, r, gx, tw);
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) Z[z_at128(L + kG128, r + 8 * k2)] = w1[k2];
+  }
+  __syncthreads();
+  // y FFT of the columns m2 < 65, its input split on the way in (Z = A + i B holds the
+  // transforms of rows q and q + 64), each result stored straight to T
+  float2* out = T + ((int64_t)b * N + ip) * N * H;
+#pragma unroll 1
+  for (int round = 0; round < 2; ++round) {
+    const int idx = L + kG128 * round;
+    if (idx >= 72) break;
+    const int col = col128(idx);
+    float2 w[16];
+#pragma unroll
+    for (int s8 = 0; s8 < 8; ++s8) {
+      const int q = r + 8 * s8;
+      const float2 zk = Z[z_at128(q, col)];
+      const float2 zm = Z[z_at128(q, (N - col) & (N - 1))];
+      w[s8] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+      w[s8 + 8] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+    }
+    fft128_group(w, r, gx, tw);
+    if (idx <= 64) {
+#pragma unroll
+      for (int k2 = 0; k2 < 16; ++k2) out[(r + 8 * k2) * H + col] = w[k2];
+    }
+  }
+  part = block_sum(part, red);
+  if (threadIdx.x == 0) atomicAdd(&bg[b], part);
+}
+
+constexpr size_t xy128_smem_bytes() {
+  return (size_t)128 * sizeof(float2) + (size_t)128 * 128 * sizeof(float) + (size_t)kG128 * kXS128 * sizeof(float2);
+}
+
+// fft_z_kernel<128, SPLIT> with the radix-16 x 8 FFT.
+template <bool SPLIT>
+__global__ void __launch_bounds__(kT128, 2)
+fft_z128_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ what, const float* __restrict__ bg,
+                const float4* __restrict__ refq, const float* __restrict__ rot, const float* __restrict__ ctf,
+                float* __restrict__ nrm, uint32_t* __restrict__ a1, int a1_ws, int a1_R, uint32_t* __restrict__ a1n,
+                int a1n_R) {
+  constexpr int N = 128, HN = 64, H = 65;
+  extern __shared__ __align__(16) float2 sm2[];
+  __shared__ float red[32];
+  float2* tw = sm2;                // 128
+  float2* buf = sm2 + 128;         // 128 (i') x kZS128
+  float2* xs = buf + N * kZS128;   // 36 x kXS128
+  const int jp = blockIdx.x, b = blockIdx.y;
+  float2* base = T + (int64_t)b * N * N * H + (int64_t)jp * H;
+  const float2* wb = what + (int64_t)jp * H;
+  const float avg = g.wsum > 0.f ? __ldg(&bg[b]) / g.wsum : 0.f;
+  load_twiddles128(tw);
+#pragma unroll 4
+  for (int e = threadIdx.x; e < N * H; e += kT128) {
+    const int ip = e / H, m2 = e - (e / H) * H;
+    const float2 t = base[(int64_t)ip * N * H + m2];
+    const float2 w = __ldg(&wb[(int64_t)ip * N * H + m2]);
+    buf[ip * kZS128 + m2] = make_float2(fmaf(avg, w.x, t.x), fmaf(avg, w.y, t.y));
+  }
+  __syncthreads();
+  {
+    const int L = threadIdx.x >> 3, r = threadIdx.x & 7;
+    float2* gx = xs + L * kXS128;
+#pragma unroll 1
+    for (int round = 0; round < 2; ++round) {
+      const int idx = L + kG128 * round;
+      if (idx >= 72) break;
+      const int col = col128(idx);
+      float2 v[16];
+#pragma unroll
+      for (int s8 = 0; s8 < 16; ++s8) v[s8] = buf[(r + 8 * s8) * kZS128 + col];
+      fft128_group(v, r, gx, tw);
+      __syncwarp();
+      if (idx <= 64) {
+#pragma unroll
+        for (int k2 = 0; k2 < 16; ++k2) buf[(r + 8 * k2) * kZS128 + col] = v[k2];
+      }
+    }
+  }
+  __syncthreads();
+  float R[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) R[q] = __ldg(&rot[b * 9 + q]);
+  const float c = (float)g.h;
+  float st = 0.f, ss = 0.f;
+#pragma unroll 2
+  for (int e = threadIdx.x; e < N * H; e += kT128) {
+    const int ip = SPLIT ? e & (N - 1) : e / H, m2 = SPLIT ? e >> 7 : e - (e / H) * H;
+    const float2 t = buf[ip * kZS128 + m2];
+    const int kp = ip < HN ? ip : ip - N;
+    const int jq = jp < HN ? jp : jp - N;
+    const int xq = m2 < HN ? m2 : m2 - H;
+    // outside the mask the sample is taken far outside the box, which reads zero (entry 0)
+    const bool in_mask = kp * kp + jq * jq + xq * xq <= g.mask_r2;
+    float2 s;
+    {
+      const int zo = (ip + HN) & (N - 1), yo = (jp + HN) & (N - 1), xw = m2 + HN;
+      const float bx = (float)xw - c, by = (float)yo - c, bz = (float)zo - c;
+      const float rx = R[0] * bx + R[1] * by + R[2] * bz + c;
+      const float ry = R[3] * bx + R[4] * by + R[5] * bz + c;
+      const float rz = in_mask ? R[6] * bx + R[7] * by + R[8] * bz + c : -4.f;
+      s = trilinear_quad(refq, N, rz, ry, rx);
+    }
+    if (in_mask && ctf) {
+      const float cv = __ldg(&ctf[(((int64_t)b * N + ip) * N + jp) * H + m2]);
+      s.x *= cv;
+      s.y *= cv;
+    }
+    st += t.x * t.x + t.y * t.y;
+    ss += s.x * s.x + s.y * s.y;
+    const float2 p = make_float2(s.x * t.x + s.y * t.y, s.x * t.y - s.y * t.x);
+    if (SPLIT) {
+      uint32_t hi, lo;
+      split_bf16x2(p.x, p.y, hi, lo);
+      if (m2 < HN) {
+        const size_t row = ((size_t)b * HN + m2) * N + jp;
+        a1[row * a1_ws + ip] = hi;
+        a1[((size_t)a1_R + row) * a1_ws + ip] = lo;
+      } else {
+        // the Nyquist plane m2 = N/2: its own pass-1 operand, rows (b, m1), K (m0, re/im)
+        const size_t row = (size_t)b * N + jp;
+        a1n[row * a1_ws + ip] = hi;
+        a1n[((size_t)a1n_R + row) * a1_ws + ip] = lo;
+      }
+    } else {
+      base[(int64_t)ip * N * H + m2] = p;
+    }
+  }
+  st = block_sum(st, red);
+  ss = block_sum(ss, red);
+  if (threadIdx.x == 0) {
+    atomicAdd(&nrm[2 * b], st);
+    atomicAdd(&nrm[2 * b + 1], ss);
+  }
+}
+
+constexpr size_t z128_smem_bytes() {
+  return (size_t)128 * sizeof(float2) + (size_t)128 * kZS128 * sizeof(float2) + (size_t)kG128 * kXS128 * sizeof(float2);
+}
+
 __global__ void fill_table_kernel(ShiftGeom g, int n, float* __restrict__ tab) {
   const int r2 = blockIdx.x * blockDim.x + threadIdx.x;
   if (r2 < n) tab[r2] = fill_weight(r2, g);
@@ -1035,7 +1356,7 @@ struct mtb_shift {
   float* fill_tab; // fill weight W by integer squared radius (device formula)
   float2* what;    // (N, N, N/2+1) plane transforms of the fill weight W / N^3
   float2* ref;     // (N, N, N) Fourier reference, fftshifted and masked
-  float4* refq;    // box 64: corner quads of ref, (N + 2) (N + 1)^2 x 32 bytes
+  float4* refq;    // boxes 64, 128: corner quads of ref, (N + 2) (N + 1)^2 x 32 bytes
   float2* E0;      // (U, N)
   float2* E1;      // (U, N)
   float2* E2;      // (U, H)
@@ -1128,6 +1449,35 @@ int shift_front_64(mtb_shift* h, const float* subtomos, const float* shift_zyx, 
   return MTB_OK;
 }
 
+int shift_front_128(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
+                    int B, cudaStream_t st, bool split) {
+  const ShiftGeom& g = h->g;
+  const int sxy = (int)xy128_smem_bytes(), sz = (int)z128_smem_bytes();
+  MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
+  mtb_prof_begin(st);
+  patch_fft_xy128_kernel<<<dim3(128, B), kT128, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, h->fill_tab, g, h->T,
+                                                            h->bg);
+  mtb_prof_end(st, "patch_fft_xy128_kernel");
+  MTB_LAUNCH_CHECK();
+  prof_mark(h, 1, st);
+  if (split) {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z128_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+    mtb_prof_begin(st);
+    fft_z128_kernel<true><<<dim3(128, B), kT128, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
+                                                            (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1,
+                                                            (uint32_t*)h->tc.A1n, h->tc.R1n);
+    mtb_prof_end(st, "fft_z128_kernel");
+  } else {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z128_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+    mtb_prof_begin(st);
+    fft_z128_kernel<false><<<dim3(128, B), kT128, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
+                                                             nullptr, 0, 0, nullptr, 0);
+    mtb_prof_end(st, "fft_z128_kernel");
+  }
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
+}
+
 // split: the z pass writes the tensor-core pass-1 operand (A1) instead of the FP32 product in T.
 int shift_front(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
                 int B, cudaStream_t st, bool split) {
@@ -1138,7 +1488,8 @@ int shift_front(mtb_shift* h, const float* subtomos, const float* shift_zyx, con
     case 32: return shift_front_n<32>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
     case 64: return B > 0 ? shift_front_64(h, subtomos, shift_zyx, rot, ctf, B, st, split)
                           : shift_front_n<64>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
-    case 128: return shift_front_n<128>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
+    case 128: return B > 0 ? shift_front_128(h, subtomos, shift_zyx, rot, ctf, B, st, split)
+                           : shift_front_n<128>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
     case 48: return shift_front_n<48>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
     case 80: return shift_front_n<80>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
     case 96: return shift_front_n<96>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
@@ -1237,7 +1588,8 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
   if (!want_tc && (!alloc((void**)&h->X1, B * g.U * N * g.H * 8) || !alloc((void**)&h->pval, B * h->ngrp * 4) ||
                    !alloc((void**)&h->pidx, B * h->ngrp * 4)))
     return fail(MTB_ERR_OOM);
-  if (N == 64 && !alloc((void**)&h->refq, (size_t)(N + 2) * (N + 1) * (N + 1) * 32)) return fail(MTB_ERR_OOM);
+  if ((N == 64 || N == 128) && !alloc((void**)&h->refq, (size_t)(N + 2) * (N + 1) * (N + 1) * 32))
+    return fail(MTB_ERR_OOM);
   if (cudaMemcpy(h->bgw_tab, wtab.data(), wtab.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->E0, e0.data(), e0.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->E1, e0.data(), e0.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
