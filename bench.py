@@ -872,6 +872,18 @@ def run_mixed(args):
                            "shift_precision": mixed.boxes[N][1].shifter.effective_precision,
                            "shift_tile_rows": spec.cfg.shift_tile_rows,
                            "tile_timings_ms": {str(k): v for k, v in spec.timings.items()}}
+    # where the time goes: one eager alternation per box size with every library launch timed
+    # (CUDA events around each launch; not the graph-replay number above)
+    from matcha_b200 import _native as nat
+
+    for N in counts:
+        cap.restore()
+        nat.profile_start(256)
+        mixed({N: (cap.volumes[N], cap.tracker[N], cap.shift[N])})
+        nat.profile_stop()
+        prof, _ = nat.profile_read()
+        per_box[str(N)]["kernel_ms"] = {k: round(v["ms"], 3)
+                                        for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])}
     print(json.dumps({
         "metric": "subtomograms/s, mixed boxes 48/64/96 (one alternation, one CUDA graph replay)",
         "value": total / (ms * 1e-3), "unit": "subtomograms/s", "ms_per_step": ms, "steps": n,

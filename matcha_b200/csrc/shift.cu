@@ -945,7 +945,9 @@ patch_fft_xy128_kernel(const float* __restrict__ vol, const float* __restrict__ 
     for (int e = threadIdx.x; e < P4; e += kT128) {
       const float4 a = in0 ? __ldg(g0 + e) : make_float4(0.f, 0.f, 0.f, 0.f);
       const float4 c = in1 ? __ldg(g1 + e) : make_float4(0.f, 0.f, 0.f, 0.f);
-      pl4[e] = make_float4(w0 * a.x + w1 * c.x, w0 * a.y + w1 * c.y, w0 * a.z + w1 * c.z, w0 * a.w + w1 * c.w);
+      const int row = e >> 5;  // 32 float4 per row; the swizzle moves whole float4
+      pl4[(row << 5) | ((e & 31) ^ ((row & 3) << 1))] =
+          make_float4(w0 * a.x + w1 * c.x, w0 * a.y + w1 * c.y, w0 * a.z + w1 * c.z, w0 * a.w + w1 * c.w);
     }
   }
   __syncthreads();
@@ -957,8 +959,11 @@ patch_fft_xy128_kernel(const float* __restrict__ vol, const float* __restrict__ 
     const float wy0 = __int_as_float(ty.z), wy1 = __int_as_float(ty.w);
     const float wx0 = s_wx[0][k], wx1 = s_wx[1][k];
     const int cx0 = s_cx[0][k], cx1 = s_cx[1][k];
-    const float a = wx0 * P0[cy0 * N + cx0] + wx1 * P0[cy0 * N + cx1];
-    const float c = wx0 * P0[cy1 * N + cx0] + wx1 * P0[cy1 * N + cx1];
+    // plane row y holds column x at x ^ 8 (y & 3): the four groups of a warp read four
+    // consecutive rows at the same columns, which then fall in four different 8-bank windows
+    const int sy0 = (cy0 & 3) << 3, sy1 = (cy1 & 3) << 3;
+    const float a = wx0 * P0[cy0 * N + (cx0 ^ sy0)] + wx1 * P0[cy0 * N + (cx1 ^ sy0)];
+    const float c = wx0 * P0[cy1 * N + (cx0 ^ sy1)] + wx1 * P0[cy1 * N + (cx1 ^ sy1)];
     const float p = wy0 * a + wy1 * c;
     const int dj = j - HN, dk = k - HN;
     const int r2 = di * di + dj * dj + dk * dk;
@@ -1075,7 +1080,7 @@ fft_z128_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ 
   for (int q = 0; q < 9; ++q) R[q] = __ldg(&rot[b * 9 + q]);
   const float c = (float)g.h;
   float st = 0.f, ss = 0.f;
-#pragma unroll 2
+#pragma unroll 4
   for (int e = threadIdx.x; e < N * H; e += kT128) {
     const int ip = SPLIT ? e & (N - 1) : e / H, m2 = SPLIT ? e >> 7 : e - (e / H) * H;
     const float2 t = buf[ip * kZS128 + m2];
@@ -1128,6 +1133,370 @@ fft_z128_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ 
 
 constexpr size_t z128_smem_bytes() {
   return (size_t)128 * sizeof(float2) + (size_t)128 * kZS128 * sizeof(float2) + (size_t)kG128 * kXS128 * sizeof(float2);
+}
+
+// ------------------------------------------------------------------ boxes 48 and 96: radix-S x 8 path
+// A line of N = 8 S points (S = 6 or 12) is x[r + 8 s] (thread r of a group of 8, register
+// s < S): an S-point DFT in registers (Cooley-Tukey over 3 and 2 or 4), the twiddles W_N^(r k1),
+// a transpose through the group's scratch, and 8-point DFTs over r for the k1 = r + 8 j < S the
+// thread owns, which give X[k1 + S k2], k2 < 8.  The group synchronises on its own 8 lanes, so
+// groups without work in a round simply skip it.  Same passes as the box-128 kernels.
+constexpr int kTG = 288;  // 36 groups of 8
+constexpr int kGG = 36;
+
+// 3-point forward DFT in place.
+__device__ __forceinline__ void dft3(float2& a, float2& b, float2& c) {
+  const float h = 0.86602540378443865f;  // sqrt(3) / 2
+  const float2 t1 = c_add(b, c);
+  const float2 t2 = make_float2(a.x - 0.5f * t1.x, a.y - 0.5f * t1.y);
+  const float2 d = c_sub(b, c);
+  const float2 t3 = make_float2(h * d.y, -h * d.x);  // -i (sqrt(3)/2) (b - c)
+  a = c_add(a, t1);
+  b = c_add(t2, t3);
+  c = c_sub(t2, t3);
+}
+
+// S-point forward DFT, natural order in and out, S = 6 (2 x 3) or 12 (4 x 3): for each residue
+// s2 of s mod n2 a 3-point DFT over s1 (s = s2 + n2 s1), the twiddles W_S^(s2 k1), then an
+// n2-point DFT over s2 for each k1: X[k1 + 3 k2].
+template <int S>
+__device__ __forceinline__ void dft_small(float2 (&v)[S]) {
+  static_assert(S == 6 || S == 12, "dft_small covers S = 6 and 12");
+  constexpr int n2 = S / 3;
+  float2 y[n2][3];
+#pragma unroll
+  for (int s2 = 0; s2 < n2; ++s2) {
+    y[s2][0] = v[s2];
+    y[s2][1] = v[s2 + n2];
+    y[s2][2] = v[s2 + 2 * n2];
+    dft3(y[s2][0], y[s2][1], y[s2][2]);
+  }
+  const float h = 0.86602540378443865f;
+  if constexpr (S == 6) {
+    // W6^1 = (1/2, -h), W6^2 = (-1/2, -h)
+    y[1][1] = cmul(y[1][1], make_float2(0.5f, -h));
+    y[1][2] = cmul(y[1][2], make_float2(-0.5f, -h));
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1) {
+      v[k1] = c_add(y[0][k1], y[1][k1]);
+      v[k1 + 3] = c_sub(y[0][k1], y[1][k1]);
+    }
+  } else {
+    // W12^m, m = s2 k1 <= 6: (cos(pi m / 6), -sin(pi m / 6))
+    const float2 w12[7] = {make_float2(1.f, 0.f),  make_float2(h, -0.5f),   make_float2(0.5f, -h),
+                           make_float2(0.f, -1.f), make_float2(-0.5f, -h),  make_float2(-h, -0.5f),
+                           make_float2(-1.f, 0.f)};
+#pragma unroll
+    for (int s2 = 1; s2 < 4; ++s2)
+#pragma unroll
+      for (int k1 = 1; k1 < 3; ++k1) y[s2][k1] = cmul(y[s2][k1], w12[s2 * k1]);
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1) {
+      // 4-point DFT over s2: X[k1 + 3 k2]
+      const float2 a = y[0][k1], b = y[1][k1], c = y[2][k1], d = y[3][k1];
+      const float2 p0 = c_add(a, c), p1 = c_sub(a, c), q0 = c_add(b, d), q1 = c_mi(c_sub(b, d));
+      v[k1] = c_add(p0, q0);
+      v[k1 + 3] = c_add(p1, q1);
+      v[k1 + 6] = c_sub(p0, q0);
+      v[k1 + 9] = c_sub(p1, q1);
+    }
+  }
+}
+
+template <int S>
+__host__ __device__ constexpr int grp_xs() {  // per-group scratch: 9 S entries, stride = 8 (mod 16)
+  return ((9 * S + 7) / 16) * 16 + 8;
+}
+
+// N-point forward FFT (N = 8 S) of one line by its 8 threads; v[s] = x[r + 8 s] on entry; on
+// exit o[j][k2] = X[(r + 8 j) + S k2] for the j with r + 8 j < S.  gmask: the group's lanes.
+template <int S>
+__device__ __forceinline__ void fft_grp(float2 (&v)[S], int r, unsigned gmask, float2* xs, const float2* tw,
+                                        float2 (&o)[2][8]) {
+  dft_small<S>(v);  // V_r[k1]
+#pragma unroll
+  for (int k1 = 1; k1 < S; ++k1) v[k1] = cmul(v[k1], tw[r * k1]);
+  __syncwarp(gmask);
+#pragma unroll
+  for (int k1 = 0; k1 < S; ++k1) xs[9 * k1 + r] = v[k1];
+  __syncwarp(gmask);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int k1 = r + 8 * j;
+    if (k1 < S) {
+#pragma unroll
+      for (int t = 0; t < 8; ++t) o[j][t] = xs[9 * k1 + t];  // V_t[k1]
+      dft8(o[j]);
+    }
+  }
+}
+
+// patch_fft_xy_kernel<N, false> for N = 48, 96 with the radix-S x 8 FFTs.
+template <int N>
+__global__ void __launch_bounds__(kTG, 2)
+patch_fft_xy_grp_kernel(const float* __restrict__ vol, const float* __restrict__ shift_zyx,
+                        const float* __restrict__ bgw_tab, const float* __restrict__ fill_tab, ShiftGeom g,
+                        float2* __restrict__ T, float* __restrict__ bg) {
+  constexpr int S = N / 8, HN = N / 2, H = N / 2 + 1;
+  constexpr int PR = N + 8;  // plane row stride (floats): four consecutive rows fall on different banks
+  constexpr int ZR = N + 1;  // x-FFT output row stride (float2)
+  constexpr int XS = grp_xs<S>();
+  constexpr size_t kRegion = (size_t)N * PR * 4 > (size_t)HN * ZR * 8 ? (size_t)N * PR * 4 : (size_t)HN * ZR * 8;
+  extern __shared__ __align__(16) float2 sm2[];
+  __shared__ float red[32];
+  __shared__ int s_cx[2][N];
+  __shared__ float s_wx[2][N];
+  __shared__ int4 s_ty[N];
+  float2* tw = sm2;                                       // N
+  float* P0 = reinterpret_cast<float*>(sm2 + N);          // the z-interpolated plane (N x PR)
+  float2* Z = reinterpret_cast<float2*>(P0);              // then the HN x ZR x-FFT output
+  float2* xs = reinterpret_cast<float2*>(reinterpret_cast<char*>(P0) + kRegion);  // kGG x XS
+  const int ip = blockIdx.x, b = blockIdx.y;
+  const int i = wrap_n<N>(ip + HN);
+  const int di = i - HN;
+  const float* v = vol + (int64_t)b * N * N * N;
+  const PatchShift ps = patch_shift(shift_zyx, b, N);
+  const float z = (float)i + ps.f[0];
+  const float z0 = floorf(z);
+  const int iz = (int)z0;
+  const float fz = z - z0;
+  load_twiddles(tw, N, N);
+  if (threadIdx.x < 2 * N) {
+    const int ax = threadIdx.x / N, j = threadIdx.x % N;
+    const float y = (float)j + ps.f[1 + ax];
+    const float y0 = floorf(y);
+    const int iy = (int)y0;
+    const float fy = y - y0;
+    const bool zero = (j == ps.zp[1 + ax]);
+    const int c0 = min(max(iy, 0), N - 1), c1 = min(max(iy + 1, 0), N - 1);
+    const float w0 = (zero || iy < 0 || iy >= N) ? 0.f : 1.f - fy;
+    const float w1 = (zero || iy + 1 < 0 || iy + 1 >= N) ? 0.f : fy;
+    if (ax == 0) {
+      s_ty[j] = make_int4(c0, c1, __float_as_int(w0), __float_as_int(w1));
+    } else {
+      s_cx[0][j] = c0;
+      s_cx[1][j] = c1;
+      s_wx[0][j] = w0;
+      s_wx[1][j] = w1;
+    }
+  }
+  {
+    constexpr int R4 = N / 4, P4 = N * R4;
+    const bool zplane = (i == ps.zp[0]);
+    const bool in0 = iz >= 0 && iz < N, in1 = iz + 1 >= 0 && iz + 1 < N;
+    const float w0 = (zplane || !in0) ? 0.f : 1.f - fz, w1 = (zplane || !in1) ? 0.f : fz;
+    const float4* g0 = reinterpret_cast<const float4*>(v + (int64_t)(in0 ? iz : 0) * N * N);
+    const float4* g1 = reinterpret_cast<const float4*>(v + (int64_t)(in1 ? iz + 1 : 0) * N * N);
+    float4* pl4 = reinterpret_cast<float4*>(P0);
+#pragma unroll 4
+    for (int e = threadIdx.x; e < P4; e += kTG) {
+      const float4 a = in0 ? __ldg(g0 + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 c = in1 ? __ldg(g1 + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const int row = e / R4;
+      pl4[row * (PR / 4) + (e - row * R4)] =
+          make_float4(w0 * a.x + w1 * c.x, w0 * a.y + w1 * c.y, w0 * a.z + w1 * c.z, w0 * a.w + w1 * c.w);
+    }
+  }
+  __syncthreads();
+  const int L = threadIdx.x >> 3, r = threadIdx.x & 7;
+  const unsigned gmask = 0xFFu << (threadIdx.x & 24);
+  float2* gx = xs + L * XS;
+  float part = 0.f;
+  auto sample = [&](int j, int k) -> float {
+    const int4 ty = s_ty[j];
+    const int cy0 = ty.x, cy1 = ty.y;
+    const float wy0 = __int_as_float(ty.z), wy1 = __int_as_float(ty.w);
+    const float wx0 = s_wx[0][k], wx1 = s_wx[1][k];
+    const int cx0 = s_cx[0][k], cx1 = s_cx[1][k];
+    const float a = wx0 * P0[cy0 * PR + cx0] + wx1 * P0[cy0 * PR + cx1];
+    const float c = wx0 * P0[cy1 * PR + cx0] + wx1 * P0[cy1 * PR + cx1];
+    const float p = wy0 * a + wy1 * c;
+    const int dj = j - HN, dk = k - HN;
+    const int r2 = di * di + dj * dj + dk * dk;
+    float keep = 1.f;  // 1 - W
+    if (r2 > g.r2_outer) {
+      part += p;
+      keep = 0.f;
+    } else if (r2 >= g.r2_inner) {
+      part += __ldg(bgw_tab + r2) * p;
+      keep = 1.f - __ldg(fill_tab + r2);
+    }
+    return keep * p * g.inv_n3;
+  };
+  // x FFT: packed lines q = L and L + 36 (rolled rows q and q + HN as real and imaginary
+  // parts), all samples taken before the plane is overwritten by Z
+  constexpr int kRounds = (HN + kGG - 1) / kGG;
+  static_assert(kRounds <= 2, "two rounds of lines at most");
+  float2 w[2][S];
+#pragma unroll
+  for (int round = 0; round < kRounds; ++round) {
+    const int q = L + kGG * round;
+    if (q < HN) {
+#pragma unroll
+      for (int s8 = 0; s8 < S; ++s8) {
+        const int kp = r + 8 * s8, k = wrap_n<N>(kp + HN);
+        w[round][s8] = make_float2(sample(q + HN, k), sample(q, k));
+      }
+    }
+  }
+  __syncthreads();  // the plane is read: Z may overwrite it
+#pragma unroll
+  for (int round = 0; round < kRounds; ++round) {
+    const int q = L + kGG * round;
+    if (q < HN) {
+      float2 o[2][8];
+      fft_grp<S>(w[round], r, gmask, gx, tw, o);
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+        if (r + 8 * j < S) {
+#pragma unroll
+          for (int k2 = 0; k2 < 8; ++k2) Z[q * ZR + r + 8 * j + S * k2] = o[j][k2];
+        }
+    }
+  }
+  __syncthreads();
+  // y FFT of the columns m2 < H, its input split on the way in (Z = A + i B holds the
+  // transforms of rows q and q + HN), each result stored straight to T
+  float2* out = T + ((int64_t)b * N + ip) * N * H;
+#pragma unroll 1
+  for (int col = L; col < H; col += kGG) {
+    float2 x[S];
+    const int cm = col == 0 ? 0 : N - col;
+#pragma unroll
+    for (int s8 = 0; s8 < S / 2; ++s8) {
+      const int q = r + 8 * s8;
+      const float2 zk = Z[q * ZR + col];
+      const float2 zm = Z[q * ZR + cm];
+      x[s8] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+      x[s8 + S / 2] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+    }
+    float2 o[2][8];
+    fft_grp<S>(x, r, gmask, gx, tw, o);
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+      if (r + 8 * j < S) {
+#pragma unroll
+        for (int k2 = 0; k2 < 8; ++k2) out[(r + 8 * j + S * k2) * H + col] = o[j][k2];
+      }
+  }
+  part = block_sum(part, red);
+  if (threadIdx.x == 0) atomicAdd(&bg[b], part);
+}
+
+template <int N>
+constexpr size_t xy_grp_smem_bytes() {
+  constexpr int HN = N / 2;
+  constexpr size_t plane = (size_t)N * (N + 8) * 4, zb = (size_t)HN * (N + 1) * 8;
+  return (size_t)N * sizeof(float2) + (plane > zb ? plane : zb) + (size_t)kGG * grp_xs<N / 8>() * sizeof(float2);
+}
+
+// fft_z_kernel<N, SPLIT> for N = 48, 96 with the radix-S x 8 FFT.
+template <int N, bool SPLIT>
+__global__ void __launch_bounds__(kTG, 2)
+fft_z_grp_kernel(ShiftGeom g, float2* __restrict__ T, const float2* __restrict__ what, const float* __restrict__ bg,
+                 const float4* __restrict__ refq, const float* __restrict__ rot, const float* __restrict__ ctf,
+                 float* __restrict__ nrm, uint32_t* __restrict__ a1, int a1_ws, int a1_R, uint32_t* __restrict__ a1n,
+                 int a1n_R) {
+  constexpr int S = N / 8, HN = N / 2, H = N / 2 + 1;
+  constexpr int XS = grp_xs<S>();
+  extern __shared__ __align__(16) float2 sm2[];
+  __shared__ float red[32];
+  float2* tw = sm2;            // N
+  float2* buf = sm2 + N;       // N (i') x H
+  float2* xs = buf + N * H;    // kGG x XS
+  const int jp = blockIdx.x, b = blockIdx.y;
+  float2* base = T + (int64_t)b * N * N * H + (int64_t)jp * H;
+  const float2* wb = what + (int64_t)jp * H;
+  const float avg = g.wsum > 0.f ? __ldg(&bg[b]) / g.wsum : 0.f;
+  load_twiddles(tw, N, N);
+#pragma unroll 4
+  for (int e = threadIdx.x; e < N * H; e += kTG) {
+    const int ip = e / H, m2 = e - (e / H) * H;
+    const float2 t = base[(int64_t)ip * N * H + m2];
+    const float2 w = __ldg(&wb[(int64_t)ip * N * H + m2]);
+    buf[ip * H + m2] = make_float2(fmaf(avg, w.x, t.x), fmaf(avg, w.y, t.y));
+  }
+  __syncthreads();
+  {
+    const int L = threadIdx.x >> 3, r = threadIdx.x & 7;
+    const unsigned gmask = 0xFFu << (threadIdx.x & 24);
+    float2* gx = xs + L * XS;
+#pragma unroll 1
+    for (int col = L; col < H; col += kGG) {
+      float2 x[S];
+#pragma unroll
+      for (int s8 = 0; s8 < S; ++s8) x[s8] = buf[(r + 8 * s8) * H + col];
+      float2 o[2][8];
+      fft_grp<S>(x, r, gmask, gx, tw, o);
+      __syncwarp(gmask);  // the group has read its column: write the transform back
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+        if (r + 8 * j < S) {
+#pragma unroll
+          for (int k2 = 0; k2 < 8; ++k2) buf[(r + 8 * j + S * k2) * H + col] = o[j][k2];
+        }
+    }
+  }
+  __syncthreads();
+  float R[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) R[q] = __ldg(&rot[b * 9 + q]);
+  const float c = (float)g.h;
+  float st = 0.f, ss = 0.f;
+#pragma unroll 4
+  for (int e = threadIdx.x; e < N * H; e += kTG) {
+    const int ip = SPLIT ? e % N : e / H, m2 = SPLIT ? e / N : e % H;
+    const float2 t = buf[ip * H + m2];
+    const int kp = ip < HN ? ip : ip - N;
+    const int jq = jp < HN ? jp : jp - N;
+    const int xq = m2 < HN ? m2 : m2 - H;
+    // outside the mask the sample is taken far outside the box, which reads zero (entry 0)
+    const bool in_mask = kp * kp + jq * jq + xq * xq <= g.mask_r2;
+    float2 s;
+    {
+      const int zo = wrap_n<N>(ip + HN), yo = wrap_n<N>(jp + HN), xw = m2 + HN;
+      const float bx = (float)xw - c, by = (float)yo - c, bz = (float)zo - c;
+      const float rx = R[0] * bx + R[1] * by + R[2] * bz + c;
+      const float ry = R[3] * bx + R[4] * by + R[5] * bz + c;
+      const float rz = in_mask ? R[6] * bx + R[7] * by + R[8] * bz + c : -4.f;
+      s = trilinear_quad(refq, N, rz, ry, rx);
+    }
+    if (in_mask && ctf) {
+      const float cv = __ldg(&ctf[(((int64_t)b * N + ip) * N + jp) * H + m2]);
+      s.x *= cv;
+      s.y *= cv;
+    }
+    st += t.x * t.x + t.y * t.y;
+    ss += s.x * s.x + s.y * s.y;
+    const float2 p = make_float2(s.x * t.x + s.y * t.y, s.x * t.y - s.y * t.x);
+    if (SPLIT) {
+      uint32_t hi, lo;
+      split_bf16x2(p.x, p.y, hi, lo);
+      if (m2 < HN) {
+        const size_t row = ((size_t)b * HN + m2) * N + jp;
+        a1[row * a1_ws + ip] = hi;
+        a1[((size_t)a1_R + row) * a1_ws + ip] = lo;
+      } else {
+        const size_t row = (size_t)b * N + jp;
+        a1n[row * a1_ws + ip] = hi;
+        a1n[((size_t)a1n_R + row) * a1_ws + ip] = lo;
+      }
+    } else {
+      base[(int64_t)ip * N * H + m2] = p;
+    }
+  }
+  st = block_sum(st, red);
+  ss = block_sum(ss, red);
+  if (threadIdx.x == 0) {
+    atomicAdd(&nrm[2 * b], st);
+    atomicAdd(&nrm[2 * b + 1], ss);
+  }
+}
+
+template <int N>
+constexpr size_t z_grp_smem_bytes() {
+  return (size_t)N * sizeof(float2) + (size_t)N * (N / 2 + 1) * sizeof(float2) +
+         (size_t)kGG * grp_xs<N / 8>() * sizeof(float2);
 }
 
 __global__ void fill_table_kernel(ShiftGeom g, int n, float* __restrict__ tab) {
@@ -1356,7 +1725,7 @@ struct mtb_shift {
   float* fill_tab; // fill weight W by integer squared radius (device formula)
   float2* what;    // (N, N, N/2+1) plane transforms of the fill weight W / N^3
   float2* ref;     // (N, N, N) Fourier reference, fftshifted and masked
-  float4* refq;    // boxes 64, 128: corner quads of ref, (N + 2) (N + 1)^2 x 32 bytes
+  float4* refq;    // boxes 48, 64, 96, 128: corner quads of ref, (N + 2) (N + 1)^2 x 32 bytes
   float2* E0;      // (U, N)
   float2* E1;      // (U, N)
   float2* E2;      // (U, H)
@@ -1478,6 +1847,36 @@ int shift_front_128(mtb_shift* h, const float* subtomos, const float* shift_zyx,
   return MTB_OK;
 }
 
+template <int N>
+int shift_front_grp(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
+                    int B, cudaStream_t st, bool split) {
+  const ShiftGeom& g = h->g;
+  const int sxy = (int)xy_grp_smem_bytes<N>(), sz = (int)z_grp_smem_bytes<N>();
+  MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy_grp_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
+  mtb_prof_begin(st);
+  patch_fft_xy_grp_kernel<N><<<dim3(N, B), kTG, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, h->fill_tab, g, h->T,
+                                                            h->bg);
+  mtb_prof_end(st, "patch_fft_xy_grp_kernel");
+  MTB_LAUNCH_CHECK();
+  prof_mark(h, 1, st);
+  if (split) {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_grp_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+    mtb_prof_begin(st);
+    fft_z_grp_kernel<N, true><<<dim3(N, B), kTG, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
+                                                            (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1,
+                                                            (uint32_t*)h->tc.A1n, h->tc.R1n);
+    mtb_prof_end(st, "fft_z_grp_kernel");
+  } else {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_grp_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+    mtb_prof_begin(st);
+    fft_z_grp_kernel<N, false><<<dim3(N, B), kTG, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
+                                                             nullptr, 0, 0, nullptr, 0);
+    mtb_prof_end(st, "fft_z_grp_kernel");
+  }
+  MTB_LAUNCH_CHECK();
+  return MTB_OK;
+}
+
 // split: the z pass writes the tensor-core pass-1 operand (A1) instead of the FP32 product in T.
 int shift_front(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
                 int B, cudaStream_t st, bool split) {
@@ -1490,9 +1889,11 @@ int shift_front(mtb_shift* h, const float* subtomos, const float* shift_zyx, con
                           : shift_front_n<64>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
     case 128: return B > 0 ? shift_front_128(h, subtomos, shift_zyx, rot, ctf, B, st, split)
                            : shift_front_n<128>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
-    case 48: return shift_front_n<48>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
+    case 48: return B > 0 ? shift_front_grp<48>(h, subtomos, shift_zyx, rot, ctf, B, st, split)
+                          : shift_front_n<48>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
     case 80: return shift_front_n<80>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
-    case 96: return shift_front_n<96>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
+    case 96: return B > 0 ? shift_front_grp<96>(h, subtomos, shift_zyx, rot, ctf, B, st, split)
+                          : shift_front_n<96>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
     default: MTB_ARG_CHECK(false, "N must be a power of two in [4, 128] or 48, 80, 96");
   }
 }
@@ -1588,7 +1989,8 @@ extern "C" int mtb_shift_create(const mtb_shift_config* cfg, mtb_shift** out) {
   if (!want_tc && (!alloc((void**)&h->X1, B * g.U * N * g.H * 8) || !alloc((void**)&h->pval, B * h->ngrp * 4) ||
                    !alloc((void**)&h->pidx, B * h->ngrp * 4)))
     return fail(MTB_ERR_OOM);
-  if ((N == 64 || N == 128) && !alloc((void**)&h->refq, (size_t)(N + 2) * (N + 1) * (N + 1) * 32))
+  if ((N == 48 || N == 64 || N == 96 || N == 128) &&
+      !alloc((void**)&h->refq, (size_t)(N + 2) * (N + 1) * (N + 1) * 32))
     return fail(MTB_ERR_OOM);
   if (cudaMemcpy(h->bgw_tab, wtab.data(), wtab.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->E0, e0.data(), e0.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
