@@ -56,6 +56,9 @@ def parse():
                    help="uneven boxes instead of the metric's shape: 4096 subtomograms drawn from boxes 48, 64, 96 "
                         "(L 24, 32, 48; own templates of 150, 400, 900 blobs), shifts in +-6, SNR U[-10, 5] dB, one "
                         "captured graph per alternation (a reported extra, not the metric)")
+    p.add_argument("--split-degree", type=int, default=None,
+                   help="--highband: also run the expansion in plain BF16 up to this degree with the hi+lo split "
+                        "above (default 40, the shape's own schedule) and report it beside the split everywhere")
     p.add_argument("--highband", action="store_true",
                    help="the high-bandlimit shape instead of the metric's: 128^3, L=64, march 16/32/48/64, "
                         "shift r=8, -5 dB (a reported extra, not the metric; --batch defaults to 512; --cpu-sample "
@@ -732,6 +735,8 @@ def run_highband(args):
 
     dev = torch.device("cuda:0")
     N, L, B = 128, 64, (args.batch if args.batch != 1000 else 512)
+    if args.split_degree is None:
+        args.split_degree = 40  # BF16 with the split correction above l = 40
     Li, uf, radius = [16, 32, 48], 8, 8
     rng = np.random.default_rng(args.seed)
     template = make_template(rng, N=N, n_blobs=1500, window=12)
@@ -743,9 +748,10 @@ def run_highband(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     n = max(1, args.steps)
 
-    def one_precision(precision):
+    def one_precision(precision, split_degree=None):
         step = AlignmentStep(StepConfig(N=N, L=L, Li=Li, batch=B, shift_search_radius=radius,
-                                        shift_upsample_factor=uf, precision=precision), dev)
+                                        shift_upsample_factor=uf, precision=precision,
+                                        expansion_split_degree=split_degree), dev)
         step.set_template(template)
         tracker = ident.clone()
         for _ in range(max(1, args.warmup)):
@@ -770,9 +776,13 @@ def run_highband(args):
         nat.profile_stop()
         prof, _ = nat.profile_read()
         res["kernel_ms"] = {k: round(v["ms"], 3) for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])}
-        prec = f"expansion {step.correlator.fle.precision}, upsampled DFT {step.shifter.effective_precision}"
+        fle = step.correlator.fle
+        prec = f"expansion {fle.precision}" + (f" (plain BF16 up to degree {split_degree}: "
+                                               f"{fle.split_tiles()[0]} of {fle.split_tiles()[1]} GEMM tiles split)"
+                                               if split_degree is not None else "") + \
+            f", upsampled DFT {step.shifter.effective_precision}"
         three = None
-        if precision != "fp32":
+        if precision != "fp32" and split_degree is None:
             tracker.copy_(ident)
             local = torch.zeros((B, 3), device=dev)
             e0.record(st)
@@ -788,7 +798,7 @@ def run_highband(args):
         torch.cuda.empty_cache()
         return ms, res, prec, three
 
-    ms, chosen, prec, three = one_precision("auto")
+    ms, chosen, prec, three = one_precision("auto", None)
     err1 = rotation_error_deg(chosen["alpha"], chosen["beta"], chosen["gamma"], q_true)
     line = {
         "metric": "subtomograms/s at 128^3 L=64 (one alternation), high-bandlimit shape",
@@ -800,6 +810,20 @@ def run_highband(args):
         "three_alternations": three, "kernel_ms_per_alternation": chosen.pop("kernel_ms"),
     }
     runs = {"chosen": chosen}
+    if args.split_degree is not None:
+        # the shape's own schedule: plain BF16 up to degree split_degree, the hi+lo split above
+        msx, sched, precx, _ = one_precision("auto", args.split_degree)
+        kern = sched.pop("kernel_ms")
+        runs[f"plain_bf16_to_l{args.split_degree}"] = sched
+        ang = lambda d: [np.asarray(d[k], dtype=np.float64) for k in ("alpha", "beta", "gamma")]
+        dv = euler_dev_deg(*ang(sched), *ang(chosen))
+        line[f"plain_bf16_to_l{args.split_degree}"] = {
+            "ms_per_alternation": msx, "value": B / (msx * 1e-3), "precision": precx,
+            "gemm_tc_kernel_ms": kern.get("gemm_tc_kernel"),
+            "vs_chosen": {"median_rot_dev_deg": float(np.median(dv)), "max_rot_dev_deg": float(dv.max()),
+                          "frac_within_0p05deg": float(np.mean(dv < 0.05)),
+                          "shift_equal_frac": float(np.mean(np.all(np.abs(sched["shift"] - chosen["shift"]) < 1e-6,
+                                                                   axis=1)))}}
     if not args.no_fp32:
         ms32, plain, prec32, _ = one_precision("fp32")
         plain.pop("kernel_ms")

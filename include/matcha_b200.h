@@ -178,11 +178,16 @@ typedef struct {
   const int* kidx;          /* [sum_l (2l+1) kpad[l]] coefficient index of (l, mu, k),
                                rows mu = -l..l, -1 = padding                            */
   int precision;            /* MTB_FLE_FP32: FP32 CUDA-core GEMM; MTB_FLE_BF16X3: tcgen05
-                               BF16 GEMM with a hi+lo split correction                  */
+                               BF16 GEMM with a hi+lo split correction; MTB_FLE_BF16_SPLIT:
+                               tcgen05 BF16 GEMM, the split correction only for the columns
+                               of degree l > split_degree                               */
+  int split_degree;         /* MTB_FLE_BF16_SPLIT: highest degree run in plain BF16 (one MMA
+                               per K step instead of three); ignored otherwise           */
 } mtb_fle_config;
 
 #define MTB_FLE_FP32 0
 #define MTB_FLE_BF16X3 1
+#define MTB_FLE_BF16_SPLIT 2
 
 typedef struct mtb_fle mtb_fle;
 
@@ -231,6 +236,11 @@ int mtb_sigma_backward_template(mtb_fle* h, const float* coeffs, int64_t coeff_s
  * memory and returns, and mtb_fle_status reports MTB_ERR_TIMEOUT.  Nothing faults or hangs.
  * MTB_ERR_ARG on an FP32 handle. */
 int mtb_fle_inject_stall(mtb_fle* h, int on);
+
+/* The tensor-core GEMM's 256-column tiles that take the hi+lo split (*n_split) of all its
+ * valid tiles (*n_tiles): every tile under MTB_FLE_BF16X3, those holding a column of degree
+ * above split_degree under MTB_FLE_BF16_SPLIT, 0 of 0 on the FP32 path. */
+int mtb_fle_split_tiles(const mtb_fle* h, int* n_split, int* n_tiles);
 
 /* ------------------------------------------------------------------------------
  * FFT shift match (RELION-style masked correlation with a local upsampled DFT).

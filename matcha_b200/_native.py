@@ -23,6 +23,7 @@ MTB_ERR_CUDA = 5
 MTB_MAX_STAGES = 16
 MTB_FLE_FP32 = 0
 MTB_FLE_BF16X3 = 1
+MTB_FLE_BF16_SPLIT = 2
 MTB_SHIFT_FP32 = 0
 MTB_SHIFT_BF16X3 = 1
 MTB_SHIFT_AUTO = 2
@@ -56,6 +57,7 @@ class MtbFleConfig(ctypes.Structure):
         ("col_lk", ctypes.c_void_p), ("col_scale", ctypes.c_void_p), ("coef_col_re", ctypes.c_void_p),
         ("coef_col_im", ctypes.c_void_p), ("coef_sign_re", ctypes.c_void_p), ("coef_sign_im", ctypes.c_void_p),
         ("kpad", ctypes.c_void_p), ("kidx", ctypes.c_void_p), ("precision", ctypes.c_int),
+        ("split_degree", ctypes.c_int),
     ]
 
 
@@ -89,6 +91,7 @@ SIGNATURES = {
     "mtb_sigma_upto": (_I, [_P, _P, _I64, _P, _I, _I, _P, _I64, _P]),
     "mtb_fle_status": (_I, [_P, _P]),
     "mtb_fle_inject_stall": (_I, [_P, _I]),
+    "mtb_fle_split_tiles": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "mtb_sigma_backward_template": (_I, [_P, _P, _I64, _P, _I64, _I, _I, _P, _P]),
     "mtb_score_backward": (_I, [_P, _I64, _I, _I, _P, _P, _P, _P, _P, _I64, _P, _P]),
     "mtb_shift_create": (_I, [ctypes.POINTER(MtbShiftConfig), ctypes.POINTER(_P)]),

@@ -31,7 +31,7 @@ class CrossCorrelationMatcher:
     def __init__(self, N: int, device: torch.device, expansion_epsilon: float = 1e-4, batchsize: int = 1,
                  reduce_memory: bool = True, bandlimit: int = None, micro_batch_split: int = 2,
                  dtype=torch.float32, radius: int = None, jl_zeros_path: str = None, cs_path: str = None,
-                 precision_mode: str = "accurate", precision: str = None):
+                 precision_mode: str = "accurate", precision: str = None, split_degree: int = None):
         self.N = N
         self.fle_basis_eps = expansion_epsilon
         self.batchsize = batchsize
@@ -53,7 +53,8 @@ class CrossCorrelationMatcher:
         self.fle = FLEBasis3D(N=self.N, bandlimit=self.bandlimit, eps=self.fle_basis_eps,
                               reduce_memory=self.reduce_memory, batchsize=self.batchsize, radius=self.radius,
                               device=self.device, dtype=torch.complex64, jl_zeros_path=jl_zeros_path,
-                              cs_path=cs_path, precision_mode=precision_mode, precision=precision)
+                              cs_path=cs_path, precision_mode=precision_mode, precision=precision,
+                              split_degree=split_degree)
         self.lmax = self.fle.lmax
         self.sigma = torch.zeros((self.batchsize, compute_size(self.lmax + 1)), dtype=torch.complex64,
                                  device=self.device)

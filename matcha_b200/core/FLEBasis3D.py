@@ -116,7 +116,7 @@ class FLEBasis3D:
     def __init__(self, N, bandlimit, eps, maxitr=None, maxfun=None, max_l=None, mode="complex",
                  sph_harm_solver="nvidia_torch", reduce_memory=True, batchsize=1, radius=1, device="cuda",
                  dtype=torch.complex128, jl_zeros_path="jl_zeros_l=3000_k=2500.mat",
-                 cs_path="cs_l=3000_k=2500.mat", precision_mode="accurate", precision=None):
+                 cs_path="cs_l=3000_k=2500.mat", precision_mode="accurate", precision=None, split_degree=None):
         if mode not in ("complex", "real"):
             raise AssertionError("mode must be 'real' or 'complex'")
         if mode == "real":
@@ -136,7 +136,12 @@ class FLEBasis3D:
             precision = "bf16x3" if str(precision_mode).strip().lower() == "fast" else "fp32"
         if precision not in ("fp32", "bf16x3"):
             raise ValueError("precision must be 'fp32' (CUDA cores) or 'bf16x3' (tensor cores, hi+lo split)")
+        if split_degree is not None and precision != "bf16x3":
+            raise ValueError("split_degree applies to precision 'bf16x3' only")
         self.precision = precision
+        # with split_degree, the tensor-core GEMM runs the columns of degree <= split_degree in
+        # plain BF16 (one MMA per K step) and keeps the hi+lo split above it
+        self.split_degree = None if split_degree is None else int(split_degree)
         tb = T.lap_eig_ball(int(N), bandlimit, float(radius), jl_zeros_path, cs_path, maxfun=maxfun, max_l=max_l)
         self.tables = tb
         self.N1, self.N, self.ne, self.lmax = tb.N1, tb.N, tb.ne, tb.lmax
@@ -158,13 +163,24 @@ class FLEBasis3D:
             arr = np.ascontiguousarray(ct[name])
             keep.append(arr)
             setattr(cfg, name, arr.ctypes.data)
-        cfg.precision = nat.MTB_FLE_BF16X3 if precision == "bf16x3" else nat.MTB_FLE_FP32
+        if precision == "fp32":
+            cfg.precision = nat.MTB_FLE_FP32
+        elif self.split_degree is None:
+            cfg.precision = nat.MTB_FLE_BF16X3
+        else:
+            cfg.precision, cfg.split_degree = nat.MTB_FLE_BF16_SPLIT, self.split_degree
         lib = nat.load()
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             nat.check(lib.mtb_fle_create(ctypes.byref(cfg), ctypes.byref(h)), "mtb_fle_create")
         self._h = h
         self._lib = lib
+
+    def split_tiles(self):
+        """(tiles of the tensor-core GEMM that take the hi+lo split, all its tiles); (0, 0) in FP32."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        nat.check(self._lib.mtb_fle_split_tiles(self._h, ctypes.byref(a), ctypes.byref(b)), "mtb_fle_split_tiles")
+        return a.value, b.value
 
     def __del__(self):
         h = getattr(self, "_h", None)

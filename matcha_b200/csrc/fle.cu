@@ -17,6 +17,7 @@
 // a_{l,k,-m} = (-1)^m conj(a_{l,k,m}) for real volumes.
 #include <math.h>
 #include <string.h>
+#include <algorithm>
 #include <vector>
 #include "common.cuh"
 #include "fle_tc.cuh"
@@ -318,12 +319,21 @@ extern "C" int mtb_fle_create(const mtb_fle_config* cfg, mtb_fle** out) {
   h->cfg = *cfg;
   auto fail = [&](int code) { mtb_fle_destroy(h); return code; };
   const int nc = cfg->n_cols, nr = cfg->n_rep, L = cfg->lmax;
-  // columns per class and position of each column inside its class block
+  // columns per class and position of each column inside its class block: by degree (stable),
+  // so that a 256-column tile of the tensor-core GEMM spans a narrow range of l
   std::vector<int> pos(nc);
+  std::vector<std::vector<int>> by_class(kClasses);
   for (int c = 0; c < nc; ++c) {
     const int k = cfg->col_class[c];
     if (k < 0 || k >= kClasses) return fail(MTB_ERR_ARG);
-    pos[c] = h->class_cols[k]++;
+    if (cfg->col_l[c] < 0 || cfg->col_l[c] > L) return fail(MTB_ERR_ARG);
+    by_class[k].push_back(c);
+  }
+  for (int k = 0; k < kClasses; ++k) {
+    std::stable_sort(by_class[k].begin(), by_class[k].end(),
+                     [&](int a, int b) { return cfg->col_l[a] < cfg->col_l[b]; });
+    for (size_t j = 0; j < by_class[k].size(); ++j) pos[by_class[k][j]] = (int)j;
+    h->class_cols[k] = (int)by_class[k].size();
   }
   int off = 0;
   for (int k = 0; k < kClasses; ++k) { h->class_off[k] = off; off += h->class_cols[k]; }
@@ -409,8 +419,16 @@ extern "C" int mtb_fle_create(const mtb_fle_config* cfg, mtb_fle** out) {
   cudaFree(d_cos); cudaFree(d_phi); cudaFree(d_r2); cudaFree(d_j); cudaFree(d_lms); cudaFree(d_cl);
   cudaFree(d_cls); cudaFree(d_pos); cudaFree(d_part); cudaFree(d_lk); cudaFree(d_scale);
   if (rc) return fail(rc);
-  if (cfg->precision == MTB_FLE_BF16X3) {
-    rc = fle_tc_prepare(&h->tc, h->basis, h->class_cols, h->class_off, nr, cfg->max_batch, nc);
+  if (cfg->precision == MTB_FLE_BF16X3 || cfg->precision == MTB_FLE_BF16_SPLIT) {
+    // per class, the highest degree of each column position (columns are sorted by degree)
+    std::vector<std::vector<int>> col_deg(kClasses);
+    for (int k = 0; k < kClasses; ++k) {
+      col_deg[k].resize(h->class_cols[k]);
+      for (size_t j = 0; j < by_class[k].size(); ++j) col_deg[k][j] = cfg->col_l[by_class[k][j]];
+    }
+    const int split_degree = cfg->precision == MTB_FLE_BF16X3 ? -1 : cfg->split_degree;
+    rc = fle_tc_prepare(&h->tc, h->basis, h->class_cols, h->class_off, nr, cfg->max_batch, nc, col_deg,
+                        split_degree);
     if (rc) return fail(rc);
     h->use_tc = true;
     // the FP32 basis was only the source of the hi/lo split: release it (at 128^3, L = 64 it
@@ -529,4 +547,11 @@ extern "C" int mtb_fle_status(mtb_fle* h, mtb_stream_t stream) {
   const int rc = fle_tc_check(&h->tc, (cudaStream_t)stream);
   if (rc) mtb_set_last_error("tensor-core FLE GEMM: a bounded wait ran out", __FILE__, __LINE__);
   return rc;
+}
+
+extern "C" int mtb_fle_split_tiles(const mtb_fle* h, int* n_split, int* n_tiles) {
+  MTB_ARG_CHECK(h && n_split && n_tiles, "null argument");
+  *n_split = h->use_tc ? h->tc.n_split_tiles : 0;
+  *n_tiles = h->use_tc ? h->tc.n_tiles : 0;
+  return MTB_OK;
 }

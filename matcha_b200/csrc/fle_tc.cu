@@ -60,6 +60,8 @@ struct TcParams {
   int coff[8];          // column offset of the class inside C
   int ldc;              // row stride of C (floats)
   int stall;            // test hook: no loads are issued, and waits give up after kStallPolls
+  int ntn;              // N tiles per class
+  const int* split;     // (8, ntn): 1 = hi+lo split (three K segments), 0 = plain BF16 (one)
 };
 
 // Poll limit of every wait while the stall hook is on: at most kStallPolls x kSuspendNs (20 ms).
@@ -102,7 +104,8 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
   const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
   if (n0 >= P.ncols[cls]) return;  // uniform per CTA
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int KB3 = 3 * P.KB;  // K blocks of the three hi/lo segments
+  // K blocks: the three hi/lo segments, or the (hi, hi) segment alone for a plain BF16 tile
+  const int KB3 = (__ldg(&P.split[cls * P.ntn + blockIdx.y]) ? 3 : 1) * P.KB;
   const int nchunks = (KB3 + kChunkKB - 1) / kChunkKB;
   const long long polls = P.stall ? kStallPolls : kSpinLimit;
 
@@ -329,7 +332,7 @@ size_t fle_tc_a_elems(int max_batch, int n_rep) {
 }
 
 int fle_tc_prepare(FleTc* t, float* const* basis, const int* class_cols, const int* class_off, int n_rep,
-                   int max_batch, int n_cols) {
+                   int max_batch, int n_cols, const std::vector<std::vector<int>>& col_deg, int split_degree) {
   memset(t, 0, sizeof(*t));
   t->Mpad = (max_batch + TM - 1) / TM * TM;
   t->Kpad = (n_rep + TK - 1) / TK * TK;
@@ -346,6 +349,24 @@ int fle_tc_prepare(FleTc* t, float* const* basis, const int* class_cols, const i
   if (cudaMalloc(&t->A, asz * 2) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->B, bsz * 2) != cudaSuccess) return MTB_ERR_OOM;
   if (cudaMalloc(&t->err, sizeof(int)) != cudaSuccess) return MTB_ERR_OOM;
+  // which tiles take the split: those holding a column of degree above split_degree
+  t->ntn = t->Npad / TN;
+  {
+    std::vector<int> flags((size_t)8 * t->ntn, 1);
+    for (int k = 0; k < 8; ++k)
+      for (int n = 0; n < t->ntn; ++n) {
+        const int c0 = n * TN;
+        if (c0 >= class_cols[k]) continue;
+        const int c1 = (c0 + TN < class_cols[k] ? c0 + TN : class_cols[k]) - 1;
+        const int top = (size_t)k < col_deg.size() && (size_t)c1 < col_deg[k].size() ? col_deg[k][c1] : 1 << 30;
+        flags[(size_t)k * t->ntn + n] = (split_degree < 0 || top > split_degree) ? 1 : 0;
+        t->n_tiles += 1;
+        t->n_split_tiles += flags[(size_t)k * t->ntn + n];
+      }
+    if (cudaMalloc(&t->split, flags.size() * sizeof(int)) != cudaSuccess) return MTB_ERR_OOM;
+    if (cudaMemcpy(t->split, flags.data(), flags.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+      return MTB_ERR_CUDA;
+  }
   if (cudaMemset(t->B, 0, bsz * 2) != cudaSuccess || cudaMemset(t->A, 0, asz * 2) != cudaSuccess ||
       cudaMemset(t->err, 0, sizeof(int)) != cudaSuccess)
     return MTB_ERR_CUDA;
@@ -366,6 +387,7 @@ void fle_tc_release(FleTc* t) {
   if (t->A) cudaFree(t->A);
   if (t->B) cudaFree(t->B);
   if (t->err) cudaFree(t->err);
+  if (t->split) cudaFree(t->split);
   memset(t, 0, sizeof(*t));
 }
 
@@ -388,6 +410,8 @@ int fle_tc_forward(FleTc* t, const float* vol, int64_t vol_stride, int B, const 
   }
   P.ldc = t->n_cols;
   P.stall = t->stall;
+  P.ntn = t->ntn;
+  P.split = t->split;
   const size_t smem = (size_t)STAGES * STAGE_BYTES + 1024;
   MTB_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 gg((B + TM - 1) / TM, t->Npad / TN, 8);

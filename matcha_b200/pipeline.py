@@ -41,6 +41,9 @@ class StepConfig:
                                      # not cover the box), "fp32" on CUDA cores, or "auto": the
                                      # expansion on tcgen05 and the upsampled DFT there where its
                                      # kernels cover the box (ShiftMatcher.effective_precision)
+    expansion_split_degree: int | None = None  # tensor-core expansion: plain BF16 for the columns
+                                     # of degree <= this, the hi+lo split above (None: split
+                                     # everywhere)
 
 
 class _Cfg(dict):
@@ -62,7 +65,9 @@ class AlignmentStep:
             raise ValueError("precision must be 'bf16x3', 'fp32' or 'auto'")
         self.correlator = CrossCorrelationMatcher(N=cfg.N, device=self.device, batchsize=cfg.batch,
                                                   bandlimit=cfg.L, radius=radius, precision_mode="fast",
-                                                  precision="fp32" if cfg.precision == "fp32" else "bf16x3")
+                                                  precision="fp32" if cfg.precision == "fp32" else "bf16x3",
+                                                  split_degree=None if cfg.precision == "fp32"
+                                                  else cfg.expansion_split_degree)
         self.matcher = Matcha(batchsize=cfg.batch, device=self.device, L_max=cfg.L,
                               matcha_config=dict(Li=list(cfg.Li) + [cfg.L], candidates=cfg.candidates,
                                                  num_steps=cfg.num_steps, oversampling_factor_K=cfg.K))

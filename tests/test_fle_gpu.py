@@ -126,6 +126,35 @@ def test_tensor_core_split_at_benchmark_shape(cuda_device):
     assert rel < 1e-4, rel
 
 
+@pytest.mark.parametrize("split_degree", [20, 40])
+def test_degree_schedule_at_benchmark_shape(cuda_device, split_degree):
+    """split_degree: the GEMM tiles whose columns are all of degree <= split_degree run in plain
+    BF16 (one MMA per K step), the others keep the hi+lo split.  Columns are sorted by degree
+    inside each parity class, so the tiles above the threshold hold the high degrees; their
+    coefficients keep the split's accuracy, the plain ones BF16's (about 2e-3 relative on noise
+    volumes, where nothing cancels the rounding)."""
+    from matcha_b200.core.FLEBasis3D import FLEBasis3D
+
+    kw = dict(N=64, bandlimit=32, eps=1e-4, batchsize=200, radius=30, device=cuda_device, dtype=torch.complex64)
+    mixed = FLEBasis3D(precision="bf16x3", split_degree=split_degree, **kw)
+    full = FLEBasis3D(precision="bf16x3", **kw)
+    fp = FLEBasis3D(precision="fp32", **kw)
+    n_split, n_tiles = mixed.split_tiles()
+    assert full.split_tiles() == (n_tiles, n_tiles) and fp.split_tiles() == (0, 0)
+    assert 0 < n_split < n_tiles, (n_split, n_tiles)
+    v = torch.randn(200, 64, 64, 64, device=cuda_device)
+    a, b = mixed.evaluate_t(v), fp.evaluate_t(v)
+    mixed.status()
+    ls = torch.from_numpy(np.asarray(mixed.ls)).to(cuda_device)
+    # a tile takes the split when any of its columns is above the threshold, so every column of
+    # degree > split_degree is in a split tile
+    hi = ls > split_degree
+    rel_hi = (torch.linalg.norm((a - b)[:, hi]) / torch.linalg.norm(b[:, hi])).item()
+    rel_all = (torch.linalg.norm(a - b) / torch.linalg.norm(b)).item()
+    assert rel_hi < 1e-4, rel_hi
+    assert rel_all < 5e-3, rel_all
+
+
 @pytest.mark.parametrize("precision,tol", [("fp32", 1e-5), ("bf16x3", 1e-4)])
 @pytest.mark.parametrize("tag,N1,bl,radius", [("c16r8", 16, 8, 8), ("c32r16", 32, 16, 16), ("c32r15", 32, 16, 15)])
 def test_evaluate_t_matches_reference_dense_basis(cuda_device, tag, N1, bl, radius, precision, tol):
