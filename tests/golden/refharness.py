@@ -118,3 +118,104 @@ def load_module(dotted):
     """Import a reference module by dotted name (after installing the stubs)."""
     _install_stubs()
     return importlib.import_module(dotted)
+
+
+# ------------------------------------------------------------------ functional shims for the driver
+# The reference's alignment driver (align_subtomograms.py, utils/rotation_ops.py,
+# utils/volume_rotation.py, utils/io_utils.py, core/ShiftMatcher.py:913) calls
+# quaternionic.array (construction, ``*``, ``conj``, ``normalized``, ``ndarray``,
+# ``to_euler_angles``, ``array.from_euler_angles``) and reads templates through
+# ``mrcfile.open(path).data``.  These stand-ins restate quaternionic 1.0's published
+# conventions ((w, x, y, z) components, Hamilton product, intrinsic z-y-z Euler angles) and
+# serve arrays registered in memory in place of MRC files.
+
+def _quaternionic_module():
+    import numpy as np
+
+    def _hamilton(a, b):
+        w1, x1, y1, z1 = np.moveaxis(a, -1, 0)
+        w2, x2, y2, z2 = np.moveaxis(b, -1, 0)
+        return np.stack([w1 * w2 - x1 * x2 - y1 * y2 - z1 * z2,
+                         w1 * x2 + x1 * w2 + y1 * z2 - z1 * y2,
+                         w1 * y2 - x1 * z2 + y1 * w2 + z1 * x2,
+                         w1 * z2 + x1 * y2 - y1 * x2 + z1 * w2], -1)
+
+    class QArray(np.ndarray):
+        def __new__(cls, data):
+            a = np.asarray(data, dtype=np.float64)
+            if a.shape[-1] != 4:
+                raise ValueError("quaternion arrays have 4 components in the last axis")
+            return a.copy().view(cls)
+
+        def __array_finalize__(self, obj):
+            pass
+
+        def __getitem__(self, item):
+            out = np.ndarray.__getitem__(self, item)
+            return out.view(QArray) if isinstance(out, np.ndarray) and out.ndim >= 1 and out.shape[-1] == 4 else out
+
+        def __mul__(self, other):
+            return QArray(_hamilton(np.asarray(self), np.asarray(other)))
+
+        @property
+        def ndarray(self):
+            return np.asarray(self).view(np.ndarray).copy()
+
+        def conj(self):
+            return QArray(np.asarray(self) * np.array([1.0, -1.0, -1.0, -1.0]))
+
+        @property
+        def normalized(self):
+            a = np.asarray(self)
+            return QArray(a / np.sqrt((a ** 2).sum(-1, keepdims=True)))
+
+        @property
+        def to_euler_angles(self):
+            q = np.asarray(self)
+            n = (q ** 2).sum(-1)
+            out = np.empty(q.shape[:-1] + (3,))
+            out[..., 0] = np.arctan2(q[..., 3], q[..., 0]) + np.arctan2(-q[..., 1], q[..., 2])
+            out[..., 1] = 2 * np.arccos(np.sqrt((q[..., 0] ** 2 + q[..., 3] ** 2) / n))
+            out[..., 2] = np.arctan2(q[..., 3], q[..., 0]) - np.arctan2(-q[..., 1], q[..., 2])
+            return out
+
+        @classmethod
+        def from_euler_angles(cls, alpha_beta_gamma, beta=None, gamma=None):
+            if beta is None:
+                abg = np.asarray(alpha_beta_gamma, dtype=np.float64)
+                a, b, g = abg[..., 0], abg[..., 1], abg[..., 2]
+            else:
+                a, b, g = (np.asarray(v, dtype=np.float64) for v in (alpha_beta_gamma, beta, gamma))
+            return cls(np.stack([np.cos(b / 2) * np.cos((a + g) / 2), -np.sin(b / 2) * np.sin((a - g) / 2),
+                                 np.sin(b / 2) * np.cos((a - g) / 2), np.cos(b / 2) * np.sin((a + g) / 2)], -1))
+
+    mod = types.ModuleType("quaternionic")
+    mod.array = QArray
+    return mod
+
+
+MRC_FILES = {}  # path -> ndarray served by the mrcfile stand-in
+
+
+def _mrcfile_module():
+    class _Mrc:
+        def __init__(self, data):
+            self.data = data
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *exc):
+            return False
+
+    mod = types.ModuleType("mrcfile")
+    mod.open = lambda path, *a, **k: _Mrc(MRC_FILES[str(path)])
+    return mod
+
+
+def install_driver_shims():
+    """Functional quaternionic and mrcfile stand-ins (replacing the empty stubs) for running
+    the reference's alignment driver on the CPU."""
+    _install_stubs()
+    sys.modules["quaternionic"] = _quaternionic_module()
+    sys.modules["mrcfile"] = _mrcfile_module()

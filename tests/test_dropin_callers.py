@@ -75,3 +75,27 @@ def test_reference_callers_bind_to_the_drop_in_signatures():
     # the alignment driver builds all three matchers and calls the search and the shift match
     assert {"CrossCorrelationMatcher", "Matcha", "ShiftMatcher", "get_sigma", "search_orientations",
             "search_shifts", "set_reference", "set_template"} <= seen, seen
+
+
+def test_recorded_driver_calls_bind_to_the_drop_in_signatures():
+    """The calls of the reference's driver recorded in caller_trace.npz (make_caller_trace.py)
+    bind to the drop-in signatures by keyword, as the driver made them; the GPU replay of the
+    same trace is tests/test_caller_trace_gpu.py."""
+    import json
+
+    from tests.helpers import golden
+
+    classes = _classes()
+    z = golden("caller_trace.npz")
+    events = json.loads(str(z["events"]))
+    calls = [e["call"] for e in events]
+    assert calls[:6] == ["Matcha", "ShiftMatcher", "CrossCorrelationMatcher", "CrossCorrelationMatcher.set_template",
+                         "ShiftMatcher.set_reference", "ShiftMatcher.get_base_shifts"], calls
+    assert calls[6:] == ["CrossCorrelationMatcher.get_sigma", "Matcha.search_orientations",
+                         "ShiftMatcher.search_shifts"] * 2, calls
+    for e in events:
+        cls, _, meth = e["call"].partition(".")
+        fn = getattr(classes[cls], meth) if meth else classes[cls].__init__
+        sig = inspect.signature(fn)
+        sig = sig.replace(parameters=list(sig.parameters.values())[1:])
+        sig.bind(**{k: None for k in e["args"]})
