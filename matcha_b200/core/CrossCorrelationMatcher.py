@@ -101,6 +101,10 @@ class CrossCorrelationMatcher:
         return self.sigma, self.bh_norms
 
     def _expand(self, volumes: torch.Tensor):
+        # the reference's driver passes the rotated patches as complex64 with a zero imaginary
+        # part (align_subtomograms.py:240-252); the expansion is of the real part
+        if volumes.is_complex():
+            volumes = volumes.real
         vol = volumes.to(device=self.device, dtype=torch.float32).contiguous()
         dev = self.device
         with torch.cuda.device(dev):

@@ -92,7 +92,7 @@ def test_reference_driver_calls_replay_on_the_drop_in_classes(cuda_device):
         elif call == "CrossCorrelationMatcher.set_template":
             kw["template_data"] = np.asarray(kw["template_data"])
             obj["ccm"].set_template(**kw)
-            ref = float(z[res["bh_norm_template"]["array"]])
+            ref = float(np.asarray(z[res["bh_norm_template"]["array"]]).reshape(-1)[0])
             assert abs(float(obj["ccm"].bh_norm_template) - ref) <= 1e-4 * ref
         elif call == "ShiftMatcher.set_reference":
             obj["shift"].set_reference(template_data=np.asarray(kw["template_data"]))
