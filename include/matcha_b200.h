@@ -283,6 +283,17 @@ int mtb_shift_set_reference(mtb_shift* h, const float* ref_fourier, mtb_stream_t
 int mtb_shift_search(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot,
                      const float* ctf, int B, float* shift_xyz, float* score, mtb_stream_t stream);
 
+/* mtb_shift_search in two halves (no counterpart in the reference): mtb_shift_begin takes the
+ * patch of each subtomogram at shift_zyx and its x/y transforms into the handle's workspace -
+ * nothing that depends on the orientation, so a caller may issue it before the orientation is
+ * known, or on another stream; mtb_shift_finish adds the rotated reference and runs the rest
+ * for the same B.  The handle holds one begun batch: mtb_shift_finish must be ordered after
+ * its mtb_shift_begin (the same stream, or an event between the two streams), and the next
+ * mtb_shift_begin after that mtb_shift_finish. */
+int mtb_shift_begin(mtb_shift* h, const float* subtomos, const float* shift_zyx, int B, mtb_stream_t stream);
+int mtb_shift_finish(mtb_shift* h, const float* rot, const float* ctf, int B, float* shift_xyz, float* score,
+                     mtb_stream_t stream);
+
 /* The shift match's correlation as a function of a continuous shift, and its gradient (no
  * counterpart in the reference, which evaluates it only on the upsampled grid,
  * ShiftMatcher.py:46-91, 94-282): for the same inputs as mtb_shift_search and query shifts

@@ -103,6 +103,8 @@ SIGNATURES = {
     "mtb_shift_profile": (_I, [_P, _I]),
     "mtb_shift_profile_read": (_I, [_P, _P, _P]),
     "mtb_shift_search": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P]),
+    "mtb_shift_begin": (_I, [_P, _P, _P, _I, _P]),
+    "mtb_shift_finish": (_I, [_P, _P, _P, _I, _P, _P, _P]),
     "mtb_update_rotation": (_I, [_P, _P, _P, _P, _I, _P, _P, _P]),
     "mtb_tracker_rotation": (_I, [_P, _I, _P, _P]),
     "mtb_shift_reference": (_I, [_P, _I, ctypes.c_float, _P, _P, _P]),

@@ -1757,7 +1757,7 @@ void prof_mark(mtb_shift* h, int k, cudaStream_t st) {
 // plane transforms of the background fill weight, once per geometry, into h->what.
 template <int N>
 int shift_front_n(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
-                  int B, cudaStream_t st, bool split) {
+                  int B, cudaStream_t st, bool split, int phases = 3) {
   const ShiftGeom& g = h->g;
   const int sxy = (int)xy_smem_bytes<N>(), sz = (int)z_smem_bytes<N>();
   if (B == 0) {
@@ -1766,134 +1766,152 @@ int shift_front_n(mtb_shift* h, const float* subtomos, const float* shift_zyx, c
     MTB_LAUNCH_CHECK();
     return MTB_OK;
   }
-  MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
-  mtb_prof_begin(st);
-  patch_fft_xy_kernel<N, false><<<dim3(N, B), kT, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, g, h->T, h->bg);
-  mtb_prof_end(st, "patch_fft_xy_kernel");
-  MTB_LAUNCH_CHECK();
-  prof_mark(h, 1, st);
-  if (split) {
-    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+  if (phases & 1) {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
     mtb_prof_begin(st);
-    fft_z_kernel<N, true><<<dim3(N, B), kT, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm,
-                                                       (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1, (uint32_t*)h->tc.A1n,
-        h->tc.R1n);
-    mtb_prof_end(st, "fft_z_kernel");
-  } else {
-    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
-    mtb_prof_begin(st);
-    fft_z_kernel<N, false><<<dim3(N, B), kT, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm, nullptr,
-                                                        0, 0, nullptr, 0);
-    mtb_prof_end(st, "fft_z_kernel");
+    patch_fft_xy_kernel<N, false><<<dim3(N, B), kT, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, g, h->T, h->bg);
+    mtb_prof_end(st, "patch_fft_xy_kernel");
+    MTB_LAUNCH_CHECK();
+    prof_mark(h, 1, st);
   }
-  MTB_LAUNCH_CHECK();
+  if (phases & 2) {
+    if (split) {
+      MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+      mtb_prof_begin(st);
+      fft_z_kernel<N, true><<<dim3(N, B), kT, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm,
+                                                         (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1, (uint32_t*)h->tc.A1n,
+          h->tc.R1n);
+      mtb_prof_end(st, "fft_z_kernel");
+    } else {
+      MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+      mtb_prof_begin(st);
+      fft_z_kernel<N, false><<<dim3(N, B), kT, sz, st>>>(g, h->T, h->what, h->bg, h->ref, rot, ctf, h->nrm, nullptr,
+                                                          0, 0, nullptr, 0);
+      mtb_prof_end(st, "fft_z_kernel");
+    }
+    MTB_LAUNCH_CHECK();
+  }
   return MTB_OK;
 }
 
 int shift_front_64(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
-                   int B, cudaStream_t st, bool split) {
+                   int B, cudaStream_t st, bool split, int phases = 3) {
   const ShiftGeom& g = h->g;
   const int sxy = (int)xy64_smem_bytes(), sz = (int)z64_smem_bytes();
-  MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
-  mtb_prof_begin(st);
-  patch_fft_xy64_kernel<<<dim3(64, B), kT64, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, h->fill_tab, g, h->T, h->bg);
-  mtb_prof_end(st, "patch_fft_xy64_kernel");
-  MTB_LAUNCH_CHECK();
-  prof_mark(h, 1, st);
-  if (split) {
-    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+  if (phases & 1) {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
     mtb_prof_begin(st);
-    fft_z64_kernel<true><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
-                                                         (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1, (uint32_t*)h->tc.A1n,
-        h->tc.R1n);
-    mtb_prof_end(st, "fft_z64_kernel");
-  } else {
-    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
-    mtb_prof_begin(st);
-    fft_z64_kernel<false><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm, nullptr,
-                                                          0, 0, nullptr, 0);
-    mtb_prof_end(st, "fft_z64_kernel");
+    patch_fft_xy64_kernel<<<dim3(64, B), kT64, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, h->fill_tab, g, h->T, h->bg);
+    mtb_prof_end(st, "patch_fft_xy64_kernel");
+    MTB_LAUNCH_CHECK();
+    prof_mark(h, 1, st);
   }
-  MTB_LAUNCH_CHECK();
+  if (phases & 2) {
+    if (split) {
+      MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+      mtb_prof_begin(st);
+      fft_z64_kernel<true><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
+                                                           (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1, (uint32_t*)h->tc.A1n,
+          h->tc.R1n);
+      mtb_prof_end(st, "fft_z64_kernel");
+    } else {
+      MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z64_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+      mtb_prof_begin(st);
+      fft_z64_kernel<false><<<dim3(64, B), kT64, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm, nullptr,
+                                                            0, 0, nullptr, 0);
+      mtb_prof_end(st, "fft_z64_kernel");
+    }
+    MTB_LAUNCH_CHECK();
+  }
   return MTB_OK;
 }
 
 int shift_front_128(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
-                    int B, cudaStream_t st, bool split) {
+                    int B, cudaStream_t st, bool split, int phases = 3) {
   const ShiftGeom& g = h->g;
   const int sxy = (int)xy128_smem_bytes(), sz = (int)z128_smem_bytes();
-  MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
-  mtb_prof_begin(st);
-  patch_fft_xy128_kernel<<<dim3(128, B), kT128, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, h->fill_tab, g, h->T,
-                                                            h->bg);
-  mtb_prof_end(st, "patch_fft_xy128_kernel");
-  MTB_LAUNCH_CHECK();
-  prof_mark(h, 1, st);
-  if (split) {
-    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z128_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+  if (phases & 1) {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
     mtb_prof_begin(st);
-    fft_z128_kernel<true><<<dim3(128, B), kT128, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
-                                                            (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1,
-                                                            (uint32_t*)h->tc.A1n, h->tc.R1n);
-    mtb_prof_end(st, "fft_z128_kernel");
-  } else {
-    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z128_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
-    mtb_prof_begin(st);
-    fft_z128_kernel<false><<<dim3(128, B), kT128, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
-                                                             nullptr, 0, 0, nullptr, 0);
-    mtb_prof_end(st, "fft_z128_kernel");
+    patch_fft_xy128_kernel<<<dim3(128, B), kT128, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, h->fill_tab, g, h->T,
+                                                              h->bg);
+    mtb_prof_end(st, "patch_fft_xy128_kernel");
+    MTB_LAUNCH_CHECK();
+    prof_mark(h, 1, st);
   }
-  MTB_LAUNCH_CHECK();
+  if (phases & 2) {
+    if (split) {
+      MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z128_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+      mtb_prof_begin(st);
+      fft_z128_kernel<true><<<dim3(128, B), kT128, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
+                                                              (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1,
+                                                              (uint32_t*)h->tc.A1n, h->tc.R1n);
+      mtb_prof_end(st, "fft_z128_kernel");
+    } else {
+      MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z128_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+      mtb_prof_begin(st);
+      fft_z128_kernel<false><<<dim3(128, B), kT128, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
+                                                               nullptr, 0, 0, nullptr, 0);
+      mtb_prof_end(st, "fft_z128_kernel");
+    }
+    MTB_LAUNCH_CHECK();
+  }
   return MTB_OK;
 }
 
 template <int N>
 int shift_front_grp(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
-                    int B, cudaStream_t st, bool split) {
+                    int B, cudaStream_t st, bool split, int phases = 3) {
   const ShiftGeom& g = h->g;
   const int sxy = (int)xy_grp_smem_bytes<N>(), sz = (int)z_grp_smem_bytes<N>();
-  MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy_grp_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
-  mtb_prof_begin(st);
-  patch_fft_xy_grp_kernel<N><<<dim3(N, B), kTG, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, h->fill_tab, g, h->T,
-                                                            h->bg);
-  mtb_prof_end(st, "patch_fft_xy_grp_kernel");
-  MTB_LAUNCH_CHECK();
-  prof_mark(h, 1, st);
-  if (split) {
-    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_grp_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+  if (phases & 1) {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(patch_fft_xy_grp_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, sxy));
     mtb_prof_begin(st);
-    fft_z_grp_kernel<N, true><<<dim3(N, B), kTG, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
-                                                            (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1,
-                                                            (uint32_t*)h->tc.A1n, h->tc.R1n);
-    mtb_prof_end(st, "fft_z_grp_kernel");
-  } else {
-    MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_grp_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
-    mtb_prof_begin(st);
-    fft_z_grp_kernel<N, false><<<dim3(N, B), kTG, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
-                                                             nullptr, 0, 0, nullptr, 0);
-    mtb_prof_end(st, "fft_z_grp_kernel");
+    patch_fft_xy_grp_kernel<N><<<dim3(N, B), kTG, sxy, st>>>(subtomos, shift_zyx, h->bgw_tab, h->fill_tab, g, h->T,
+                                                              h->bg);
+    mtb_prof_end(st, "patch_fft_xy_grp_kernel");
+    MTB_LAUNCH_CHECK();
+    prof_mark(h, 1, st);
   }
-  MTB_LAUNCH_CHECK();
+  if (phases & 2) {
+    if (split) {
+      MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_grp_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+      mtb_prof_begin(st);
+      fft_z_grp_kernel<N, true><<<dim3(N, B), kTG, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
+                                                              (uint32_t*)h->tc.A1, h->tc.KB12 * 32, h->tc.R1,
+                                                              (uint32_t*)h->tc.A1n, h->tc.R1n);
+      mtb_prof_end(st, "fft_z_grp_kernel");
+    } else {
+      MTB_CUDA_TRY(cudaFuncSetAttribute(fft_z_grp_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sz));
+      mtb_prof_begin(st);
+      fft_z_grp_kernel<N, false><<<dim3(N, B), kTG, sz, st>>>(g, h->T, h->what, h->bg, h->refq, rot, ctf, h->nrm,
+                                                               nullptr, 0, 0, nullptr, 0);
+      mtb_prof_end(st, "fft_z_grp_kernel");
+    }
+    MTB_LAUNCH_CHECK();
+  }
   return MTB_OK;
 }
 
 // split: the z pass writes the tensor-core pass-1 operand (A1) instead of the FP32 product in T.
+// phases: bit 0 the patch and x/y transforms (independent of the orientation), bit 1 the z
+// pass with the rotated reference (B > 0; B == 0 computes the fill weight's transforms).
 int shift_front(mtb_shift* h, const float* subtomos, const float* shift_zyx, const float* rot, const float* ctf,
-                int B, cudaStream_t st, bool split) {
+                int B, cudaStream_t st, bool split, int phases = 3) {
   switch (h->g.N) {
-    case 4: return shift_front_n<4>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
-    case 8: return shift_front_n<8>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
-    case 16: return shift_front_n<16>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
-    case 32: return shift_front_n<32>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
-    case 64: return B > 0 ? shift_front_64(h, subtomos, shift_zyx, rot, ctf, B, st, split)
-                          : shift_front_n<64>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
-    case 128: return B > 0 ? shift_front_128(h, subtomos, shift_zyx, rot, ctf, B, st, split)
-                           : shift_front_n<128>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
-    case 48: return B > 0 ? shift_front_grp<48>(h, subtomos, shift_zyx, rot, ctf, B, st, split)
-                          : shift_front_n<48>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
-    case 80: return shift_front_n<80>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
-    case 96: return B > 0 ? shift_front_grp<96>(h, subtomos, shift_zyx, rot, ctf, B, st, split)
-                          : shift_front_n<96>(h, subtomos, shift_zyx, rot, ctf, B, st, split);
+    case 4: return shift_front_n<4>(h, subtomos, shift_zyx, rot, ctf, B, st, split, phases);
+    case 8: return shift_front_n<8>(h, subtomos, shift_zyx, rot, ctf, B, st, split, phases);
+    case 16: return shift_front_n<16>(h, subtomos, shift_zyx, rot, ctf, B, st, split, phases);
+    case 32: return shift_front_n<32>(h, subtomos, shift_zyx, rot, ctf, B, st, split, phases);
+    case 64: return B > 0 ? shift_front_64(h, subtomos, shift_zyx, rot, ctf, B, st, split, phases)
+                          : shift_front_n<64>(h, subtomos, shift_zyx, rot, ctf, B, st, split, phases);
+    case 128: return B > 0 ? shift_front_128(h, subtomos, shift_zyx, rot, ctf, B, st, split, phases)
+                           : shift_front_n<128>(h, subtomos, shift_zyx, rot, ctf, B, st, split, phases);
+    case 48: return B > 0 ? shift_front_grp<48>(h, subtomos, shift_zyx, rot, ctf, B, st, split, phases)
+                          : shift_front_n<48>(h, subtomos, shift_zyx, rot, ctf, B, st, split, phases);
+    case 80: return shift_front_n<80>(h, subtomos, shift_zyx, rot, ctf, B, st, split, phases);
+    case 96: return B > 0 ? shift_front_grp<96>(h, subtomos, shift_zyx, rot, ctf, B, st, split, phases)
+                          : shift_front_n<96>(h, subtomos, shift_zyx, rot, ctf, B, st, split, phases);
     default: MTB_ARG_CHECK(false, "N must be a power of two in [4, 128] or 48, 80, 96");
   }
 }
@@ -2060,13 +2078,35 @@ extern "C" int mtb_shift_search(mtb_shift* h, const float* subtomos, const float
   MTB_ARG_CHECK(B >= 0 && B <= h->cfg.max_batch, "batch exceeds max_batch");
   if (B == 0) return MTB_OK;
   MTB_ARG_CHECK(subtomos && shift_zyx && rot && shift_xyz && score, "null pointer");
+  int rc = mtb_shift_begin(h, subtomos, shift_zyx, B, stream);
+  if (rc) return rc;
+  return mtb_shift_finish(h, rot, ctf, B, shift_xyz, score, stream);
+}
+
+extern "C" int mtb_shift_begin(mtb_shift* h, const float* subtomos, const float* shift_zyx, int B,
+                               mtb_stream_t stream) {
+  MTB_ARG_CHECK(h, "null handle");
+  MTB_ARG_CHECK(B >= 0 && B <= h->cfg.max_batch, "batch exceeds max_batch");
+  if (B == 0) return MTB_OK;
+  MTB_ARG_CHECK(subtomos && shift_zyx, "null pointer");
   cudaStream_t st = (cudaStream_t)stream;
-  const ShiftGeom& g = h->g;
-  const int N = g.N, H = g.H, U = g.U;
   MTB_CUDA_TRY(cudaMemsetAsync(h->bg, 0, (size_t)B * 4, st));
   MTB_CUDA_TRY(cudaMemsetAsync(h->nrm, 0, (size_t)B * 8, st));
   prof_mark(h, 0, st);
-  int rc = shift_front(h, subtomos, shift_zyx, rot, ctf, B, st, h->use_tc);
+  return shift_front(h, subtomos, shift_zyx, nullptr, nullptr, B, st, h->use_tc, 1);
+}
+
+extern "C" int mtb_shift_finish(mtb_shift* h, const float* rot, const float* ctf, int B, float* shift_xyz,
+                                float* score, mtb_stream_t stream) {
+  MTB_ARG_CHECK(h, "null handle");
+  MTB_ARG_CHECK(h->has_ref, "shift reference is not set");
+  MTB_ARG_CHECK(B >= 0 && B <= h->cfg.max_batch, "batch exceeds max_batch");
+  if (B == 0) return MTB_OK;
+  MTB_ARG_CHECK(rot && shift_xyz && score, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  const ShiftGeom& g = h->g;
+  const int N = g.N, H = g.H, U = g.U;
+  int rc = shift_front(h, nullptr, nullptr, rot, ctf, B, st, h->use_tc, 2);
   if (rc) return rc;
   prof_mark(h, 2, st);
   if (h->use_tc) {
