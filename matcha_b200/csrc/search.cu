@@ -52,7 +52,8 @@ size_t grid_smem_bytes(int L0, int K, int JB) {
   return (size_t)(nk + n * P + JB * P * P + JB * P * n) * sizeof(float2) + (size_t)JB * nk * sizeof(float);
 }
 
-// Beta values per pass: four when they fit, else one.
+// Beta values per pass: four when they fit, else one (at L0 = 16 two would fit, but the
+// 150 KB they take leave room for one CTA per SM instead of two, which measured slower).
 int grid_jb(int L0, int K) { return grid_smem_bytes(L0, K, 4) <= kGridSmemCap ? 4 : 1; }
 size_t grid_smem_bytes(int L0, int K) { return grid_smem_bytes(L0, K, grid_jb(L0, K)); }
 
@@ -301,11 +302,16 @@ int grid_launch_t(const float2* sigma, int64_t stride, int B, const float* dtab,
   return MTB_OK;
 }
 
-// The grid search for L0 = 8, n = 32 (the reference's default march) with its index
-// arithmetic fixed at compile time; other grids take the general instantiation.
+// The grid search for L0 = 8, 12, 16 with K = 2 (the marches of boxes 64, 96 and 128 at
+// bandlimit N/2) with its index arithmetic fixed at compile time; other grids take the general
+// instantiation.
 int grid_launch(const float2* sigma, int64_t stride, int B, const float* dtab, int L0, int K, int C, float* a,
                 float* b, float* g, float* grid, cudaStream_t st) {
   if (L0 == 8 && K == 2 && C <= 16) return grid_launch_t<8, 32, 16>(sigma, stride, B, dtab, L0, K, C, a, b, g, grid, st);
+  if (L0 == 12 && K == 2 && C <= 16)
+    return grid_launch_t<12, 48, 16>(sigma, stride, B, dtab, L0, K, C, a, b, g, grid, st);
+  if (L0 == 16 && K == 2 && C <= 16)
+    return grid_launch_t<16, 64, 16>(sigma, stride, B, dtab, L0, K, C, a, b, g, grid, st);
   if (C <= 16) return grid_launch_t<0, 0, 16>(sigma, stride, B, dtab, L0, K, C, a, b, g, grid, st);
   return grid_launch_t<0, 0, kMaxCand>(sigma, stride, B, dtab, L0, K, C, a, b, g, grid, st);
 }

@@ -17,7 +17,7 @@ def _matcha(B, Lmax, Li, C=10, steps=1, compat=False, device="cuda:0"):
                   compat_top_block=compat)
 
 
-@pytest.mark.parametrize("L0,K", [(4, 2), (8, 2), (8, 1), (16, 2)])
+@pytest.mark.parametrize("L0,K", [(4, 2), (8, 2), (8, 1), (12, 2), (16, 2)])
 def test_grid_matches_oracle(cuda_device, L0, K):
     from matcha_b200.core.SOFFT import SOFFT
 
@@ -29,23 +29,26 @@ def test_grid_matches_oracle(cuda_device, L0, K):
     np.testing.assert_allclose(f, ref, atol=2e-5 * np.abs(ref).max())
 
 
-def test_grid_topk_indices_bit_exact_on_clear_peaks(cuda_device):
-    rng = np.random.default_rng(5)
-    B, Lmax, C = 6, 16, 10
+@pytest.mark.parametrize("L0,Lmax", [(8, 16), (12, 24), (16, 32)])
+def test_grid_topk_indices_bit_exact_on_clear_peaks(cuda_device, L0, Lmax):
+    """L0 = 8, 12, 16 (n = 32, 48, 64): the compile-time instantiations of the grid kernel."""
+    rng = np.random.default_rng(5 + L0)
+    B, C = 6, 10
+    n = 4 * L0
     sig, _ = synthetic_sigma(rng, B, Lmax)
-    m = _matcha(B, Lmax, [8, 12], C=C)
+    m = _matcha(B, Lmax, [L0, Lmax], C=C)
     a, b, g = m._grid_search_so3fft(torch.from_numpy(sig).to(cuda_device))
-    f = M.sofft_eval(sig.astype(np.complex128), 8, 2)
+    f = M.sofft_eval(sig.astype(np.complex128), L0, 2)
     ids, vals = M.topk_grid(f, C + 1)
-    ra, rb, rg = M.ids_to_angles(ids[:, :C], 32, dtype=np.float32)
+    ra, rb, rg = M.ids_to_angles(ids[:, :C], n, dtype=np.float32)
     margin = (vals[:, :-1] - vals[:, 1:]) / np.abs(vals[:, :1])
     for bi in range(B):
         for c in range(C):
             # a rank is only well defined when it is separated from the next value
             if margin[bi, c] > 1e-5 and (c == 0 or margin[bi, c - 1] > 1e-5):
                 # angles are float32(index) * float32(step), as torch computes them
-                got = np.rint([b[bi, c].item() / (np.pi / 31), a[bi, c].item() / (np.pi / 16),
-                               g[bi, c].item() / (np.pi / 16)]).astype(int)
+                got = np.rint([b[bi, c].item() / (np.pi / (n - 1)), a[bi, c].item() / (2 * np.pi / n),
+                               g[bi, c].item() / (2 * np.pi / n)]).astype(int)
                 assert tuple(got) == tuple(ids[bi, c]), (bi, c, got, ids[bi, c])
                 np.testing.assert_allclose([a[bi, c].item(), b[bi, c].item(), g[bi, c].item()],
                                            [ra[bi, c], rb[bi, c], rg[bi, c]], atol=1e-6)
