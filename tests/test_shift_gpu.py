@@ -74,6 +74,36 @@ def test_shift_matches_oracle(cuda_device, N, uf, r, precision):
         np.testing.assert_allclose(score[b], sc_ref, rtol=tol)
 
 
+@pytest.mark.parametrize("N,uf,r,B", [(128, 4, 1, 1), (96, 8, 6, 1), (32, 8, 15, 2), (48, 2, 0, 5)])
+def test_shift_tensor_path_edges_match_oracle(cuda_device, N, uf, r, B):
+    """Edges of the tensor-core geometry: a single subtomogram (one partial row tile per pass),
+    U = 248 at box 32 (N-tile and pass-3 tile at their 256-column limit, the two TMEM
+    accumulators filling its 512 columns) and U = 2 at box 48."""
+    rng = np.random.default_rng(N * 7 + r)
+    tmpl = blob_template(rng, N, 60, N * 0.3, (1.5, 3.0), mask_radius=N * 0.4)
+    q = haar_quaternions(rng, B)
+    vols = rotate_volumes_reference(np.repeat(tmpl[None], B, 0), q)
+    vols = (vols + 0.5 * rng.standard_normal(vols.shape)).astype(np.float32)
+    prior = rng.uniform(-1.0, 1.0, (B, 3)).astype(np.float32)
+    sm = _matcher(N, B, uf, r, cuda_device, precision="bf16x3")
+    sm.set_reference(tmpl)
+    shift, score = sm.search_shifts(subtomos=torch.from_numpy(vols).to(cuda_device), ctfs=None,
+                                    shift_zyx=torch.from_numpy(prior).to(cuda_device), rotation_tracker=q)
+    sm.status()
+    assert sm.effective_precision == "bf16x3"
+    shift, score = shift.cpu().numpy(), score.cpu().numpy()
+    ref = OS.load_reference_full(tmpl, N, 1.0)
+    ang = OS.euler_zyz_deg_from_quat_conj(q)
+    for b in range(B):
+        (s_ref, sc_ref), parts = OS.estimate_shift_like_relion(ref, vols[b], prior[b], ang[b], uf, r,
+                                                               return_parts=True)
+        grid = parts["grid"].ravel()
+        top2 = np.sort(grid)[-2:]
+        if (top2[1] - top2[0]) > 1e-4 * abs(top2[1]):
+            np.testing.assert_allclose(shift[b], s_ref, atol=1e-6)
+        np.testing.assert_allclose(score[b], sc_ref, rtol=1e-4)
+
+
 def test_shift_requires_reference(cuda_device):
     sm = _matcher(16, 1, 4, 1, cuda_device)
     with pytest.raises(RuntimeError):
