@@ -372,14 +372,38 @@ DRAM_BYTES_PER_SUBTOMO = {"patch_fft_xy64_kernel": 1_910_000, "fft_z64_kernel": 
                           "updft1_tc_kernel": 2_205_000, "updft23_tc_kernel": 1_525_000}
 
 
+# ---------------------------------------------------------------- ranks
+def dist_env():
+    """(world size, rank, local rank) from the launcher's environment (one process per GPU)."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def max_over_ranks(value: float, world: int, device) -> float:
+    """The largest of the ranks' values: a replica job's step time is its slowest rank's (an
+    all_reduce of the timing only; the ranks exchange no data).  The identity on one rank."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(world: int, batch: int, ms: float) -> float:
+    """Subtomograms per second of the whole job: every rank aligns its own batch of ``batch``
+    in the max-over-ranks step time ``ms`` (weak scaling)."""
+    return world * batch / (ms * 1e-3)
+
+
 # ---------------------------------------------------------------- our implementation
 def run_ours(args):
     import torch
     import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = dist_env()
     if world > 1:
         from datetime import timedelta
 
@@ -431,10 +455,8 @@ def run_ours(args):
     ms = start.elapsed_time(end) / args.steps
     prof, dropped = nat.profile_read()
     launches = sum(v["launches"] for v in prof.values())
+    ms = max_over_ranks(ms, world, dev)
     if world > 1:
-        tms = torch.tensor([ms], device=dev)
-        dist.all_reduce(tms, op=dist.ReduceOp.MAX)
-        ms = float(tms.item())
         dist.barrier()
     # end-to-end through the public API with host buffers
     # (AlignmentStep.align_host: the volumes' host-to-device copy overlaps the alignment in
@@ -461,10 +483,7 @@ def run_ours(args):
     e2e_end.record(st)
     torch.cuda.synchronize()
     e2e_ms = e2e_start.elapsed_time(e2e_end) / e2e_steps
-    if world > 1:
-        t2 = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t2.item())
+    e2e_ms = max_over_ranks(e2e_ms, world, dev)
     # accuracy of the chosen path on the full batch (one more step; the end-to-end runs' pieces
     # overwrote the step's output buffers), kept for the comparison with the oracle below
     out = one()
@@ -496,11 +515,8 @@ def run_ours(args):
         prof32, _ = nat.profile_read()
         ms32 = e32s.elapsed_time(e32e) / n32
         plain_out = {k: o32[k].cpu().numpy() for k in ("alpha", "beta", "gamma", "shift")}
-        if world > 1:
-            t32 = torch.tensor([ms32], device=dev)
-            dist.all_reduce(t32, op=dist.ReduceOp.MAX)
-            ms32 = float(t32.item())
-        plain = {"value": world * B / (ms32 * 1e-3), "ms_per_step": ms32, "steps": n32,
+        ms32 = max_over_ranks(ms32, world, dev)
+        plain = {"value": whole_job_value(world, B, ms32), "ms_per_step": ms32, "steps": n32,
                  "chosen_speedup": ms32 / ms, "kernels_ms_per_step": {k: v["ms"] / n32 for k, v in prof32.items()}}
         del step32
     # three alternations per batch, as an alignment run makes them: each prepares the batch at
@@ -531,15 +547,12 @@ def run_ours(args):
         step.prepare(vols, zeros3, tracker)
     ep1.record(st)
     torch.cuda.synchronize()
-    ms_prep = ep0.elapsed_time(ep1) / 5
-    if world > 1:
-        t3 = torch.tensor([ms3], device=dev)
-        dist.all_reduce(t3, op=dist.ReduceOp.MAX)
-        ms3 = float(t3.item())
+    ms_prep = max_over_ranks(ep0.elapsed_time(ep1) / 5, world, dev)
+    ms3 = max_over_ranks(ms3, world, dev)
     # rotation error of the tracker after the third alternation (the last run's)
     trk = tracker.cpu().numpy()
     err3 = tracker_error_deg(trk, q_true)
-    alternations = {"value": world * B / (ms3 * 1e-3), "unit": "subtomograms/s", "alternations": 3,
+    alternations = {"value": whole_job_value(world, B, ms3), "unit": "subtomograms/s", "alternations": 3,
                     "ms_per_batch": ms3, "runs": n3, "prepare_ms_per_alternation": ms_prep,
                     "median_rot_err_deg": float(np.median(err3)), "p90_rot_err_deg": float(np.percentile(err3, 90))}
     err = rotation_error_deg(chosen["alpha"], chosen["beta"], chosen["gamma"], q_true)
@@ -567,7 +580,7 @@ def run_ours(args):
     clocks = clk.summary()
     line = {
         "metric": METRIC,
-        "value": world * B / (ms * 1e-3),
+        "value": whole_job_value(world, B, ms),
         "unit": "subtomograms/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -597,8 +610,8 @@ def run_ours(args):
         "plain_fp32": plain,
         "three_alternations": alternations,
         "one_alternation_with_preparation": {"ms_per_step": ms + ms_prep,
-                                             "value": world * B / ((ms + ms_prep) * 1e-3)},
-        "e2e": {"value": world * B / (e2e_ms * 1e-3), "unit": "subtomograms/s",
+                                             "value": whole_job_value(world, B, ms + ms_prep)},
+        "e2e": {"value": whole_job_value(world, B, e2e_ms), "unit": "subtomograms/s",
                 "h2d_bytes_per_step": int(B * N_BOX ** 3 * 4), "d2h_bytes_per_step": int(B * 8 * 4)},
         "gpu_launches": int(launches),
         "profile_dropped_launches": dropped,
@@ -636,8 +649,8 @@ def run_reference(args):
     """The oracle restatement of the reference's alternation on the host cores, on the first
     ``--cpu-sample`` subtomograms of the same batch the GPU arm aligns (same generator, same
     seeds, built on the CPU)."""
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    _, rank, _ = dist_env()
+    if rank != 0:  # under torchrun rank 0 alone times the host cores; the others exit 0
         return
     import torch
 
