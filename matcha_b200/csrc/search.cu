@@ -45,17 +45,26 @@ __device__ __forceinline__ bool better(float v1, int i1, float v2, int i2) {
 
 constexpr size_t kGridSmemCap = 200 * 1024;
 
-// Dynamic shared memory of the grid kernel: sigma (l < L0), the twiddle matrix, and the
-// F, G buffers of JB beta values.
-size_t grid_smem_bytes(int L0, int K, int JB) {
+constexpr size_t kGridTwoPerSm = 112 * 1024;  // dynamic shared memory that leaves room for two CTAs
+
+// Dynamic shared memory of the grid kernel: sigma (l < L0), the twiddle matrix, the F, G
+// buffers of JB beta values and, when staged, their d-table rows.
+size_t grid_smem_bytes(int L0, int K, int JB, bool staged) {
   const int n = 2 * L0 * K, P = 2 * L0 - 1, nk = mtb_dsize(L0 - 1);
-  return (size_t)(nk + n * P + JB * P * P + JB * P * n) * sizeof(float2) + (size_t)JB * nk * sizeof(float);
+  return (size_t)(nk + n * P + JB * P * P + JB * P * n) * sizeof(float2) +
+         (staged ? (size_t)JB * nk * sizeof(float) : 0);
 }
 
-// Beta values per pass: four when they fit, else one (at L0 = 16 two would fit, but the
-// 150 KB they take leave room for one CTA per SM instead of two, which measured slower).
-int grid_jb(int L0, int K) { return grid_smem_bytes(L0, K, 4) <= kGridSmemCap ? 4 : 1; }
-size_t grid_smem_bytes(int L0, int K) { return grid_smem_bytes(L0, K, grid_jb(L0, K)); }
+// Beta values per pass: four with their d-table rows staged in shared memory when they fit;
+// else two read straight from the (L2-resident) table when two CTAs still fit an SM (at
+// L0 = 16 two staged rows take 150 KB, room for one CTA per SM, which measured slower than one
+// staged row with two CTAs); else one, staged.
+int grid_jb(int L0, int K) {
+  if (grid_smem_bytes(L0, K, 4, true) <= kGridSmemCap) return 4;
+  return grid_smem_bytes(L0, K, 2, false) <= kGridTwoPerSm ? 2 : 1;
+}
+bool grid_staged(int L0, int K) { return grid_jb(L0, K) != 2; }
+size_t grid_smem_bytes(int L0, int K) { return grid_smem_bytes(L0, K, grid_jb(L0, K), grid_staged(L0, K)); }
 
 // SOFFT on the (n x n x n) grid (beta_j = j pi/(n-1), alpha_a = 2 pi a/n, gamma_g = 2 pi g/n)
 // for one subtomogram per CTA, kGridJB beta values per pass:
@@ -66,7 +75,7 @@ size_t grid_smem_bytes(int L0, int K) { return grid_smem_bytes(L0, K, grid_jb(L0
 // L0T, NT > 0 fix L0 and n at compile time (the index arithmetic then folds to constants);
 // 0 takes them from the arguments.  KC >= C is the capacity of each thread's kept set, held
 // in registers (statically indexed).
-template <int L0T, int NT, int KC>
+template <int L0T, int NT, int KC, bool STAGED>
 __global__ void __launch_bounds__(kGridThreads)
 so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
                      const float* __restrict__ dtab, int L0_arg, int n_arg, int C, int JB,
@@ -125,20 +134,21 @@ so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
   const float inv_n2 = 1.f / (float)(n * n);
   for (int j0 = 0; j0 < n; j0 += JB) {
     const int jn = min(JB, n - j0);
-    for (int e = tid; e < jn * nk; e += blockDim.x) sD[e] = __ldg(&dtab[(int64_t)j0 * nk + e]);
+    if (STAGED)
+      for (int e = tid; e < jn * nk; e += blockDim.x) sD[e] = __ldg(&dtab[(int64_t)j0 * nk + e]);
     __syncthreads();
     for (int q = tid; q < jn * P * P; q += blockDim.x) {
       const int jb = q / (P * P), qq = q - jb * (P * P);
       const int mp = qq / P - (L0 - 1), m = qq % P - (L0 - 1);
       const int l0 = max(abs(mp), abs(m));
-      const float* dj = sD + jb * nk;
+      const float* dj = STAGED ? sD + jb * nk : dtab + (int64_t)(j0 + jb) * nk;
       float re = 0.f, im = 0.f;
       if (L0T > 0) {
 #pragma unroll
         for (int l = 0; l < L0T; ++l) {
           if (l >= l0) {
             const int idx = mtb_dsize(l - 1) + (mp + l) * (2 * l + 1) + (m + l);
-            const float d = dj[idx];
+            const float d = STAGED ? dj[idx] : __ldg(dj + idx);
             re += d * sg[idx].x;
             im += d * sg[idx].y;
           }
@@ -146,7 +156,7 @@ so3_grid_topk_kernel(const float2* __restrict__ sigma, int64_t stride, int B,
       } else {
         for (int l = l0; l < L0; ++l) {
           const int idx = mtb_dsize(l - 1) + (mp + l) * (2 * l + 1) + (m + l);
-          const float d = dj[idx];
+          const float d = STAGED ? dj[idx] : __ldg(dj + idx);
           re += d * sg[idx].x;
           im += d * sg[idx].y;
         }
@@ -292,11 +302,19 @@ template <int L0T, int NT, int KC>
 int grid_launch_t(const float2* sigma, int64_t stride, int B, const float* dtab, int L0, int K, int C, float* a,
                   float* b, float* g, float* grid, cudaStream_t st) {
   const size_t smem = grid_smem_bytes(L0, K);
-  MTB_CUDA_TRY(cudaFuncSetAttribute(so3_grid_topk_kernel<L0T, NT, KC>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int jb = grid_jb(L0, K);
   mtb_prof_begin(st);
-  so3_grid_topk_kernel<L0T, NT, KC><<<B, kGridThreads, smem, st>>>(sigma, stride, B, dtab, L0, 2 * L0 * K, C,
-                                                               grid_jb(L0, K), a, b, g, grid);
+  if (grid_staged(L0, K)) {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(so3_grid_topk_kernel<L0T, NT, KC, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    so3_grid_topk_kernel<L0T, NT, KC, true><<<B, kGridThreads, smem, st>>>(sigma, stride, B, dtab, L0, 2 * L0 * K,
+                                                                       C, jb, a, b, g, grid);
+  } else {
+    MTB_CUDA_TRY(cudaFuncSetAttribute(so3_grid_topk_kernel<L0T, NT, KC, false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    so3_grid_topk_kernel<L0T, NT, KC, false><<<B, kGridThreads, smem, st>>>(sigma, stride, B, dtab, L0, 2 * L0 * K,
+                                                                        C, jb, a, b, g, grid);
+  }
   mtb_prof_end(st, "so3_grid_topk_kernel");
   MTB_LAUNCH_CHECK();
   return MTB_OK;
