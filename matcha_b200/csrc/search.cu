@@ -45,8 +45,6 @@ __device__ __forceinline__ bool better(float v1, int i1, float v2, int i2) {
 
 constexpr size_t kGridSmemCap = 200 * 1024;
 
-constexpr size_t kGridTwoPerSm = 112 * 1024;  // dynamic shared memory that leaves room for two CTAs
-
 // Dynamic shared memory of the grid kernel: sigma (l < L0), the twiddle matrix, the F, G
 // buffers of JB beta values and, when staged, their d-table rows.
 size_t grid_smem_bytes(int L0, int K, int JB, bool staged) {
@@ -55,16 +53,44 @@ size_t grid_smem_bytes(int L0, int K, int JB, bool staged) {
          (staged ? (size_t)JB * nk * sizeof(float) : 0);
 }
 
-// Beta values per pass: four with their d-table rows staged in shared memory when they fit;
-// else two read straight from the (L2-resident) table when two CTAs still fit an SM (at
-// L0 = 16 two staged rows take 150 KB, room for one CTA per SM, which measured slower than one
-// staged row with two CTAs); else one, staged.
-int grid_jb(int L0, int K) {
-  if (grid_smem_bytes(L0, K, 4, true) <= kGridSmemCap) return 4;
-  return grid_smem_bytes(L0, K, 2, false) <= kGridTwoPerSm ? 2 : 1;
+// CTAs of the grid kernel an SM holds with `smem` bytes of dynamic shared memory (228 KB per
+// SM, 1 KB reserved and the static arrays per CTA), at most four (the register limit of the
+// 64-register instantiations at 256 threads).
+int grid_ctas_per_sm(size_t smem) {
+  const int c = (int)((size_t)228 * 1024 / (smem + 1024 + 256));
+  return c < 4 ? c : 4;
 }
-bool grid_staged(int L0, int K) { return grid_jb(L0, K) != 2; }
-size_t grid_smem_bytes(int L0, int K) { return grid_smem_bytes(L0, K, grid_jb(L0, K), grid_staged(L0, K)); }
+
+struct GridPlan {
+  int jb;       // beta values per pass
+  bool staged;  // their d-table rows copied into shared memory (else read from the L2-resident table)
+};
+
+// The pass shape: the most CTAs per SM first (the kernel is latency-bound: a CTA runs its
+// passes one after another, three barriers each), then the most beta values per pass (fewer
+// passes), then staged rows.  At L0 = 16 this is two unstaged rows, two CTAs per SM (staged,
+// the two rows take 150 KB and leave one).
+GridPlan grid_plan(int L0, int K) {
+  GridPlan best{0, true};
+  int best_c = 0;
+  for (int jb : {8, 4, 2, 1})
+    for (bool staged : {true, false}) {
+      const size_t sm = grid_smem_bytes(L0, K, jb, staged);
+      if (sm > kGridSmemCap) continue;
+      const int c = grid_ctas_per_sm(sm);
+      if (c > best_c || (c == best_c && jb > best.jb)) {
+        best = GridPlan{jb, staged};
+        best_c = c;
+      }
+    }
+  return best;
+}
+int grid_jb(int L0, int K) { return grid_plan(L0, K).jb; }
+bool grid_staged(int L0, int K) { return grid_plan(L0, K).staged; }
+size_t grid_smem_bytes(int L0, int K) {
+  const GridPlan p = grid_plan(L0, K);
+  return p.jb ? grid_smem_bytes(L0, K, p.jb, p.staged) : kGridSmemCap + 1;  // jb 0: nothing fits
+}
 
 // SOFFT on the (n x n x n) grid (beta_j = j pi/(n-1), alpha_a = 2 pi a/n, gamma_g = 2 pi g/n)
 // for one subtomogram per CTA, kGridJB beta values per pass:
