@@ -25,8 +25,16 @@
 // accumulator (two alternating buffers in tensor memory), plus the Nyquist term in FP32, to
 // a running argmax key per subtomogram, a chunk behind the writers.  A2 K-blocks and pass-3
 // chunks take turns in a ring of two or three shared-memory slots, so the next tile's A2
-// loads while this tile's pass 3 runs.  Neither X2 nor the U^3 grid reaches memory.  All
-// device waits are bounded; a wait that runs out sets err and the CTA winds down.
+// loads while this tile's pass 3 runs.  Neither X2 nor the U^3 grid reaches memory.
+//
+// The fused kernel needs 2U <= 256 and whole u0 groups per 128-row tile (boxes 16, 32, 64).
+// Other even boxes up to 128 (48, 80, 96, 128) and U up to 256 run the passes unfused: pass 2
+// is the pass-1 kernel again, its epilogue writing X2 as the pass-3 operand A3 to memory (rows
+// (b, u0 U + u1) padded to a multiple of 128 per subtomogram), and updft3_tc_kernel runs pass 3
+// with the Nyquist term and the argmax.  Where 2U > 256 or E1 would not fit in shared memory
+// beside two A stages, the N-tile of passes 1 and 2 is cut into column parts, one per CTA, the
+// CTAs of one row tile adjacent in the grid so that A is read from memory once.  All device
+// waits are bounded; a wait that runs out sets err and the CTA winds down.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <math.h>
