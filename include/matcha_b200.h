@@ -256,8 +256,9 @@ typedef struct {
   float mask_radius;     /* box_size / (2 voxel_size), setup_utils.py:292-295; <0: N/2 */
   float cosine_width;    /* 5.0 in the reference (setup_utils.py:295)               */
   int precision;         /* MTB_SHIFT_FP32: upsampled DFT on CUDA cores; MTB_SHIFT_BF16X3:
-                            tcgen05 BF16 GEMMs with a hi+lo split, MTB_ERR_ARG from create on a
-                            box / upsampled region the tensor-core kernels do not cover;
+                            tcgen05 BF16 GEMMs with a hi+lo split (every even box from 16 to
+                            128 the shift match takes, U = ceil(uf (2r + 1)) <= 256), MTB_ERR_ARG
+                            from create on a box / upsampled region they do not cover;
                             MTB_SHIFT_AUTO: the tensor cores where they cover it, else FP32 */
   int tile_rows;         /* FP32 upsampled DFT: rows u0 per CTA of its passes 2+3 (0: 2), the tile
                             shape matcha_b200.autotune chooses per box; no effect on the result */
