@@ -69,6 +69,11 @@ typedef struct mtb_search mtb_search;
 int mtb_search_create(const mtb_search_config* cfg, mtb_search** out);
 void mtb_search_destroy(mtb_search* h);
 
+/* Host-only query of the grid kernel's pass shape for (L0, K) (no counterpart in the
+ * reference): beta values per pass, whether their d-table rows are staged in shared memory,
+ * and its dynamic shared memory.  MTB_ERR_ARG when the grid does not fit shared memory. */
+int mtb_so3_grid_plan(int L0, int K, int* beta_per_pass, int* staged, int64_t* smem);
+
 /* Grid search: f(beta_j, alpha_a, gamma_g) on the (2 L0 K)^3 grid, top-`candidates`
  * peaks per subtomogram, converted to Euler angles (radians).
  * sigma: (B, sigma_stride) complex64, at least dsize(L0-1) entries per row.
@@ -312,6 +317,15 @@ int mtb_shift_score_grad(mtb_shift* h, const float* subtomos, const float* shift
 /* The precision a handle runs the upsampled DFT in (MTB_SHIFT_FP32 or MTB_SHIFT_BF16X3):
  * what MTB_SHIFT_AUTO resolved to.  No counterpart in the reference (a query of this build). */
 int mtb_shift_precision(const mtb_shift* h, int* precision);
+
+/* Host-only query of the tensor-core upsampled DFT's launch geometry for box N and upsampled
+ * region U (no device, no allocation; no counterpart in the reference): whether passes 2 and 3
+ * run fused, the column parts of the passes-1/2 N-tile and each part's width in columns, the
+ * pipeline stages of the pass-1/2 kernel and of the separate pass-3 kernel (0 when fused),
+ * and the largest dynamic shared memory of its kernels.  MTB_ERR_ARG where the tensor-core
+ * kernels do not cover (N, U). */
+int mtb_shift_tc_plan(int N, int U, int* fused, int* column_parts, int* n_tile, int* stages1, int* stages3,
+                      int64_t* smem_max);
 
 /* Synchronises stream; MTB_ERR_TIMEOUT if a bounded device-side wait of the tensor-core
  * path gave up since the handle was created (then its results are invalid). */

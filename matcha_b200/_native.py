@@ -104,6 +104,8 @@ SIGNATURES = {
     "mtb_shift_profile_read": (_I, [_P, _P, _P]),
     "mtb_shift_search": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P]),
     "mtb_shift_begin": (_I, [_P, _P, _P, _I, _P]),
+    "mtb_shift_tc_plan": (_I, [_I, _I] + [ctypes.POINTER(_I)] * 5 + [ctypes.POINTER(_I64)]),
+    "mtb_so3_grid_plan": (_I, [_I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I64)]),
     "mtb_shift_finish": (_I, [_P, _P, _P, _I, _P, _P, _P]),
     "mtb_update_rotation": (_I, [_P, _P, _P, _P, _I, _P, _P, _P]),
     "mtb_tracker_rotation": (_I, [_P, _I, _P, _P]),

@@ -702,3 +702,13 @@ extern "C" int mtb_search_orientations_static(const mtb_search_config* cfg, cons
   MTB_LAUNCH_CHECK();
   return MTB_OK;
 }
+
+extern "C" int mtb_so3_grid_plan(int L0, int K, int* beta_per_pass, int* staged, int64_t* smem) {
+  MTB_ARG_CHECK(L0 >= 1 && K >= 1 && beta_per_pass && staged && smem, "bad argument");
+  const GridPlan p = grid_plan(L0, K);
+  MTB_ARG_CHECK(p.jb > 0, "grid search too large for shared memory (reduce L0 or K)");
+  *beta_per_pass = p.jb;
+  *staged = p.staged ? 1 : 0;
+  *smem = (int64_t)grid_smem_bytes(L0, K);
+  return MTB_OK;
+}

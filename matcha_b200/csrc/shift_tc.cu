@@ -913,7 +913,9 @@ struct Geometry {
   size_t smem1, smem23, smem3;
 };
 
-bool geometry(int N, int U, Geometry* o) {
+// The geometry of the fused (passes 2+3 in one kernel) or the unfused kernels; false when it
+// does not fit the MMA shapes, tensor memory or shared memory.
+bool geometry_as(int N, int U, bool fused, Geometry* o) {
   if (N < 16 || N > 128 || (N & 1)) return false;
   if (U < 1 || U > 256) return false;
   Geometry g;
@@ -921,7 +923,8 @@ bool geometry(int N, int U, Geometry* o) {
   g.NT3 = (U + 15) / 16 * 16;
   g.KB12 = (2 * N + TK - 1) / TK;
   g.KB3 = (N + TK - 1) / TK;  // K of pass 3: (m2 < N/2, re/im)
-  g.fused = (N == 16 || N == 32 || N == 64) && 2 * U <= 256;
+  g.fused = fused;
+  if (fused && !((N == 16 || N == 32 || N == 64) && 2 * U <= 256)) return false;
   g.NT12 = (2 * U + 15) / 16 * 16;
   g.G = TM / g.HH;
   g.TPB = (U + g.G - 1) / g.G;
@@ -967,11 +970,38 @@ bool geometry(int N, int U, Geometry* o) {
   return true;
 }
 
+// The fused kernels where they fit (boxes 16, 32, 64 with 2U <= 256, within the shared
+// memory of two operand slots), else the unfused ones.
+bool geometry(int N, int U, Geometry* o) {
+  return geometry_as(N, U, true, o) || geometry_as(N, U, false, o);
+}
+
 }  // namespace
 
 int shift_tc_fits(int N, int U) {
   Geometry g;
   return geometry(N, U, &g) ? MTB_OK : MTB_ERR_ARG;
+}
+
+extern "C" int mtb_shift_tc_plan(int N, int U, int* fused, int* column_parts, int* n_tile, int* stages1,
+                                 int* stages3, int64_t* smem_max) {
+  MTB_ARG_CHECK(fused && column_parts && n_tile && stages1 && stages3 && smem_max, "null pointer");
+  Geometry g;
+  if (!geometry(N, U, &g)) {
+    mtb_set_last_error("the tensor-core shift kernels do not cover this box and upsampled region", __FILE__,
+                       __LINE__);
+    return MTB_ERR_ARG;
+  }
+  *fused = g.fused ? 1 : 0;
+  *column_parts = g.NS;
+  *n_tile = g.NT12;
+  *stages1 = g.stages1;
+  *stages3 = g.fused ? 0 : g.stages3;
+  size_t m = g.smem1;
+  if (g.fused && g.smem23 > m) m = g.smem23;
+  if (!g.fused && g.smem3 > m) m = g.smem3;
+  *smem_max = (int64_t)m;
+  return MTB_OK;
 }
 
 int shift_tc_prepare(ShiftTc* t, int N, int H, int U, int uf, float dftshift, int max_batch) {

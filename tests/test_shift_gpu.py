@@ -74,11 +74,12 @@ def test_shift_matches_oracle(cuda_device, N, uf, r, precision):
         np.testing.assert_allclose(score[b], sc_ref, rtol=tol)
 
 
-@pytest.mark.parametrize("N,uf,r,B", [(128, 4, 1, 1), (96, 8, 6, 1), (32, 8, 15, 2), (48, 2, 0, 5)])
+@pytest.mark.parametrize("N,uf,r,B", [(128, 4, 1, 1), (96, 8, 6, 1), (32, 8, 15, 2), (48, 2, 0, 5), (64, 4, 15, 2)])
 def test_shift_tensor_path_edges_match_oracle(cuda_device, N, uf, r, B):
     """Edges of the tensor-core geometry: a single subtomogram (one partial row tile per pass),
     U = 248 at box 32 (N-tile and pass-3 tile at their 256-column limit, the two TMEM
-    accumulators filling its 512 columns) and U = 2 at box 48."""
+    accumulators filling its 512 columns), U = 2 at box 48, and U = 124 at box 64 (2U fits the
+    fused kernel's N-tile but its shared memory does not: the unfused passes run)."""
     rng = np.random.default_rng(N * 7 + r)
     tmpl = blob_template(rng, N, 60, N * 0.3, (1.5, 3.0), mask_radius=N * 0.4)
     q = haar_quaternions(rng, B)
