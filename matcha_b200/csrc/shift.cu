@@ -176,7 +176,6 @@ __device__ void load_twiddles(float2* tw, int L, int count) {
   }
 }
 
-__device__ void load_twiddles(float2* tw, int L) { load_twiddles(tw, L, L / 2); }
 
 // Boxes that are not powers of two (48, 80, 96) take the same kernels with the radix-2 FFTs
 // replaced by direct DFTs (O(N^2) per line, natural-order output) and the index rolls done by
