@@ -8,6 +8,7 @@
     python bench_cases.py graph 64     # one alternation, 64^3 L 32: eager calls vs a CUDA graph
     python bench_cases.py shift 1000 --stages   # plus ShiftMatcher.profile per kernel group
     python bench_cases.py shift 64 --box 128 --radius 8 --kernels   # 128^3, r 8: time per kernel
+    python bench_cases.py fftbound 4 --box 128  # cuFFT of the 2x oversampled grid (comparison only)
 
 Each case builds its inputs on the device from a fixed seed (random volumes, Haar rotations,
 random shifts; a synthetic sigma with a known optimum for the search), runs the stage three
@@ -174,7 +175,33 @@ def _graph(B: int, reps: int) -> int:
     return 0
 
 
-CASES = {"shift": _shift, "search": _search, "fle": _fle, "prepare": _prepare, "reader": None, "graph": None}
+def _fftbound(B: int, reps: int, box: int) -> int:
+    """A lower bound for the FFT-plus-shell form of the expansion (the reference's NUFFT path)
+    at box N: one complex64 FFT of each volume's 2x oversampled (2N)^3 grid, the NUFFT's own
+    FFT alone (no spreading, no spherical-harmonic or radial step), timed with cuFFT through
+    torch.fft on B volumes.  A comparison measurement only: nothing in the library calls cuFFT."""
+    import torch
+
+    dev = torch.device("cuda:0")
+    n = 2 * box
+    x = torch.randn((B, n, n, n), device=dev, dtype=torch.complex64)
+    for _ in range(3):
+        torch.fft.fftn(x, dim=(1, 2, 3))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        torch.fft.fftn(x, dim=(1, 2, 3))
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    print(f"fftbound box {box}: ({n})^3 complex64 FFT, {B} volumes: {ms:.3f} ms per call, "
+          f"{1e3 * ms / B:.1f} us per volume")
+    return 0
+
+
+CASES = {"shift": _shift, "search": _search, "fle": _fle, "prepare": _prepare, "reader": None, "graph": None,
+         "fftbound": None}
 
 
 def main(argv=None) -> int:
@@ -183,7 +210,7 @@ def main(argv=None) -> int:
     p.add_argument("batch", type=int)
     p.add_argument("--reps", type=int, default=5)
     p.add_argument("--stages", action="store_true", help="shift only: time each kernel group with CUDA events")
-    p.add_argument("--box", type=int, default=64, help="shift only: box size")
+    p.add_argument("--box", type=int, default=64, help="shift and fftbound: box size")
     p.add_argument("--radius", type=int, default=5, help="shift only: search radius (voxels)")
     p.add_argument("--precision", default="bf16x3", help="shift only: bf16x3, fp32 or auto")
     p.add_argument("--kernels", action="store_true",
@@ -196,6 +223,8 @@ def main(argv=None) -> int:
         return 2
     if a.case == "graph":
         return _graph(a.batch, a.reps)
+    if a.case == "fftbound":
+        return _fftbound(a.batch, a.reps, a.box)
     dev = torch.device("cuda:0")
     if a.case == "shift":
         run = _shift(a.batch, dev, a.box, a.radius, a.precision)
