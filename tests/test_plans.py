@@ -78,3 +78,23 @@ def test_every_grid_plan_fits():
             p = _grid_plan(L0, K)
             assert p is not None, (L0, K)
             assert p[0] in (1, 2, 4, 8) and p[2] <= GRID_CAP, (L0, K, p)
+
+
+def test_capacity_plan_is_the_affine_fit_of_two_probes(monkeypatch):
+    """matcha_b200.autotune.plan_capacity on the host logic alone: the step's memory measured at
+    two capacities (here a stand-in of fixed + per-subtomogram bytes), the margin on the slope,
+    the batch's own volumes added, and the largest capacity within the budget."""
+    torch = pytest.importorskip("torch")
+    from matcha_b200 import autotune
+    from matcha_b200.pipeline import StepConfig
+
+    fixed, per = 700_000_000, 3_000_000
+    monkeypatch.setattr(autotune, "step_bytes", lambda cfg, cap, dev: fixed + per * cap)
+    cfg = StepConfig(N=64, L=32, batch=128)
+    plan = autotune.plan_capacity(cfg, "cpu", budget_bytes=20_000_000_000, probe=(128, 384), margin=1.1)
+    slope = int(-(-1.1 * per // 1))  # ceil(margin x per)
+    assert plan.bytes_per_subtomo == slope + 4 * 64 ** 3
+    assert plan.bytes_fixed == fixed + per * 128 - slope * 128
+    assert plan.capacity == (20_000_000_000 - plan.bytes_fixed) // plan.bytes_per_subtomo
+    assert plan.bytes_fixed + plan.capacity * plan.bytes_per_subtomo <= 20_000_000_000
+    del torch
