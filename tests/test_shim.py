@@ -39,4 +39,4 @@ def test_bench_cases_need_a_device(monkeypatch):
 
     monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
     assert profile_cases.main(["shift", "2"]) == 2
-    assert set(profile_cases.CASES) == {"shift", "search", "fle", "prepare", "reader", "graph"}
+    assert set(profile_cases.CASES) == {"shift", "search", "fle", "prepare", "reader", "graph", "fftbound"}
